@@ -1,0 +1,443 @@
+#!/usr/bin/env python
+"""Benchmark of the GPU spherical harmonic transforms.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+                    [--workload glq2047|dh2799x16|...]
+
+One step = one forward and one inverse transform of every field of the
+workload: MakeGridGLQ then SHExpandGLQ (or the DH pair).  The metric is
+transforms/s, one transform being one direction of one field, summed over
+all GPUs.  Inputs are seeded synthetic power-law coefficients (no dataset is
+involved); nodes and weights come from the GPU PreGLQ.
+
+Prints one JSON line (rank 0).  Multi-GPU runs (torchrun) are independent
+replicas: the transforms of a field do not shard across GPUs in this
+workload, each rank runs the same per-GPU work and the slowest rank's time
+is used (weak scaling).
+
+--impl reference times the reference algorithm on the host cores: the CPU
+oracle (a statement-by-statement C restatement of the SHTOOLS Fortran, which
+cannot be compiled here) on a bounded sample of ring pairs, all host threads.
+"""
+import argparse
+import concurrent.futures
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "transforms/s at lmax 2047 & 2799: mixed-prec vs FP64 GPU, rel err vs FP64"
+
+WORKLOADS = {
+    # config 2: plain FP64 GLQ, single field, lmax 2047, 2048 x 4095 grid
+    "glq2047": dict(kind="glq", lmax=2047, nfield=1, sampling=1, beta=2.0,
+                    seed=2000),
+    # config 5 shape in FP64: 16 DH fields, lmax 2799, sampling 2
+    "dh2799x16": dict(kind="dh", lmax=2799, nfield=16, sampling=2, beta=3.0,
+                      seed=5000),
+    # config 3 shape: 8 DH fields, lmax 719, sampling 2
+    "dh719x8": dict(kind="dh", lmax=719, nfield=8, sampling=2, beta=2.0,
+                    seed=3000),
+    # config 1 shape: one DH field, lmax 255, sampling 2
+    "dh255": dict(kind="dh", lmax=255, nfield=1, sampling=2, beta=2.0,
+                  seed=1000),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--workload", default="glq2047", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="target duration of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def flops_per_transform(w):
+    """Algorithmic FP64 flops of the Legendre stage of one transform: per
+    ring pair and (l, m), 4 for the three-term recursion and 4 for the two
+    multiply-adds of the contraction (F_rec + F_contr with 2*nlat*N_lm each)."""
+    L = w["lmax"]
+    nlm = (L + 1) * (L + 2) // 2
+    nlat = L + 1 if w["kind"] == "glq" else 2 * L + 2
+    return 8.0 * (nlat / 2.0) * nlm
+
+
+def power_law(L, seed, beta):
+    from oracle.oracle import power_law_cilm  # same seeded recipe, numpy only
+    return power_law_cilm(L, seed, beta)
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle on all host threads, bounded sample of ring pairs
+# ---------------------------------------------------------------------------
+def cpu_sample(w, seconds, threads=None):
+    import numpy as np
+    from oracle import oracle as O
+    L = w["lmax"]
+    threads = threads or len(os.sched_getaffinity(0))
+    c = power_law(L, w["seed"], w["beta"])
+    if w["kind"] == "glq":
+        zero, wt = O.shglq(L)
+        npair = (L + 2) // 2
+        grid = np.random.default_rng(1).standard_normal((L + 1, 2 * L + 1))
+    else:
+        n = 2 * L + 2
+        npair = n // 2 + 1
+        grid = np.random.default_rng(1).standard_normal((n, w["sampling"] * n))
+
+    def run(lo, hi):
+        if w["kind"] == "glq":
+            O.makegrid_glq(c, zero=zero, pair_window=(lo, hi))
+            O.shexpand_glq(grid, w=wt, zero=zero, pair_window=(lo, hi))
+        else:
+            O.makegrid_dh(c, sampling=w["sampling"], pair_window=(lo, hi))
+            O.shexpand_dh(grid, sampling=w["sampling"], pair_window=(lo, hi))
+
+    # calibrate: one pair on one thread
+    t0 = time.perf_counter()
+    run(npair // 3, npair // 3 + 1)
+    t1 = max(time.perf_counter() - t0, 1e-4)
+    per_thread = max(1, min(npair // threads if threads <= npair else 1,
+                            int(seconds / t1)))
+    windows = []
+    stride = max(1, npair // threads)
+    for t in range(threads):
+        lo = min(npair - per_thread, (t * stride) % max(1, npair - per_thread + 1))
+        windows.append((max(0, lo), max(0, lo) + per_thread))
+
+    def one_step():
+        t0 = time.perf_counter()
+        with concurrent.futures.ThreadPoolExecutor(threads) as ex:
+            list(ex.map(lambda wd: run(*wd), windows))
+        dt = time.perf_counter() - t0
+        pairs_done = per_thread * threads
+        # each (synthesis + analysis) over all pairs is 2 transforms of one field
+        transforms = 2.0 * pairs_done / npair
+        return transforms / dt, dt
+
+    sample = ("%d ring pairs of %d per thread x %d threads, synthesis+analysis, "
+              "single field; transforms/s scaled by the ring fraction"
+              % (per_thread, npair, threads))
+    return one_step, sample, threads
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.out.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for line in self.out:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def fp64_peak(torch, dev):
+    """Measured FP64 FMA throughput of this GPU (TFLOP/s), from the probe."""
+    import ctypes
+    path = os.path.join(ROOT, "shtools_b200", "lib", "libshtc_probe.so")
+    lib = ctypes.CDLL(path)
+    lib.shtc_probe_dfma.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_void_p]
+    props = torch.cuda.get_device_properties(dev)
+    blocks = props.multi_processor_count * 8
+    iters = 4096
+    out = torch.empty(blocks * 256, dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream(dev)
+    best = 0.0
+    for rep in range(4):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        rc = lib.shtc_probe_dfma(ctypes.c_void_p(out.data_ptr()), blocks, iters,
+                                 ctypes.c_void_p(st.cuda_stream))
+        b.record(st)
+        b.synchronize()
+        assert rc == 0
+        ms = a.elapsed_time(b)
+        flops = blocks * 256.0 * iters * 16 * 8 * 2
+        if rep > 0:
+            best = max(best, flops / (ms * 1e-3) / 1e12)
+    return best
+
+
+def max_over_ranks(x, device=None):
+    """Max of a float over all ranks of the default process group (the
+    slowest replica sets the time); identity without a process group."""
+    import torch
+    if not (torch.distributed.is_available() and torch.distributed.is_initialized()):
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def load_traffic(name):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get(name)
+    except Exception:
+        return None
+
+
+def run_cuda(args, w, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import shtools_b200 as sht
+    from shtools_b200 import _lib
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    L, F = w["lmax"], w["nfield"]
+    cil = np.stack([power_law(L, w["seed"] + i, w["beta"]) for i in range(F)])
+    c_host = torch.from_numpy(cil).pin_memory()
+    c = c_host.to(dev)
+    if w["kind"] == "glq":
+        zero_t, w_t = sht.PreGLQ(-1.0, 1.0, L + 1, device=dev)
+        zero, wts = zero_t.cpu().numpy(), w_t.cpu().numpy()
+        synth = lambda x: sht.MakeGridGLQ(x, zero=zero)
+        anal = lambda g: sht.SHExpandGLQ(g, w=wts, zero=zero)
+    else:
+        s = w["sampling"]
+        synth = lambda x: sht.MakeGridDH(x, sampling=s)
+        anal = lambda g: sht.SHExpandDH(g, sampling=s)
+
+    def step(x):
+        g = synth(x)
+        return g, anal(g)
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    st = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        g, back = step(c)
+    torch.cuda.synchronize(dev)
+    # accuracy of the round trip (size-independent property, per degree)
+    bb = back.cpu().numpy()
+    num = np.sqrt(((bb - cil) ** 2).sum(axis=(1, 3)))
+    den = np.sqrt((cil ** 2).sum(axis=(1, 3)))
+    rt_err = float((num / np.where(den > 0, den, 1)).max())
+
+    peak = fp64_peak(torch, dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # ---- device-resident timed region --------------------------------------
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize(dev)
+    lib.shtc_timing_enable(1)
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            flush.fill_(float(i))             # L2 flush outside the step events
+            evs[i][0].record(st)
+            g, back = step(c)
+            evs[i][1].record(st)
+        torch.cuda.synchronize(dev)
+    barrier()
+    lib.shtc_timing_enable(0)
+    import ctypes
+    ms = (ctypes.c_double * 6)()
+    cnt = (ctypes.c_int * 6)()
+    lib.shtc_timing_collect(ms, cnt, 6)
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = max_over_ranks(sum(step_ms), dev)
+    transforms = 2.0 * F * args.steps * world
+    value = transforms / (total_ms * 1e-3)
+
+    # ---- end-to-end through the public API with host buffers ---------------
+    g_host = torch.empty(tuple(g.shape), dtype=torch.float64).pin_memory()
+    b_host = torch.empty(tuple(back.shape), dtype=torch.float64).pin_memory()
+    e2e_steps = max(1, min(args.steps, 5))
+    barrier()
+    torch.cuda.synchronize(dev)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for i in range(e2e_steps):
+        xd = c_host.to(dev, non_blocking=True)          # H2D coefficients
+        gd = synth(xd)
+        g_host.copy_(gd, non_blocking=True)              # D2H grid
+        gd2 = g_host.to(dev, non_blocking=True)          # H2D grid
+        bd = anal(gd2)
+        b_host.copy_(bd, non_blocking=True)              # D2H coefficients
+    b.record(st)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(a.elapsed_time(b), dev)
+    e2e_value = 2.0 * F * e2e_steps * world / (e2e_ms * 1e-3)
+    h2d = c_host.numel() * 8 + g_host.numel() * 8
+    d2h = g_host.numel() * 8 + b_host.numel() * 8
+
+    # ---- roofline of the dominant kernel ------------------------------------
+    names = ["pack", "legendre_synth", "fft_c2r", "fft_r2c", "legendre_anal",
+             "unpack"]
+    dom = max((1, 4), key=lambda i: ms[i])
+    per_launch_ms = ms[dom] / max(1, cnt[dom])
+    fl = flops_per_transform(w) * F
+    achieved = fl / (per_launch_ms * 1e-3) / 1e12
+    traffic = load_traffic("%s_%s" % (names[dom], args.workload))
+    stage = {names[i]: {"ms_per_launch": (ms[i] / cnt[i]) if cnt[i] else None,
+                        "launches": cnt[i],
+                        "share": ms[i] / max(1e-9, sum(ms))} for i in range(6)}
+    res = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "transforms/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic seeded power-law coefficients, S(l)=(l+1)^-%g" % w["beta"],
+        "config": {"workload": args.workload, "kind": w["kind"], "lmax": L,
+                   "fields_per_gpu": F, "sampling": w["sampling"],
+                   "precision": "fp64", "step": "synthesis + analysis",
+                   "l2": "flushed between steps (256 MiB write, outside step events)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "roofline": {"kernel": names[dom], "bound": "fp64", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None,
+                     "peak_source": "measured FP64 FMA probe, this run "
+                                    "(MEASURED_PEAKS.json has no FP64 entry)",
+                     "flops_per_launch": fl, "traffic": traffic},
+        "stages": stage,
+        "roundtrip_max_perdeg_err": rt_err,
+        "e2e": {"value": e2e_value, "unit": "transforms/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps,
+                "path": "torch API from pinned host buffers: H2D cilm, "
+                        "synthesis, D2H grid, H2D grid, analysis, D2H cilm"},
+        "gpu_launches": int(sum(cnt)),
+        "clocks": clk.summary(),
+    }
+    return res
+
+
+def main():
+    args = parse()
+    w = WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        # the reference arm runs on rank 0's host cores only
+        if rank != 0:
+            return 0
+        one_step, sample, threads = cpu_sample(w, args.cpu_seconds / 3)
+        for _ in range(args.warmup):
+            one_step()
+        vals, dts = [], []
+        for _ in range(args.steps):
+            v, dt = one_step()
+            vals.append(v)
+            dts.append(dt)
+        value = args.steps / sum(1.0 / v for v in vals)   # harmonic mean
+        res = {"metric": METRIC, "impl": "reference", "value": value,
+               "unit": "transforms/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": 1e3 * sum(dts) / len(dts),
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "f64", "data": "synthetic seeded power-law coefficients",
+               "config": {"workload": args.workload, "kind": w["kind"],
+                          "lmax": w["lmax"], "fields": w["nfield"],
+                          "sampling": w["sampling"]},
+               "cpu_baseline": {"value": value, "unit": "transforms/s",
+                                "cores": threads, "kind": "port",
+                                "sample": sample},
+               "e2e": {"value": value, "unit": "transforms/s",
+                       "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(res))
+        return 0
+    if world > 1:
+        import torch
+        import datetime
+        torch.distributed.init_process_group(
+            "nccl", timeout=datetime.timedelta(seconds=120))
+    res = run_cuda(args, w, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        one_step, sample, threads = cpu_sample(w, args.cpu_seconds / 2)
+        v, dt = one_step()
+        res["cpu_baseline"] = {"value": v, "unit": "transforms/s",
+                               "cores": threads, "kind": "port",
+                               "sample": sample + " (%.1f s)" % dt}
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

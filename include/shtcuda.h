@@ -1,0 +1,207 @@
+/*
+ * shtcuda.h -- C ABI of libshtcuda, the B200 (sm_100a) engine for the real
+ * spherical harmonic transforms of SHTOOLS on Driscoll-Healy (DH) and
+ * Gauss-Legendre (GLQ) grids.
+ *
+ * Two layers are exported:
+ *
+ *  1. The device API (shtc_*): plans, caller-owned device buffers, a CUDA
+ *     stream argument, batches of fields, arbitrary element strides, int
+ *     status return.  Nothing in a transform call allocates or synchronises;
+ *     the caller passes a workspace of shtc_workspace_bytes() bytes.
+ *
+ *  2. Host-array drop-ins with exactly the names, arguments and Fortran
+ *     column-major layouts of the reference C interface include/shtools.h
+ *     (lines cited per function).  They copy to the GPU, run the device API
+ *     and copy back, so a program linked against libSHTOOLS for these
+ *     routines can link against libshtcuda instead.
+ *
+ * Status codes keep the meanings of the reference's exitstatus
+ * (src/MakeGridDH.f95:62-70, src/MakeGridGLQ.f95:196, src/PreGLQ.f95:129-139)
+ * and add codes for GPU-side failures.
+ */
+#ifndef SHTCUDA_H
+#define SHTCUDA_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define SHTC_API __attribute__((visibility("default")))
+#else
+#define SHTC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SHTC_OK 0
+#define SHTC_EDIM 1      /* improper dimensions of an input array            */
+#define SHTC_EBOUND 2    /* improper bounds for an input variable            */
+#define SHTC_EALLOC 3    /* error allocating memory                          */
+#define SHTC_EIO 4       /* file IO error (unused; kept for the code table)  */
+#define SHTC_ENOZERO 5   /* GLQ nodes missing or PreGLQ did not converge     */
+#define SHTC_ECUDA 6     /* CUDA runtime or kernel launch error              */
+#define SHTC_EHANDLE 7   /* null plan handle or null required pointer        */
+#define SHTC_EUNSUP 8    /* FFT length or size beyond the supported range    */
+#define SHTC_EWORK 9     /* workspace smaller than shtc_workspace_bytes()    */
+
+#define SHTC_GRID_DH 1
+#define SHTC_GRID_GLQ 2
+
+typedef struct shtc_plan shtc_plan;
+
+/* Library version as 10000*major + 100*minor + patch. */
+SHTC_API int shtc_version(void);
+
+/* Human-readable text of a status code (static storage). */
+SHTC_API const char* shtc_status_string(int status);
+
+/* ------------------------------------------------------------------------ */
+/* Plans.  A plan holds the device tables of one grid and option set:       */
+/* recursion factors ff1/ff2 (MakeGridDH.f95:321-381), sectoral start       */
+/* values, the u^m/1e-280 rescale table, ring geometry, quadrature weights  */
+/* and the longitude FFT plan.  Creation allocates device memory and        */
+/* synchronises the stream; transforms on a plan do neither.                */
+/* lmax_calc < 0 means lmax_calc = lmax.                                    */
+/* ------------------------------------------------------------------------ */
+
+/* DH grid of n = 2*lmax+2 rings, sampling*n longitudes (MakeGridDH.f95:109-156). */
+SHTC_API int shtc_plan_create_dh(shtc_plan** plan, int lmax, int sampling, int lmax_calc,
+                        int norm, int csphase, int extend, void* stream);
+
+/* GLQ grid of lmax+1 rings, 2*lmax+1 longitudes (MakeGridGLQ.f95:108-109).
+ * zero/w: host arrays of lmax+1 nodes (descending) and weights, e.g. from
+ * SHGLQ; NULL computes them with the GPU PreGLQ. */
+SHTC_API int shtc_plan_create_glq(shtc_plan** plan, int lmax, const double* zero,
+                         const double* w, int lmax_calc, int norm, int csphase,
+                         int extend, void* stream);
+
+SHTC_API int shtc_plan_destroy(shtc_plan* plan);
+
+/* info[0..15] = kind, lmax, lmax_comp, norm, csphase, sampling, extend,
+ * nlat, nlon, nlat_out, nlon_out, npair, nlm, device_bytes, bluestein,
+ * fft_mode */
+SHTC_API int shtc_plan_info(const shtc_plan* plan, long long* info, int ninfo);
+
+/* Device workspace bytes needed by any transform of nfield fields. */
+SHTC_API size_t shtc_workspace_bytes(const shtc_plan* plan, int nfield);
+
+/* ------------------------------------------------------------------------ */
+/* Transforms on device buffers.  Strides are in elements.                 */
+/*   cilm: element (f, k, l, m) at cilm[f*csf + k*csk + l*csl + m*csm],     */
+/*         k = 0 cosine (Clm), k = 1 sine (Slm), 0 <= l, m < cilm_dim.       */
+/*   grid: element (f, i, j) at grid[f*gsf + i*gsr + j*gsc].                */
+/* ------------------------------------------------------------------------ */
+
+/* MakeGridDH / MakeGridGLQ: cilm -> grid of nlat_out x nlon_out. */
+SHTC_API int shtc_synthesis(const shtc_plan* plan, const double* cilm, long long csf,
+                   long long csk, long long csl, long long csm, int cilm_dim,
+                   double* grid, long long gsf, long long gsr, long long gsc,
+                   int nfield, void* work, size_t work_bytes, void* stream);
+
+/* SHExpandDH / SHExpandGLQ: grid of nlat x nlon -> cilm (cilm_dim >=
+ * lmax_comp+1; entries beyond lmax_comp and with m > l are set to zero). */
+SHTC_API int shtc_analysis(const shtc_plan* plan, const double* grid, long long gsf,
+                  long long gsr, long long gsc, double* cilm, long long csf,
+                  long long csk, long long csl, long long csm, int cilm_dim,
+                  int nfield, void* work, size_t work_bytes, void* stream);
+
+/* Adjoint of shtc_synthesis: grid cotangent (nlat_out x nlon_out) ->
+ * coefficient cotangent.  The Legendre functions are recomputed, not
+ * stored. */
+SHTC_API int shtc_synthesis_adjoint(const shtc_plan* plan, const double* grid,
+                           long long gsf, long long gsr, long long gsc,
+                           double* cilm, long long csf, long long csk,
+                           long long csl, long long csm, int cilm_dim,
+                           int nfield, void* work, size_t work_bytes,
+                           void* stream);
+
+/* Adjoint of shtc_analysis: coefficient cotangent -> grid cotangent
+ * (nlat x nlon): the quadrature-weighted transpose of the analysis. */
+SHTC_API int shtc_analysis_adjoint(const shtc_plan* plan, const double* cilm,
+                          long long csf, long long csk, long long csl,
+                          long long csm, int cilm_dim, double* grid,
+                          long long gsf, long long gsr, long long gsc,
+                          int nfield, void* work, size_t work_bytes,
+                          void* stream);
+
+/* Quadrature on the GPU (device output arrays).
+ * PreGLQ.f95:1-151: n nodes (descending) and weights on [x1, x2];
+ * returns SHTC_ENOZERO if Newton's iteration does not converge.  Synchronises
+ * the stream. */
+SHTC_API int shtc_preglq(double x1, double x2, int n, double* zero, double* w,
+                void* stream);
+/* DHaj.f95:1-107: the n (+extend) Driscoll-Healy weights. */
+SHTC_API int shtc_dhaj(int n, double* aj, int extend, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Stage timing (no counterpart in the reference, which times whole calls  */
+/* with cpu_time, examples/fortran/TimingAccuracy/TimingAccuracyDH.f95:96). */
+/* When enabled, each kernel stage of a transform is bracketed by CUDA      */
+/* events on its stream; collect() waits for them and returns the summed    */
+/* milliseconds and launch counts per stage id.                             */
+/* ------------------------------------------------------------------------ */
+#define SHTC_STAGE_PACK 0
+#define SHTC_STAGE_LEGENDRE_SYNTH 1
+#define SHTC_STAGE_FFT_C2R 2
+#define SHTC_STAGE_FFT_R2C 3
+#define SHTC_STAGE_LEGENDRE_ANAL 4
+#define SHTC_STAGE_UNPACK 5
+#define SHTC_NUM_STAGES 6
+
+SHTC_API int shtc_timing_enable(int on);
+SHTC_API int shtc_timing_collect(double* ms, int* counts, int nstages);
+
+/* ------------------------------------------------------------------------ */
+/* Drop-ins of the reference C interface, include/shtools.h.  Host arrays,  */
+/* Fortran column-major: cilm(2, cilm_dim, cilm_dim), grid(d0, d1).  NULL  */
+/* optional arguments take the reference defaults.  The plx arguments of   */
+/* the GLQ routines (precomputed Legendre tables) are accepted only as     */
+/* NULL; a non-NULL plx returns exitstatus 2.                              */
+/* ------------------------------------------------------------------------ */
+
+/* include/shtools.h:104-116 (src/MakeGridDH.f95:1) */
+SHTC_API void MakeGridDH(double* griddh, const int griddh_d0, const int griddh_d1,
+                int* n, const double* cilm, const int cilm_dim, const int lmax,
+                const int* norm, const int* sampling, const int* csphase,
+                const int* lmax_calc, const int* extend, int* exitstatus);
+
+/* include/shtools.h:92-103 (src/SHExpandDH.f95:1) */
+SHTC_API void SHExpandDH(const double* grid, const int grid_d0, const int grid_d1,
+                const int n, double* cilm, const int cilm_dim, int* lmax,
+                const int* norm, const int* sampling, const int* csphase,
+                const int* lmax_calc, int* exitstatus);
+
+/* include/shtools.h:153-165 (src/MakeGridGLQ.f95:1) */
+SHTC_API void MakeGridGLQ(double* gridglq, const int gridglq_d0, const int gridglq_d1,
+                 const double* cilm, const int cilm_dim, const int lmax,
+                 const double* plx, const double* zero, const int* norm,
+                 const int* csphase, const int* lmax_calc, const int* extend,
+                 int* exitstatus);
+
+/* include/shtools.h:142-152 (src/SHExpandGLQ.f95:1); gridglq is
+ * (lmax+1, 2*lmax+1) column-major as in src/cWrapper.f95:340 */
+SHTC_API void SHExpandGLQ(double* cilm, const int cilm_dim, const int lmax,
+                 const double* gridglq, const double* w, const double* plx,
+                 const double* zero, const int* norm, const int* csphase,
+                 const int* lmax_calc, int* exitstatus);
+
+/* include/shtools.h:134-141 (src/SHGLQ.f95:1); plx must be NULL */
+SHTC_API void SHGLQ(const int lmax, double* zero, double* w, double* plx,
+           const int* norm, const int* csphase, const int* cnorm,
+           int* exitstatus);
+
+/* include/shtools.h:1025-1030 (src/PreGLQ.f95:1) */
+SHTC_API void PreGLQ(const double x1, const double x2, const int n, double* zero,
+            double* w, int* exitstatus);
+
+/* include/shtools.h:1034-1038 (src/DHaj.f95:1) */
+SHTC_API void DHaj(const int n, double* aj, const int aj_d0, const int* extend,
+          int* exitstatus);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHTCUDA_H */

@@ -1,0 +1,106 @@
+"""ctypes binding of libshtcuda (include/shtcuda.h).
+
+The library is loaded from the package tree (shtools_b200/lib/libshtcuda.so).
+There is no fallback: if the library is missing, or no CUDA device is
+visible, every transform raises.  PyTorch supplies device memory and the
+current CUDA stream; the arithmetic happens in the library's kernels.
+"""
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, "lib", "libshtcuda.so")
+
+_P = ctypes.c_void_p
+_LL = ctypes.c_longlong
+_I = ctypes.c_int
+_D = ctypes.c_double
+_SZ = ctypes.c_size_t
+_DP = ctypes.POINTER(ctypes.c_double)
+_IP = ctypes.POINTER(ctypes.c_int)
+
+_lock = threading.Lock()
+_lib = None
+
+# exported C-ABI symbols, in the order of include/shtcuda.h
+EXPORTS = (
+    "shtc_version", "shtc_status_string", "shtc_plan_create_dh",
+    "shtc_plan_create_glq", "shtc_plan_destroy", "shtc_plan_info",
+    "shtc_workspace_bytes", "shtc_synthesis", "shtc_analysis",
+    "shtc_synthesis_adjoint", "shtc_analysis_adjoint", "shtc_preglq",
+    "shtc_dhaj", "MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ",
+    "SHGLQ", "PreGLQ", "DHaj",
+)
+
+
+class SHTCudaError(RuntimeError):
+    """A libshtcuda call returned a non-zero status (reference exit codes 1-5
+    plus GPU-side codes 6-9)."""
+
+    def __init__(self, status, what=""):
+        self.status = int(status)
+        msg = status_string(status)
+        super().__init__("%s%s (status %d)" % (what + ": " if what else "", msg,
+                                               self.status))
+
+
+def _bind(L):
+    L.shtc_version.restype = _I
+    L.shtc_status_string.restype = ctypes.c_char_p
+    L.shtc_status_string.argtypes = [_I]
+    L.shtc_plan_create_dh.argtypes = [ctypes.POINTER(_P), _I, _I, _I, _I, _I, _I, _P]
+    L.shtc_plan_create_glq.argtypes = [ctypes.POINTER(_P), _I, _DP, _DP, _I, _I, _I,
+                                       _I, _P]
+    L.shtc_plan_destroy.argtypes = [_P]
+    L.shtc_plan_info.argtypes = [_P, ctypes.POINTER(_LL), _I]
+    L.shtc_workspace_bytes.restype = _SZ
+    L.shtc_workspace_bytes.argtypes = [_P, _I]
+    coef = [_P, _LL, _LL, _LL, _LL, _I]
+    grid = [_P, _LL, _LL, _LL]
+    tail = [_I, _P, _SZ, _P]
+    L.shtc_synthesis.argtypes = [_P] + coef + grid + tail
+    L.shtc_analysis.argtypes = [_P] + grid + coef + tail
+    L.shtc_synthesis_adjoint.argtypes = [_P] + grid + coef + tail
+    L.shtc_analysis_adjoint.argtypes = [_P] + coef + grid + tail
+    L.shtc_preglq.argtypes = [_D, _D, _I, _P, _P, _P]
+    L.shtc_dhaj.argtypes = [_I, _P, _I, _P]
+    L.MakeGridDH.argtypes = [_DP, _I, _I, _IP, _DP, _I, _I, _IP, _IP, _IP, _IP, _IP,
+                             _IP]
+    L.SHExpandDH.argtypes = [_DP, _I, _I, _I, _DP, _I, _IP, _IP, _IP, _IP, _IP, _IP]
+    L.MakeGridGLQ.argtypes = [_DP, _I, _I, _DP, _I, _I, _DP, _DP, _IP, _IP, _IP, _IP,
+                              _IP]
+    L.SHExpandGLQ.argtypes = [_DP, _I, _I, _DP, _DP, _DP, _DP, _IP, _IP, _IP, _IP]
+    L.SHGLQ.argtypes = [_I, _DP, _DP, _DP, _IP, _IP, _IP, _IP]
+    L.PreGLQ.argtypes = [_D, _D, _I, _DP, _DP, _IP]
+    L.DHaj.argtypes = [_I, _DP, _I, _IP, _IP]
+    for name in ("MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ", "SHGLQ",
+                 "PreGLQ", "DHaj"):
+        getattr(L, name).restype = None
+    return L
+
+
+def load(path=None):
+    """Load (once) and return the ctypes handle of libshtcuda."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            p = path or LIBPATH
+            if not os.path.exists(p):
+                raise RuntimeError(
+                    "libshtcuda is not built (%s missing): run "
+                    "`python -m shtools_b200.build`" % p)
+            _lib = _bind(ctypes.CDLL(p))
+        return _lib
+
+
+def status_string(status):
+    try:
+        return load().shtc_status_string(int(status)).decode()
+    except Exception:  # library missing: generic text
+        return "status %d" % status
+
+
+def check(status, what=""):
+    if status != 0:
+        raise SHTCudaError(status, what)

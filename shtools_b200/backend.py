@@ -1,0 +1,132 @@
+"""The 'cuda' backend of pyshtools.
+
+A module with the function signatures of the reference's non-Fortran backend
+(pyshtools/backends/ducc0_wrapper.py:454, 659, 837, 1003): numpy arrays in,
+numpy arrays out, the arithmetic on the GPU.  After ``register()``,
+``pyshtools.backends.select_preferred_backend('cuda')`` makes
+``SHCoeffs.expand()`` and ``SHGrid.expand()`` run here unchanged
+(pyshtools/shclasses/shcoeffs.py:4343-4377, shgrid.py:2105, 3011).
+
+Only the real DH and GLQ transforms are implemented on the GPU.  The other
+names that the backend injectors rebind (pyshtools/expand/__init__.py:91-111,
+pyshtools/rotate/__init__.py:18-21) are taken from the reference's own
+'shtools' backend when pyshtools is importable, so that switching backends
+never removes a function; without pyshtools they raise NotImplementedError.
+"""
+import sys
+
+import numpy as np
+
+from . import transforms as _t
+
+__all__ = ["MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ", "SHGLQ",
+           "MakeGridDHC", "SHExpandDHC", "MakeGridGLQC", "SHExpandGLQC",
+           "MakeGradientDH", "SHRotateRealCoef", "available", "register",
+           "set_nthreads"]
+
+
+def available():
+    """True when libshtcuda loads and a CUDA device is visible."""
+    try:
+        import torch
+        from . import _lib
+        _lib.load()
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def set_nthreads(ntnew):
+    """Accepted for interface compatibility with the ducc backend; the GPU
+    backend has no host thread pool."""
+    return None
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def MakeGridDH(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
+               extend=False):
+    """griddh = MakeGridDH(cilm, [lmax, norm, sampling, csphase, lmax_calc,
+    extend]) -- see src/MakeGridDH.f95:1 and ducc0_wrapper.py:454."""
+    return _np(_t.MakeGridDH(np.asarray(cilm, dtype=np.float64), lmax=lmax,
+                             norm=norm, sampling=sampling, csphase=csphase,
+                             lmax_calc=lmax_calc, extend=extend))
+
+
+def SHExpandDH(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None):
+    """cilm = SHExpandDH(griddh, [norm, sampling, csphase, lmax_calc]) -- see
+    src/SHExpandDH.f95:1 and ducc0_wrapper.py:659."""
+    return _np(_t.SHExpandDH(np.asarray(griddh, dtype=np.float64), norm=norm,
+                             sampling=sampling, csphase=csphase,
+                             lmax_calc=lmax_calc))
+
+
+def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
+                extend=False):
+    """gridglq = MakeGridGLQ(cilm, [zero, lmax, norm, csphase, lmax_calc,
+    extend]) -- see src/MakeGridGLQ.f95:1 and ducc0_wrapper.py:837.  With
+    zero=None the nodes come from the GPU PreGLQ."""
+    return _np(_t.MakeGridGLQ(np.asarray(cilm, dtype=np.float64), zero=zero,
+                              lmax=lmax, norm=norm, csphase=csphase,
+                              lmax_calc=lmax_calc, extend=extend))
+
+
+def SHExpandGLQ(gridglq, w=None, zero=None, norm=1, csphase=1, lmax_calc=None):
+    """cilm = SHExpandGLQ(gridglq, [w, zero, norm, csphase, lmax_calc]) -- see
+    src/SHExpandGLQ.f95:1 and ducc0_wrapper.py:1003."""
+    return _np(_t.SHExpandGLQ(np.asarray(gridglq, dtype=np.float64), w=w,
+                              zero=zero, norm=norm, csphase=csphase,
+                              lmax_calc=lmax_calc))
+
+
+def SHGLQ(lmax):
+    """zero, w = SHGLQ(lmax) -- Gauss-Legendre nodes and weights from the GPU
+    PreGLQ (src/SHGLQ.f95:188)."""
+    return _t.SHGLQ(lmax)
+
+
+def _fallback(name):
+    """The reference 'shtools' backend's function of this name."""
+    try:
+        from pyshtools.backends import shtools as _ref_shtools
+        return getattr(_ref_shtools, name)
+    except Exception:
+        return None
+
+
+def _passthrough(name):
+    def fn(*args, **kwargs):
+        f = _fallback(name)
+        if f is None:
+            raise NotImplementedError(
+                "%s is not part of the GPU transforms (real DH/GLQ only) and "
+                "the reference 'shtools' backend is not importable" % name)
+        return f(*args, **kwargs)
+    fn.__name__ = name
+    fn.__doc__ = ("Delegates to the reference 'shtools' backend: the GPU "
+                  "backend implements the real DH and GLQ transforms only.")
+    return fn
+
+
+MakeGridDHC = _passthrough("MakeGridDHC")
+SHExpandDHC = _passthrough("SHExpandDHC")
+MakeGridGLQC = _passthrough("MakeGridGLQC")
+SHExpandGLQC = _passthrough("SHExpandGLQC")
+MakeGradientDH = _passthrough("MakeGradientDH")
+SHRotateRealCoef = _passthrough("SHRotateRealCoef")
+
+
+def register(registry=None):
+    """Add this module as backend 'cuda' to the pyshtools backend registry
+    (pyshtools/backends/backends.py:27).  ``registry`` may be given
+    explicitly (a module with ``_available_backends``); otherwise
+    pyshtools.backends.backends is used.  pyshtools/backends/__init__.py:29
+    deletes the name ``backends`` from its package, so the module is taken
+    from sys.modules.  Returns the registry module."""
+    if registry is None:
+        import pyshtools  # noqa: F401
+        registry = sys.modules["pyshtools.backends.backends"]
+    registry._available_backends["cuda"] = sys.modules[__name__]
+    return registry

@@ -1,0 +1,429 @@
+// C ABI of libshtcuda: device transforms, their adjoints, and the host-array
+// drop-ins of the reference C interface (include/shtools.h).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "shtc_internal.cuh"
+
+using namespace shtc;
+
+extern "C" int shtc_version(void) { return 100; }
+
+extern "C" const char* shtc_status_string(int s) {
+    switch (s) {
+        case SHTC_OK: return "No errors.";
+        case SHTC_EDIM: return "Improper dimensions of input array.";
+        case SHTC_EBOUND: return "Improper bounds for input variable.";
+        case SHTC_EALLOC: return "Error allocating memory.";
+        case SHTC_EIO: return "File IO error.";
+        case SHTC_ENOZERO: return "Gauss-Legendre nodes missing or not converged.";
+        case SHTC_ECUDA: return "CUDA runtime or kernel launch error.";
+        case SHTC_EHANDLE: return "Null plan handle or required pointer.";
+        case SHTC_EUNSUP: return "Transform size not supported.";
+        case SHTC_EWORK: return "Workspace too small.";
+        default: return "Unknown status.";
+    }
+}
+
+// workspace layout: [coef region | spec region], each 256-byte aligned
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+static size_t coef_region(const shtc_plan* P, int nfield) {
+    const int tiles = anal_tiles(P);
+    return align256((size_t)P->nlm * nfield * sizeof(double2) * (tiles > 1 ? tiles : 1));
+}
+
+static size_t spec_region(const shtc_plan* P, int nfield) {
+    return align256((size_t)nfield * P->npair * (P->lc + 1) * 2 * sizeof(double2));
+}
+
+extern "C" size_t shtc_workspace_bytes(const shtc_plan* P, int nfield) {
+    if (!P || nfield < 1) return 0;
+    return coef_region(P, nfield) + spec_region(P, nfield);
+}
+
+static int check_call(const shtc_plan* P, const void* a, const void* b,
+                      int nfield, void* work, size_t wb) {
+    if (!P || !a || !b) return SHTC_EHANDLE;
+    if (nfield < 1) return SHTC_EBOUND;
+    if (!work || wb < shtc_workspace_bytes(P, nfield)) return SHTC_EWORK;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != P->device) return SHTC_EHANDLE;
+    return SHTC_OK;
+}
+
+extern "C" int shtc_synthesis(const shtc_plan* P, const double* cilm,
+                              long long csf, long long csk, long long csl,
+                              long long csm, int cdim, double* grid,
+                              long long gsf, long long gsr, long long gsc,
+                              int nfield, void* work, size_t wb, void* stream) {
+    int rc = check_call(P, cilm, grid, nfield, work, wb);
+    if (rc) return rc;
+    if (cdim < 1) return SHTC_EDIM;
+    cudaStream_t st = (cudaStream_t)stream;
+    double2* packed = (double2*)work;
+    double2* spec = (double2*)((char*)work + coef_region(P, nfield));
+    stage_begin(SHTC_STAGE_PACK, st);
+    rc = launch_pack_coef(P, cilm, csf, csk, csl, csm, cdim, packed, nfield, 0, st);
+    stage_end(SHTC_STAGE_PACK, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_LEGENDRE_SYNTH, st);
+    rc = launch_legendre_synth(P, packed, spec, nfield, st);
+    stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_FFT_C2R, st);
+    rc = launch_fft_c2r(P, spec, grid, gsf, gsr, gsc, nfield, 0, st);
+    stage_end(SHTC_STAGE_FFT_C2R, st);
+    return rc;
+}
+
+extern "C" int shtc_analysis(const shtc_plan* P, const double* grid,
+                             long long gsf, long long gsr, long long gsc,
+                             double* cilm, long long csf, long long csk,
+                             long long csl, long long csm, int cdim, int nfield,
+                             void* work, size_t wb, void* stream) {
+    int rc = check_call(P, grid, cilm, nfield, work, wb);
+    if (rc) return rc;
+    if (cdim < P->lc + 1) return SHTC_EDIM;
+    cudaStream_t st = (cudaStream_t)stream;
+    double2* partial = (double2*)work;
+    double2* spec = (double2*)((char*)work + coef_region(P, nfield));
+    const int tiles = anal_tiles(P);
+    stage_begin(SHTC_STAGE_FFT_R2C, st);
+    rc = launch_fft_r2c(P, grid, gsf, gsr, gsc, spec, nfield, 1, 0, st);
+    stage_end(SHTC_STAGE_FFT_R2C, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
+    rc = launch_legendre_anal(P, spec, partial, tiles, nfield, st);
+    stage_end(SHTC_STAGE_LEGENDRE_ANAL, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_UNPACK, st);
+    rc = launch_unpack_coef(P, partial, tiles, cilm, csf, csk, csl, csm, cdim, nfield,
+                            1, st);
+    stage_end(SHTC_STAGE_UNPACK, st);
+    return rc;
+}
+
+extern "C" int shtc_synthesis_adjoint(const shtc_plan* P, const double* grid,
+                                      long long gsf, long long gsr,
+                                      long long gsc, double* cilm,
+                                      long long csf, long long csk,
+                                      long long csl, long long csm, int cdim,
+                                      int nfield, void* work, size_t wb,
+                                      void* stream) {
+    int rc = check_call(P, grid, cilm, nfield, work, wb);
+    if (rc) return rc;
+    if (cdim < 1) return SHTC_EDIM;
+    cudaStream_t st = (cudaStream_t)stream;
+    double2* partial = (double2*)work;
+    double2* spec = (double2*)((char*)work + coef_region(P, nfield));
+    const int tiles = anal_tiles(P);
+    stage_begin(SHTC_STAGE_FFT_R2C, st);
+    rc = launch_fft_r2c(P, grid, gsf, gsr, gsc, spec, nfield, 0, P->extend, st);
+    stage_end(SHTC_STAGE_FFT_R2C, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
+    rc = launch_legendre_anal(P, spec, partial, tiles, nfield, st);
+    stage_end(SHTC_STAGE_LEGENDRE_ANAL, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_UNPACK, st);
+    rc = launch_unpack_coef(P, partial, tiles, cilm, csf, csk, csl, csm, cdim, nfield,
+                            0, st);
+    stage_end(SHTC_STAGE_UNPACK, st);
+    return rc;
+}
+
+extern "C" int shtc_analysis_adjoint(const shtc_plan* P, const double* cilm,
+                                     long long csf, long long csk,
+                                     long long csl, long long csm, int cdim,
+                                     double* grid, long long gsf, long long gsr,
+                                     long long gsc, int nfield, void* work,
+                                     size_t wb, void* stream) {
+    int rc = check_call(P, cilm, grid, nfield, work, wb);
+    if (rc) return rc;
+    if (cdim < 1) return SHTC_EDIM;
+    cudaStream_t st = (cudaStream_t)stream;
+    double2* packed = (double2*)work;
+    double2* spec = (double2*)((char*)work + coef_region(P, nfield));
+    stage_begin(SHTC_STAGE_PACK, st);
+    rc = launch_pack_coef(P, cilm, csf, csk, csl, csm, cdim, packed, nfield, 1, st);
+    stage_end(SHTC_STAGE_PACK, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_LEGENDRE_SYNTH, st);
+    rc = launch_legendre_synth(P, packed, spec, nfield, st);
+    stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_FFT_C2R, st);
+    rc = launch_fft_c2r(P, spec, grid, gsf, gsr, gsc, nfield, 1, st);
+    stage_end(SHTC_STAGE_FFT_C2R, st);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// host drop-ins of include/shtools.h
+// ---------------------------------------------------------------------------
+namespace {
+
+struct PlanKey {
+    int kind, lmax, lc, norm, csphase, sampling, extend, device;
+    std::vector<double> zero;
+    bool operator<(const PlanKey& o) const {
+        return std::tie(kind, lmax, lc, norm, csphase, sampling, extend, device, zero) <
+               std::tie(o.kind, o.lmax, o.lc, o.norm, o.csphase, o.sampling, o.extend,
+                        o.device, o.zero);
+    }
+};
+
+std::mutex g_mu;
+std::map<PlanKey, shtc_plan*> g_plans;
+
+// Plans of the host drop-ins are cached per option set and device for the
+// life of the process, like the reference's saved tables.
+int cached_plan(int kind, int lmax, int lc, int norm, int csphase, int sampling,
+                int extend, const double* zero, const double* w, shtc_plan** out,
+                cudaStream_t st) {
+    PlanKey k;
+    k.kind = kind; k.lmax = lmax; k.lc = lc; k.norm = norm; k.csphase = csphase;
+    k.sampling = sampling; k.extend = extend;
+    cudaGetDevice(&k.device);
+    if (zero) k.zero.assign(zero, zero + lmax + 1);
+    if (w) k.zero.insert(k.zero.end(), w, w + lmax + 1);
+    std::lock_guard<std::mutex> g(g_mu);
+    auto it = g_plans.find(k);
+    if (it != g_plans.end()) { *out = it->second; return SHTC_OK; }
+    shtc_plan* p = nullptr;
+    int rc = kind == SHTC_GRID_DH
+                 ? shtc_plan_create_dh(&p, lmax, sampling, lc, norm, csphase, extend, st)
+                 : shtc_plan_create_glq(&p, lmax, zero, w, lc, norm, csphase, extend, st);
+    if (rc) return rc;
+    g_plans[k] = p;
+    *out = p;
+    return SHTC_OK;
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+    int alloc(size_t b) { return cudaMalloc(&p, b ? b : 8) == cudaSuccess ? SHTC_OK : SHTC_EALLOC; }
+};
+
+void set_status(int* exitstatus, int rc) {
+    if (exitstatus) *exitstatus = rc;
+}
+
+int opt(const int* p, int def) { return p ? *p : def; }
+
+}  // namespace
+
+extern "C" void MakeGridDH(double* griddh, const int d0, const int d1, int* n,
+                           const double* cilm, const int cdim, const int lmax,
+                           const int* norm, const int* sampling,
+                           const int* csphase, const int* lmax_calc,
+                           const int* extend, int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    const int nn = 2 * lmax + 2;
+    if (n) *n = nn;
+    const int samp = opt(sampling, 1), ext = opt(extend, 0), nrm = opt(norm, 1),
+              cs = opt(csphase, 1);
+    if (samp != 1 && samp != 2) return set_status(exitstatus, SHTC_EBOUND);
+    if (ext != 0 && ext != 1) return set_status(exitstatus, SHTC_EBOUND);
+    const int nlat_out = nn + ext, nlon_out = samp * nn + ext;
+    if (d0 < nlat_out || d1 < nlon_out) return set_status(exitstatus, SHTC_EDIM);
+    if (nrm < 1 || nrm > 4) return set_status(exitstatus, SHTC_EBOUND);
+    if (cs != 1 && cs != -1) return set_status(exitstatus, SHTC_EBOUND);
+    int lc = lmax < cdim - 1 ? lmax : cdim - 1;
+    if (lmax_calc) {
+        if (*lmax_calc > lmax) return set_status(exitstatus, SHTC_EBOUND);
+        if (*lmax_calc < lc) lc = *lmax_calc;
+    }
+    if (lc < 0) return set_status(exitstatus, SHTC_EDIM);
+    cudaStream_t st = cudaStreamPerThread;
+    shtc_plan* P = nullptr;
+    int rc = cached_plan(SHTC_GRID_DH, lmax, lc, nrm, cs, samp, ext, nullptr, nullptr, &P, st);
+    if (rc) return set_status(exitstatus, rc);
+    DevBuf dc, dg, dw;
+    const size_t wb = shtc_workspace_bytes(P, 1);
+    if ((rc = dc.alloc(sizeof(double) * 2 * (size_t)cdim * cdim)) ||
+        (rc = dg.alloc(sizeof(double) * (size_t)d0 * d1)) || (rc = dw.alloc(wb)))
+        return set_status(exitstatus, rc);
+    rc = map_cuda(cudaMemcpyAsync(dc.p, cilm, sizeof(double) * 2 * (size_t)cdim * cdim,
+                                  cudaMemcpyHostToDevice, st));
+    if (!rc) rc = shtc_synthesis(P, (const double*)dc.p, 0, 1, 2, 2LL * cdim, cdim,
+                                 (double*)dg.p, 0, 1, d0, 1, dw.p, wb, st);
+    if (!rc) rc = map_cuda(cudaMemcpy2DAsync(griddh, sizeof(double) * d0, dg.p,
+                                             sizeof(double) * d0,
+                                             sizeof(double) * nlat_out, nlon_out,
+                                             cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
+    set_status(exitstatus, rc);
+}
+
+extern "C" void SHExpandDH(const double* grid, const int d0, const int d1,
+                           const int n, double* cilm, const int cdim, int* lmax,
+                           const int* norm, const int* sampling,
+                           const int* csphase, const int* lmax_calc,
+                           int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    const int L = n / 2 - 1;
+    if (lmax) *lmax = L;
+    int lc = L;
+    if (lmax_calc) {
+        if (*lmax_calc > L) return set_status(exitstatus, SHTC_EBOUND);
+        lc = *lmax_calc < L ? *lmax_calc : L;
+    }
+    const int samp = opt(sampling, 1), nrm = opt(norm, 1), cs = opt(csphase, 1);
+    if (samp != 1 && samp != 2) return set_status(exitstatus, SHTC_EBOUND);
+    if (n % 2 != 0) return set_status(exitstatus, SHTC_EBOUND);
+    if (cdim < lc + 1) return set_status(exitstatus, SHTC_EDIM);
+    if (d0 < n || d1 < samp * n) return set_status(exitstatus, SHTC_EDIM);
+    if (cs != 1 && cs != -1) return set_status(exitstatus, SHTC_EBOUND);
+    if (nrm < 1 || nrm > 4) return set_status(exitstatus, SHTC_EBOUND);
+    cudaStream_t st = cudaStreamPerThread;
+    shtc_plan* P = nullptr;
+    int rc = cached_plan(SHTC_GRID_DH, L, lc, nrm, cs, samp, 0, nullptr, nullptr, &P, st);
+    if (rc) return set_status(exitstatus, rc);
+    DevBuf dc, dg, dw;
+    const size_t wb = shtc_workspace_bytes(P, 1);
+    if ((rc = dc.alloc(sizeof(double) * 2 * (size_t)cdim * cdim)) ||
+        (rc = dg.alloc(sizeof(double) * (size_t)d0 * d1)) || (rc = dw.alloc(wb)))
+        return set_status(exitstatus, rc);
+    rc = map_cuda(cudaMemcpyAsync(dg.p, grid, sizeof(double) * (size_t)d0 * d1,
+                                  cudaMemcpyHostToDevice, st));
+    if (!rc) rc = shtc_analysis(P, (const double*)dg.p, 0, 1, d0, (double*)dc.p, 0, 1, 2,
+                                2LL * cdim, cdim, 1, dw.p, wb, st);
+    if (!rc) rc = map_cuda(cudaMemcpyAsync(cilm, dc.p, sizeof(double) * 2 * (size_t)cdim * cdim,
+                                           cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
+    set_status(exitstatus, rc);
+}
+
+extern "C" void MakeGridGLQ(double* gridglq, const int d0, const int d1,
+                            const double* cilm, const int cdim, const int lmax,
+                            const double* plx, const double* zero,
+                            const int* norm, const int* csphase,
+                            const int* lmax_calc, const int* extend,
+                            int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    const int ext = opt(extend, 0), nrm = opt(norm, 1), cs = opt(csphase, 1);
+    if (ext != 0 && ext != 1) return set_status(exitstatus, SHTC_EBOUND);
+    const int nlat = lmax + 1, nlon_out = 2 * lmax + 1 + ext;
+    if (d1 < nlon_out || d0 < nlat) return set_status(exitstatus, SHTC_EDIM);
+    if (plx) return set_status(exitstatus, SHTC_EBOUND);
+    if (!zero) return set_status(exitstatus, SHTC_ENOZERO);
+    if (nrm < 1 || nrm > 4) return set_status(exitstatus, SHTC_EBOUND);
+    if (cs != 1 && cs != -1) return set_status(exitstatus, SHTC_EBOUND);
+    int lc = lmax < cdim - 1 ? lmax : cdim - 1;
+    if (lmax_calc) {
+        if (*lmax_calc > lmax) return set_status(exitstatus, SHTC_EBOUND);
+        if (*lmax_calc < lc) lc = *lmax_calc;
+    }
+    if (lc < 0) return set_status(exitstatus, SHTC_EDIM);
+    cudaStream_t st = cudaStreamPerThread;
+    shtc_plan* P = nullptr;
+    // the analysis weights are not needed for a synthesis: nodes only
+    int rc = cached_plan(SHTC_GRID_GLQ, lmax, lc, nrm, cs, 1, ext, zero, nullptr, &P, st);
+    if (rc) return set_status(exitstatus, rc);
+    DevBuf dc, dg, dw;
+    const size_t wb = shtc_workspace_bytes(P, 1);
+    if ((rc = dc.alloc(sizeof(double) * 2 * (size_t)cdim * cdim)) ||
+        (rc = dg.alloc(sizeof(double) * (size_t)d0 * d1)) || (rc = dw.alloc(wb)))
+        return set_status(exitstatus, rc);
+    rc = map_cuda(cudaMemcpyAsync(dc.p, cilm, sizeof(double) * 2 * (size_t)cdim * cdim,
+                                  cudaMemcpyHostToDevice, st));
+    if (!rc) rc = shtc_synthesis(P, (const double*)dc.p, 0, 1, 2, 2LL * cdim, cdim,
+                                 (double*)dg.p, 0, 1, d0, 1, dw.p, wb, st);
+    if (!rc) rc = map_cuda(cudaMemcpy2DAsync(gridglq, sizeof(double) * d0, dg.p,
+                                             sizeof(double) * d0, sizeof(double) * nlat,
+                                             nlon_out, cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
+    set_status(exitstatus, rc);
+}
+
+extern "C" void SHExpandGLQ(double* cilm, const int cdim, const int lmax,
+                            const double* gridglq, const double* w,
+                            const double* plx, const double* zero,
+                            const int* norm, const int* csphase,
+                            const int* lmax_calc, int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    int lc = lmax;
+    if (lmax_calc) {
+        if (*lmax_calc > lmax) return set_status(exitstatus, SHTC_EBOUND);
+        lc = *lmax_calc < lmax ? *lmax_calc : lmax;
+    }
+    if (cdim < lc + 1) return set_status(exitstatus, SHTC_EDIM);
+    if (!w) return set_status(exitstatus, SHTC_EDIM);
+    if (plx) return set_status(exitstatus, SHTC_EBOUND);
+    if (!zero) return set_status(exitstatus, SHTC_ENOZERO);
+    const int nrm = opt(norm, 1), cs = opt(csphase, 1);
+    if (nrm < 1 || nrm > 4) return set_status(exitstatus, SHTC_EBOUND);
+    if (cs != 1 && cs != -1) return set_status(exitstatus, SHTC_EBOUND);
+    const int nlat = lmax + 1, nlon = 2 * lmax + 1;
+    cudaStream_t st = cudaStreamPerThread;
+    shtc_plan* P = nullptr;
+    int rc = cached_plan(SHTC_GRID_GLQ, lmax, lc, nrm, cs, 1, 0, zero, w, &P, st);
+    if (rc) return set_status(exitstatus, rc);
+    DevBuf dc, dg, dw;
+    const size_t wb = shtc_workspace_bytes(P, 1);
+    if ((rc = dc.alloc(sizeof(double) * 2 * (size_t)cdim * cdim)) ||
+        (rc = dg.alloc(sizeof(double) * (size_t)nlat * nlon)) || (rc = dw.alloc(wb)))
+        return set_status(exitstatus, rc);
+    rc = map_cuda(cudaMemcpyAsync(dg.p, gridglq, sizeof(double) * (size_t)nlat * nlon,
+                                  cudaMemcpyHostToDevice, st));
+    if (!rc) rc = shtc_analysis(P, (const double*)dg.p, 0, 1, nlat, (double*)dc.p, 0, 1, 2,
+                                2LL * cdim, cdim, 1, dw.p, wb, st);
+    if (!rc) rc = map_cuda(cudaMemcpyAsync(cilm, dc.p, sizeof(double) * 2 * (size_t)cdim * cdim,
+                                           cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
+    set_status(exitstatus, rc);
+}
+
+extern "C" void PreGLQ(const double x1, const double x2, const int n,
+                       double* zero, double* w, int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    if (n < 1 || !zero || !w) return set_status(exitstatus, SHTC_EDIM);
+    cudaStream_t st = cudaStreamPerThread;
+    DevBuf dz, dw;
+    int rc;
+    if ((rc = dz.alloc(sizeof(double) * n)) || (rc = dw.alloc(sizeof(double) * n)))
+        return set_status(exitstatus, rc);
+    rc = shtc_preglq(x1, x2, n, (double*)dz.p, (double*)dw.p, st);
+    if (!rc) rc = map_cuda(cudaMemcpyAsync(zero, dz.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaMemcpyAsync(w, dw.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
+    set_status(exitstatus, rc);
+}
+
+extern "C" void SHGLQ(const int lmax, double* zero, double* w, double* plx,
+                      const int* norm, const int* csphase, const int* cnorm,
+                      int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    if (plx) return set_status(exitstatus, SHTC_EBOUND);
+    if (lmax < 0) return set_status(exitstatus, SHTC_EBOUND);
+    PreGLQ(-1.0, 1.0, lmax + 1, zero, w, exitstatus);
+}
+
+extern "C" void DHaj(const int n, double* aj, const int aj_d0, const int* extend,
+                     int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    const int ext = opt(extend, 0);
+    if (n % 2 != 0) return set_status(exitstatus, SHTC_EBOUND);
+    if (ext != 0 && ext != 1) return set_status(exitstatus, SHTC_EBOUND);
+    if (aj_d0 < n + ext) return set_status(exitstatus, SHTC_EDIM);
+    cudaStream_t st = cudaStreamPerThread;
+    DevBuf da;
+    int rc;
+    if ((rc = da.alloc(sizeof(double) * (n + ext)))) return set_status(exitstatus, rc);
+    rc = shtc_dhaj(n, (double*)da.p, ext, st);
+    if (!rc) rc = map_cuda(cudaMemcpyAsync(aj, da.p, sizeof(double) * (n + ext),
+                                           cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
+    set_status(exitstatus, rc);
+}

@@ -1,0 +1,119 @@
+// Internal declarations shared by the libshtcuda translation units.
+//
+// Terminology (follows the reference Fortran, src/MakeGridDH.f95 and
+// src/MakeGridGLQ.f95):
+//   L      bandwidth (lmax) that fixes the grid
+//   lc     lmax_comp = min(L, lmax_calc, cilm_dim-1): highest degree computed
+//   ring   one latitude row of the grid
+//   pair   a northern ring and its mirror ring (z -> -z) that share one
+//          Legendre recursion through P_lm(-z) = (-1)^(l+m) P_lm(z)
+//   spec   per (pair, m) Fourier coefficients of the two rings; the hand-off
+//          buffer between the Legendre kernels and the longitude FFTs
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "../../include/shtcuda.h"
+
+namespace shtc {
+
+// The Holmes-Featherstone scale factor of the reference (MakeGridDH.f95:228).
+constexpr double kScalef = 1.0e-280;
+
+// Maximum FFT radix handled by the in-shared-memory Stockham passes; other
+// prime factors go through Bluestein's algorithm.
+constexpr int kMaxRadix = 13;
+constexpr int kMaxFactors = 40;
+
+struct FftPlan {
+    int n;             // real transform length (grid columns, nlong)
+    int mode;          // 0: two rings in one complex length-n FFT (odd n)
+                       // 1: one ring via a complex FFT of length n/2 (even n)
+    int m;             // complex FFT length executed in shared memory
+    int nfac;          // radices of the length-m (or Bluestein) FFT
+    int fac[kMaxFactors];
+    int bluestein;     // 1 if m has a prime factor > kMaxRadix
+    int mb;            // Bluestein convolution length (power of two)
+    double2* d_tw;     // exp(-2 pi i t / len), t < len; len = mb if bluestein else m
+    double2* d_twn;    // mode 1: exp(-2 pi i k / n), k < n/2
+    double2* d_chirp;  // Bluestein: exp(-i pi t^2 / m), t < m
+    double2* d_kern;   // Bluestein: FFT_mb of the conjugate chirp kernel
+    size_t smem;       // dynamic shared memory bytes per CTA
+    int threads;       // CTA size
+};
+
+}  // namespace shtc
+
+// The opaque plan handle of the C ABI.
+struct shtc_plan {
+    int kind;          // SHTC_GRID_DH or SHTC_GRID_GLQ
+    int lmax;          // L
+    int lc;            // lmax_comp
+    int norm;          // 1..4
+    int csphase;       // +1 / -1
+    int sampling;      // DH: 1 or 2; GLQ: 1
+    int extend;        // synthesis output has the extra column (and DH row)
+    int nlat;          // rings of the grid without the extend row
+    int nlon;          // longitudes without the extend column (FFT length)
+    int nlat_out;      // synthesis output rows (with extend)
+    int nlon_out;      // synthesis output columns (with extend)
+    int npair;         // ring pairs
+    long long nlm;     // packed (l, m) count, (lc+1)(lc+2)/2
+    // device tables (owned)
+    double2* d_rec;    // {ff1, ff2} per packed (l, m)
+    double* d_pmm;     // sectoral start value per m
+    double* d_rtab;    // rescale factor u^m / scalef per (m, pair)
+    double* d_z;       // cos(colatitude) of the northern ring of each pair
+    int* d_rowN;       // synthesis rows of a pair (-1: none)
+    int* d_rowS;
+    int* d_arowN;      // analysis rows of a pair (-1: not used)
+    int* d_arowS;
+    double* d_wN;      // analysis ring weights (quadrature x 2pi or sqrt(2pi)...)
+    double* d_wS;
+    double* d_nrm;     // per packed (l, m): analysis normalisation divisor
+    shtc::FftPlan fft;
+    size_t device_bytes;
+    int device;        // CUDA device the tables live on
+};
+
+namespace shtc {
+
+// Packed (l, m) layout: for m = 0..lc, l = m..lc; offset of (m, m).
+__host__ __device__ inline long long packed_off(int m, int lc) {
+    return (long long)m * (2LL * lc + 3 - m) / 2;
+}
+
+// plan.cu
+int build_fft_plan(FftPlan* f, int n, cudaStream_t stream);
+void free_fft_plan(FftPlan* f);
+
+// kernels.cu launchers (return cudaGetLastError() mapped to SHTC codes)
+int launch_pack_coef(const shtc_plan* P, const double* cilm, long long sf,
+                     long long sk, long long sl, long long sm, int cdim,
+                     double2* packed, int nfield, int scale_mode,
+                     cudaStream_t st);
+int launch_legendre_synth(const shtc_plan* P, const double2* packed,
+                          double2* spec, int nfield, cudaStream_t st);
+int launch_fft_c2r(const shtc_plan* P, const double2* spec, double* grid,
+                   long long gf, long long grs, long long gcs, int nfield,
+                   int weighted, cudaStream_t st);
+int launch_fft_r2c(const shtc_plan* P, const double* grid, long long gf,
+                   long long grs, long long gcs, double2* spec, int nfield,
+                   int weighted, int fold_extend, cudaStream_t st);
+int launch_legendre_anal(const shtc_plan* P, const double2* spec,
+                         double2* partial, int ntiles_out, int nfield,
+                         cudaStream_t st);
+int launch_unpack_coef(const shtc_plan* P, const double2* partial, int ntiles,
+                       double* cilm, long long sf, long long sk, long long sl,
+                       long long sm, int cdim, int nfield, int normalise,
+                       cudaStream_t st);
+int anal_tiles(const shtc_plan* P);
+int map_cuda(cudaError_t e);
+
+// timing.cu: event brackets around kernel stages (SHTC_STAGE_* ids)
+void stage_begin(int stage, cudaStream_t st);
+void stage_end(int stage, cudaStream_t st);
+
+}  // namespace shtc

@@ -1,0 +1,431 @@
+"""Torch front end of the CUDA transforms: plans, device tensors, batches and
+autograd.
+
+Functions take and return CUDA tensors (float64).  A leading batch of fields
+is allowed: cilm of shape (..., 2, D, D), grids of shape (..., nlat, nlon).
+Argument names, defaults and lmax / lmax_calc resolution follow the
+reference's Python API (src/pyshtools.pyf:235-376 and the Fortran routines):
+
+    MakeGridDH (cilm, lmax, norm, sampling, csphase, lmax_calc, extend)
+    SHExpandDH (grid, norm, sampling, csphase, lmax_calc)
+    MakeGridGLQ(cilm, zero, lmax, norm, csphase, lmax_calc, extend)
+    SHExpandGLQ(grid, w, zero, norm, csphase, lmax_calc)
+
+All four are differentiable: the backward pass runs the hand-written
+adjoint kernels (the weighted transpose transforms, which recompute the
+Legendre functions).
+"""
+import threading
+
+import numpy as np
+import torch
+
+from . import _lib
+
+GRID_DH = 1
+GRID_GLQ = 2
+
+
+def _stream_ptr(device):
+    return ctypes_void(torch.cuda.current_stream(device).cuda_stream)
+
+
+def ctypes_void(x):
+    import ctypes
+    return ctypes.c_void_p(int(x))
+
+
+class Plan:
+    """Device tables for one grid and option set (wraps shtc_plan).
+
+    Creation synchronises the current stream; transforms do not.
+    """
+
+    def __init__(self, kind, lmax, lmax_calc=None, norm=1, csphase=1,
+                 sampling=1, extend=0, zero=None, w=None, device=None):
+        import ctypes
+        self.lib = _lib.load()
+        if device is None:
+            device = torch.device("cuda", torch.cuda.current_device())
+        device = torch.device(device)
+        if device.index is None:
+            device = torch.device("cuda", torch.cuda.current_device())
+        self.device = device
+        lc = -1 if lmax_calc is None else int(lmax_calc)
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            st = _stream_ptr(self.device)
+            if kind == GRID_DH:
+                rc = self.lib.shtc_plan_create_dh(ctypes.byref(h), int(lmax),
+                                                  int(sampling), lc, int(norm),
+                                                  int(csphase), int(extend), st)
+            else:
+                zp = wp = None
+                if zero is not None:
+                    self._zero = np.ascontiguousarray(zero, dtype=np.float64)
+                    zp = self._zero.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+                if w is not None:
+                    self._w = np.ascontiguousarray(w, dtype=np.float64)
+                    wp = self._w.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+                rc = self.lib.shtc_plan_create_glq(ctypes.byref(h), int(lmax), zp, wp,
+                                                   lc, int(norm), int(csphase),
+                                                   int(extend), st)
+        _lib.check(rc, "plan creation")
+        self.handle = h
+        info = (ctypes.c_longlong * 16)()
+        _lib.check(self.lib.shtc_plan_info(h, info, 16))
+        keys = ("kind", "lmax", "lmax_comp", "norm", "csphase", "sampling",
+                "extend", "nlat", "nlon", "nlat_out", "nlon_out", "npair", "nlm",
+                "device_bytes", "bluestein", "fft_mode")
+        self.info = {k: int(v) for k, v in zip(keys, info)}
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self.lib.shtc_plan_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+    @property
+    def lc(self):
+        return self.info["lmax_comp"]
+
+    def workspace(self, nfield):
+        nb = int(self.lib.shtc_workspace_bytes(self.handle, int(nfield)))
+        return torch.empty(nb, dtype=torch.uint8, device=self.device), nb
+
+    # -- raw transforms on (F, 2, D, D) / (F, rows, cols) float64 tensors ----
+    def _run(self, fn, src, dst, nfield, src_is_coef):
+        ws, nb = self.workspace(nfield)
+        with torch.cuda.device(self.device):
+            st = _stream_ptr(self.device)
+            c, g = (src, dst) if src_is_coef else (dst, src)
+            cargs = (ctypes_void(c.data_ptr()), c.stride(0), c.stride(1),
+                     c.stride(2), c.stride(3), c.shape[2])
+            gargs = (ctypes_void(g.data_ptr()), g.stride(0), g.stride(1),
+                     g.stride(2))
+            args = (cargs + gargs) if src_is_coef else (gargs + cargs)
+            rc = fn(self.handle, *args, int(nfield), ctypes_void(ws.data_ptr()),
+                    nb, st)
+        _lib.check(rc, fn.__name__)
+
+    def synthesis(self, cilm, out=None):
+        F = cilm.shape[0]
+        if out is None:
+            out = torch.empty((F, self.info["nlat_out"], self.info["nlon_out"]),
+                              dtype=torch.float64, device=self.device)
+        self._run(self.lib.shtc_synthesis, cilm, out, F, True)
+        return out
+
+    def analysis(self, grid, cdim=None, out=None):
+        F = grid.shape[0]
+        cdim = self.lc + 1 if cdim is None else cdim
+        if out is None:
+            out = torch.empty((F, 2, cdim, cdim), dtype=torch.float64,
+                              device=self.device)
+        self._run(self.lib.shtc_analysis, grid, out, F, False)
+        return out
+
+    def synthesis_adjoint(self, grid, cdim):
+        F = grid.shape[0]
+        out = torch.empty((F, 2, cdim, cdim), dtype=torch.float64,
+                          device=self.device)
+        self._run(self.lib.shtc_synthesis_adjoint, grid, out, F, False)
+        return out
+
+    def analysis_adjoint(self, cilm):
+        F = cilm.shape[0]
+        out = torch.empty((F, self.info["nlat"], self.info["nlon"]),
+                          dtype=torch.float64, device=self.device)
+        self._run(self.lib.shtc_analysis_adjoint, cilm, out, F, True)
+        return out
+
+
+_cache_lock = threading.Lock()
+_plans = {}
+
+
+def get_plan(kind, lmax, lmax_calc, norm, csphase, sampling=1, extend=0,
+             zero=None, w=None, device=None):
+    """Cached Plan for the option set (thread-safe)."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None \
+        else torch.device(device)
+    if dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    zkey = None if zero is None else np.asarray(zero, dtype=np.float64).tobytes()
+    wkey = None if w is None else np.asarray(w, dtype=np.float64).tobytes()
+    key = (kind, int(lmax), int(lmax_calc), int(norm), int(csphase),
+           int(sampling), int(extend), dev.index, zkey, wkey)
+    with _cache_lock:
+        p = _plans.get(key)
+        if p is None:
+            p = Plan(kind, lmax, lmax_calc, norm, csphase, sampling, extend,
+                     zero, w, dev)
+            _plans[key] = p
+        return p
+
+
+def clear_plan_cache():
+    with _cache_lock:
+        _plans.clear()
+
+
+# ---------------------------------------------------------------------------
+# argument resolution (Fortran semantics, MakeGridDH.f95:109-251)
+# ---------------------------------------------------------------------------
+def _check_common(norm, csphase):
+    if norm not in (1, 2, 3, 4):
+        raise ValueError("norm must be 1 (geodesy), 2 (Schmidt), 3 "
+                         "(unnormalized) or 4 (orthonormalized); got %r" % (norm,))
+    if csphase not in (1, -1):
+        raise ValueError("csphase must be 1 or -1; got %r" % (csphase,))
+
+
+def _resolve_synth(shape, lmax, lmax_calc):
+    """lmax and lmax_comp of a synthesis from the cilm shape, as the
+    reference: lmax defaults to the cilm degree, lmax_calc to lmax, and
+    lmax_comp = min(lmax, cilm degree, lmax_calc) (MakeGridDH.f95:230-251,
+    src/pyshtools.pyf:266-268)."""
+    if len(shape) < 3 or shape[-3] < 2 or shape[-1] != shape[-2]:
+        raise ValueError("cilm must be dimensioned as (..., 2, lmax+1, lmax+1); "
+                         "got %s" % (tuple(shape),))
+    D = int(shape[-1])
+    lmax = D - 1 if lmax is None else int(lmax)
+    if lmax < 0:
+        raise ValueError("lmax must be >= 0")
+    if lmax_calc is None:
+        lmax_calc = lmax
+    if lmax_calc > lmax:
+        raise ValueError("lmax_calc (%d) must be less than or equal to lmax (%d)"
+                         % (lmax_calc, lmax))
+    lc = min(lmax, D - 1, int(lmax_calc))
+    return lmax, lc
+
+
+def _resolve_anal_dh(shape, sampling, lmax_calc):
+    """lmax = n/2-1 and lmax_comp of SHExpandDH (SHExpandDH.f95:118-235)."""
+    if sampling not in (1, 2):
+        raise ValueError("sampling must be 1 (n by n) or 2 (n by 2n); got %r"
+                         % (sampling,))
+    if len(shape) < 2:
+        raise ValueError("griddh must be two-dimensional; got %s" % (tuple(shape),))
+    n = int(shape[-2])
+    if n % 2 != 0 or n < 2:
+        raise ValueError("The number of samples in latitude, n, must be even; "
+                         "got %d" % n)
+    if shape[-1] < sampling * n:
+        raise ValueError("griddh must be dimensioned as (n, %s); got %s"
+                         % ("n" if sampling == 1 else "2n", tuple(shape)))
+    lmax = n // 2 - 1
+    lc = lmax if lmax_calc is None else int(lmax_calc)
+    if lc > lmax:
+        raise ValueError("lmax_calc (%d) must be less than or equal to lmax (%d)"
+                         % (lc, lmax))
+    return lmax, lc
+
+
+def _resolve_anal_glq(shape, lmax_calc):
+    """lmax = nlat-1 and lmax_comp of SHExpandGLQ (SHExpandGLQ.f95:98-160)."""
+    if len(shape) < 2:
+        raise ValueError("gridglq must be two-dimensional; got %s" % (tuple(shape),))
+    lmax = int(shape[-2]) - 1
+    if shape[-1] < 2 * lmax + 1:
+        raise ValueError("gridglq must be dimensioned as (lmax+1, 2*lmax+1); "
+                         "got %s" % (tuple(shape),))
+    lc = lmax if lmax_calc is None else int(lmax_calc)
+    if lc > lmax:
+        raise ValueError("lmax_calc (%d) must be less than or equal to lmax (%d)"
+                         % (lc, lmax))
+    return lmax, lc
+
+
+def _flat(t, tail):
+    lead = t.shape[:t.dim() - tail]
+    return t.reshape((-1,) + tuple(t.shape[t.dim() - tail:])), lead
+
+
+def _as_cuda64(t, what):
+    if isinstance(t, np.ndarray):
+        t = torch.from_numpy(t)
+    if not isinstance(t, torch.Tensor):
+        t = torch.as_tensor(t)
+    if not t.is_cuda:
+        t = t.to("cuda")
+    if t.dtype != torch.float64:
+        t = t.to(torch.float64)
+    return t
+
+
+# ---------------------------------------------------------------------------
+# autograd functions
+# ---------------------------------------------------------------------------
+class _Synthesis(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, cilm, plan):
+        c, lead = _flat(cilm[..., :2, :, :], 3)
+        g = plan.synthesis(c)
+        ctx.plan = plan
+        ctx.cdim = cilm.shape[-1]
+        ctx.lead = lead
+        ctx.cshape = cilm.shape
+        return g.reshape(tuple(lead) + tuple(g.shape[1:]))
+
+    @staticmethod
+    def backward(ctx, gout):
+        plan = ctx.plan
+        g, _ = _flat(gout.contiguous(), 2)
+        gc = plan.synthesis_adjoint(g, ctx.cdim)
+        gc = gc.reshape(tuple(ctx.lead) + tuple(gc.shape[1:]))
+        if ctx.cshape[-3] > 2:
+            pad = torch.zeros(ctx.cshape, dtype=gc.dtype, device=gc.device)
+            pad[..., :2, :, :] = gc
+            gc = pad
+        return gc, None
+
+
+class _Analysis(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, grid, plan, cdim):
+        nlat, nlon = plan.info["nlat"], plan.info["nlon"]
+        g, lead = _flat(grid, 2)
+        c = plan.analysis(g[:, :nlat, :nlon], cdim)
+        ctx.plan = plan
+        ctx.lead = lead
+        ctx.gshape = grid.shape
+        return c.reshape(tuple(lead) + tuple(c.shape[1:]))
+
+    @staticmethod
+    def backward(ctx, gc):
+        plan = ctx.plan
+        c, _ = _flat(gc.contiguous(), 3)
+        g = plan.analysis_adjoint(c)
+        g = g.reshape(tuple(ctx.lead) + tuple(g.shape[1:]))
+        if tuple(g.shape) != tuple(ctx.gshape):
+            full = torch.zeros(ctx.gshape, dtype=g.dtype, device=g.device)
+            full[..., :g.shape[-2], :g.shape[-1]] = g
+            g = full
+        return g, None, None
+
+
+# ---------------------------------------------------------------------------
+# public API
+# ---------------------------------------------------------------------------
+def MakeGridDH(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
+               extend=False):
+    """Driscoll-Healy synthesis on the GPU (src/MakeGridDH.f95:1).
+
+    cilm: (..., 2, D, D) float64.  Returns (..., n+extend, sampling*n+extend)
+    with n = 2*lmax+2; row 0 is 90 N, column 0 is 0 E.
+    """
+    _check_common(norm, csphase)
+    if sampling not in (1, 2):
+        raise ValueError("sampling must be 1 (n by n) or 2 (n by 2n); got %r"
+                         % (sampling,))
+    lmax, lc = _resolve_synth(np.shape(cilm), lmax, lmax_calc)
+    cilm = _as_cuda64(cilm, "cilm")
+    plan = get_plan(GRID_DH, lmax, lc, norm, csphase, sampling, int(bool(extend)),
+                    device=cilm.device)
+    return _Synthesis.apply(cilm, plan)
+
+
+def SHExpandDH(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None):
+    """Driscoll-Healy analysis on the GPU (src/SHExpandDH.f95:1).
+
+    griddh: (..., n, >= sampling*n) float64 with n even.  Returns
+    (..., 2, lmax_calc+1, lmax_calc+1).
+    """
+    _check_common(norm, csphase)
+    lmax, lc = _resolve_anal_dh(np.shape(griddh), sampling, lmax_calc)
+    grid = _as_cuda64(griddh, "griddh")
+    plan = get_plan(GRID_DH, lmax, lc, norm, csphase, sampling, 0,
+                    device=grid.device)
+    return _Analysis.apply(grid, plan, lc + 1)
+
+
+def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
+                extend=False):
+    """Gauss-Legendre synthesis on the GPU (src/MakeGridGLQ.f95:1).
+
+    zero: the lmax+1 Gauss-Legendre nodes (e.g. from SHGLQ); None computes
+    them with the GPU PreGLQ.  Returns (..., lmax+1, 2*lmax+1+extend).
+    """
+    _check_common(norm, csphase)
+    lmax, lc = _resolve_synth(np.shape(cilm), lmax, lmax_calc)
+    z = None if zero is None else _host64(zero, lmax + 1, "zero")
+    cilm = _as_cuda64(cilm, "cilm")
+    plan = get_plan(GRID_GLQ, lmax, lc, norm, csphase, 1, int(bool(extend)),
+                    zero=z, device=cilm.device)
+    return _Synthesis.apply(cilm, plan)
+
+
+def SHExpandGLQ(gridglq, w=None, zero=None, norm=1, csphase=1,
+                lmax_calc=None):
+    """Gauss-Legendre analysis on the GPU (src/SHExpandGLQ.f95:1).
+
+    gridglq: (..., lmax+1, >= 2*lmax+1).  w, zero: weights and nodes from
+    SHGLQ; None computes them with the GPU PreGLQ.
+    """
+    _check_common(norm, csphase)
+    lmax, lc = _resolve_anal_glq(np.shape(gridglq), lmax_calc)
+    nlat = lmax + 1
+    z = None if zero is None else _host64(zero, nlat, "zero")
+    wh = None if w is None else _host64(w, nlat, "w")
+    grid = _as_cuda64(gridglq, "gridglq")
+    if (z is None) != (wh is None):
+        # one given: complete the pair from the GPU PreGLQ
+        zz, ww = SHGLQ(lmax, device=grid.device)
+        z = zz if z is None else z
+        wh = ww if wh is None else wh
+    plan = get_plan(GRID_GLQ, lmax, lc, norm, csphase, 1, 0, zero=z, w=wh,
+                    device=grid.device)
+    return _Analysis.apply(grid, plan, lc + 1)
+
+
+def _host64(a, n, what):
+    if isinstance(a, torch.Tensor):
+        a = a.detach().cpu().numpy()
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel())
+    if a.size < n:
+        raise ValueError("%s must be dimensioned as (%d); got %d" % (what, n, a.size))
+    return a[:n]
+
+
+# ---------------------------------------------------------------------------
+# quadrature (GPU)
+# ---------------------------------------------------------------------------
+def PreGLQ(x1, x2, n, device=None):
+    """Gauss-Legendre nodes (descending) and weights on [x1, x2], computed on
+    the GPU (src/PreGLQ.f95:1).  Returns two float64 CUDA tensors."""
+    lib = _lib.load()
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None \
+        else torch.device(device)
+    zero = torch.empty(int(n), dtype=torch.float64, device=dev)
+    w = torch.empty(int(n), dtype=torch.float64, device=dev)
+    with torch.cuda.device(dev):
+        rc = lib.shtc_preglq(float(x1), float(x2), int(n),
+                             ctypes_void(zero.data_ptr()),
+                             ctypes_void(w.data_ptr()), _stream_ptr(dev))
+    _lib.check(rc, "PreGLQ")
+    return zero, w
+
+
+def SHGLQ(lmax, device=None):
+    """Nodes and weights of the lmax+1 point Gauss-Legendre quadrature
+    (src/SHGLQ.f95:188), as host numpy arrays computed on the GPU."""
+    z, w = PreGLQ(-1.0, 1.0, int(lmax) + 1, device)
+    return z.cpu().numpy(), w.cpu().numpy()
+
+
+def DHaj(n, extend=0, device=None):
+    """Driscoll-Healy weights a_j (src/DHaj.f95:1) computed on the GPU."""
+    lib = _lib.load()
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None \
+        else torch.device(device)
+    aj = torch.empty(int(n) + int(extend), dtype=torch.float64, device=dev)
+    with torch.cuda.device(dev):
+        rc = lib.shtc_dhaj(int(n), ctypes_void(aj.data_ptr()), int(extend),
+                           _stream_ptr(dev))
+    _lib.check(rc, "DHaj")
+    return aj

@@ -1,0 +1,278 @@
+"""GPU parity tests: libshtcuda against the oracle (restated reference) on
+identical seeded inputs.
+
+Tolerances (FP64 path, the gate of the transforms):
+  * grids: max |grid_gpu - grid_oracle| / max |grid_oracle| <= 1e-12;
+  * coefficients: per-degree relative error
+        e(l) = ||c_gpu(l,:) - c_oracle(l,:)||_2 / ||c_oracle(l,:)||_2 <= 1e-11
+    (norm 3, unnormalised and unstable beyond degree ~15 in the reference,
+    uses the max-abs error relative to the grid magnitude instead).
+Full-size cases (lmax 2047 and 2799) compare a window of ring pairs that the
+oracle computes exactly, plus size-independent properties (round trips,
+linearity), because a full oracle transform takes minutes on one core.
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GRID_TOL = 1e-12
+DEG_TOL = 1e-11
+
+
+def perdeg(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    num = np.sqrt(((a - b) ** 2).sum(axis=(0, 2)))
+    den = np.sqrt((b ** 2).sum(axis=(0, 2)))
+    den[den == 0] = 1.0
+    return num / den
+
+
+def grid_rel(a, b):
+    return np.abs(np.asarray(a) - np.asarray(b)).max() / np.abs(np.asarray(b)).max()
+
+
+def coef_check(gpu, ref, norm, grid=None):
+    if norm == 3:
+        # unnormalised functions reach (2l-1)!! ~ 1e15 at l = 15: the sums
+        # cancel catastrophically, so the error scale is the grid magnitude
+        scale = np.abs(grid).max() if grid is not None else np.abs(ref).max()
+        assert np.abs(gpu - ref).max() / scale < 1e-15 * max(1.0, ref.shape[-1] ** 2)
+    else:
+        e = perdeg(gpu, ref)
+        assert e.max() <= DEG_TOL, (e.max(), e.argmax())
+
+
+def _golden():
+    data = np.load(os.path.join(HERE, "golden", "transforms_small.npz"))
+    keys = sorted({k.split("__")[0] for k in data.files})
+    return data, keys
+
+
+_DATA, _KEYS = _golden()
+
+
+def _parse(key):
+    kind, L, norm, cs, samp, ext, lc = key.split("_")
+    return (kind, int(L[1:]), int(norm[1:]), int(cs[1:]), int(samp[1:]),
+            int(ext[1:]), int(lc[2:]))
+
+
+@pytest.mark.parametrize("key", _KEYS)
+def test_golden_synthesis_and_analysis(cuda, key):
+    kind, L, norm, cs, samp, ext, lc = _parse(key)
+    c = _DATA[key + "__cilm"]
+    gref = _DATA[key + "__grid"]
+    bref = _DATA[key + "__back"]
+    ct = torch.from_numpy(c).cuda()
+    if kind == "dh":
+        g = cuda.MakeGridDH(ct, norm=norm, sampling=samp, csphase=cs,
+                            lmax_calc=lc, extend=bool(ext))
+        n = 2 * L + 2
+        b = cuda.SHExpandDH(torch.from_numpy(gref[:n, :samp * n]).cuda(),
+                            norm=norm, sampling=samp, csphase=cs, lmax_calc=lc)
+    else:
+        z = _DATA[key + "__zero"]
+        w = _DATA[key + "__w"]
+        g = cuda.MakeGridGLQ(ct, zero=z, norm=norm, csphase=cs, lmax_calc=lc,
+                             extend=bool(ext))
+        b = cuda.SHExpandGLQ(torch.from_numpy(gref[:, :2 * L + 1]).cuda(), w=w,
+                             zero=z, norm=norm, csphase=cs, lmax_calc=lc)
+    g = g.cpu().numpy()
+    b = b.cpu().numpy()
+    assert g.shape == gref.shape
+    assert grid_rel(g, gref) <= (GRID_TOL if norm != 3 else 1e-11)
+    assert b.shape == bref.shape
+    coef_check(b, bref, norm, gref)
+
+
+@pytest.mark.parametrize("norm", [1, 2, 4])
+@pytest.mark.parametrize("csphase", [1, -1])
+def test_config1_dh255_sampling2(cuda, oracle, norm, csphase):
+    """Plain DH round trip, lmax 255, sampling 2 (512 x 1024), seeded
+    power-law coefficients; full comparison with the oracle."""
+    L = 255
+    c = oracle.power_law_cilm(L, 1000, beta=2.0)
+    g_ref = oracle.makegrid_dh(c, norm=norm, sampling=2, csphase=csphase)
+    b_ref = oracle.shexpand_dh(g_ref, norm=norm, sampling=2, csphase=csphase)
+    g = cuda.MakeGridDH(torch.from_numpy(c).cuda(), norm=norm, sampling=2,
+                        csphase=csphase).cpu().numpy()
+    assert grid_rel(g, g_ref) <= GRID_TOL
+    b = cuda.SHExpandDH(torch.from_numpy(g_ref).cuda(), norm=norm, sampling=2,
+                        csphase=csphase).cpu().numpy()
+    coef_check(b, b_ref, norm)
+
+
+def _window_synthesis_check(cuda, oracle, kind, L, seed, pairs, **kw):
+    c = oracle.power_law_cilm(L, seed, beta=kw.pop("beta", 2.0))
+    ct = torch.from_numpy(c).cuda()
+    if kind == "glq":
+        z, w = oracle.shglq(L)
+        g = cuda.MakeGridGLQ(ct, zero=z, **kw).cpu().numpy()
+        nlat = L + 1
+    else:
+        g = cuda.MakeGridDH(ct, **kw).cpu().numpy()
+        nlat = 2 * L + 2
+    for (lo, hi) in pairs:
+        if kind == "glq":
+            gr = oracle.makegrid_glq(c, zero=z, pair_window=(lo, hi), **kw)
+            rows = [r for p in range(lo, hi) for r in (p, nlat - 1 - p)]
+        else:
+            gr = oracle.makegrid_dh(c, pair_window=(lo, hi), **kw)
+            rows = [r for p in range(lo, hi) for r in (p, nlat - p)]
+        rows = sorted(set(r for r in rows if r < gr.shape[0]))
+        ref = gr[rows]
+        assert grid_rel(g[rows], ref) <= GRID_TOL, (lo, hi)
+    return c, g
+
+
+def _window_analysis_check(cuda, oracle, kind, L, seed, pairs, **kw):
+    """Analysis of a grid that is zero outside a few ring pairs equals the
+    oracle's analysis restricted to those pairs (the analysis is a sum over
+    rings), at full size."""
+    rng = np.random.default_rng(seed)
+    if kind == "glq":
+        nlat, nlon = L + 1, 2 * L + 1
+        z, w = oracle.shglq(L)
+    else:
+        samp = kw.get("sampling", 1)
+        nlat, nlon = 2 * L + 2, kw.get("sampling", 1) * (2 * L + 2)
+    grid = np.zeros((nlat, nlon))
+    for (lo, hi) in pairs:
+        for p in range(lo, hi):
+            grid[p] = rng.standard_normal(nlon)
+            s = (nlat - 1 - p) if kind == "glq" else (nlat - p)
+            if s < nlat:
+                grid[s] = rng.standard_normal(nlon)
+    gt = torch.from_numpy(grid).cuda()
+    if kind == "glq":
+        b = cuda.SHExpandGLQ(gt, w=w, zero=z, **kw).cpu().numpy()
+        ref = sum(oracle.shexpand_glq(grid, w=w, zero=z, pair_window=pw, **kw)
+                  for pw in pairs)
+    else:
+        b = cuda.SHExpandDH(gt, **kw).cpu().numpy()
+        ref = sum(oracle.shexpand_dh(grid, pair_window=pw, **kw) for pw in pairs)
+    e = perdeg(b, ref)
+    assert e.max() <= DEG_TOL, (e.max(), e.argmax())
+
+
+def test_config2_glq2047_window(cuda, oracle):
+    """Plain FP64 GLQ, lmax 2047 (2048 x 4095): synthesis rows of ring pairs
+    near the pole, at mid latitude and at the equator agree with the oracle;
+    the analysis of those rings agrees per degree."""
+    L = 2047
+    pairs = [(0, 2), (400, 402), (1022, 1024)]
+    _window_synthesis_check(cuda, oracle, "glq", L, 2000, pairs)
+    _window_analysis_check(cuda, oracle, "glq", L, 2001, pairs)
+
+
+def test_config3_dh719_sampling2_window(cuda, oracle):
+    L = 719
+    pairs = [(0, 2), (300, 302), (719, 721)]
+    _window_synthesis_check(cuda, oracle, "dh", L, 3000, pairs, sampling=2,
+                            extend=1)
+    _window_analysis_check(cuda, oracle, "dh", L, 3001, pairs, sampling=2)
+
+
+def test_config5_dh2799_window(cuda, oracle):
+    """lmax 2799, sampling 2 (5600 x 11200): rings next to the pole (where
+    the scaled recursion values reach 1e305), at mid latitude and at the
+    equator."""
+    L = 2799
+    pairs = [(0, 2), (1400, 1401), (2799, 2801)]
+    _window_synthesis_check(cuda, oracle, "dh", L, 5000, pairs, sampling=2,
+                            beta=3.0)
+    _window_analysis_check(cuda, oracle, "dh", L, 5001, pairs, sampling=2)
+
+
+def test_roundtrip_glq2047(cuda, oracle):
+    """Size-independent property at full size: analysis(synthesis(c)) = c to
+    the accuracy of the algorithm (the reference itself reaches ~5e-11 per
+    degree at lmax 2047 for S(l) = (l+1)^-2)."""
+    L = 2047
+    c = oracle.power_law_cilm(L, 2002)
+    ct = torch.from_numpy(c).cuda()
+    g = cuda.MakeGridGLQ(ct)
+    b = cuda.SHExpandGLQ(g).cpu().numpy()
+    assert perdeg(b, c).max() < 1e-9
+
+
+def test_linearity_batched(cuda, oracle):
+    """A batch of fields gives the same result as the fields one by one, and
+    the transforms are linear."""
+    L = 95
+    cs = np.stack([oracle.power_law_cilm(L, 100 + i) for i in range(8)])
+    ct = torch.from_numpy(cs).cuda()
+    for samp in (1, 2):
+        g = cuda.MakeGridDH(ct, sampling=samp)
+        for i in (0, 5):
+            gi = cuda.MakeGridDH(ct[i], sampling=samp)
+            assert torch.allclose(g[i], gi, rtol=0, atol=1e-13 * gi.abs().max().item())
+        gsum = cuda.MakeGridDH(ct[0] + 2.0 * ct[1], sampling=samp)
+        assert torch.allclose(gsum, g[0] + 2.0 * g[1], rtol=0,
+                              atol=1e-12 * gsum.abs().max().item())
+        b = cuda.SHExpandDH(g, sampling=samp)
+        b0 = cuda.SHExpandDH(g[3], sampling=samp)
+        assert torch.allclose(b[3], b0, rtol=0, atol=1e-14)
+
+
+def test_preglq_dhaj_gpu(cuda, oracle):
+    for n in (1, 2, 7, 64, 512, 2048):
+        z, w = cuda.PreGLQ(-1.0, 1.0, n)
+        zr, wr = oracle.preglq(-1.0, 1.0, n)
+        assert np.abs(z.cpu().numpy() - zr).max() <= 1e-15
+        # the weights take P'_n at the last-but-one Newton iterate
+        # (PreGLQ.f95:121-146); a one-ulp different starting guess moves that
+        # iterate, so polar weights agree to ~n^2 * 1e-15 relative
+        assert (np.abs(w.cpu().numpy() - wr) / wr).max() <= 1e-8
+    for n in (4, 130, 1440, 5600):
+        a = cuda.DHaj(n).cpu().numpy()
+        ar = oracle.dhaj(n)
+        assert np.abs(a - ar).max() <= 1e-15 * np.abs(ar).max() * 10
+    a = cuda.DHaj(8, extend=1).cpu().numpy()
+    assert a.shape == (9,) and a[-1] == 0.0
+
+
+def test_odd_lengths_bluestein(cuda, oracle):
+    """GLQ grids whose longitude FFT length 2*lmax+1 has a prime factor above
+    13 go through Bluestein's algorithm (config 4 sizes)."""
+    for L in (31, 36, 58, 100, 256, 509):
+        c = oracle.power_law_cilm(L, 4000 + L)
+        z, w = oracle.shglq(L)
+        g = cuda.MakeGridGLQ(torch.from_numpy(c).cuda(), zero=z).cpu().numpy()
+        gr = oracle.makegrid_glq(c, zero=z)
+        assert grid_rel(g, gr) <= GRID_TOL, L
+        b = cuda.SHExpandGLQ(torch.from_numpy(gr).cuda(), w=w, zero=z).cpu().numpy()
+        br = oracle.shexpand_glq(gr, w=w, zero=z)
+        e = perdeg(b, br)
+        assert e.max() <= DEG_TOL, (L, e.max())
+
+
+def test_lmax_calc_and_padding(cuda, oracle):
+    """lmax > cilm degree zero-pads; lmax_calc < lmax truncates
+    (MakeGridDH.f95:72-75, 244-249)."""
+    c = oracle.power_law_cilm(20, 77)
+    g = cuda.MakeGridDH(torch.from_numpy(c).cuda(), lmax=31).cpu().numpy()
+    gr = oracle.makegrid_dh(c, lmax=31)
+    assert g.shape == gr.shape == (64, 64)
+    assert grid_rel(g, gr) <= GRID_TOL
+    g = cuda.MakeGridDH(torch.from_numpy(c).cuda(), lmax_calc=9).cpu().numpy()
+    gr = oracle.makegrid_dh(c, lmax_calc=9)
+    assert grid_rel(g, gr) <= GRID_TOL
+
+
+def test_errors_raise_before_launch(cuda):
+    c = torch.zeros(2, 5, 5, dtype=torch.float64, device="cuda")
+    with pytest.raises(ValueError):
+        cuda.MakeGridDH(c, norm=5)
+    with pytest.raises(ValueError):
+        cuda.MakeGridDH(c, sampling=3)
+    with pytest.raises(ValueError):
+        cuda.MakeGridDH(c, lmax_calc=9)
+    with pytest.raises(ValueError):
+        cuda.SHExpandDH(torch.zeros(7, 7, dtype=torch.float64, device="cuda"))
