@@ -135,6 +135,24 @@ SHTC_API int shtc_preglq(double x1, double x2, int n, double* zero, double* w,
 /* DHaj.f95:1-107: the n (+extend) Driscoll-Healy weights. */
 SHTC_API int shtc_dhaj(int n, double* aj, int extend, void* stream);
 
+/* Synthesis without allocation.  No counterpart in the reference: it is
+ * shtc_synthesis with the workspace taken from a fixed array inside the
+ * library, for callers that must not allocate device memory inside their own
+ * calls (memory owned by a pool or budget manager, or loops that cannot
+ * afford cudaMalloc's implicit synchronisation).  The array holds
+ * SHTC_NOALLOC_SCRATCH_BYTES on every GPU that loads the library, until
+ * exit.  Transforms needing more (shtc_workspace_bytes(plan, nfield) above
+ * that size, e.g. one DH field beyond lmax ~600) return SHTC_EWORK without
+ * launching.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and caches it: make it before any stream
+ * capture.  All calls share the array; calls that overlap on the GPU race. */
+#define SHTC_NOALLOC_SCRATCH_BYTES (16u << 20)
+SHTC_API int shtc_synthesis_noalloc(const shtc_plan* plan, const double* cilm,
+                                    long long csf, long long csk, long long csl,
+                                    long long csm, int cilm_dim, double* grid,
+                                    long long gsf, long long gsr, long long gsc,
+                                    int nfield, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Stage timing (no counterpart in the reference, which times whole calls  */
 /* with cpu_time, examples/fortran/TimingAccuracy/TimingAccuracyDH.f95:96). */
