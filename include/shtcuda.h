@@ -84,6 +84,14 @@ SHTC_API int shtc_plan_destroy(shtc_plan* plan);
  * fft_mode */
 SHTC_API int shtc_plan_info(const shtc_plan* plan, long long* info, int ninfo);
 
+/* Tile shapes of the Legendre kernels (no counterpart in the reference):
+ * ring pairs per thread of the single-field synthesis, and ring pairs per
+ * thread and warps per CTA of the analysis; each 1, 2, 4 or 8, or 0 for the
+ * built-in heuristic.  Used by the autotuner; query shtc_workspace_bytes
+ * after changing them. */
+SHTC_API int shtc_plan_set_tuning(shtc_plan* plan, int synth_T, int anal_T,
+                                  int anal_W);
+
 /* Device workspace bytes needed by any transform of nfield fields. */
 SHTC_API size_t shtc_workspace_bytes(const shtc_plan* plan, int nfield);
 

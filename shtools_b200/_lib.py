@@ -27,6 +27,8 @@ _lib = None
 EXPORTS = (
     "shtc_version", "shtc_status_string", "shtc_plan_create_dh",
     "shtc_plan_create_glq", "shtc_plan_destroy", "shtc_plan_info",
+    "shtc_plan_set_tuning", "shtc_timing_enable", "shtc_timing_collect",
+    "shtc_synthesis_noalloc",
     "shtc_workspace_bytes", "shtc_synthesis", "shtc_analysis",
     "shtc_synthesis_adjoint", "shtc_analysis_adjoint", "shtc_preglq",
     "shtc_dhaj", "MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ",
@@ -54,6 +56,7 @@ def _bind(L):
                                        _I, _P]
     L.shtc_plan_destroy.argtypes = [_P]
     L.shtc_plan_info.argtypes = [_P, ctypes.POINTER(_LL), _I]
+    L.shtc_plan_set_tuning.argtypes = [_P, _I, _I, _I]
     L.shtc_workspace_bytes.restype = _SZ
     L.shtc_workspace_bytes.argtypes = [_P, _I]
     coef = [_P, _LL, _LL, _LL, _LL, _I]

@@ -45,6 +45,20 @@ __device__ __forceinline__ double rec_step(double z, double2 f, double q1,
 
 int map_cuda(cudaError_t e) { return e == cudaSuccess ? SHTC_OK : SHTC_ECUDA; }
 
+// 16-byte asynchronous global -> shared copies (sm_80+ cp.async), used to
+// prefetch the next chunk of per-degree data while the current one is used.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::);
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
 // ---------------------------------------------------------------------------
 // coefficient packing
 // ---------------------------------------------------------------------------
@@ -93,14 +107,46 @@ __global__ void k_pack_coef(const double* __restrict__ cilm, long long sf,
 // holds the c2r input of the ring: (a_m - i b_m) * (m ? 1/2 : 1) with
 // a_m = sum_l C_lm P_lm, b_m = sum_l S_lm P_lm (MakeGridDH.f95:566-612).
 template <int T, int NF>
+__device__ __forceinline__ void synth_step(bool odd, double2 f, const double2* c,
+                                           const double* z, double* q1, double* q2,
+                                           double (*eR)[NF], double (*eI)[NF],
+                                           double (*oR)[NF], double (*oI)[NF]) {
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+        const double p = rec_step(z[t], f, q1[t], q2[t]);
+        q2[t] = q1[t];
+        q1[t] = p;
+#pragma unroll
+        for (int j = 0; j < NF; ++j) {
+            if (odd) {
+                oR[t][j] = fma(c[j].x, p, oR[t][j]);
+                oI[t][j] = fma(c[j].y, p, oI[t][j]);
+            } else {
+                eR[t][j] = fma(c[j].x, p, eR[t][j]);
+                eI[t][j] = fma(c[j].y, p, eI[t][j]);
+            }
+        }
+    }
+}
+
+// CTA = (ring-pair tile, order m); the grid runs m = 0, 1, ... so the
+// longest recursions start first and the hardware scheduler balances the
+// triangular work.  Per degree the CTA needs {ff1, ff2} and NF x {C, S}
+// (16 bytes each); chunks of kSynthChunk degrees are copied into shared
+// memory with cp.async one chunk ahead of their use.
+constexpr int kSynthChunk = 32;
+
+template <int T, int NF>
 __global__ void __launch_bounds__(128)
 k_legendre_synth(const double2* __restrict__ rec, const double* __restrict__ pmm,
                  const double* __restrict__ rtab, const double* __restrict__ zp,
                  const double2* __restrict__ coef, double2* __restrict__ spec,
                  int lc, int npair, int nfield) {
-    const int x = blockIdx.x;
+    constexpr int R = 1 + NF;                       // 16-byte items per degree
+    __shared__ __align__(16) double2 stage[2][kSynthChunk * R];
+    const int m = blockIdx.y;
     const int f0 = blockIdx.z * NF;
-    const int p0 = blockIdx.y * (blockDim.x * T) + threadIdx.x;
+    const int p0 = blockIdx.x * (blockDim.x * T) + threadIdx.x;
     double z[T];
     int pv[T];
 #pragma unroll
@@ -108,95 +154,84 @@ k_legendre_synth(const double2* __restrict__ rec, const double* __restrict__ pmm
         pv[t] = p0 + t * blockDim.x;
         z[t] = pv[t] < npair ? zp[pv[t]] : 0.0;
     }
-    for (int pass = 0; pass < 2; ++pass) {
-        const int m = pass ? lc - x : x;
-        if (pass && m <= x) break;
-        const long long o = packed_off(m, lc);
-        const double2* __restrict__ rm = rec + o;
-        const double2* __restrict__ cm = coef + o * nfield + f0;
-        const double start = pmm[m];
-        double q1[T], q2[T];
-        double eR[T][NF], eI[T][NF], oR[T][NF], oI[T][NF];
-#pragma unroll
-        for (int j = 0; j < NF; ++j) {
-            const double2 c = cm[j];
-#pragma unroll
-            for (int t = 0; t < T; ++t) {
-                eR[t][j] = c.x * start;
-                eI[t][j] = c.y * start;
-                oR[t][j] = 0.0;
-                oI[t][j] = 0.0;
-            }
+    const long long o = packed_off(m, lc);
+    const double2* __restrict__ rm = rec + o;
+    const double2* __restrict__ cm = coef + o * nfield + f0;
+    const int nsteps = lc - m;                      // degrees l = m+1 .. lc
+    const int nchunks = (nsteps + kSynthChunk - 1) / kSynthChunk;
+
+    auto load_chunk = [&](int c) {
+        double2* dst = stage[c & 1];
+        const int s0 = 1 + c * kSynthChunk;
+        for (int it = threadIdx.x; it < kSynthChunk * R; it += blockDim.x) {
+            const int k = it / R, j = it - k * R;
+            const int sidx = s0 + k;
+            if (sidx <= nsteps)
+                cp_async16(&dst[it], j == 0 ? (const void*)&rm[sidx]
+                                            : (const void*)&cm[(long long)sidx * nfield + (j - 1)]);
         }
+        cp_async_commit();
+    };
+    if (nchunks > 0) load_chunk(0);
+
+    const double start = pmm[m];
+    double q1[T], q2[T];
+    double eR[T][NF], eI[T][NF], oR[T][NF], oI[T][NF];
 #pragma unroll
-        for (int t = 0; t < T; ++t) { q1[t] = start; q2[t] = 0.0; }
-        const int nsteps = lc - m;
-        int s = 1;
-        for (; s + 1 <= nsteps; s += 2) {
-            const double2 fa = rm[s];
-            const double2 fb = rm[s + 1];
-            double2 ca[NF], cb[NF];
-#pragma unroll
-            for (int j = 0; j < NF; ++j) {
-                ca[j] = cm[(long long)s * nfield + j];
-                cb[j] = cm[(long long)(s + 1) * nfield + j];
-            }
-#pragma unroll
-            for (int t = 0; t < T; ++t) {
-                const double p = rec_step(z[t], fa, q1[t], q2[t]);
-                q2[t] = q1[t];
-                q1[t] = p;
-#pragma unroll
-                for (int j = 0; j < NF; ++j) {
-                    oR[t][j] = fma(ca[j].x, p, oR[t][j]);
-                    oI[t][j] = fma(ca[j].y, p, oI[t][j]);
-                }
-            }
-#pragma unroll
-            for (int t = 0; t < T; ++t) {
-                const double p = rec_step(z[t], fb, q1[t], q2[t]);
-                q2[t] = q1[t];
-                q1[t] = p;
-#pragma unroll
-                for (int j = 0; j < NF; ++j) {
-                    eR[t][j] = fma(cb[j].x, p, eR[t][j]);
-                    eI[t][j] = fma(cb[j].y, p, eI[t][j]);
-                }
-            }
-        }
-        if (s <= nsteps) {
-            const double2 fa = rm[s];
-            double2 ca[NF];
-#pragma unroll
-            for (int j = 0; j < NF; ++j) ca[j] = cm[(long long)s * nfield + j];
-#pragma unroll
-            for (int t = 0; t < T; ++t) {
-                const double p = rec_step(z[t], fa, q1[t], q2[t]);
-#pragma unroll
-                for (int j = 0; j < NF; ++j) {
-                    oR[t][j] = fma(ca[j].x, p, oR[t][j]);
-                    oI[t][j] = fma(ca[j].y, p, oI[t][j]);
-                }
-            }
-        }
-        const double h = m ? 0.5 : 1.0;
+    for (int j = 0; j < NF; ++j) {
+        const double2 c = cm[j];
 #pragma unroll
         for (int t = 0; t < T; ++t) {
-            if (pv[t] >= npair) continue;
-            const double r = rtab[(long long)m * npair + pv[t]];
+            eR[t][j] = c.x * start;
+            eI[t][j] = c.y * start;
+            oR[t][j] = 0.0;
+            oI[t][j] = 0.0;
+        }
+    }
 #pragma unroll
-            for (int j = 0; j < NF; ++j) {
-                double nR = 0.0, nI = 0.0, sR = 0.0, sI = 0.0;
-                if (r != 0.0) {
-                    nR = (eR[t][j] + oR[t][j]) * r;
-                    nI = (eI[t][j] + oI[t][j]) * r;
-                    sR = (eR[t][j] - oR[t][j]) * r;
-                    sI = (eI[t][j] - oI[t][j]) * r;
-                }
-                double2* o2 = spec + (((long long)(f0 + j) * npair + pv[t]) * (lc + 1) + m) * 2;
-                o2[0] = make_double2(nR * h, -nI * h);
-                o2[1] = make_double2(sR * h, -sI * h);
+    for (int t = 0; t < T; ++t) { q1[t] = start; q2[t] = 0.0; }
+
+    for (int c = 0; c < nchunks; ++c) {
+        if (c + 1 < nchunks) {
+            load_chunk(c + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double2* st = stage[c & 1];
+        const int cn = min(kSynthChunk, nsteps - c * kSynthChunk);
+        // s = 1 + c*kSynthChunk + k: odd for even k (the chunk length is even)
+        if (cn == kSynthChunk) {
+#pragma unroll
+            for (int k = 0; k < kSynthChunk; ++k)
+                synth_step<T, NF>((k & 1) == 0, st[k * R], &st[k * R + 1], z, q1, q2,
+                                  eR, eI, oR, oI);
+        } else {
+            for (int k = 0; k < cn; ++k)
+                synth_step<T, NF>((k & 1) == 0, st[k * R], &st[k * R + 1], z, q1, q2,
+                                  eR, eI, oR, oI);
+        }
+        __syncthreads();
+    }
+
+    const double h = m ? 0.5 : 1.0;
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+        if (pv[t] >= npair) continue;
+        const double r = rtab[(long long)m * npair + pv[t]];
+#pragma unroll
+        for (int j = 0; j < NF; ++j) {
+            double nR = 0.0, nI = 0.0, sR = 0.0, sI = 0.0;
+            if (r != 0.0) {
+                nR = (eR[t][j] + oR[t][j]) * r;
+                nI = (eI[t][j] + oI[t][j]) * r;
+                sR = (eR[t][j] - oR[t][j]) * r;
+                sI = (eI[t][j] - oI[t][j]) * r;
             }
+            double2* o2 = spec + (((long long)(f0 + j) * npair + pv[t]) * (lc + 1) + m) * 2;
+            o2[0] = make_double2(nR * h, -nI * h);
+            o2[1] = make_double2(sR * h, -sI * h);
         }
     }
 }
@@ -215,6 +250,30 @@ k_legendre_synth(const double2* __restrict__ rec, const double* __restrict__ pmm
 constexpr int kAnalChunk = 16;
 constexpr int kAnalPad = 33;
 
+// one degree step of the analysis for T ring pairs: returns the lane's sums
+// over its pairs of P * G, G the symmetric (even l-m) or antisymmetric (odd)
+// combination of the two rings
+template <int T>
+__device__ __forceinline__ void anal_step(bool odd, double2 fr, const double* z,
+                                          double* q1, double* q2,
+                                          const double* gsR, const double* gsI,
+                                          const double* gaR, const double* gaI,
+                                          double& accR, double& accI) {
+    accR = 0.0;
+    accI = 0.0;
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+        const double p = rec_step(z[t], fr, q1[t], q2[t]);
+        q2[t] = q1[t];
+        q1[t] = p;
+        accR = fma(p, odd ? gaR[t] : gsR[t], accR);
+        accI = fma(p, odd ? gaI[t] : gsI[t], accI);
+    }
+}
+
+// CTA = (ring-pair tile, order m), m = 0, 1, ... in launch order (longest
+// first).  The {ff1, ff2} of each chunk of kAnalChunk degrees are prefetched
+// into shared memory with cp.async one chunk ahead.
 template <int T>
 __global__ void __launch_bounds__(256)
 k_legendre_anal(const double2* __restrict__ rec, const double* __restrict__ pmm,
@@ -222,15 +281,17 @@ k_legendre_anal(const double2* __restrict__ rec, const double* __restrict__ pmm,
                 const double2* __restrict__ spec, double2* __restrict__ partial,
                 int lc, int npair, long long nlm, int nfield) {
     extern __shared__ double smem_anal[];
+    __shared__ __align__(16) double2 rstage[2][kAnalChunk];
     const int nwarps = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     double* bufRe = smem_anal + warp * (2 * kAnalChunk * kAnalPad);
     double* bufIm = bufRe + kAnalChunk * kAnalPad;
-    double* wsum = smem_anal + nwarps * (2 * kAnalChunk * kAnalPad);  // [nwarps][32]
+    // two buffers of per-warp chunk sums, alternating between chunks
+    double* wsum = smem_anal + nwarps * (2 * kAnalChunk * kAnalPad);   // [2][nwarps][32]
 
-    const int x = blockIdx.x;
-    const int tile = blockIdx.y;
+    const int tile = blockIdx.x;
+    const int m = blockIdx.y;
     const int f = blockIdx.z;
     const int p0 = tile * (blockDim.x * T) + threadIdx.x;
     double z[T];
@@ -242,94 +303,113 @@ k_legendre_anal(const double2* __restrict__ rec, const double* __restrict__ pmm,
     }
     const double2* __restrict__ sp = spec + (long long)f * npair * (lc + 1) * 2;
     double2* __restrict__ outp = partial + ((long long)tile * nfield + f) * nlm;
+    const long long o = packed_off(m, lc);
+    const double2* __restrict__ rm = rec + o;
+    const int nsteps = lc - m + 1;   // degrees l = m .. lc, s = l - m
+    const int nchunks = (nsteps + kAnalChunk - 1) / kAnalChunk;
+    auto load_chunk = [&](int c) {
+        const int sidx = c * kAnalChunk + threadIdx.x;
+        if (threadIdx.x < kAnalChunk && sidx < nsteps)
+            cp_async16(&rstage[c & 1][threadIdx.x], &rm[sidx]);
+        cp_async_commit();
+    };
+    load_chunk(0);
 
-    for (int pass = 0; pass < 2; ++pass) {
-        const int m = pass ? lc - x : x;
-        if (pass && m <= x) break;
-        const long long o = packed_off(m, lc);
-        const double2* __restrict__ rm = rec + o;
-        const double start = pmm[m];
-        // symmetric (l-m even) and antisymmetric (l-m odd) combinations
-        double gsR[T], gsI[T], gaR[T], gaI[T], q1[T], q2[T];
+    const double start = pmm[m];
+    // symmetric (l-m even) and antisymmetric (l-m odd) combinations
+    double gsR[T], gsI[T], gaR[T], gaI[T], q1[T], q2[T];
 #pragma unroll
-        for (int t = 0; t < T; ++t) {
-            gsR[t] = gsI[t] = gaR[t] = gaI[t] = 0.0;
-            if (pv[t] < npair) {
-                const double r = rtab[(long long)m * npair + pv[t]];
-                if (r != 0.0) {
-                    const double2 a = sp[((long long)pv[t] * (lc + 1) + m) * 2 + 0];
-                    const double2 b = sp[((long long)pv[t] * (lc + 1) + m) * 2 + 1];
-                    const double aR = a.x * r, aI = a.y * r;
-                    const double bR = b.x * r, bI = b.y * r;
-                    gsR[t] = aR + bR; gsI[t] = aI + bI;
-                    gaR[t] = aR - bR; gaI[t] = aI - bI;
-                }
+    for (int t = 0; t < T; ++t) {
+        gsR[t] = gsI[t] = gaR[t] = gaI[t] = 0.0;
+        if (pv[t] < npair) {
+            const double r = rtab[(long long)m * npair + pv[t]];
+            if (r != 0.0) {
+                const double2 a = sp[((long long)pv[t] * (lc + 1) + m) * 2 + 0];
+                const double2 b = sp[((long long)pv[t] * (lc + 1) + m) * 2 + 1];
+                const double aR = a.x * r, aI = a.y * r;
+                const double bR = b.x * r, bI = b.y * r;
+                gsR[t] = aR + bR; gsI[t] = aI + bI;
+                gaR[t] = aR - bR; gaI[t] = aI - bI;
             }
-            q1[t] = start;
-            q2[t] = 0.0;
         }
-        const int nsteps = lc - m + 1;   // degrees l = m .. lc
-        for (int c0 = 0; c0 < nsteps; c0 += kAnalChunk) {
-            const int cn = min(kAnalChunk, nsteps - c0);
-            for (int k = 0; k < cn; ++k) {
-                const int s = c0 + k;       // l - m
-                double accR = 0.0, accI = 0.0;
-                if (s == 0) {
+        q1[t] = start;
+        q2[t] = 0.0;
+    }
+    int buf = 0;
+    for (int c = 0; c < nchunks; ++c) {
+        const int c0 = c * kAnalChunk;
+        const int cn = min(kAnalChunk, nsteps - c0);
+        if (c + 1 < nchunks) {
+            load_chunk(c + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double2* wcoef = rstage[c & 1];
+        double accR, accI;
+        if (cn == kAnalChunk) {
+            // c0 is a multiple of the (even) chunk length: the parity of
+            // s = c0 + k is that of k, fixed by the unrolling
+#pragma unroll
+            for (int k = 0; k < kAnalChunk; ++k) {
+                if (k == 0 && c0 == 0) {
+                    accR = 0.0;
+                    accI = 0.0;
 #pragma unroll
                     for (int t = 0; t < T; ++t) {
                         accR = fma(q1[t], gsR[t], accR);
                         accI = fma(q1[t], gsI[t], accI);
                     }
                 } else {
-                    const double2 fr = rm[s];
-                    if (s & 1) {
-#pragma unroll
-                        for (int t = 0; t < T; ++t) {
-                            const double p = rec_step(z[t], fr, q1[t], q2[t]);
-                            q2[t] = q1[t];
-                            q1[t] = p;
-                            accR = fma(p, gaR[t], accR);
-                            accI = fma(p, gaI[t], accI);
-                        }
-                    } else {
-#pragma unroll
-                        for (int t = 0; t < T; ++t) {
-                            const double p = rec_step(z[t], fr, q1[t], q2[t]);
-                            q2[t] = q1[t];
-                            q1[t] = p;
-                            accR = fma(p, gsR[t], accR);
-                            accI = fma(p, gsI[t], accI);
-                        }
-                    }
+                    anal_step<T>((k & 1) != 0, wcoef[k], z, q1, q2, gsR, gsI, gaR, gaI,
+                                 accR, accI);
                 }
                 bufRe[k * kAnalPad + lane] = accR;
                 bufIm[k * kAnalPad + lane] = accI;
             }
-            __syncwarp();
-            // lane j < 16 sums the real parts of degree c0+j, lane j >= 16 the
-            // imaginary parts of degree c0+j-16, over the 32 lanes of the warp
-            {
-                const int row = lane & (kAnalChunk - 1);
-                const double* b = (lane < kAnalChunk ? bufRe : bufIm) + row * kAnalPad;
-                double sum = 0.0;
-                if (row < cn) {
-#pragma unroll 8
-                    for (int i = 0; i < 32; ++i) sum += b[i];
+        } else {
+            for (int k = 0; k < cn; ++k) {
+                if (k == 0 && c0 == 0) {
+                    accR = 0.0;
+                    accI = 0.0;
+#pragma unroll
+                    for (int t = 0; t < T; ++t) {
+                        accR = fma(q1[t], gsR[t], accR);
+                        accI = fma(q1[t], gsI[t], accI);
+                    }
+                } else {
+                    anal_step<T>((k & 1) != 0, wcoef[k], z, q1, q2, gsR, gsI, gaR, gaI,
+                                 accR, accI);
                 }
-                wsum[warp * 32 + lane] = sum;
+                bufRe[k * kAnalPad + lane] = accR;
+                bufIm[k * kAnalPad + lane] = accI;
             }
-            __syncthreads();
-            if (warp == 0) {
-                double sum = 0.0;
-                for (int w = 0; w < nwarps; ++w) sum += wsum[w * 32 + lane];
-                const int row = lane & (kAnalChunk - 1);
-                if (row < cn) {
-                    double* dst = reinterpret_cast<double*>(outp + o + c0 + row);
-                    dst[lane < kAnalChunk ? 0 : 1] = sum;
-                }
-            }
-            __syncthreads();
         }
+        __syncwarp();
+        // lane j < 16 sums the real parts of degree c0+j, lane j >= 16 the
+        // imaginary parts of degree c0+j-16, over the 32 lanes of the warp
+        {
+            const int row = lane & (kAnalChunk - 1);
+            const double* b = (lane < kAnalChunk ? bufRe : bufIm) + row * kAnalPad;
+            double sum = 0.0;
+            if (row < cn) {
+#pragma unroll 8
+                for (int i = 0; i < 32; ++i) sum += b[i];
+            }
+            wsum[(buf * nwarps + warp) * 32 + lane] = sum;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double sum = 0.0;
+            for (int w = 0; w < nwarps; ++w) sum += wsum[(buf * nwarps + w) * 32 + lane];
+            const int row = lane & (kAnalChunk - 1);
+            if (row < cn) {
+                double* dst = reinterpret_cast<double*>(outp + o + c0 + row);
+                dst[lane < kAnalChunk ? 0 : 1] = sum;
+            }
+        }
+        buf ^= 1;
     }
 }
 
@@ -396,10 +476,38 @@ __device__ __forceinline__ double2 twv(const double2* tw, int t) {
     return w;
 }
 
-// radix-R DFT of v[] in place; cs/sn hold cos/sin(2 pi j / R)
+// cos and sin of 2*pi*u/R for the odd radices, 1 <= u <= (R-1)/2 (values
+// of the circular functions rounded to double, evaluated in extended
+// precision).  With the butterfly loops unrolled, u is a compile-time
+// constant and these fold to immediates.
+__host__ __device__ constexpr double root_cos(int R, int u) {
+    return R == 3 ? -0.5
+         : R == 5 ? (u == 1 ? 0.30901699437494745 : -0.8090169943749475)
+         : R == 7 ? (u == 1 ? 0.6234898018587335 : u == 2 ? -0.2225209339563144
+                             : -0.9009688679024191)
+         : R == 11 ? (u == 1 ? 0.8412535328311812 : u == 2 ? 0.41541501300188644
+                     : u == 3 ? -0.14231483827328514 : u == 4 ? -0.6548607339452851
+                     : -0.9594929736144974)
+         : (u == 1 ? 0.8854560256532099 : u == 2 ? 0.5680647467311558
+            : u == 3 ? 0.12053668025532305 : u == 4 ? -0.3546048870425356
+            : u == 5 ? -0.7485107481711011 : -0.970941817426052);
+}
+__host__ __device__ constexpr double root_sin(int R, int u) {
+    return R == 3 ? 0.8660254037844386
+         : R == 5 ? (u == 1 ? 0.9510565162951535 : 0.5877852522924731)
+         : R == 7 ? (u == 1 ? 0.7818314824680298 : u == 2 ? 0.9749279121818236
+                             : 0.4338837391175581)
+         : R == 11 ? (u == 1 ? 0.5406408174555976 : u == 2 ? 0.9096319953545183
+                     : u == 3 ? 0.9898214418809327 : u == 4 ? 0.7557495743542583
+                     : 0.28173255684142967)
+         : (u == 1 ? 0.46472317204376856 : u == 2 ? 0.8229838658936564
+            : u == 3 ? 0.992708874098054 : u == 4 ? 0.9350162426854148
+            : u == 5 ? 0.6631226582407952 : 0.23931566428755777);
+}
+
+// radix-R DFT of v[] in place (R = 2, 4, or an odd prime <= 13)
 template <int R, int SIGN>
-__device__ __forceinline__ void dft_small(double2* v, const double* cs,
-                                          const double* sn) {
+__device__ __forceinline__ void dft_small(double2* v) {
     if (R == 2) {
         const double2 a = v[0], b = v[1];
         v[0] = make_double2(a.x + b.x, a.y + b.y);
@@ -416,7 +524,7 @@ __device__ __forceinline__ void dft_small(double2* v, const double* cs,
         v[1] = make_double2(d0.x + e.x, d0.y + e.y);
         v[3] = make_double2(d0.x - e.x, d0.y - e.y);
     } else {
-        // odd R: pair q with R-q
+        // odd R: pair q with R-q; y_s = x0 + sum_q cos(2pi sq/R) a_q -+ i sum_q sin b_q
         constexpr int H = (R - 1) / 2;
         double2 a[H + 1], b[H + 1];
         double2 y0 = v[0];
@@ -435,10 +543,13 @@ __device__ __forceinline__ void dft_small(double2* v, const double* cs,
 #pragma unroll
             for (int q = 1; q <= H; ++q) {
                 const int t = (s * q) % R;
-                re.x = fma(cs[t], a[q].x, re.x);
-                re.y = fma(cs[t], a[q].y, re.y);
-                im.x = fma(sn[t], b[q].x, im.x);
-                im.y = fma(sn[t], b[q].y, im.y);
+                const int u = t <= H ? t : R - t;
+                const double c = root_cos(R, u);
+                const double sn = t <= H ? root_sin(R, u) : -root_sin(R, u);
+                re.x = fma(c, a[q].x, re.x);
+                re.y = fma(c, a[q].y, re.y);
+                im.x = fma(sn, b[q].x, im.x);
+                im.y = fma(sn, b[q].y, im.y);
             }
             // forward: y_s = re - i im, y_{R-s} = re + i im
             if (SIGN < 0) {
@@ -452,18 +563,13 @@ __device__ __forceinline__ void dft_small(double2* v, const double* cs,
     }
 }
 
+// One Stockham pass of radix R from x to y (ping-pong shared buffers).
 template <int R, int SIGN>
-__device__ void fft_pass(const double2* __restrict__ x, double2* __restrict__ y,
-                         int M, int ns, const double2* __restrict__ tw) {
+__device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
+                                         double2* __restrict__ y, int M, int ns,
+                                         const double2* __restrict__ tw) {
     const int nr = M / R;
     const int step = M / (ns * R);
-    double cs[R], sn[R];
-#pragma unroll
-    for (int j = 0; j < R; ++j) {
-        const double2 w = tw[j * nr];
-        cs[j] = w.x;
-        sn[j] = -w.y;
-    }
     for (int j = threadIdx.x; j < nr; j += blockDim.x) {
         const int k = j % ns;
         double2 v[R];
@@ -473,7 +579,7 @@ __device__ void fft_pass(const double2* __restrict__ x, double2* __restrict__ y,
 #pragma unroll
             for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twv<SIGN>(tw, k * q * step));
         }
-        dft_small<R, SIGN>(v, cs, sn);
+        dft_small<R, SIGN>(v);
         const int d = (j - k) * R + k;
 #pragma unroll
         for (int q = 0; q < R; ++q) y[d + q * ns] = v[q];
@@ -516,9 +622,8 @@ struct FftArgs {
     const double2* kern;
 };
 
-// Complex DFT of length F.m of buf (length >= F.mb when Bluestein) with sign
-// SIGN; buf and tmp each hold F.mb (Bluestein) or F.m elements.  Returns the
-// pointer holding the result.
+// Complex DFT of length F.m of buf with sign SIGN; buf and tmp each hold
+// F.mb (Bluestein) or F.m elements.  Returns the pointer holding the result.
 template <int SIGN>
 __device__ double2* fft_exec(const FftArgs& F, double2* buf, double2* tmp) {
     __syncthreads();
@@ -563,7 +668,7 @@ __device__ double2* fft_exec(const FftArgs& F, double2* buf, double2* tmp) {
 // (even n): CTA = (pair*2 + ring, field), the ring is computed by a complex
 // length-n/2 inverse DFT and the even/odd split.  Output rows are scaled by
 // the ring weight when wN/wS are given (analysis adjoint).
-__global__ void __launch_bounds__(256) k_fft_c2r(FftArgs F, const double2* __restrict__ spec,
+__global__ void __launch_bounds__(512) k_fft_c2r(FftArgs F, const double2* __restrict__ spec,
                           double* __restrict__ grid, long long gf, long long grs,
                           long long gcs, const int* __restrict__ rowN,
                           const int* __restrict__ rowS,
@@ -594,7 +699,7 @@ __global__ void __launch_bounds__(256) k_fft_c2r(FftArgs F, const double2* __res
             a[k] = make_double2(xn.x - xs.y, xn.y + xs.x);
             if (k > 0) a[n - k] = make_double2(xn.x + xs.y, -xn.y + xs.x);
         }
-        double2* r = fft_exec<+1>(F, a, b);
+        const double2* r = fft_exec<+1>(F, a, b);
         const double sN = wN ? wN[p] * wscale : 1.0;
         const double sS = wS ? wS[p] * wscale : 1.0;
         double* gN = rN >= 0 ? grid + f * gf + rN * grs : nullptr;
@@ -629,7 +734,7 @@ __global__ void __launch_bounds__(256) k_fft_c2r(FftArgs F, const double2* __res
             const double2 wb = cmul(w, B);
             a[k] = make_double2(A.x - wb.y, A.y + wb.x);
         }
-        double2* r = fft_exec<+1>(F, a, b);
+        const double2* r = fft_exec<+1>(F, a, b);
         const double sc = (h ? (wS ? wS[p] * wscale : 1.0) : (wN ? wN[p] * wscale : 1.0));
         double* g = grid + f * gf + row * grs;
         for (int j = threadIdx.x; j < M; j += blockDim.x) {
@@ -644,7 +749,7 @@ __global__ void __launch_bounds__(256) k_fft_c2r(FftArgs F, const double2* __res
 // r2c: grid rows -> spec (m = 0..lc), each multiplied by the ring weight
 // (times wscale) as (Re, -Im), the reference's fcoef (SHExpandGLQ.f95:535-547).
 // fold_extend adds column n into column 0 (adjoint of the extend copy).
-__global__ void __launch_bounds__(256) k_fft_r2c(FftArgs F, const double* __restrict__ grid,
+__global__ void __launch_bounds__(512) k_fft_r2c(FftArgs F, const double* __restrict__ grid,
                           long long gf, long long grs, long long gcs,
                           double2* __restrict__ spec, const int* __restrict__ rowN,
                           const int* __restrict__ rowS,
@@ -672,7 +777,7 @@ __global__ void __launch_bounds__(256) k_fft_r2c(FftArgs F, const double* __rest
             }
             a[j] = make_double2(xn, xs);
         }
-        double2* r = fft_exec<-1>(F, a, b);
+        const double2* r = fft_exec<-1>(F, a, b);
         const double sN = wN ? wN[p] * wscale : wscale;
         const double sS = wS ? wS[p] * wscale : wscale;
         double2* X = spec + ((long long)f * npair + p) * (lc + 1) * 2;
@@ -702,7 +807,7 @@ __global__ void __launch_bounds__(256) k_fft_r2c(FftArgs F, const double* __rest
             if (fold_extend && j == 0) x0 += g[(long long)n * gcs];
             a[j] = make_double2(x0, x1);
         }
-        double2* r = fft_exec<-1>(F, a, b);
+        const double2* r = fft_exec<-1>(F, a, b);
         const double sc = h ? (wS ? wS[p] * wscale : wscale) : (wN ? wN[p] * wscale : wscale);
         for (int k = threadIdx.x; k <= lc; k += blockDim.x) {
             const double2 zk = r[k == M ? 0 : k];
@@ -745,7 +850,7 @@ static void launch_synth_t(const shtc_plan* P, const double2* packed,
                            double2* spec, int nfield, cudaStream_t st) {
     const int threads = 128;
     const int tiles = (P->npair + threads * T - 1) / (threads * T);
-    dim3 grid(P->lc / 2 + 1, tiles, nfield / NF);
+    dim3 grid(tiles, P->lc + 1, nfield / NF);
     k_legendre_synth<T, NF><<<grid, threads, 0, st>>>(
         P->d_rec, P->d_pmm, P->d_rtab, P->d_z, packed, spec, P->lc, P->npair,
         nfield);
@@ -753,14 +858,22 @@ static void launch_synth_t(const shtc_plan* P, const double2* packed,
 
 int launch_legendre_synth(const shtc_plan* P, const double2* packed,
                           double2* spec, int nfield, cudaStream_t st) {
+    const int np = P->npair;
     if (nfield % 4 == 0 && nfield >= 8) {
         launch_synth_t<2, 4>(P, packed, spec, nfield, st);
     } else if (nfield % 2 == 0 && nfield >= 2) {
-        launch_synth_t<2, 2>(P, packed, spec, nfield, st);
-    } else if (P->npair > 256) {
-        launch_synth_t<4, 1>(P, packed, spec, nfield, st);
+        if (np > 512) launch_synth_t<4, 2>(P, packed, spec, nfield, st);
+        else launch_synth_t<2, 2>(P, packed, spec, nfield, st);
     } else {
-        launch_synth_t<1, 1>(P, packed, spec, nfield, st);
+        // heuristic from the autotuner's sweeps on B200 (lmax 63..2799)
+        int T = P->tune_synth_T;
+        if (T == 0) T = np > 768 ? 8 : (np > 256 ? 2 : 1);
+        switch (T) {
+            case 8: launch_synth_t<8, 1>(P, packed, spec, nfield, st); break;
+            case 4: launch_synth_t<4, 1>(P, packed, spec, nfield, st); break;
+            case 2: launch_synth_t<2, 1>(P, packed, spec, nfield, st); break;
+            default: launch_synth_t<1, 1>(P, packed, spec, nfield, st); break;
+        }
     }
     return map_cuda(cudaGetLastError());
 }
@@ -768,10 +881,14 @@ int launch_legendre_synth(const shtc_plan* P, const double2* packed,
 // analysis CTA shape: T pairs per thread, W warps
 static void anal_shape(const shtc_plan* P, int* T, int* W, int* tiles) {
     const int np = P->npair;
-    int t = np >= 1024 ? 4 : (np >= 256 ? 2 : 1);
-    int w = (np + 32 * t - 1) / (32 * t);
-    if (w > 8) w = 8;
-    if (w < 1) w = 1;
+    int w = P->tune_anal_W ? P->tune_anal_W : 2;
+    int t = P->tune_anal_T;
+    if (t == 0) {
+        // largest T (at most 4) that leaves at least two CTA tiles of ring
+        // pairs: what the autotuner's sweeps on B200 select for lmax 63..2799
+        t = 1;
+        while (t < 4 && 32 * w * (2 * t) <= np / 2) t *= 2;
+    }
     *T = t;
     *W = w;
     *tiles = (np + 32 * t * w - 1) / (32 * t * w);
@@ -789,12 +906,12 @@ static int launch_anal_t(const shtc_plan* P, const double2* spec,
                          cudaStream_t st) {
     const int threads = 32 * W;
     const size_t smem = (size_t)W * (2 * kAnalChunk * kAnalPad) * sizeof(double)
-                        + (size_t)W * 32 * sizeof(double);
+                        + (size_t)2 * W * 32 * sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(k_legendre_anal<T>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return map_cuda(e);
-    dim3 grid(P->lc / 2 + 1, tiles, nfield);
+    dim3 grid(tiles, P->lc + 1, nfield);
     k_legendre_anal<T><<<grid, threads, smem, st>>>(
         P->d_rec, P->d_pmm, P->d_rtab, P->d_z, spec, partial, P->lc, P->npair,
         P->nlm, nfield);
@@ -808,6 +925,7 @@ int launch_legendre_anal(const shtc_plan* P, const double2* spec,
     anal_shape(P, &T, &W, &tiles);
     if (tiles != ntiles_out) return SHTC_EBOUND;
     switch (T) {
+        case 8: return launch_anal_t<8>(P, spec, partial, nfield, W, tiles, st);
         case 4: return launch_anal_t<4>(P, spec, partial, nfield, W, tiles, st);
         case 2: return launch_anal_t<2>(P, spec, partial, nfield, W, tiles, st);
         default: return launch_anal_t<1>(P, spec, partial, nfield, W, tiles, st);

@@ -278,12 +278,13 @@ int build_fft_plan(FftPlan* f, int n, cudaStream_t st) {
         }
     }
     const int len = f->bluestein ? f->mb : f->m;
+    // two shared buffers: Stockham passes ping-pong between them
     f->smem = 2 * (size_t)len * sizeof(double2);
     int maxsmem = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (maxsmem > 0 && f->smem > (size_t)maxsmem) return SHTC_EUNSUP;
-    f->threads = 256;
+    f->threads = len > 2048 ? 512 : (len > 512 ? 256 : 128);
     auto up = [&](double2** d, const std::vector<double2>& h) -> int {
         if (h.empty()) { *d = nullptr; return SHTC_OK; }
         if (cudaMalloc((void**)d, h.size() * sizeof(double2)) != cudaSuccess) return SHTC_EALLOC;
@@ -650,6 +651,17 @@ extern "C" int shtc_dhaj(int n, double* aj, int extend, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     k_dhaj<<<(n + extend + 127) / 128, 128, 0, st>>>(n, aj, extend);
     return map_cuda(cudaGetLastError());
+}
+
+extern "C" int shtc_plan_set_tuning(shtc_plan* P, int synth_T, int anal_T,
+                                    int anal_W) {
+    if (!P) return SHTC_EHANDLE;
+    auto ok = [](int v) { return v == 0 || v == 1 || v == 2 || v == 4 || v == 8; };
+    if (!ok(synth_T) || !ok(anal_T) || !ok(anal_W)) return SHTC_EBOUND;
+    P->tune_synth_T = synth_T;
+    P->tune_anal_T = anal_T;
+    P->tune_anal_W = anal_W;
+    return SHTC_OK;
 }
 
 extern "C" int shtc_plan_info(const shtc_plan* P, long long* info, int ninfo) {

@@ -74,6 +74,9 @@ struct shtc_plan {
     double* d_wS;
     double* d_nrm;     // per packed (l, m): analysis normalisation divisor
     shtc::FftPlan fft;
+    int tune_synth_T;  // ring pairs per thread of the synthesis (0: heuristic)
+    int tune_anal_T;   // ring pairs per thread of the analysis (0: heuristic)
+    int tune_anal_W;   // warps per CTA of the analysis (0: heuristic)
     size_t device_bytes;
     int device;        // CUDA device the tables live on
 };

@@ -148,8 +148,11 @@ _plans = {}
 
 
 def get_plan(kind, lmax, lmax_calc, norm, csphase, sampling=1, extend=0,
-             zero=None, w=None, device=None):
-    """Cached Plan for the option set (thread-safe)."""
+             zero=None, w=None, device=None, tune=None):
+    """Cached Plan for the option set (thread-safe).  New plans are
+    autotuned when ``tune`` is true or the environment sets SHTC_AUTOTUNE=1
+    (shtools_b200.autotune)."""
+    import os
     dev = torch.device("cuda", torch.cuda.current_device()) if device is None \
         else torch.device(device)
     if dev.index is None:
@@ -164,6 +167,9 @@ def get_plan(kind, lmax, lmax_calc, norm, csphase, sampling=1, extend=0,
             p = Plan(kind, lmax, lmax_calc, norm, csphase, sampling, extend,
                      zero, w, dev)
             _plans[key] = p
+            if tune or (tune is None and os.environ.get("SHTC_AUTOTUNE") == "1"):
+                from . import autotune
+                autotune.tune_plan(p)
         return p
 
 
