@@ -134,6 +134,64 @@ SHTC_API int shtc_analysis_adjoint(const shtc_plan* plan, const double* cilm,
                           int nfield, void* work, size_t work_bytes,
                           void* stream);
 
+/* ------------------------------------------------------------------------ */
+/* Batches of fields on several grids (no single counterpart in the         */
+/* reference, which transforms one field per call): e.g. thousands of GLQ   */
+/* fields of uneven lmax.  A batch references existing plans (one per grid  */
+/* and option set, extend = 0), which must outlive it; the nf fields of a   */
+/* plan share its Legendre recursion.  A batched transform is one pack      */
+/* launch, one persistent Legendre launch over cost-sorted work items and   */
+/* one launch for all longitude FFTs (plus an unpack for the analysis), so  */
+/* it can be captured in a CUDA graph.  Caller arrays hold the groups one   */
+/* after another: per group (nf, 2, lc+1, lc+1) coefficients and            */
+/* (nf, nlat, nlon) grids, C order, at the offsets of shtc_batch_layout.    */
+/* ------------------------------------------------------------------------ */
+typedef struct shtc_batch shtc_batch;
+SHTC_API int shtc_batch_create(shtc_batch** batch, int nplans,
+                               shtc_plan* const* plans, const int* nfields,
+                               void* stream);
+SHTC_API int shtc_batch_destroy(shtc_batch* batch);
+/* cilm_off / grid_off: nplans+1 element offsets (the last is the total). */
+SHTC_API int shtc_batch_layout(const shtc_batch* batch, long long* cilm_off,
+                               long long* grid_off);
+SHTC_API size_t shtc_batch_workspace_bytes(const shtc_batch* batch);
+SHTC_API int shtc_batch_synthesis(const shtc_batch* batch, const double* cilm,
+                                  double* grid, void* work, size_t work_bytes,
+                                  void* stream);
+SHTC_API int shtc_batch_analysis(const shtc_batch* batch, const double* grid,
+                                 double* cilm, void* work, size_t work_bytes,
+                                 void* stream);
+
+/* The same four transforms with the element type of each array given by a
+ * dtype code, SHTC_F64 or SHTC_F32 (no counterpart in the reference, which is
+ * float64 only).  Arithmetic stays in FP64 inside the kernels; float32
+ * arrays are converted on load and store (e.g. float32 grids with float64
+ * coefficients, or both float32). */
+#define SHTC_F64 0
+#define SHTC_F32 1
+SHTC_API int shtc_synthesis_ex(const shtc_plan* plan, const void* cilm, int cilm_dtype,
+                               long long csf, long long csk, long long csl,
+                               long long csm, int cilm_dim, void* grid, int grid_dtype,
+                               long long gsf, long long gsr, long long gsc, int nfield,
+                               void* work, size_t work_bytes, void* stream);
+SHTC_API int shtc_analysis_ex(const shtc_plan* plan, const void* grid, int grid_dtype,
+                              long long gsf, long long gsr, long long gsc, void* cilm,
+                              int cilm_dtype, long long csf, long long csk,
+                              long long csl, long long csm, int cilm_dim, int nfield,
+                              void* work, size_t work_bytes, void* stream);
+SHTC_API int shtc_synthesis_adjoint_ex(const shtc_plan* plan, const void* grid,
+                                       int grid_dtype, long long gsf, long long gsr,
+                                       long long gsc, void* cilm, int cilm_dtype,
+                                       long long csf, long long csk, long long csl,
+                                       long long csm, int cilm_dim, int nfield,
+                                       void* work, size_t work_bytes, void* stream);
+SHTC_API int shtc_analysis_adjoint_ex(const shtc_plan* plan, const void* cilm,
+                                      int cilm_dtype, long long csf, long long csk,
+                                      long long csl, long long csm, int cilm_dim,
+                                      void* grid, int grid_dtype, long long gsf,
+                                      long long gsr, long long gsc, int nfield,
+                                      void* work, size_t work_bytes, void* stream);
+
 /* Quadrature on the GPU (device output arrays).
  * PreGLQ.f95:1-151: n nodes (descending) and weights on [x1, x2];
  * returns SHTC_ENOZERO if Newton's iteration does not converge.  Synchronises

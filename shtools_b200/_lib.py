@@ -30,7 +30,11 @@ EXPORTS = (
     "shtc_plan_set_tuning", "shtc_timing_enable", "shtc_timing_collect",
     "shtc_synthesis_noalloc",
     "shtc_workspace_bytes", "shtc_synthesis", "shtc_analysis",
-    "shtc_synthesis_adjoint", "shtc_analysis_adjoint", "shtc_preglq",
+    "shtc_synthesis_adjoint", "shtc_analysis_adjoint", "shtc_synthesis_ex",
+    "shtc_analysis_ex", "shtc_synthesis_adjoint_ex", "shtc_analysis_adjoint_ex",
+    "shtc_batch_create", "shtc_batch_destroy", "shtc_batch_layout",
+    "shtc_batch_workspace_bytes", "shtc_batch_synthesis", "shtc_batch_analysis",
+    "shtc_preglq",
     "shtc_dhaj", "MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ",
     "SHGLQ", "PreGLQ", "DHaj",
 )
@@ -66,6 +70,12 @@ def _bind(L):
     L.shtc_analysis.argtypes = [_P] + grid + coef + tail
     L.shtc_synthesis_adjoint.argtypes = [_P] + grid + coef + tail
     L.shtc_analysis_adjoint.argtypes = [_P] + coef + grid + tail
+    coefx = [_P, _I, _LL, _LL, _LL, _LL, _I]
+    gridx = [_P, _I, _LL, _LL, _LL]
+    L.shtc_synthesis_ex.argtypes = [_P] + coefx + gridx + tail
+    L.shtc_analysis_ex.argtypes = [_P] + gridx + coefx + tail
+    L.shtc_synthesis_adjoint_ex.argtypes = [_P] + gridx + coefx + tail
+    L.shtc_analysis_adjoint_ex.argtypes = [_P] + coefx + gridx + tail
     L.shtc_preglq.argtypes = [_D, _D, _I, _P, _P, _P]
     L.shtc_dhaj.argtypes = [_I, _P, _I, _P]
     L.MakeGridDH.argtypes = [_DP, _I, _I, _IP, _DP, _I, _I, _IP, _IP, _IP, _IP, _IP,

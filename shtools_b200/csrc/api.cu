@@ -60,19 +60,25 @@ static int check_call(const shtc_plan* P, const void* a, const void* b,
     return SHTC_OK;
 }
 
-extern "C" int shtc_synthesis(const shtc_plan* P, const double* cilm,
-                              long long csf, long long csk, long long csl,
-                              long long csm, int cdim, double* grid,
-                              long long gsf, long long gsr, long long gsc,
-                              int nfield, void* work, size_t wb, void* stream) {
+static int check_dtypes(int a, int b) {
+    auto ok = [](int d) { return d == SHTC_F64 || d == SHTC_F32; };
+    return ok(a) && ok(b) ? SHTC_OK : SHTC_EBOUND;
+}
+
+extern "C" int shtc_synthesis_ex(const shtc_plan* P, const void* cilm, int cdt,
+                                 long long csf, long long csk, long long csl,
+                                 long long csm, int cdim, void* grid, int gdt,
+                                 long long gsf, long long gsr, long long gsc,
+                                 int nfield, void* work, size_t wb, void* stream) {
     int rc = check_call(P, cilm, grid, nfield, work, wb);
     if (rc) return rc;
+    if ((rc = check_dtypes(cdt, gdt))) return rc;
     if (cdim < 1) return SHTC_EDIM;
     cudaStream_t st = (cudaStream_t)stream;
     double2* packed = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
     stage_begin(SHTC_STAGE_PACK, st);
-    rc = launch_pack_coef(P, cilm, csf, csk, csl, csm, cdim, packed, nfield, 0, st);
+    rc = launch_pack_coef(P, cilm, cdt, csf, csk, csl, csm, cdim, packed, nfield, 0, st);
     stage_end(SHTC_STAGE_PACK, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_SYNTH, st);
@@ -80,25 +86,26 @@ extern "C" int shtc_synthesis(const shtc_plan* P, const double* cilm,
     stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_FFT_C2R, st);
-    rc = launch_fft_c2r(P, spec, grid, gsf, gsr, gsc, nfield, 0, st);
+    rc = launch_fft_c2r(P, spec, grid, gdt, gsf, gsr, gsc, nfield, 0, st);
     stage_end(SHTC_STAGE_FFT_C2R, st);
     return rc;
 }
 
-extern "C" int shtc_analysis(const shtc_plan* P, const double* grid,
-                             long long gsf, long long gsr, long long gsc,
-                             double* cilm, long long csf, long long csk,
-                             long long csl, long long csm, int cdim, int nfield,
-                             void* work, size_t wb, void* stream) {
+extern "C" int shtc_analysis_ex(const shtc_plan* P, const void* grid, int gdt,
+                                long long gsf, long long gsr, long long gsc,
+                                void* cilm, int cdt, long long csf, long long csk,
+                                long long csl, long long csm, int cdim, int nfield,
+                                void* work, size_t wb, void* stream) {
     int rc = check_call(P, grid, cilm, nfield, work, wb);
     if (rc) return rc;
+    if ((rc = check_dtypes(cdt, gdt))) return rc;
     if (cdim < P->lc + 1) return SHTC_EDIM;
     cudaStream_t st = (cudaStream_t)stream;
     double2* partial = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
     const int tiles = anal_tiles(P);
     stage_begin(SHTC_STAGE_FFT_R2C, st);
-    rc = launch_fft_r2c(P, grid, gsf, gsr, gsc, spec, nfield, 1, 0, st);
+    rc = launch_fft_r2c(P, grid, gdt, gsf, gsr, gsc, spec, nfield, 1, 0, st);
     stage_end(SHTC_STAGE_FFT_R2C, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
@@ -106,28 +113,28 @@ extern "C" int shtc_analysis(const shtc_plan* P, const double* grid,
     stage_end(SHTC_STAGE_LEGENDRE_ANAL, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_UNPACK, st);
-    rc = launch_unpack_coef(P, partial, tiles, cilm, csf, csk, csl, csm, cdim, nfield,
+    rc = launch_unpack_coef(P, partial, tiles, cilm, cdt, csf, csk, csl, csm, cdim, nfield,
                             1, st);
     stage_end(SHTC_STAGE_UNPACK, st);
     return rc;
 }
 
-extern "C" int shtc_synthesis_adjoint(const shtc_plan* P, const double* grid,
-                                      long long gsf, long long gsr,
-                                      long long gsc, double* cilm,
-                                      long long csf, long long csk,
-                                      long long csl, long long csm, int cdim,
-                                      int nfield, void* work, size_t wb,
-                                      void* stream) {
+extern "C" int shtc_synthesis_adjoint_ex(const shtc_plan* P, const void* grid, int gdt,
+                                         long long gsf, long long gsr, long long gsc,
+                                         void* cilm, int cdt, long long csf,
+                                         long long csk, long long csl, long long csm,
+                                         int cdim, int nfield, void* work, size_t wb,
+                                         void* stream) {
     int rc = check_call(P, grid, cilm, nfield, work, wb);
     if (rc) return rc;
+    if ((rc = check_dtypes(cdt, gdt))) return rc;
     if (cdim < 1) return SHTC_EDIM;
     cudaStream_t st = (cudaStream_t)stream;
     double2* partial = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
     const int tiles = anal_tiles(P);
     stage_begin(SHTC_STAGE_FFT_R2C, st);
-    rc = launch_fft_r2c(P, grid, gsf, gsr, gsc, spec, nfield, 0, P->extend, st);
+    rc = launch_fft_r2c(P, grid, gdt, gsf, gsr, gsc, spec, nfield, 0, P->extend, st);
     stage_end(SHTC_STAGE_FFT_R2C, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
@@ -135,26 +142,26 @@ extern "C" int shtc_synthesis_adjoint(const shtc_plan* P, const double* grid,
     stage_end(SHTC_STAGE_LEGENDRE_ANAL, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_UNPACK, st);
-    rc = launch_unpack_coef(P, partial, tiles, cilm, csf, csk, csl, csm, cdim, nfield,
+    rc = launch_unpack_coef(P, partial, tiles, cilm, cdt, csf, csk, csl, csm, cdim, nfield,
                             0, st);
     stage_end(SHTC_STAGE_UNPACK, st);
     return rc;
 }
 
-extern "C" int shtc_analysis_adjoint(const shtc_plan* P, const double* cilm,
-                                     long long csf, long long csk,
-                                     long long csl, long long csm, int cdim,
-                                     double* grid, long long gsf, long long gsr,
-                                     long long gsc, int nfield, void* work,
-                                     size_t wb, void* stream) {
+extern "C" int shtc_analysis_adjoint_ex(const shtc_plan* P, const void* cilm, int cdt,
+                                        long long csf, long long csk, long long csl,
+                                        long long csm, int cdim, void* grid, int gdt,
+                                        long long gsf, long long gsr, long long gsc,
+                                        int nfield, void* work, size_t wb, void* stream) {
     int rc = check_call(P, cilm, grid, nfield, work, wb);
     if (rc) return rc;
+    if ((rc = check_dtypes(cdt, gdt))) return rc;
     if (cdim < 1) return SHTC_EDIM;
     cudaStream_t st = (cudaStream_t)stream;
     double2* packed = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
     stage_begin(SHTC_STAGE_PACK, st);
-    rc = launch_pack_coef(P, cilm, csf, csk, csl, csm, cdim, packed, nfield, 1, st);
+    rc = launch_pack_coef(P, cilm, cdt, csf, csk, csl, csm, cdim, packed, nfield, 1, st);
     stage_end(SHTC_STAGE_PACK, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_SYNTH, st);
@@ -162,9 +169,43 @@ extern "C" int shtc_analysis_adjoint(const shtc_plan* P, const double* cilm,
     stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_FFT_C2R, st);
-    rc = launch_fft_c2r(P, spec, grid, gsf, gsr, gsc, nfield, 1, st);
+    rc = launch_fft_c2r(P, spec, grid, gdt, gsf, gsr, gsc, nfield, 1, st);
     stage_end(SHTC_STAGE_FFT_C2R, st);
     return rc;
+}
+
+extern "C" int shtc_synthesis(const shtc_plan* P, const double* cilm, long long csf,
+                              long long csk, long long csl, long long csm, int cdim,
+                              double* grid, long long gsf, long long gsr, long long gsc,
+                              int nfield, void* work, size_t wb, void* stream) {
+    return shtc_synthesis_ex(P, cilm, SHTC_F64, csf, csk, csl, csm, cdim, grid, SHTC_F64,
+                             gsf, gsr, gsc, nfield, work, wb, stream);
+}
+
+extern "C" int shtc_analysis(const shtc_plan* P, const double* grid, long long gsf,
+                             long long gsr, long long gsc, double* cilm, long long csf,
+                             long long csk, long long csl, long long csm, int cdim,
+                             int nfield, void* work, size_t wb, void* stream) {
+    return shtc_analysis_ex(P, grid, SHTC_F64, gsf, gsr, gsc, cilm, SHTC_F64, csf, csk, csl,
+                            csm, cdim, nfield, work, wb, stream);
+}
+
+extern "C" int shtc_synthesis_adjoint(const shtc_plan* P, const double* grid,
+                                      long long gsf, long long gsr, long long gsc,
+                                      double* cilm, long long csf, long long csk,
+                                      long long csl, long long csm, int cdim,
+                                      int nfield, void* work, size_t wb, void* stream) {
+    return shtc_synthesis_adjoint_ex(P, grid, SHTC_F64, gsf, gsr, gsc, cilm, SHTC_F64, csf,
+                                     csk, csl, csm, cdim, nfield, work, wb, stream);
+}
+
+extern "C" int shtc_analysis_adjoint(const shtc_plan* P, const double* cilm,
+                                     long long csf, long long csk, long long csl,
+                                     long long csm, int cdim, double* grid, long long gsf,
+                                     long long gsr, long long gsc, int nfield, void* work,
+                                     size_t wb, void* stream) {
+    return shtc_analysis_adjoint_ex(P, cilm, SHTC_F64, csf, csk, csl, csm, cdim, grid,
+                                    SHTC_F64, gsf, gsr, gsc, nfield, work, wb, stream);
 }
 
 // ---------------------------------------------------------------------------

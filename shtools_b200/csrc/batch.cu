@@ -1,0 +1,430 @@
+// Batched transforms of many fields on several grids (e.g. GLQ grids of
+// uneven lmax): one persistent Legendre launch over (grid group, order m,
+// ring tile, field chunk) work items, plus one launch each for packing and
+// for all longitude FFTs, so a whole batch is a handful of launches that a
+// CUDA graph can capture and replay.
+//
+// A batch references plans (one per distinct grid and option set); fields
+// of one plan form a group and share the Legendre recursion.  Work items are
+// sorted by cost, longest first, and handed out through a global counter:
+// the persistent CTAs then finish together (longest-processing-time-first
+// scheduling).  Layout of the caller's arrays: the groups one after another,
+// a group holding nf fields as (nf, 2, lc+1, lc+1) coefficients and
+// (nf, nlat, nlon) grids, C order (offsets from shtc_batch_layout).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "fft.cuh"
+#include "legendre.cuh"
+#include "shtc_internal.cuh"
+
+namespace shtc {
+
+struct BatchGroup {
+    const double2* rec;
+    const double* pmm;
+    const double* rtab;
+    const double* z;
+    const int* rowN;
+    const int* rowS;
+    const int* arowN;
+    const int* arowS;
+    const double* wN;
+    const double* wS;
+    const double* nrm3;
+    int lc, npair, nf, norm, nlat, nlon, fft_jobs, tiles;
+    double inv_nlon;
+    long long nlm;
+    long long cilm_off;   // caller coefficients (doubles)
+    long long grid_off;   // caller grids (doubles)
+    long long pack_off;   // workspace: packed coefficients / analysis partials (double2)
+    long long spec_off;   // workspace: ring spectra (double2)
+};
+
+constexpr int kBatchSynthNF = 4;
+constexpr int kBatchThreads = 128;        // ring pairs per tile (T = 1)
+constexpr int kBatchAnalWarps = 4;
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+// pack: item (g, m); coefficients (nf, 2, D, D) -> packed [(l,m)][nf] {C, S}
+__global__ void k_batch_pack(const BatchGroup* __restrict__ G,
+                             const int2* __restrict__ items,
+                             const double* __restrict__ cilm,
+                             double2* __restrict__ work) {
+    const int2 it = items[blockIdx.x];
+    const BatchGroup& g = G[it.x];
+    const int m = it.y, lc = g.lc, D = lc + 1, nf = g.nf;
+    const long long o = packed_off(m, lc);
+    const double* c = cilm + g.cilm_off;
+    double2* pk = work + g.pack_off;
+    for (int l = m + threadIdx.x; l <= lc; l += blockDim.x) {
+        for (int f = 0; f < nf; ++f) {
+            const double* b = c + (long long)f * 2 * D * D + (long long)l * D + m;
+            const double cs = b[0];
+            const double sn = m == 0 ? 0.0 : b[(long long)D * D];
+            pk[(o + (l - m)) * nf + f] = make_double2(cs, sn);
+        }
+    }
+}
+
+// unpack: item (g, m); tile sums, normalisation (SHExpandDH.f95:674-702)
+__global__ void k_batch_unpack(const BatchGroup* __restrict__ G,
+                               const int2* __restrict__ items,
+                               const double2* __restrict__ work,
+                               double* __restrict__ cilm) {
+    const double pi = 3.141592653589793238462643383279502884;
+    const int2 it = items[blockIdx.x];
+    const BatchGroup& g = G[it.x];
+    const int m = it.y, lc = g.lc, D = lc + 1, nf = g.nf;
+    const long long o = packed_off(m, lc);
+    const double2* part = work + g.pack_off;
+    double* c = cilm + g.cilm_off;
+    for (int l = m + threadIdx.x; l <= lc; l += blockDim.x) {
+        const long long idx = o + (l - m);
+        for (int f = 0; f < nf; ++f) {
+            double cs = 0.0, sn = 0.0;
+            for (int t = 0; t < g.tiles; ++t) {
+                const double2 v = part[((long long)t * nf + f) * g.nlm + idx];
+                cs += v.x;
+                sn += v.y;
+            }
+            switch (g.norm) {
+                case 1: cs = cs / (4 * pi); sn = sn / (4 * pi); break;
+                case 2:
+                    cs = cs * (2 * l + 1) / (4 * pi);
+                    sn = sn * (2 * l + 1) / (4 * pi);
+                    break;
+                case 3: cs = cs / g.nrm3[idx]; sn = sn / g.nrm3[idx]; break;
+                default: break;
+            }
+            double* b = c + (long long)f * 2 * D * D + (long long)l * D + m;
+            b[0] = cs;
+            b[(long long)D * D] = m == 0 ? 0.0 : sn;
+        }
+    }
+}
+
+__device__ __forceinline__ int next_item(int* counter, int* s_item) {
+    if (threadIdx.x == 0) *s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = *s_item;
+    __syncthreads();
+    return it;
+}
+
+// persistent synthesis: item (g, m, tile, f0)
+__global__ void __launch_bounds__(kBatchThreads)
+k_batch_synth(const BatchGroup* __restrict__ G, const int4* __restrict__ items,
+              int nitems, int* __restrict__ counter, double2* __restrict__ work) {
+    __shared__ __align__(16) SynthStage<kBatchSynthNF> sm;
+    __shared__ int s_item;
+    for (;;) {
+        const int i = next_item(counter, &s_item);
+        if (i >= nitems) return;
+        const int4 w = items[i];
+        const BatchGroup& g = G[w.x];
+        synth_order<1, kBatchSynthNF>(sm, g.rec, g.pmm, g.rtab, g.z, work + g.pack_off,
+                                      work + g.spec_off, g.lc, g.npair, g.nf, w.y, w.z,
+                                      w.w, min(kBatchSynthNF, g.nf - w.w));
+    }
+}
+
+// persistent analysis: item (g, m, tile, f)
+__global__ void __launch_bounds__(32 * kBatchAnalWarps)
+k_batch_anal(const BatchGroup* __restrict__ G, const int4* __restrict__ items,
+             int nitems, int* __restrict__ counter, double2* __restrict__ work) {
+    extern __shared__ double smem_anal[];
+    __shared__ __align__(16) double2 rstage[2][kAnalChunk];
+    __shared__ int s_item;
+    for (;;) {
+        const int i = next_item(counter, &s_item);
+        if (i >= nitems) return;
+        const int4 w = items[i];
+        const BatchGroup& g = G[w.x];
+        const int f = w.w;
+        anal_order<1>(smem_anal, rstage, g.rec, g.pmm, g.rtab, g.z,
+                      work + g.spec_off + (long long)f * g.npair * (g.lc + 1) * 2,
+                      work + g.pack_off + ((long long)w.z * g.nf + f) * g.nlm, g.lc,
+                      g.npair, w.y, w.z);
+    }
+}
+
+// FFT jobs: item (g, f, job); the group's FftArgs are read from memory
+__global__ void __launch_bounds__(512)
+k_batch_c2r(const BatchGroup* __restrict__ G, const FftArgs* __restrict__ FA,
+            const int4* __restrict__ jobs, const double2* __restrict__ work,
+            double* __restrict__ grid) {
+    extern __shared__ double2 smem_fft[];
+    const int4 j = jobs[blockIdx.x];
+    const BatchGroup& g = G[j.x];
+    const FftArgs F = FA[j.x];
+    fft_c2r_body<double>(F, smem_fft, j.z, j.y, work + g.spec_off, grid + g.grid_off,
+                 (long long)g.nlat * g.nlon, g.nlon, 1, g.rowN, g.rowS, nullptr,
+                 nullptr, 1.0, g.lc, g.npair, 0);
+}
+
+__global__ void __launch_bounds__(512)
+k_batch_r2c(const BatchGroup* __restrict__ G, const FftArgs* __restrict__ FA,
+            const int4* __restrict__ jobs, const double* __restrict__ grid,
+            double2* __restrict__ work) {
+    extern __shared__ double2 smem_fft[];
+    const int4 j = jobs[blockIdx.x];
+    const BatchGroup& g = G[j.x];
+    const FftArgs F = FA[j.x];
+    fft_r2c_body<double>(F, smem_fft, j.z, j.y, grid + g.grid_off, (long long)g.nlat * g.nlon,
+                 g.nlon, 1, work + g.spec_off, g.arowN, g.arowS, g.wN, g.wS,
+                 g.inv_nlon, g.lc, g.npair, 0);
+}
+
+}  // namespace shtc
+
+using namespace shtc;
+
+struct shtc_batch {
+    int ngroup = 0;
+    int device = 0;
+    std::vector<BatchGroup> h_groups;
+    BatchGroup* d_groups = nullptr;
+    FftArgs* d_fft = nullptr;
+    int2* d_pitems = nullptr;
+    int npitems = 0;
+    int4* d_sitems = nullptr;
+    int nsitems = 0;
+    int4* d_aitems = nullptr;
+    int naitems = 0;
+    int4* d_jobs = nullptr;
+    int njobs = 0;
+    int* d_counter = nullptr;
+    size_t work_bytes = 0;
+    size_t fft_smem = 0;
+    int fft_threads = 128;
+    int synth_ctas = 0;
+    int anal_ctas = 0;
+    long long cilm_total = 0;
+    long long grid_total = 0;
+};
+
+static void batch_free(shtc_batch* B) {
+    cudaFree(B->d_groups);
+    cudaFree(B->d_fft);
+    cudaFree(B->d_pitems);
+    cudaFree(B->d_sitems);
+    cudaFree(B->d_aitems);
+    cudaFree(B->d_jobs);
+    cudaFree(B->d_counter);
+}
+
+template <typename Tp>
+static int upload(Tp** d, const std::vector<Tp>& h, cudaStream_t st) {
+    if (cudaMalloc((void**)d, sizeof(Tp) * (h.empty() ? 1 : h.size())) != cudaSuccess)
+        return SHTC_EALLOC;
+    if (h.empty()) return SHTC_OK;
+    return map_cuda(cudaMemcpyAsync(*d, h.data(), sizeof(Tp) * h.size(),
+                                    cudaMemcpyHostToDevice, st));
+}
+
+extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
+                                          shtc_plan* const* plans,
+                                          const int* nfields, void* stream) {
+    if (!out || !plans || !nfields || ngroup < 1) return SHTC_EHANDLE;
+    *out = nullptr;
+    cudaStream_t st = (cudaStream_t)stream;
+    shtc_batch* B = new (std::nothrow) shtc_batch();
+    if (!B) return SHTC_EALLOC;
+    cudaGetDevice(&B->device);
+    B->ngroup = ngroup;
+    std::vector<FftArgs> fa(ngroup);
+    long long pack = 0, spec = 0, coff = 0, goff = 0;
+    size_t smem = 0;
+    int threads = 128;
+    struct Cost { double c; int4 it; };
+    std::vector<Cost> sc, ac;
+    std::vector<int2> pitems;
+    std::vector<int4> jobs;
+    for (int gi = 0; gi < ngroup; ++gi) {
+        const shtc_plan* P = plans[gi];
+        const int nf = nfields[gi];
+        if (!P || nf < 1 || P->device != B->device || P->extend != 0) {
+            delete B;
+            return P && P->extend != 0 ? SHTC_EBOUND : SHTC_EHANDLE;
+        }
+        BatchGroup g;
+        g.rec = P->d_rec; g.pmm = P->d_pmm; g.rtab = P->d_rtab; g.z = P->d_z;
+        g.rowN = P->d_rowN; g.rowS = P->d_rowS; g.arowN = P->d_arowN;
+        g.arowS = P->d_arowS; g.wN = P->d_wN; g.wS = P->d_wS; g.nrm3 = P->d_nrm;
+        g.lc = P->lc; g.npair = P->npair; g.nf = nf; g.norm = P->norm;
+        g.nlat = P->nlat; g.nlon = P->nlon;
+        g.fft_jobs = P->fft.mode == 0 ? P->npair : 2 * P->npair;
+        g.tiles = (P->npair + kBatchThreads - 1) / kBatchThreads;
+        g.inv_nlon = 1.0 / (double)P->nlon;
+        g.nlm = P->nlm;
+        g.cilm_off = coff;
+        g.grid_off = goff;
+        g.pack_off = pack;
+        g.spec_off = spec;
+        coff += (long long)nf * 2 * (P->lc + 1) * (P->lc + 1);
+        goff += (long long)nf * P->nlat * P->nlon;
+        pack += (long long)P->nlm * nf * std::max(1, g.tiles);
+        spec += (long long)nf * P->npair * (P->lc + 1) * 2;
+        B->h_groups.push_back(g);
+        fa[gi] = fft_args(P->fft);
+        smem = std::max(smem, P->fft.smem);
+        threads = std::max(threads, P->fft.threads);
+        // work items, with costs for longest-first ordering
+        const int lc = P->lc;
+        for (int m = 0; m <= lc; ++m) {
+            pitems.push_back(make_int2(gi, m));
+            for (int t = 0; t < g.tiles; ++t) {
+                const int pairs = std::min(kBatchThreads, P->npair - t * kBatchThreads);
+                for (int f0 = 0; f0 < nf; f0 += kBatchSynthNF) {
+                    const int nv = std::min(kBatchSynthNF, nf - f0);
+                    sc.push_back({(double)(lc - m + 1) * pairs * (4.0 + 2.0 * nv),
+                                  make_int4(gi, m, t, f0)});
+                }
+                for (int f = 0; f < nf; ++f)
+                    ac.push_back({(double)(lc - m + 1) * pairs * 6.0, make_int4(gi, m, t, f)});
+            }
+        }
+        for (int f = 0; f < nf; ++f)
+            for (int j = 0; j < g.fft_jobs; ++j) jobs.push_back(make_int4(gi, f, j, 0));
+    }
+    // the spectra follow all packed-coefficient regions in the workspace
+    for (BatchGroup& g : B->h_groups) g.spec_off += pack;
+    auto by_cost = [](const Cost& a, const Cost& b) { return a.c > b.c; };
+    std::stable_sort(sc.begin(), sc.end(), by_cost);
+    std::stable_sort(ac.begin(), ac.end(), by_cost);
+    std::vector<int4> si(sc.size()), ai(ac.size());
+    for (size_t i = 0; i < sc.size(); ++i) si[i] = sc[i].it;
+    for (size_t i = 0; i < ac.size(); ++i) ai[i] = ac[i].it;
+    B->npitems = (int)pitems.size();
+    B->nsitems = (int)si.size();
+    B->naitems = (int)ai.size();
+    B->njobs = (int)jobs.size();
+    B->fft_smem = smem;
+    B->fft_threads = threads;
+    B->cilm_total = coff;
+    B->grid_total = goff;
+    B->work_bytes = (size_t)(pack + spec) * sizeof(double2);
+    int rc = SHTC_OK;
+    if (!rc) rc = upload(&B->d_groups, B->h_groups, st);
+    if (!rc) rc = upload(&B->d_fft, fa, st);
+    if (!rc) rc = upload(&B->d_pitems, pitems, st);
+    if (!rc) rc = upload(&B->d_sitems, si, st);
+    if (!rc) rc = upload(&B->d_aitems, ai, st);
+    if (!rc) rc = upload(&B->d_jobs, jobs, st);
+    if (!rc && cudaMalloc((void**)&B->d_counter, 2 * sizeof(int)) != cudaSuccess)
+        rc = SHTC_EALLOC;
+    if (!rc) {
+        int sm = 0, per = 0;
+        cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, B->device);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_synth, kBatchThreads, 0);
+        B->synth_ctas = sm * std::max(1, per);
+        const size_t asmem = anal_smem_bytes(kBatchAnalWarps);
+        cudaFuncSetAttribute(k_batch_anal, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)asmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_anal,
+                                                      32 * kBatchAnalWarps, asmem);
+        B->anal_ctas = sm * std::max(1, per);
+        if (B->fft_smem > 48 * 1024) {
+            cudaFuncSetAttribute(k_batch_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)B->fft_smem);
+            cudaFuncSetAttribute(k_batch_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)B->fft_smem);
+        }
+        rc = map_cuda(cudaStreamSynchronize(st));
+    }
+    if (rc) {
+        batch_free(B);
+        delete B;
+        return rc;
+    }
+    *out = B;
+    return SHTC_OK;
+}
+
+extern "C" SHTC_API int shtc_batch_destroy(shtc_batch* B) {
+    if (!B) return SHTC_EHANDLE;
+    batch_free(B);
+    delete B;
+    return SHTC_OK;
+}
+
+extern "C" SHTC_API size_t shtc_batch_workspace_bytes(const shtc_batch* B) {
+    return B ? B->work_bytes : 0;
+}
+
+extern "C" SHTC_API int shtc_batch_layout(const shtc_batch* B, long long* cilm_off,
+                                          long long* grid_off) {
+    if (!B || !cilm_off || !grid_off) return SHTC_EHANDLE;
+    for (int g = 0; g < B->ngroup; ++g) {
+        cilm_off[g] = B->h_groups[g].cilm_off;
+        grid_off[g] = B->h_groups[g].grid_off;
+    }
+    cilm_off[B->ngroup] = B->cilm_total;
+    grid_off[B->ngroup] = B->grid_total;
+    return SHTC_OK;
+}
+
+static int batch_check(const shtc_batch* B, const void* a, const void* b,
+                       void* work, size_t wb) {
+    if (!B || !a || !b) return SHTC_EHANDLE;
+    if (!work || wb < B->work_bytes) return SHTC_EWORK;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    return dev == B->device ? SHTC_OK : SHTC_EHANDLE;
+}
+
+extern "C" SHTC_API int shtc_batch_synthesis(const shtc_batch* B, const double* cilm,
+                                             double* grid, void* work, size_t wb,
+                                             void* stream) {
+    int rc = batch_check(B, cilm, grid, work, wb);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    double2* w = (double2*)work;
+    stage_begin(SHTC_STAGE_PACK, st);
+    k_batch_pack<<<B->npitems, 128, 0, st>>>(B->d_groups, B->d_pitems, cilm, w);
+    stage_end(SHTC_STAGE_PACK, st);
+    if ((rc = map_cuda(cudaGetLastError()))) return rc;
+    if ((rc = map_cuda(cudaMemsetAsync(B->d_counter, 0, sizeof(int), st)))) return rc;
+    stage_begin(SHTC_STAGE_LEGENDRE_SYNTH, st);
+    k_batch_synth<<<B->synth_ctas, kBatchThreads, 0, st>>>(B->d_groups, B->d_sitems,
+                                                           B->nsitems, B->d_counter, w);
+    stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
+    if ((rc = map_cuda(cudaGetLastError()))) return rc;
+    stage_begin(SHTC_STAGE_FFT_C2R, st);
+    k_batch_c2r<<<B->njobs, B->fft_threads, B->fft_smem, st>>>(B->d_groups, B->d_fft,
+                                                               B->d_jobs, w, grid);
+    stage_end(SHTC_STAGE_FFT_C2R, st);
+    return map_cuda(cudaGetLastError());
+}
+
+extern "C" SHTC_API int shtc_batch_analysis(const shtc_batch* B, const double* grid,
+                                            double* cilm, void* work, size_t wb,
+                                            void* stream) {
+    int rc = batch_check(B, grid, cilm, work, wb);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    double2* w = (double2*)work;
+    stage_begin(SHTC_STAGE_FFT_R2C, st);
+    k_batch_r2c<<<B->njobs, B->fft_threads, B->fft_smem, st>>>(B->d_groups, B->d_fft,
+                                                               B->d_jobs, grid, w);
+    stage_end(SHTC_STAGE_FFT_R2C, st);
+    if ((rc = map_cuda(cudaGetLastError()))) return rc;
+    if ((rc = map_cuda(cudaMemsetAsync(B->d_counter, 0, sizeof(int), st)))) return rc;
+    stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
+    k_batch_anal<<<B->anal_ctas, 32 * kBatchAnalWarps, anal_smem_bytes(kBatchAnalWarps),
+                   st>>>(B->d_groups, B->d_aitems, B->naitems, B->d_counter, w);
+    stage_end(SHTC_STAGE_LEGENDRE_ANAL, st);
+    if ((rc = map_cuda(cudaGetLastError()))) return rc;
+    if ((rc = map_cuda(cudaMemsetAsync(cilm, 0, sizeof(double) * B->cilm_total, st))))
+        return rc;
+    stage_begin(SHTC_STAGE_UNPACK, st);
+    k_batch_unpack<<<B->npitems, 128, 0, st>>>(B->d_groups, B->d_pitems, w, cilm);
+    stage_end(SHTC_STAGE_UNPACK, st);
+    return map_cuda(cudaGetLastError());
+}

@@ -1,0 +1,375 @@
+// Device code of the longitude FFTs (c2r for synthesis, r2c for analysis),
+// shared by the per-plan kernels (kernels.cu) and the batched kernels
+// (batch.cu).  Stockham autosort passes ping-pong between two shared
+// buffers; radix 2, 3, 4, 5, 7, 11, 13 butterflies; Bluestein's algorithm
+// for lengths with other prime factors.  Conventions are those of FFTW's
+// unnormalised r2c / c2r (src/FFTW3.f95:212-271).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "shtc_internal.cuh"
+
+namespace shtc {
+
+// ---------------------------------------------------------------------------
+// FFT: Stockham autosort passes in shared memory
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// table entries are exp(-2 pi i t / len); SIGN > 0 takes the conjugate
+template <int SIGN>
+__device__ __forceinline__ double2 twv(const double2* tw, int t) {
+    double2 w = tw[t];
+    if (SIGN > 0) w.y = -w.y;
+    return w;
+}
+
+// cos and sin of 2*pi*u/R for the odd radices, 1 <= u <= (R-1)/2 (values
+// of the circular functions rounded to double, evaluated in extended
+// precision).  With the butterfly loops unrolled, u is a compile-time
+// constant and these fold to immediates.
+__host__ __device__ constexpr double root_cos(int R, int u) {
+    return R == 3 ? -0.5
+         : R == 5 ? (u == 1 ? 0.30901699437494745 : -0.8090169943749475)
+         : R == 7 ? (u == 1 ? 0.6234898018587335 : u == 2 ? -0.2225209339563144
+                             : -0.9009688679024191)
+         : R == 11 ? (u == 1 ? 0.8412535328311812 : u == 2 ? 0.41541501300188644
+                     : u == 3 ? -0.14231483827328514 : u == 4 ? -0.6548607339452851
+                     : -0.9594929736144974)
+         : (u == 1 ? 0.8854560256532099 : u == 2 ? 0.5680647467311558
+            : u == 3 ? 0.12053668025532305 : u == 4 ? -0.3546048870425356
+            : u == 5 ? -0.7485107481711011 : -0.970941817426052);
+}
+__host__ __device__ constexpr double root_sin(int R, int u) {
+    return R == 3 ? 0.8660254037844386
+         : R == 5 ? (u == 1 ? 0.9510565162951535 : 0.5877852522924731)
+         : R == 7 ? (u == 1 ? 0.7818314824680298 : u == 2 ? 0.9749279121818236
+                             : 0.4338837391175581)
+         : R == 11 ? (u == 1 ? 0.5406408174555976 : u == 2 ? 0.9096319953545183
+                     : u == 3 ? 0.9898214418809327 : u == 4 ? 0.7557495743542583
+                     : 0.28173255684142967)
+         : (u == 1 ? 0.46472317204376856 : u == 2 ? 0.8229838658936564
+            : u == 3 ? 0.992708874098054 : u == 4 ? 0.9350162426854148
+            : u == 5 ? 0.6631226582407952 : 0.23931566428755777);
+}
+
+// radix-R DFT of v[] in place (R = 2, 4, or an odd prime <= 13)
+template <int R, int SIGN>
+__device__ __forceinline__ void dft_small(double2* v) {
+    if (R == 2) {
+        const double2 a = v[0], b = v[1];
+        v[0] = make_double2(a.x + b.x, a.y + b.y);
+        v[1] = make_double2(a.x - b.x, a.y - b.y);
+    } else if (R == 4) {
+        const double2 s0 = make_double2(v[0].x + v[2].x, v[0].y + v[2].y);
+        const double2 d0 = make_double2(v[0].x - v[2].x, v[0].y - v[2].y);
+        const double2 s1 = make_double2(v[1].x + v[3].x, v[1].y + v[3].y);
+        const double2 d1 = make_double2(v[1].x - v[3].x, v[1].y - v[3].y);
+        // forward: multiply d1 by -i; backward: by +i
+        const double2 e = SIGN < 0 ? make_double2(d1.y, -d1.x) : make_double2(-d1.y, d1.x);
+        v[0] = make_double2(s0.x + s1.x, s0.y + s1.y);
+        v[2] = make_double2(s0.x - s1.x, s0.y - s1.y);
+        v[1] = make_double2(d0.x + e.x, d0.y + e.y);
+        v[3] = make_double2(d0.x - e.x, d0.y - e.y);
+    } else {
+        // odd R: pair q with R-q; y_s = x0 + sum_q cos(2pi sq/R) a_q -+ i sum_q sin b_q
+        constexpr int H = (R - 1) / 2;
+        double2 a[H + 1], b[H + 1];
+        double2 y0 = v[0];
+#pragma unroll
+        for (int q = 1; q <= H; ++q) {
+            a[q] = make_double2(v[q].x + v[R - q].x, v[q].y + v[R - q].y);
+            b[q] = make_double2(v[q].x - v[R - q].x, v[q].y - v[R - q].y);
+            y0.x += a[q].x;
+            y0.y += a[q].y;
+        }
+        const double2 x0 = v[0];
+        v[0] = y0;
+#pragma unroll
+        for (int s = 1; s <= H; ++s) {
+            double2 re = x0, im = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int q = 1; q <= H; ++q) {
+                const int t = (s * q) % R;
+                const int u = t <= H ? t : R - t;
+                const double c = root_cos(R, u);
+                const double sn = t <= H ? root_sin(R, u) : -root_sin(R, u);
+                re.x = fma(c, a[q].x, re.x);
+                re.y = fma(c, a[q].y, re.y);
+                im.x = fma(sn, b[q].x, im.x);
+                im.y = fma(sn, b[q].y, im.y);
+            }
+            // forward: y_s = re - i im, y_{R-s} = re + i im
+            if (SIGN < 0) {
+                v[s] = make_double2(re.x + im.y, re.y - im.x);
+                v[R - s] = make_double2(re.x - im.y, re.y + im.x);
+            } else {
+                v[s] = make_double2(re.x - im.y, re.y + im.x);
+                v[R - s] = make_double2(re.x + im.y, re.y - im.x);
+            }
+        }
+    }
+}
+
+// One Stockham pass of radix R from x to y (ping-pong shared buffers).
+template <int R, int SIGN>
+__device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
+                                         double2* __restrict__ y, int M, int ns,
+                                         const double2* __restrict__ tw) {
+    const int nr = M / R;
+    const int step = M / (ns * R);
+    for (int j = threadIdx.x; j < nr; j += blockDim.x) {
+        const int k = j % ns;
+        double2 v[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = x[j + q * nr];
+        if (k != 0) {
+#pragma unroll
+            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twv<SIGN>(tw, k * q * step));
+        }
+        dft_small<R, SIGN>(v);
+        const int d = (j - k) * R + k;
+#pragma unroll
+        for (int q = 0; q < R; ++q) y[d + q * ns] = v[q];
+    }
+}
+
+// Runs the passes; the data starts in a, the result pointer is returned.
+template <int SIGN>
+__device__ double2* fft_run(double2* a, double2* b, int M, const int* fac,
+                            int nfac, const double2* __restrict__ tw) {
+    int ns = 1;
+    for (int i = 0; i < nfac; ++i) {
+        __syncthreads();
+        const int r = fac[i];
+        switch (r) {
+            case 2: fft_pass<2, SIGN>(a, b, M, ns, tw); break;
+            case 3: fft_pass<3, SIGN>(a, b, M, ns, tw); break;
+            case 4: fft_pass<4, SIGN>(a, b, M, ns, tw); break;
+            case 5: fft_pass<5, SIGN>(a, b, M, ns, tw); break;
+            case 7: fft_pass<7, SIGN>(a, b, M, ns, tw); break;
+            case 11: fft_pass<11, SIGN>(a, b, M, ns, tw); break;
+            case 13: fft_pass<13, SIGN>(a, b, M, ns, tw); break;
+            default: break;
+        }
+        ns *= r;
+        double2* t = a;
+        a = b;
+        b = t;
+    }
+    __syncthreads();
+    return a;
+}
+
+struct FftArgs {
+    int n, mode, m, nfac, bluestein, mb;
+    int fac[kMaxFactors];
+    const double2* tw;
+    const double2* twn;
+    const double2* chirp;
+    const double2* kern;
+};
+
+// Complex DFT of length F.m of buf with sign SIGN; buf and tmp each hold
+// F.mb (Bluestein) or F.m elements.  Returns the pointer holding the result.
+template <int SIGN>
+__device__ double2* fft_exec(const FftArgs& F, double2* buf, double2* tmp) {
+    __syncthreads();
+    if (!F.bluestein) return fft_run<SIGN>(buf, tmp, F.m, F.fac, F.nfac, F.tw);
+    // Bluestein: X_k = c_k sum_j (x_j c_j) conj(c_{k-j}), c_t = exp(-+ i pi t^2/m)
+    const int m = F.m, mb = F.mb;
+    for (int t = threadIdx.x; t < mb; t += blockDim.x) {
+        if (t < m) {
+            double2 c = F.chirp[t];
+            if (SIGN > 0) c.y = -c.y;
+            buf[t] = cmul(buf[t], c);
+        } else {
+            buf[t] = make_double2(0.0, 0.0);
+        }
+    }
+    double2* r = fft_run<-1>(buf, tmp, mb, F.fac, F.nfac, F.tw);
+    double2* o = (r == buf) ? tmp : buf;
+    for (int t = threadIdx.x; t < mb; t += blockDim.x) {
+        double2 kf;
+        if (SIGN < 0) {
+            kf = F.kern[t];
+        } else {
+            kf = F.kern[(mb - t) & (mb - 1)];
+            kf.y = -kf.y;
+        }
+        r[t] = cmul(r[t], kf);
+    }
+    double2* r2 = fft_run<+1>(r, o, mb, F.fac, F.nfac, F.tw);
+    const double inv = 1.0 / (double)mb;
+    for (int t = threadIdx.x; t < m; t += blockDim.x) {
+        double2 c = F.chirp[t];
+        if (SIGN > 0) c.y = -c.y;
+        const double2 v = make_double2(r2[t].x * inv, r2[t].y * inv);
+        r2[t] = cmul(v, c);
+    }
+    __syncthreads();
+    return r2;
+}
+
+// c2r: spec -> grid.  mode 0 (odd n): CTA = (pair, field), the two rings are
+// the real and imaginary parts of one complex length-n inverse DFT.  mode 1
+// (even n): CTA = (pair*2 + ring, field), the ring is computed by a complex
+// length-n/2 inverse DFT and the even/odd split.  Output rows are scaled by
+// the ring weight when wN/wS are given (analysis adjoint).
+template <typename GT>
+__device__ __forceinline__ void fft_c2r_body(
+    const FftArgs& F, double2* smem_fft, int job, int f,
+    const double2* __restrict__ spec, GT* __restrict__ grid, long long gf,
+    long long grs, long long gcs, const int* __restrict__ rowN,
+    const int* __restrict__ rowS, const double* __restrict__ wN,
+    const double* __restrict__ wS, double wscale, int lc, int npair,
+    int extend_col) {
+    const int len = F.bluestein ? F.mb : F.m;
+    double2* a = smem_fft;
+    double2* b = smem_fft + len;
+    const int n = F.n;
+    if (F.mode == 0) {
+        const int p = job;
+        const int rN = rowN[p], rS = rowS[p];
+        const double2* X = spec + ((long long)f * npair + p) * (lc + 1) * 2;
+        for (int k = threadIdx.x; k < n; k += blockDim.x) a[k] = make_double2(0.0, 0.0);
+        __syncthreads();
+        for (int k = threadIdx.x; k <= lc; k += blockDim.x) {
+            double2 xn = X[2 * k + 0];
+            double2 xs = rS >= 0 ? X[2 * k + 1] : make_double2(0.0, 0.0);
+            if (k == 0) {
+                xn.y = 0.0;
+                xs.y = 0.0;
+            }
+            // Z_k = X^N_k + i X^S_k ; Z_{n-k} = conj(X^N_k) + i conj(X^S_k)
+            a[k] = make_double2(xn.x - xs.y, xn.y + xs.x);
+            if (k > 0) a[n - k] = make_double2(xn.x + xs.y, -xn.y + xs.x);
+        }
+        const double2* r = fft_exec<+1>(F, a, b);
+        const double sN = wN ? wN[p] * wscale : 1.0;
+        const double sS = wS ? wS[p] * wscale : 1.0;
+        GT* gN = rN >= 0 ? grid + f * gf + rN * grs : nullptr;
+        GT* gS = rS >= 0 ? grid + f * gf + rS * grs : nullptr;
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const double2 v = r[j];
+            if (gN) gN[j * gcs] = (GT)(v.x * sN);
+            if (gS) gS[j * gcs] = (GT)(v.y * sS);
+        }
+        if (extend_col && threadIdx.x == 0) {
+            if (gN) gN[(long long)n * gcs] = (GT)(r[0].x * sN);
+            if (gS) gS[(long long)n * gcs] = (GT)(r[0].y * sS);
+        }
+    } else {
+        const int p = job >> 1;
+        const int h = job & 1;
+        const int row = h ? rowS[p] : rowN[p];
+        if (row < 0) return;
+        const int M = F.m;   // n/2
+        const double2* X = spec + ((long long)f * npair + p) * (lc + 1) * 2 + h;
+        // Z'_k = (X_k + conj X_{M-k}) + i w^{-k} (X_k - conj X_{M-k}), w = exp(-2 pi i/n)
+        for (int k = threadIdx.x; k < M; k += blockDim.x) {
+            double2 xk = k <= lc ? X[2 * k] : make_double2(0.0, 0.0);
+            if (k == 0) xk.y = 0.0;
+            const int km = M - k;
+            double2 xm = (km <= lc && km < M) ? X[2 * km] : make_double2(0.0, 0.0);
+            if (km == 0) xm.y = 0.0;
+            const double2 A = make_double2(xk.x + xm.x, xk.y - xm.y);
+            const double2 B = make_double2(xk.x - xm.x, xk.y + xm.y);
+            double2 w = F.twn[k];
+            w.y = -w.y;                         // exp(+2 pi i k/n)
+            const double2 wb = cmul(w, B);
+            a[k] = make_double2(A.x - wb.y, A.y + wb.x);
+        }
+        const double2* r = fft_exec<+1>(F, a, b);
+        const double sc = (h ? (wS ? wS[p] * wscale : 1.0) : (wN ? wN[p] * wscale : 1.0));
+        GT* g = grid + f * gf + row * grs;
+        for (int j = threadIdx.x; j < M; j += blockDim.x) {
+            const double2 v = r[j];
+            g[(2LL * j) * gcs] = (GT)(v.x * sc);
+            g[(2LL * j + 1) * gcs] = (GT)(v.y * sc);
+        }
+        if (extend_col && threadIdx.x == 0) g[(long long)n * gcs] = (GT)(r[0].x * sc);
+    }
+}
+
+// r2c: grid rows -> spec (m = 0..lc), each multiplied by the ring weight
+// (times wscale) as (Re, -Im), the reference's fcoef (SHExpandGLQ.f95:535-547).
+// fold_extend adds column n into column 0 (adjoint of the extend copy).
+template <typename GT>
+__device__ __forceinline__ void fft_r2c_body(
+    const FftArgs& F, double2* smem_fft, int job, int f,
+    const GT* __restrict__ grid, long long gf, long long grs, long long gcs,
+    double2* __restrict__ spec, const int* __restrict__ rowN,
+    const int* __restrict__ rowS, const double* __restrict__ wN,
+    const double* __restrict__ wS, double wscale, int lc, int npair,
+    int fold_extend) {
+    const int len = F.bluestein ? F.mb : F.m;
+    double2* a = smem_fft;
+    double2* b = smem_fft + len;
+    const int n = F.n;
+    if (F.mode == 0) {
+        const int p = job;
+        const int rN = rowN[p], rS = rowS[p];
+        const GT* gN = rN >= 0 ? grid + f * gf + rN * grs : nullptr;
+        const GT* gS = rS >= 0 ? grid + f * gf + rS * grs : nullptr;
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            double xn = gN ? (double)gN[j * gcs] : 0.0;
+            double xs = gS ? (double)gS[j * gcs] : 0.0;
+            if (fold_extend && j == 0) {
+                if (gN) xn += (double)gN[(long long)n * gcs];
+                if (gS) xs += (double)gS[(long long)n * gcs];
+            }
+            a[j] = make_double2(xn, xs);
+        }
+        const double2* r = fft_exec<-1>(F, a, b);
+        const double sN = wN ? wN[p] * wscale : wscale;
+        const double sS = wS ? wS[p] * wscale : wscale;
+        double2* X = spec + ((long long)f * npair + p) * (lc + 1) * 2;
+        for (int k = threadIdx.x; k <= lc; k += blockDim.x) {
+            const double2 zk = r[k];
+            const double2 zm = r[k == 0 ? 0 : n - k];
+            // X^N = (Z_k + conj Z_{n-k})/2 ; X^S = (Z_k - conj Z_{n-k})/(2i)
+            const double nr = 0.5 * (zk.x + zm.x), ni = 0.5 * (zk.y - zm.y);
+            const double sr = 0.5 * (zk.y + zm.y), si = -0.5 * (zk.x - zm.x);
+            X[2 * k + 0] = make_double2(sN * nr, -(sN * ni));
+            X[2 * k + 1] = make_double2(sS * sr, -(sS * si));
+        }
+    } else {
+        const int p = job >> 1;
+        const int h = job & 1;
+        const int row = h ? rowS[p] : rowN[p];
+        double2* X = spec + ((long long)f * npair + p) * (lc + 1) * 2 + h;
+        if (row < 0) {
+            for (int k = threadIdx.x; k <= lc; k += blockDim.x) X[2 * k] = make_double2(0.0, 0.0);
+            return;
+        }
+        const int M = F.m;
+        const GT* g = grid + f * gf + row * grs;
+        for (int j = threadIdx.x; j < M; j += blockDim.x) {
+            double x0 = (double)g[(2LL * j) * gcs];
+            const double x1 = (double)g[(2LL * j + 1) * gcs];
+            if (fold_extend && j == 0) x0 += (double)g[(long long)n * gcs];
+            a[j] = make_double2(x0, x1);
+        }
+        const double2* r = fft_exec<-1>(F, a, b);
+        const double sc = h ? (wS ? wS[p] * wscale : wscale) : (wN ? wN[p] * wscale : wscale);
+        for (int k = threadIdx.x; k <= lc; k += blockDim.x) {
+            const double2 zk = r[k == M ? 0 : k];
+            const double2 zm = r[k == 0 ? 0 : M - k];
+            // E = (Z_k + conj Z_{M-k})/2, O = (Z_k - conj Z_{M-k})/(2i), X = E + w^k O
+            const double2 E = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+            const double2 O = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
+            const double2 wo = cmul(F.twn[k], O);
+            const double xr = E.x + wo.x, xi = E.y + wo.y;
+            X[2 * k] = make_double2(sc * xr, -(sc * xi));
+        }
+    }
+}
+
+// FftArgs of a plan's FFT (kernels.cu)
+FftArgs fft_args(const FftPlan& f);
+
+}  // namespace shtc

@@ -93,23 +93,23 @@ int build_fft_plan(FftPlan* f, int n, cudaStream_t stream);
 void free_fft_plan(FftPlan* f);
 
 // kernels.cu launchers (return cudaGetLastError() mapped to SHTC codes)
-int launch_pack_coef(const shtc_plan* P, const double* cilm, long long sf,
+int launch_pack_coef(const shtc_plan* P, const void* cilm, int dtype, long long sf,
                      long long sk, long long sl, long long sm, int cdim,
                      double2* packed, int nfield, int scale_mode,
                      cudaStream_t st);
 int launch_legendre_synth(const shtc_plan* P, const double2* packed,
                           double2* spec, int nfield, cudaStream_t st);
-int launch_fft_c2r(const shtc_plan* P, const double2* spec, double* grid,
+int launch_fft_c2r(const shtc_plan* P, const double2* spec, void* grid, int dtype,
                    long long gf, long long grs, long long gcs, int nfield,
                    int weighted, cudaStream_t st);
-int launch_fft_r2c(const shtc_plan* P, const double* grid, long long gf,
+int launch_fft_r2c(const shtc_plan* P, const void* grid, int dtype, long long gf,
                    long long grs, long long gcs, double2* spec, int nfield,
                    int weighted, int fold_extend, cudaStream_t st);
 int launch_legendre_anal(const shtc_plan* P, const double2* spec,
                          double2* partial, int ntiles_out, int nfield,
                          cudaStream_t st);
 int launch_unpack_coef(const shtc_plan* P, const double2* partial, int ntiles,
-                       double* cilm, long long sf, long long sk, long long sl,
+                       void* cilm, int dtype, long long sf, long long sk, long long sl,
                        long long sm, int cdim, int nfield, int normalise,
                        cudaStream_t st);
 int anal_tiles(const shtc_plan* P);

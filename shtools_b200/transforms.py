@@ -96,51 +96,55 @@ class Plan:
         nb = int(self.lib.shtc_workspace_bytes(self.handle, int(nfield)))
         return torch.empty(nb, dtype=torch.uint8, device=self.device), nb
 
-    # -- raw transforms on (F, 2, D, D) / (F, rows, cols) float64 tensors ----
+    # -- raw transforms on (F, 2, D, D) / (F, rows, cols) tensors -------------
+    # float64 or float32 arrays; the kernels compute in FP64 either way
     def _run(self, fn, src, dst, nfield, src_is_coef):
         ws, nb = self.workspace(nfield)
         with torch.cuda.device(self.device):
             st = _stream_ptr(self.device)
             c, g = (src, dst) if src_is_coef else (dst, src)
-            cargs = (ctypes_void(c.data_ptr()), c.stride(0), c.stride(1),
-                     c.stride(2), c.stride(3), c.shape[2])
-            gargs = (ctypes_void(g.data_ptr()), g.stride(0), g.stride(1),
-                     g.stride(2))
+            cargs = (ctypes_void(c.data_ptr()), _DTYPE[c.dtype], c.stride(0),
+                     c.stride(1), c.stride(2), c.stride(3), c.shape[2])
+            gargs = (ctypes_void(g.data_ptr()), _DTYPE[g.dtype], g.stride(0),
+                     g.stride(1), g.stride(2))
             args = (cargs + gargs) if src_is_coef else (gargs + cargs)
             rc = fn(self.handle, *args, int(nfield), ctypes_void(ws.data_ptr()),
                     nb, st)
         _lib.check(rc, fn.__name__)
 
-    def synthesis(self, cilm, out=None):
+    def synthesis(self, cilm, out=None, dtype=None):
         F = cilm.shape[0]
         if out is None:
             out = torch.empty((F, self.info["nlat_out"], self.info["nlon_out"]),
-                              dtype=torch.float64, device=self.device)
-        self._run(self.lib.shtc_synthesis, cilm, out, F, True)
+                              dtype=dtype or cilm.dtype, device=self.device)
+        self._run(self.lib.shtc_synthesis_ex, cilm, out, F, True)
         return out
 
-    def analysis(self, grid, cdim=None, out=None):
+    def analysis(self, grid, cdim=None, out=None, dtype=None):
         F = grid.shape[0]
         cdim = self.lc + 1 if cdim is None else cdim
         if out is None:
-            out = torch.empty((F, 2, cdim, cdim), dtype=torch.float64,
+            out = torch.empty((F, 2, cdim, cdim), dtype=dtype or grid.dtype,
                               device=self.device)
-        self._run(self.lib.shtc_analysis, grid, out, F, False)
+        self._run(self.lib.shtc_analysis_ex, grid, out, F, False)
         return out
 
-    def synthesis_adjoint(self, grid, cdim):
+    def synthesis_adjoint(self, grid, cdim, dtype=None):
         F = grid.shape[0]
-        out = torch.empty((F, 2, cdim, cdim), dtype=torch.float64,
+        out = torch.empty((F, 2, cdim, cdim), dtype=dtype or grid.dtype,
                           device=self.device)
-        self._run(self.lib.shtc_synthesis_adjoint, grid, out, F, False)
+        self._run(self.lib.shtc_synthesis_adjoint_ex, grid, out, F, False)
         return out
 
-    def analysis_adjoint(self, cilm):
+    def analysis_adjoint(self, cilm, dtype=None):
         F = cilm.shape[0]
         out = torch.empty((F, self.info["nlat"], self.info["nlon"]),
-                          dtype=torch.float64, device=self.device)
-        self._run(self.lib.shtc_analysis_adjoint, cilm, out, F, True)
+                          dtype=dtype or cilm.dtype, device=self.device)
+        self._run(self.lib.shtc_analysis_adjoint_ex, cilm, out, F, True)
         return out
+
+
+_DTYPE = {torch.float64: 0, torch.float32: 1}
 
 
 _cache_lock = threading.Lock()
@@ -252,16 +256,27 @@ def _flat(t, tail):
     return t.reshape((-1,) + tuple(t.shape[t.dim() - tail:])), lead
 
 
-def _as_cuda64(t, what):
+def _as_cuda(t, what):
+    """CUDA tensor of dtype float64 or float32 (other dtypes -> float64)."""
     if isinstance(t, np.ndarray):
         t = torch.from_numpy(t)
     if not isinstance(t, torch.Tensor):
         t = torch.as_tensor(t)
     if not t.is_cuda:
         t = t.to("cuda")
-    if t.dtype != torch.float64:
+    if t.dtype not in _DTYPE:
         t = t.to(torch.float64)
     return t
+
+
+def _out_dtype(dtype):
+    if dtype is None:
+        return None
+    dtype = torch.float64 if dtype in (np.float64, "float64") else \
+        torch.float32 if dtype in (np.float32, "float32") else dtype
+    if dtype not in _DTYPE:
+        raise ValueError("dtype must be float64 or float32; got %r" % (dtype,))
+    return dtype
 
 
 # ---------------------------------------------------------------------------
@@ -269,89 +284,96 @@ def _as_cuda64(t, what):
 # ---------------------------------------------------------------------------
 class _Synthesis(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, cilm, plan):
+    def forward(ctx, cilm, plan, dtype):
         c, lead = _flat(cilm[..., :2, :, :], 3)
-        g = plan.synthesis(c)
+        g = plan.synthesis(c, dtype=dtype)
         ctx.plan = plan
         ctx.cdim = cilm.shape[-1]
         ctx.lead = lead
         ctx.cshape = cilm.shape
+        ctx.cdtype = cilm.dtype
         return g.reshape(tuple(lead) + tuple(g.shape[1:]))
 
     @staticmethod
     def backward(ctx, gout):
         plan = ctx.plan
         g, _ = _flat(gout.contiguous(), 2)
-        gc = plan.synthesis_adjoint(g, ctx.cdim)
+        gc = plan.synthesis_adjoint(g, ctx.cdim, dtype=ctx.cdtype)
         gc = gc.reshape(tuple(ctx.lead) + tuple(gc.shape[1:]))
         if ctx.cshape[-3] > 2:
             pad = torch.zeros(ctx.cshape, dtype=gc.dtype, device=gc.device)
             pad[..., :2, :, :] = gc
             gc = pad
-        return gc, None
+        return gc, None, None
 
 
 class _Analysis(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, grid, plan, cdim):
+    def forward(ctx, grid, plan, cdim, dtype):
         nlat, nlon = plan.info["nlat"], plan.info["nlon"]
         g, lead = _flat(grid, 2)
-        c = plan.analysis(g[:, :nlat, :nlon], cdim)
+        c = plan.analysis(g[:, :nlat, :nlon], cdim, dtype=dtype)
         ctx.plan = plan
         ctx.lead = lead
         ctx.gshape = grid.shape
+        ctx.gdtype = grid.dtype
         return c.reshape(tuple(lead) + tuple(c.shape[1:]))
 
     @staticmethod
     def backward(ctx, gc):
         plan = ctx.plan
         c, _ = _flat(gc.contiguous(), 3)
-        g = plan.analysis_adjoint(c)
+        g = plan.analysis_adjoint(c, dtype=ctx.gdtype)
         g = g.reshape(tuple(ctx.lead) + tuple(g.shape[1:]))
         if tuple(g.shape) != tuple(ctx.gshape):
             full = torch.zeros(ctx.gshape, dtype=g.dtype, device=g.device)
             full[..., :g.shape[-2], :g.shape[-1]] = g
             g = full
-        return g, None, None
+        return g, None, None, None
 
 
 # ---------------------------------------------------------------------------
 # public API
 # ---------------------------------------------------------------------------
 def MakeGridDH(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
-               extend=False):
+               extend=False, dtype=None):
     """Driscoll-Healy synthesis on the GPU (src/MakeGridDH.f95:1).
 
-    cilm: (..., 2, D, D) float64.  Returns (..., n+extend, sampling*n+extend)
-    with n = 2*lmax+2; row 0 is 90 N, column 0 is 0 E.
+    cilm: (..., 2, D, D) float64 or float32.  Returns (..., n+extend,
+    sampling*n+extend) with n = 2*lmax+2; row 0 is 90 N, column 0 is 0 E.
+    dtype: element type of the grid (default: that of cilm); the arithmetic
+    is FP64 either way.
     """
     _check_common(norm, csphase)
     if sampling not in (1, 2):
         raise ValueError("sampling must be 1 (n by n) or 2 (n by 2n); got %r"
                          % (sampling,))
     lmax, lc = _resolve_synth(np.shape(cilm), lmax, lmax_calc)
-    cilm = _as_cuda64(cilm, "cilm")
+    dtype = _out_dtype(dtype)
+    cilm = _as_cuda(cilm, "cilm")
     plan = get_plan(GRID_DH, lmax, lc, norm, csphase, sampling, int(bool(extend)),
                     device=cilm.device)
-    return _Synthesis.apply(cilm, plan)
+    return _Synthesis.apply(cilm, plan, dtype)
 
 
-def SHExpandDH(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None):
+def SHExpandDH(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None,
+               dtype=None):
     """Driscoll-Healy analysis on the GPU (src/SHExpandDH.f95:1).
 
-    griddh: (..., n, >= sampling*n) float64 with n even.  Returns
-    (..., 2, lmax_calc+1, lmax_calc+1).
+    griddh: (..., n, >= sampling*n) float64 or float32 with n even.  Returns
+    (..., 2, lmax_calc+1, lmax_calc+1) of ``dtype`` (default: the grid's).
     """
     _check_common(norm, csphase)
     lmax, lc = _resolve_anal_dh(np.shape(griddh), sampling, lmax_calc)
-    grid = _as_cuda64(griddh, "griddh")
+    dtype = _out_dtype(dtype)
+    grid = _as_cuda(griddh, "griddh")
     plan = get_plan(GRID_DH, lmax, lc, norm, csphase, sampling, 0,
                     device=grid.device)
-    return _Analysis.apply(grid, plan, lc + 1)
+    return _Analysis.apply(grid, plan, lc + 1, dtype)
 
 
 def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
-                extend=False):
+                extend=False, dtype=None):
     """Gauss-Legendre synthesis on the GPU (src/MakeGridGLQ.f95:1).
 
     zero: the lmax+1 Gauss-Legendre nodes (e.g. from SHGLQ); None computes
@@ -359,15 +381,16 @@ def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
     """
     _check_common(norm, csphase)
     lmax, lc = _resolve_synth(np.shape(cilm), lmax, lmax_calc)
+    dtype = _out_dtype(dtype)
     z = None if zero is None else _host64(zero, lmax + 1, "zero")
-    cilm = _as_cuda64(cilm, "cilm")
+    cilm = _as_cuda(cilm, "cilm")
     plan = get_plan(GRID_GLQ, lmax, lc, norm, csphase, 1, int(bool(extend)),
                     zero=z, device=cilm.device)
-    return _Synthesis.apply(cilm, plan)
+    return _Synthesis.apply(cilm, plan, dtype)
 
 
 def SHExpandGLQ(gridglq, w=None, zero=None, norm=1, csphase=1,
-                lmax_calc=None):
+                lmax_calc=None, dtype=None):
     """Gauss-Legendre analysis on the GPU (src/SHExpandGLQ.f95:1).
 
     gridglq: (..., lmax+1, >= 2*lmax+1).  w, zero: weights and nodes from
@@ -375,10 +398,11 @@ def SHExpandGLQ(gridglq, w=None, zero=None, norm=1, csphase=1,
     """
     _check_common(norm, csphase)
     lmax, lc = _resolve_anal_glq(np.shape(gridglq), lmax_calc)
+    dtype = _out_dtype(dtype)
     nlat = lmax + 1
     z = None if zero is None else _host64(zero, nlat, "zero")
     wh = None if w is None else _host64(w, nlat, "w")
-    grid = _as_cuda64(gridglq, "gridglq")
+    grid = _as_cuda(gridglq, "gridglq")
     if (z is None) != (wh is None):
         # one given: complete the pair from the GPU PreGLQ
         zz, ww = SHGLQ(lmax, device=grid.device)
@@ -386,7 +410,7 @@ def SHExpandGLQ(gridglq, w=None, zero=None, norm=1, csphase=1,
         wh = ww if wh is None else wh
     plan = get_plan(GRID_GLQ, lmax, lc, norm, csphase, 1, 0, zero=z, w=wh,
                     device=grid.device)
-    return _Analysis.apply(grid, plan, lc + 1)
+    return _Analysis.apply(grid, plan, lc + 1, dtype)
 
 
 def _host64(a, n, what):
