@@ -119,8 +119,8 @@ template <int R, int SIGN>
 __device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
                                          double2* __restrict__ y, int M, int ns,
                                          const double2* __restrict__ tw) {
+    // tw: this pass's twiddles, entry (q-1)*ns + k
     const int nr = M / R;
-    const int step = M / (ns * R);
     for (int j = threadIdx.x; j < nr; j += blockDim.x) {
         const int k = j % ns;
         double2 v[R];
@@ -128,7 +128,7 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
         for (int q = 0; q < R; ++q) v[q] = x[j + q * nr];
         if (k != 0) {
 #pragma unroll
-            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twv<SIGN>(tw, k * q * step));
+            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twv<SIGN>(tw, (q - 1) * ns + k));
         }
         dft_small<R, SIGN>(v);
         const int d = (j - k) * R + k;
@@ -140,25 +140,27 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
 // Runs the passes; the data starts in a, the result pointer is returned.
 template <int SIGN>
 __device__ double2* fft_run(double2* a, double2* b, int M, const int* fac,
-                            int nfac, const double2* __restrict__ tw) {
+                            int nfac, const double2* __restrict__ tw,
+                            const int* tw_off) {
     int ns = 1;
     for (int i = 0; i < nfac; ++i) {
         __syncthreads();
         const int r = fac[i];
+        const double2* t = tw + tw_off[i];
         switch (r) {
-            case 2: fft_pass<2, SIGN>(a, b, M, ns, tw); break;
-            case 3: fft_pass<3, SIGN>(a, b, M, ns, tw); break;
-            case 4: fft_pass<4, SIGN>(a, b, M, ns, tw); break;
-            case 5: fft_pass<5, SIGN>(a, b, M, ns, tw); break;
-            case 7: fft_pass<7, SIGN>(a, b, M, ns, tw); break;
-            case 11: fft_pass<11, SIGN>(a, b, M, ns, tw); break;
-            case 13: fft_pass<13, SIGN>(a, b, M, ns, tw); break;
+            case 2: fft_pass<2, SIGN>(a, b, M, ns, t); break;
+            case 3: fft_pass<3, SIGN>(a, b, M, ns, t); break;
+            case 4: fft_pass<4, SIGN>(a, b, M, ns, t); break;
+            case 5: fft_pass<5, SIGN>(a, b, M, ns, t); break;
+            case 7: fft_pass<7, SIGN>(a, b, M, ns, t); break;
+            case 11: fft_pass<11, SIGN>(a, b, M, ns, t); break;
+            case 13: fft_pass<13, SIGN>(a, b, M, ns, t); break;
             default: break;
         }
         ns *= r;
-        double2* t = a;
+        double2* sw = a;
         a = b;
-        b = t;
+        b = sw;
     }
     __syncthreads();
     return a;
@@ -167,6 +169,7 @@ __device__ double2* fft_run(double2* a, double2* b, int M, const int* fac,
 struct FftArgs {
     int n, mode, m, nfac, bluestein, mb;
     int fac[kMaxFactors];
+    int tw_off[kMaxFactors];
     const double2* tw;
     const double2* twn;
     const double2* chirp;
@@ -178,7 +181,7 @@ struct FftArgs {
 template <int SIGN>
 __device__ double2* fft_exec(const FftArgs& F, double2* buf, double2* tmp) {
     __syncthreads();
-    if (!F.bluestein) return fft_run<SIGN>(buf, tmp, F.m, F.fac, F.nfac, F.tw);
+    if (!F.bluestein) return fft_run<SIGN>(buf, tmp, F.m, F.fac, F.nfac, F.tw, F.tw_off);
     // Bluestein: X_k = c_k sum_j (x_j c_j) conj(c_{k-j}), c_t = exp(-+ i pi t^2/m)
     const int m = F.m, mb = F.mb;
     for (int t = threadIdx.x; t < mb; t += blockDim.x) {
@@ -190,7 +193,7 @@ __device__ double2* fft_exec(const FftArgs& F, double2* buf, double2* tmp) {
             buf[t] = make_double2(0.0, 0.0);
         }
     }
-    double2* r = fft_run<-1>(buf, tmp, mb, F.fac, F.nfac, F.tw);
+    double2* r = fft_run<-1>(buf, tmp, mb, F.fac, F.nfac, F.tw, F.tw_off);
     double2* o = (r == buf) ? tmp : buf;
     for (int t = threadIdx.x; t < mb; t += blockDim.x) {
         double2 kf;
@@ -202,7 +205,7 @@ __device__ double2* fft_exec(const FftArgs& F, double2* buf, double2* tmp) {
         }
         r[t] = cmul(r[t], kf);
     }
-    double2* r2 = fft_run<+1>(r, o, mb, F.fac, F.nfac, F.tw);
+    double2* r2 = fft_run<+1>(r, o, mb, F.fac, F.nfac, F.tw, F.tw_off);
     const double inv = 1.0 / (double)mb;
     for (int t = threadIdx.x; t < m; t += blockDim.x) {
         double2 c = F.chirp[t];
@@ -237,6 +240,7 @@ __device__ __forceinline__ void fft_c2r_body(
         const double2* X = spec + ((long long)f * npair + p) * (lc + 1) * 2;
         for (int k = threadIdx.x; k < n; k += blockDim.x) a[k] = make_double2(0.0, 0.0);
         __syncthreads();
+#pragma unroll 4
         for (int k = threadIdx.x; k <= lc; k += blockDim.x) {
             double2 xn = X[2 * k + 0];
             double2 xs = rS >= 0 ? X[2 * k + 1] : make_double2(0.0, 0.0);
@@ -253,6 +257,7 @@ __device__ __forceinline__ void fft_c2r_body(
         const double sS = wS ? wS[p] * wscale : 1.0;
         GT* gN = rN >= 0 ? grid + f * gf + rN * grs : nullptr;
         GT* gS = rS >= 0 ? grid + f * gf + rS * grs : nullptr;
+#pragma unroll 4
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
             const double2 v = r[j];
             if (gN) gN[j * gcs] = (GT)(v.x * sN);
@@ -270,6 +275,7 @@ __device__ __forceinline__ void fft_c2r_body(
         const int M = F.m;   // n/2
         const double2* X = spec + ((long long)f * npair + p) * (lc + 1) * 2 + h;
         // Z'_k = (X_k + conj X_{M-k}) + i w^{-k} (X_k - conj X_{M-k}), w = exp(-2 pi i/n)
+#pragma unroll 4
         for (int k = threadIdx.x; k < M; k += blockDim.x) {
             double2 xk = k <= lc ? X[2 * k] : make_double2(0.0, 0.0);
             if (k == 0) xk.y = 0.0;
@@ -286,6 +292,7 @@ __device__ __forceinline__ void fft_c2r_body(
         const double2* r = fft_exec<+1>(F, a, b);
         const double sc = (h ? (wS ? wS[p] * wscale : 1.0) : (wN ? wN[p] * wscale : 1.0));
         GT* g = grid + f * gf + row * grs;
+#pragma unroll 4
         for (int j = threadIdx.x; j < M; j += blockDim.x) {
             const double2 v = r[j];
             g[(2LL * j) * gcs] = (GT)(v.x * sc);
@@ -315,6 +322,7 @@ __device__ __forceinline__ void fft_r2c_body(
         const int rN = rowN[p], rS = rowS[p];
         const GT* gN = rN >= 0 ? grid + f * gf + rN * grs : nullptr;
         const GT* gS = rS >= 0 ? grid + f * gf + rS * grs : nullptr;
+#pragma unroll 4
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
             double xn = gN ? (double)gN[j * gcs] : 0.0;
             double xs = gS ? (double)gS[j * gcs] : 0.0;
@@ -328,6 +336,7 @@ __device__ __forceinline__ void fft_r2c_body(
         const double sN = wN ? wN[p] * wscale : wscale;
         const double sS = wS ? wS[p] * wscale : wscale;
         double2* X = spec + ((long long)f * npair + p) * (lc + 1) * 2;
+#pragma unroll 4
         for (int k = threadIdx.x; k <= lc; k += blockDim.x) {
             const double2 zk = r[k];
             const double2 zm = r[k == 0 ? 0 : n - k];
@@ -348,6 +357,7 @@ __device__ __forceinline__ void fft_r2c_body(
         }
         const int M = F.m;
         const GT* g = grid + f * gf + row * grs;
+#pragma unroll 4
         for (int j = threadIdx.x; j < M; j += blockDim.x) {
             double x0 = (double)g[(2LL * j) * gcs];
             const double x1 = (double)g[(2LL * j + 1) * gcs];
@@ -356,6 +366,7 @@ __device__ __forceinline__ void fft_r2c_body(
         }
         const double2* r = fft_exec<-1>(F, a, b);
         const double sc = h ? (wS ? wS[p] * wscale : wscale) : (wN ? wN[p] * wscale : wscale);
+#pragma unroll 4
         for (int k = threadIdx.x; k <= lc; k += blockDim.x) {
             const double2 zk = r[k == M ? 0 : k];
             const double2 zm = r[k == 0 ? 0 : M - k];

@@ -191,7 +191,10 @@ FftArgs fft_args(const FftPlan& f) {
     FftArgs a;
     a.n = f.n; a.mode = f.mode; a.m = f.m; a.nfac = f.nfac;
     a.bluestein = f.bluestein; a.mb = f.mb;
-    for (int i = 0; i < kMaxFactors; ++i) a.fac[i] = i < f.nfac ? f.fac[i] : 0;
+    for (int i = 0; i < kMaxFactors; ++i) {
+        a.fac[i] = i < f.nfac ? f.fac[i] : 0;
+        a.tw_off[i] = i < f.nfac ? f.tw_off[i] : 0;
+    }
     a.tw = f.d_tw; a.twn = f.d_twn; a.chirp = f.d_chirp; a.kern = f.d_kern;
     return a;
 }
@@ -227,7 +230,12 @@ static void launch_synth_t(const shtc_plan* P, const double2* packed,
 int launch_legendre_synth(const shtc_plan* P, const double2* packed,
                           double2* spec, int nfield, cudaStream_t st) {
     const int np = P->npair;
-    if (nfield % 4 == 0 && nfield >= 8) {
+    if (nfield % 8 == 0) {
+        // one recursion per 8 fields; T = 1 keeps the 8 x 4 accumulators in
+        // registers
+        if (np > 512) launch_synth_t<2, 8>(P, packed, spec, nfield, st);
+        else launch_synth_t<1, 8>(P, packed, spec, nfield, st);
+    } else if (nfield % 4 == 0) {
         launch_synth_t<2, 4>(P, packed, spec, nfield, st);
     } else if (nfield % 2 == 0 && nfield >= 2) {
         if (np > 512) launch_synth_t<4, 2>(P, packed, spec, nfield, st);

@@ -208,13 +208,27 @@ static int factor_len(int n, int* fac) {
     return k;
 }
 
-static void roots_table(int len, std::vector<double2>& out) {
-    out.resize(len);
+// Twiddles of every Stockham pass, pass after pass: for the pass of radix R
+// applied after sub-transforms of size ns, entry (q-1)*ns + k holds
+// exp(-2 pi i k q / (ns R)), so that threads of consecutive k read
+// consecutive entries.
+static void pass_twiddles(int len, const int* fac, int nfac, std::vector<double2>& out,
+                          int* off) {
+    out.clear();
     const long double tp = 2.0L * 3.141592653589793238462643383279502884L;
-    for (int t = 0; t < len; ++t) {
-        const long double a = tp * (long double)t / (long double)len;
-        out[t] = make_double2((double)cosl(a), (double)(-sinl(a)));
+    int ns = 1;
+    for (int i = 0; i < nfac; ++i) {
+        const int R = fac[i];
+        off[i] = (int)out.size();
+        for (int q = 1; q < R; ++q)
+            for (int k = 0; k < ns; ++k) {
+                const long long t = ((long long)k * q) % ((long long)ns * R);
+                const long double a = tp * (long double)t / (long double)(ns * R);
+                out.push_back(make_double2((double)cosl(a), (double)(-sinl(a))));
+            }
+        ns *= R;
     }
+    (void)len;
 }
 
 int build_fft_plan(FftPlan* f, int n, cudaStream_t st) {
@@ -231,7 +245,6 @@ int build_fft_plan(FftPlan* f, int n, cudaStream_t st) {
         while (mb < 2 * f->m - 1) mb <<= 1;
         f->mb = mb;
         nf = factor_len(mb, fac);
-        roots_table(mb, tw);
         chirp.resize(f->m);
         const long double pi = 3.141592653589793238462643383279502884L;
         for (long long t = 0; t < f->m; ++t) {
@@ -263,10 +276,9 @@ int build_fft_plan(FftPlan* f, int n, cudaStream_t st) {
             }
             kern[k] = make_double2((double)sr, (double)si);
         }
-    } else {
-        roots_table(f->m, tw);
     }
     if (nf > kMaxFactors) return SHTC_EUNSUP;
+    pass_twiddles(f->bluestein ? f->mb : f->m, fac, nf, tw, f->tw_off);
     f->nfac = nf;
     for (int i = 0; i < nf; ++i) f->fac[i] = fac[i];
     if (f->mode == 1) {

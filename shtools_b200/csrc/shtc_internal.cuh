@@ -36,7 +36,9 @@ struct FftPlan {
     int fac[kMaxFactors];
     int bluestein;     // 1 if m has a prime factor > kMaxRadix
     int mb;            // Bluestein convolution length (power of two)
-    double2* d_tw;     // exp(-2 pi i t / len), t < len; len = mb if bluestein else m
+    double2* d_tw;     // per-pass twiddles: pass i at tw_off[i], entry (q-1)*ns+k
+                       // = exp(-2 pi i k q / (ns R)), of the length-(mb or m) FFT
+    int tw_off[kMaxFactors];
     double2* d_twn;    // mode 1: exp(-2 pi i k / n), k < n/2
     double2* d_chirp;  // Bluestein: exp(-i pi t^2 / m), t < m
     double2* d_kern;   // Bluestein: FFT_mb of the conjugate chirp kernel
