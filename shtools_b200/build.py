@@ -42,7 +42,7 @@ def deps():
 
 def flags(extra=()):
     return ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC",
-            "-Xcompiler", "-O2", "-Xcompiler", "-fvisibility=hidden", "--shared", "-DSHTC_EXACT_RECURSION=1",
+            "-Xcompiler", "-O2", "-Xcompiler", "-fvisibility=hidden", "--shared",
             "-I" + os.path.join(ROOT, "include"), *extra]
 
 

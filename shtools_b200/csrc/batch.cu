@@ -51,7 +51,8 @@ constexpr int kBatchAnalWarps = 4;
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
-// pack: item (g, m); coefficients (nf, 2, D, D) -> packed [(l,m)][nf] {C, S}
+// pack: item (g, m); coefficients (nf, 2, D, D) -> packed [(l,m)][nf] {C, S},
+// premultiplied by D(l - m) of the rescaled recursion
 __global__ void k_batch_pack(const BatchGroup* __restrict__ G,
                              const int2* __restrict__ items,
                              const double* __restrict__ cilm,
@@ -63,11 +64,13 @@ __global__ void k_batch_pack(const BatchGroup* __restrict__ G,
     const double* c = cilm + g.cilm_off;
     double2* pk = work + g.pack_off;
     for (int l = m + threadIdx.x; l <= lc; l += blockDim.x) {
+        // D(l - m) of the rescaled recursion (legendre.cuh)
+        const double d = g.rec[o + (l - m)].y;
         for (int f = 0; f < nf; ++f) {
             const double* b = c + (long long)f * 2 * D * D + (long long)l * D + m;
             const double cs = b[0];
             const double sn = m == 0 ? 0.0 : b[(long long)D * D];
-            pk[(o + (l - m)) * nf + f] = make_double2(cs, sn);
+            pk[(o + (l - m)) * nf + f] = make_double2(cs * d, sn * d);
         }
     }
 }
@@ -147,10 +150,10 @@ k_batch_anal(const BatchGroup* __restrict__ G, const int4* __restrict__ items,
         const int4 w = items[i];
         const BatchGroup& g = G[w.x];
         const int f = w.w;
-        anal_order<1>(smem_anal, rstage, g.rec, g.pmm, g.rtab, g.z,
-                      work + g.spec_off + (long long)f * g.npair * (g.lc + 1) * 2,
-                      work + g.pack_off + ((long long)w.z * g.nf + f) * g.nlm, g.lc,
-                      g.npair, w.y, w.z);
+        anal_order<1, 1>(smem_anal, rstage, g.rec, g.pmm, g.rtab, g.z,
+                         work + g.spec_off + (long long)f * g.npair * (g.lc + 1) * 2, 0,
+                         work + g.pack_off + ((long long)w.z * g.nf + f) * g.nlm, 0, g.lc,
+                         g.npair, w.y, w.z, 1);
     }
 }
 
@@ -324,7 +327,7 @@ extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
         cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, B->device);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_synth, kBatchThreads, 0);
         B->synth_ctas = sm * std::max(1, per);
-        const size_t asmem = anal_smem_bytes(kBatchAnalWarps);
+        const size_t asmem = anal_smem_bytes(kBatchAnalWarps, 1);
         cudaFuncSetAttribute(k_batch_anal, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)asmem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_anal,
@@ -417,7 +420,7 @@ extern "C" SHTC_API int shtc_batch_analysis(const shtc_batch* B, const double* g
     if ((rc = map_cuda(cudaGetLastError()))) return rc;
     if ((rc = map_cuda(cudaMemsetAsync(B->d_counter, 0, sizeof(int), st)))) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
-    k_batch_anal<<<B->anal_ctas, 32 * kBatchAnalWarps, anal_smem_bytes(kBatchAnalWarps),
+    k_batch_anal<<<B->anal_ctas, 32 * kBatchAnalWarps, anal_smem_bytes(kBatchAnalWarps, 1),
                    st>>>(B->d_groups, B->d_aitems, B->naitems, B->d_counter, w);
     stage_end(SHTC_STAGE_LEGENDRE_ANAL, st);
     if ((rc = map_cuda(cudaGetLastError()))) return rc;

@@ -45,29 +45,49 @@ __device__ __forceinline__ double anal_norm_factor(int norm, int l,
     }
 }
 
+// (l, m) tiles of kCoefTile x kCoefTile staged in shared memory: the
+// coefficient arrays (C order, contiguous along m) and the packed arrays
+// (contiguous along l for one m) are then both accessed along their fast
+// dimension.
+constexpr int kCoefTile = 32;
+constexpr int kCoefRows = 8;   // blockDim = (kCoefTile, kCoefRows)
+
 template <typename CT>
-__global__ void k_pack_coef(const CT* __restrict__ cilm, long long sf,
-                            long long sk, long long sl, long long sm, int cdim,
-                            double2* __restrict__ packed, int lc, int nfield,
-                            int norm, const double* __restrict__ nrm3,
-                            int scale_mode) {
-    const int m = blockIdx.y;
-    const int l = m + blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kCoefTile * kCoefRows)
+k_pack_coef(const CT* __restrict__ cilm, long long sf, long long sk, long long sl,
+            long long sm, int cdim, double2* __restrict__ packed, int lc, int nfield,
+            int norm, const double* __restrict__ nrm3, int scale_mode,
+            const double2* __restrict__ rec) {
+    __shared__ double2 tile[kCoefTile][kCoefTile + 1];   // [m - m0][l - l0]
+    const int l0 = blockIdx.x * kCoefTile, m0 = blockIdx.y * kCoefTile;
     const int f = blockIdx.z;
-    if (l > lc) return;
-    const long long idx = packed_off(m, lc) + (l - m);
-    double c = 0.0, s = 0.0;
-    if (l < cdim) {
-        const CT* b = cilm + f * sf + l * sl + m * sm;
-        c = (double)b[0];
-        s = (m == 0) ? 0.0 : (double)b[sk];
+    if (m0 > l0 + kCoefTile - 1) return;   // tile above the diagonal (uniform)
+    const int tx = threadIdx.x;
+    for (int j = threadIdx.y; j < kCoefTile; j += kCoefRows) {
+        const int l = l0 + j, m = m0 + tx;
+        double c = 0.0, s = 0.0;
+        if (m <= l && l <= lc && l < cdim) {
+            const CT* b = cilm + f * sf + l * sl + m * sm;
+            c = (double)b[0];
+            s = (m == 0) ? 0.0 : (double)b[sk];
+        }
+        tile[tx][j] = make_double2(c, s);
     }
-    if (scale_mode == 1) {
-        const double a = anal_norm_factor(norm, l, nrm3, idx);
-        c *= a;
-        s *= a;
+    __syncthreads();
+    for (int j = threadIdx.y; j < kCoefTile; j += kCoefRows) {
+        const int m = m0 + j, l = l0 + tx;
+        if (m > l || l > lc) continue;
+        const long long idx = packed_off(m, lc) + (l - m);
+        double2 v = tile[j][tx];
+        if (scale_mode == 1) {
+            const double a = anal_norm_factor(norm, l, nrm3, idx);
+            v.x *= a;
+            v.y *= a;
+        }
+        // D(l - m) of the rescaled recursion (legendre.cuh)
+        const double d = rec[idx].y;
+        packed[idx * nfield + f] = make_double2(v.x * d, v.y * d);
     }
-    packed[idx * nfield + f] = make_double2(c, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -92,7 +112,7 @@ k_legendre_synth(const double2* __restrict__ rec, const double* __restrict__ pmm
                        blockIdx.y, blockIdx.x, blockIdx.z * NF, NF);
 }
 
-template <int T>
+template <int T, int NF>
 __global__ void __launch_bounds__(256)
 k_legendre_anal(const double2* __restrict__ rec, const double* __restrict__ pmm,
                 const double* __restrict__ rtab, const double* __restrict__ zp,
@@ -100,11 +120,11 @@ k_legendre_anal(const double2* __restrict__ rec, const double* __restrict__ pmm,
                 int lc, int npair, long long nlm, int nfield) {
     extern __shared__ double smem_anal[];
     __shared__ __align__(16) double2 rstage[2][kAnalChunk];
-    const int f = blockIdx.z;
-    anal_order<T>(smem_anal, rstage, rec, pmm, rtab, zp,
-                  spec + (long long)f * npair * (lc + 1) * 2,
-                  partial + ((long long)blockIdx.x * nfield + f) * nlm, lc, npair,
-                  blockIdx.y, blockIdx.x);
+    const int f0 = blockIdx.z * NF;
+    const long long sstride = (long long)npair * (lc + 1) * 2;
+    anal_order<T, NF>(smem_anal, rstage, rec, pmm, rtab, zp, spec + f0 * sstride, sstride,
+                      partial + ((long long)blockIdx.x * nfield + f0) * nlm, nlm, lc, npair,
+                      blockIdx.y, blockIdx.x, min(NF, nfield - f0));
 }
 
 // ---------------------------------------------------------------------------
@@ -113,47 +133,57 @@ k_legendre_anal(const double2* __restrict__ rec, const double* __restrict__ pmm,
 // normalise 1: divide by the integral of Ylm^2 exactly as the reference
 // (SHExpandDH.f95:674-702); 0: no normalisation (synthesis adjoint).
 template <typename CT>
-__global__ void k_unpack_coef(const double2* __restrict__ partial, int ntiles,
-                              CT* __restrict__ cilm, long long sf,
-                              long long sk, long long sl, long long sm, int cdim,
-                              int lc, long long nlm, int nfield, int norm,
-                              const double* __restrict__ nrm3, int normalise) {
+__global__ void __launch_bounds__(kCoefTile * kCoefRows)
+k_unpack_coef(const double2* __restrict__ partial, int ntiles, CT* __restrict__ cilm,
+              long long sf, long long sk, long long sl, long long sm, int cdim, int lc,
+              long long nlm, int nfield, int norm, const double* __restrict__ nrm3,
+              int normalise) {
     const double pi = 3.141592653589793238462643383279502884;
-    const int m = blockIdx.y;
-    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ double2 tile[kCoefTile][kCoefTile + 1];   // [m - m0][l - l0]
+    const int l0 = blockIdx.x * kCoefTile, m0 = blockIdx.y * kCoefTile;
     const int f = blockIdx.z;
-    if (l >= cdim) return;
-    double c = 0.0, s = 0.0;
-    if (m <= l && l <= lc) {
-        const long long idx = packed_off(m, lc) + (l - m);
-        for (int t = 0; t < ntiles; ++t) {
-            const double2 v = partial[((long long)t * nfield + f) * nlm + idx];
-            c += v.x;
-            s += v.y;
-        }
-        if (normalise) {
-            switch (norm) {
-                case 1:
-                    c = c / (4 * pi);
-                    s = s / (4 * pi);
-                    break;
-                case 2:
-                    c = c * (2 * l + 1) / (4 * pi);
-                    s = s * (2 * l + 1) / (4 * pi);
-                    break;
-                case 3:
-                    c = c / nrm3[idx];
-                    s = s / nrm3[idx];
-                    break;
-                default:
-                    break;
+    const int tx = threadIdx.x;
+    for (int j = threadIdx.y; j < kCoefTile; j += kCoefRows) {
+        const int m = m0 + j, l = l0 + tx;
+        double c = 0.0, s = 0.0;
+        if (m <= l && l <= lc && l < cdim) {
+            const long long idx = packed_off(m, lc) + (l - m);
+            for (int t = 0; t < ntiles; ++t) {
+                const double2 v = partial[((long long)t * nfield + f) * nlm + idx];
+                c += v.x;
+                s += v.y;
             }
+            if (normalise) {
+                switch (norm) {
+                    case 1:
+                        c = c / (4 * pi);
+                        s = s / (4 * pi);
+                        break;
+                    case 2:
+                        c = c * (2 * l + 1) / (4 * pi);
+                        s = s * (2 * l + 1) / (4 * pi);
+                        break;
+                    case 3:
+                        c = c / nrm3[idx];
+                        s = s / nrm3[idx];
+                        break;
+                    default:
+                        break;
+                }
+            }
+            if (m == 0) s = 0.0;
         }
-        if (m == 0) s = 0.0;
+        tile[j][tx] = make_double2(c, s);
     }
-    CT* b = cilm + f * sf + l * sl + m * sm;
-    b[0] = (CT)c;
-    b[sk] = (CT)s;
+    __syncthreads();
+    for (int j = threadIdx.y; j < kCoefTile; j += kCoefRows) {
+        const int l = l0 + j, m = m0 + tx;
+        if (l >= cdim || m >= cdim) continue;
+        const double2 v = tile[tx][j];
+        CT* b = cilm + f * sf + l * sl + m * sm;
+        b[0] = (CT)v.x;
+        b[sk] = (CT)v.y;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -204,15 +234,16 @@ int launch_pack_coef(const shtc_plan* P, const void* cilm, int dtype, long long 
                      double2* packed, int nfield, int scale_mode,
                      cudaStream_t st) {
     const int lc = P->lc;
-    dim3 grid((lc + 1 + 127) / 128, lc + 1, nfield);
+    const int nt = (lc + kCoefTile) / kCoefTile;
+    const dim3 grid(nt, nt, nfield), block(kCoefTile, kCoefRows);
     if (dtype == SHTC_F32)
-        k_pack_coef<float><<<grid, 128, 0, st>>>((const float*)cilm, sf, sk, sl, sm, cdim,
+        k_pack_coef<float><<<grid, block, 0, st>>>((const float*)cilm, sf, sk, sl, sm, cdim,
                                                  packed, lc, nfield, P->norm, P->d_nrm,
-                                                 scale_mode);
+                                                 scale_mode, P->d_rec);
     else
-        k_pack_coef<double><<<grid, 128, 0, st>>>((const double*)cilm, sf, sk, sl, sm, cdim,
+        k_pack_coef<double><<<grid, block, 0, st>>>((const double*)cilm, sf, sk, sl, sm, cdim,
                                                   packed, lc, nfield, P->norm, P->d_nrm,
-                                                  scale_mode);
+                                                  scale_mode, P->d_rec);
     return map_cuda(cudaGetLastError());
 }
 
@@ -276,21 +307,36 @@ int anal_tiles(const shtc_plan* P) {
     return tiles;
 }
 
-template <int T>
+template <int T, int NF>
 static int launch_anal_t(const shtc_plan* P, const double2* spec,
                          double2* partial, int nfield, int W, int tiles,
                          cudaStream_t st) {
     const int threads = 32 * W;
-    const size_t smem = anal_smem_bytes(W);
-    cudaError_t e = cudaFuncSetAttribute(k_legendre_anal<T>,
+    const size_t smem = anal_smem_bytes(W, NF);
+    cudaError_t e = cudaFuncSetAttribute(k_legendre_anal<T, NF>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return map_cuda(e);
-    dim3 grid(tiles, P->lc + 1, nfield);
-    k_legendre_anal<T><<<grid, threads, smem, st>>>(
+    dim3 grid(tiles, P->lc + 1, (nfield + NF - 1) / NF);
+    k_legendre_anal<T, NF><<<grid, threads, smem, st>>>(
         P->d_rec, P->d_pmm, P->d_rtab, P->d_z, spec, partial, P->lc, P->npair,
         P->nlm, nfield);
     return map_cuda(cudaGetLastError());
+}
+
+// Fields share the recursion in groups of NF.  The group's G values take
+// 4*T*NF registers, so NF is chosen to keep T*NF <= 8 (about 128 registers):
+// NF = 4 for T <= 2, 2 for T = 4, 1 for T = 8.
+template <int T>
+static int launch_anal_nf(const shtc_plan* P, const double2* spec, double2* partial,
+                          int nfield, int W, int tiles, cudaStream_t st) {
+    if constexpr (T <= 2) {
+        if (nfield % 4 == 0) return launch_anal_t<T, 4>(P, spec, partial, nfield, W, tiles, st);
+    }
+    if constexpr (T <= 4) {
+        if (nfield % 2 == 0) return launch_anal_t<T, 2>(P, spec, partial, nfield, W, tiles, st);
+    }
+    return launch_anal_t<T, 1>(P, spec, partial, nfield, W, tiles, st);
 }
 
 int launch_legendre_anal(const shtc_plan* P, const double2* spec,
@@ -300,10 +346,10 @@ int launch_legendre_anal(const shtc_plan* P, const double2* spec,
     anal_shape(P, &T, &W, &tiles);
     if (tiles != ntiles_out) return SHTC_EBOUND;
     switch (T) {
-        case 8: return launch_anal_t<8>(P, spec, partial, nfield, W, tiles, st);
-        case 4: return launch_anal_t<4>(P, spec, partial, nfield, W, tiles, st);
-        case 2: return launch_anal_t<2>(P, spec, partial, nfield, W, tiles, st);
-        default: return launch_anal_t<1>(P, spec, partial, nfield, W, tiles, st);
+        case 8: return launch_anal_nf<8>(P, spec, partial, nfield, W, tiles, st);
+        case 4: return launch_anal_nf<4>(P, spec, partial, nfield, W, tiles, st);
+        case 2: return launch_anal_nf<2>(P, spec, partial, nfield, W, tiles, st);
+        default: return launch_anal_nf<1>(P, spec, partial, nfield, W, tiles, st);
     }
 }
 
@@ -312,13 +358,14 @@ int launch_unpack_coef(const shtc_plan* P, const double2* partial, int ntiles,
                        long long sm, int cdim, int nfield, int normalise,
                        cudaStream_t st) {
     const int lc = P->lc;
-    dim3 grid((cdim + 127) / 128, cdim, nfield);
+    const int nt = (cdim + kCoefTile - 1) / kCoefTile;
+    const dim3 grid(nt, nt, nfield), block(kCoefTile, kCoefRows);
     if (dtype == SHTC_F32)
-        k_unpack_coef<float><<<grid, 128, 0, st>>>(partial, ntiles, (float*)cilm, sf, sk,
+        k_unpack_coef<float><<<grid, block, 0, st>>>(partial, ntiles, (float*)cilm, sf, sk,
                                                    sl, sm, cdim, lc, P->nlm, nfield,
                                                    P->norm, P->d_nrm, normalise);
     else
-        k_unpack_coef<double><<<grid, 128, 0, st>>>(partial, ntiles, (double*)cilm, sf, sk,
+        k_unpack_coef<double><<<grid, block, 0, st>>>(partial, ntiles, (double*)cilm, sf, sk,
                                                     sl, sm, cdim, lc, P->nlm, nfield,
                                                     P->norm, P->d_nrm, normalise);
     return map_cuda(cudaGetLastError());

@@ -6,6 +6,21 @@
 // the three-term recursion
 //     P(l) = z*ff1(l,m)*P(l-1) - ff2(l,m)*P(l-2)
 // runs on the scaled values, and the sums are multiplied by u^m * 1e280.
+//
+// The recursion is run in a rescaled form with two FP64 operations per
+// degree instead of four.  With s = l - m, a(s) = ff1, b(s) = ff2 and
+// segments of kRecSegment degrees (s0, s0 + kRecSegment], s0 a multiple of
+// kRecSegment,
+//     P(s) = D(s) * Q(s),   D(s) = a(s0+1) * ... * a(s),
+//     Q(s) = z * Q(s-1) - beta(s) * Q(s-2),   beta(s) = b(s) / (a(s) a(s-1)),
+// which is the same recursion (D(s-2)/D(s) = 1/(a(s) a(s-1)) across a
+// segment start too, once both recursion values are multiplied by the
+// segment's last D when it ends).  The table rec[] holds {beta(s), D(s)};
+// synthesis coefficients are premultiplied by D(s) when packed and analysis
+// sums are multiplied by D(s) when reduced.  Every a(s) >= 1, so Q <= P in
+// magnitude; D stays below ~1e24 for lmax <= 2800 and the Q values stay in
+// the normal double range.
+//
 // One work item is one order m for one tile of ring pairs (and one group of
 // fields); each thread owns T ring pairs, and the per-degree data of the
 // order is read once per item into shared memory and broadcast to all rings.
@@ -17,16 +32,21 @@
 
 namespace shtc {
 
-// P(l) = (z*ff1)*P(l-1) - ff2*P(l-2), rounded as the reference's
-// non-fused expression when SHTC_EXACT_RECURSION is set (4 ops), otherwise
-// with one fused multiply-add (3 ops).
+// one step of the rescaled recursion: Q(s) = z*Q(s-1) - beta(s)*Q(s-2),
+// f = {beta(s), D(s)}
 __device__ __forceinline__ double rec_step(double z, double2 f, double q1,
                                            double q2) {
-#if SHTC_EXACT_RECURSION
-    return __dsub_rn(__dmul_rn(__dmul_rn(z, f.x), q1), __dmul_rn(f.y, q2));
-#else
-    return fma(z * f.x, q1, -(f.y * q2));
-#endif
+    return fma(z, q1, -(f.x * q2));
+}
+
+// end of a recursion segment: both recursion values back to P units
+template <int T>
+__device__ __forceinline__ void rec_rescale(double d, double* q1, double* q2) {
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+        q1[t] *= d;
+        q2[t] *= d;
+    }
 }
 
 // 16-byte asynchronous global -> shared copies (sm_80+ cp.async), used to
@@ -73,6 +93,7 @@ __device__ __forceinline__ void synth_step(bool odd, double2 f, const double2* c
 // chunks of kSynthChunk degrees are copied into shared memory with cp.async
 // one chunk ahead of their use.
 constexpr int kSynthChunk = 32;
+static_assert(kSynthChunk % kRecSegment == 0, "chunks hold whole segments");
 
 template <int NF>
 struct SynthStage {
@@ -149,15 +170,22 @@ __device__ __forceinline__ void synth_order(
         const double2* st = sm.buf[c & 1];
         const int cn = min(kSynthChunk, nsteps - c * kSynthChunk);
         // s = 1 + c*kSynthChunk + k: odd for even k (the chunk length is even)
+        // segments end at s = 32c + 16 and 32c + 32, i.e. k = 15 and 31
         if (cn == kSynthChunk) {
 #pragma unroll
-            for (int k = 0; k < kSynthChunk; ++k)
+            for (int k = 0; k < kSynthChunk; ++k) {
                 synth_step<T, NF>((k & 1) == 0, st[k * R], &st[k * R + 1], z, q1, q2,
                                   eR, eI, oR, oI);
+                if ((k & (kRecSegment - 1)) == kRecSegment - 1)
+                    rec_rescale<T>(st[k * R].y, q1, q2);
+            }
         } else {
-            for (int k = 0; k < cn; ++k)
+            for (int k = 0; k < cn; ++k) {
                 synth_step<T, NF>((k & 1) == 0, st[k * R], &st[k * R + 1], z, q1, q2,
                                   eR, eI, oR, oI);
+                if ((k & (kRecSegment - 1)) == kRecSegment - 1)
+                    rec_rescale<T>(st[k * R].y, q1, q2);
+            }
         }
         __syncthreads();
     }
@@ -188,62 +216,83 @@ __device__ __forceinline__ void synth_order(
 // analysis
 // ---------------------------------------------------------------------------
 // Input spec[((f*npair + p)*(lc+1) + m)*2 + h] = weighted (Re, -Im) Fourier
-// coefficients of the rings (SHExpandDH.f95:470-479).  For each (l, m) the
-// sum over ring pairs of P_lm(z_p) * (F_north +- F_south) * u^m/scalef is
-// reduced across the CTA: each lane sums its T pairs, a shared-memory
-// transpose sums the 32 lanes of a warp for 16 consecutive degrees at a time,
-// and warp 0 adds the warps in a fixed order (deterministic).  With more than
-// one tile per order the per-tile sums go to partial[tile][...] and the
-// unpack kernel adds them, again in a fixed order.
-constexpr int kAnalChunk = 16;
+// coefficients of the rings (SHExpandDH.f95:470-479).  For each (l, m) and
+// field the sum over ring pairs of P_lm(z_p) * (F_north +- F_south) *
+// u^m/scalef is reduced across the CTA: each lane sums its T pairs, a
+// shared-memory transpose sums the 32 lanes of a warp for a chunk of
+// degrees at a time, and warp 0 adds the warps in a fixed order
+// (deterministic).  With more than one tile per order the per-tile sums go
+// to partial[tile][field][...] and the unpack kernel adds them, again in a
+// fixed order.  NF fields share one recursion: per degree a lane does 2T
+// recursion operations and 2*T*NF multiply-adds.
+constexpr int kAnalChunk = 16;   // degrees per stage of staged {beta, D}
 constexpr int kAnalPad = 33;
+static_assert(kAnalChunk == kRecSegment, "segment ends fall on stage starts");
 
-// dynamic shared memory of an analysis CTA of W warps
-__host__ __device__ inline size_t anal_smem_bytes(int W) {
-    return (size_t)W * (2 * kAnalChunk * kAnalPad) * sizeof(double) +
-           (size_t)2 * W * 32 * sizeof(double);
+// degrees per transpose chunk for NF fields: 2*NF*CH = 32 rows, one per lane
+__host__ __device__ constexpr int anal_chunk(int NF) { return kAnalChunk / NF; }
+
+// dynamic shared memory of an analysis CTA of W warps for NF fields
+__host__ __device__ inline size_t anal_smem_bytes(int W, int NF) {
+    return (size_t)W * 32 * kAnalPad * sizeof(double) +             // per-warp transpose
+           (size_t)2 * W * (2 * NF * kAnalChunk) * sizeof(double);  // per-warp stage sums x2
 }
 
-// one degree step of the analysis for T ring pairs: the lane's sums over its
+// one degree step for T ring pairs and NF fields: the lane's sums over its
 // pairs of P * G, G the symmetric (even l-m) or antisymmetric (odd)
-// combination of the two rings
-template <int T>
+// combination of the two rings of each pair
+template <int T, int NF>
 __device__ __forceinline__ void anal_step(bool odd, double2 fr, const double* z,
                                           double* q1, double* q2,
-                                          const double* gsR, const double* gsI,
-                                          const double* gaR, const double* gaI,
-                                          double& accR, double& accI) {
-    accR = 0.0;
-    accI = 0.0;
+                                          const double (*gsR)[NF], const double (*gsI)[NF],
+                                          const double (*gaR)[NF], const double (*gaI)[NF],
+                                          double* accR, double* accI) {
+    double p[T];
 #pragma unroll
     for (int t = 0; t < T; ++t) {
-        const double p = rec_step(z[t], fr, q1[t], q2[t]);
+        p[t] = rec_step(z[t], fr, q1[t], q2[t]);
         q2[t] = q1[t];
-        q1[t] = p;
-        accR = fma(p, odd ? gaR[t] : gsR[t], accR);
-        accI = fma(p, odd ? gaI[t] : gsI[t], accI);
+        q1[t] = p[t];
+    }
+#pragma unroll
+    for (int j = 0; j < NF; ++j) {
+        double r = 0.0, i = 0.0;
+#pragma unroll
+        for (int t = 0; t < T; ++t) {
+            r = fma(p[t], odd ? gaR[t][j] : gsR[t][j], r);
+            i = fma(p[t], odd ? gaI[t][j] : gsI[t][j], i);
+        }
+        accR[j] = r;
+        accI[j] = i;
     }
 }
 
-// Analysis of order m for the ring pairs of tile `tile` of one field:
-//   sp:   the field's spec, [pair][m][ring]
-//   outp: the tile's packed {C, S} sums of the field, [packed (l, m)]
-// smem: anal_smem_bytes(W) bytes; rstage: 2 x kAnalChunk staged {ff1, ff2}.
+// Analysis of order m for the ring pairs of tile `tile` and the fields
+// f0 .. f0+nvalid-1 (nvalid <= NF):
+//   sp:   spec of field f0, [pair][m][ring]; field j at sp + j*sstride
+//   outp: the tile's packed {C, S} sums of field f0, [packed (l, m)];
+//         field j at outp + j*ostride
+// smem: anal_smem_bytes(W, NF) bytes; rstage: 2 x kAnalChunk staged
+// {beta, D}.  Degrees go in stages of kAnalChunk (one CTA barrier each),
+// each stage in NF transpose chunks of kAnalChunk/NF degrees (warp-local).
 // Ends with the tile's sums written by warp 0 after a barrier; the caller
 // must pass another barrier before reusing the shared memory.
-template <int T>
+template <int T, int NF>
 __device__ __forceinline__ void anal_order(
     double* smem, double2 (*rstage)[kAnalChunk], const double2* __restrict__ rec,
     const double* __restrict__ pmm, const double* __restrict__ rtab,
-    const double* __restrict__ zp, const double2* __restrict__ sp,
-    double2* __restrict__ outp, int lc, int npair, int m, int tile) {
+    const double* __restrict__ zp, const double2* __restrict__ sp, long long sstride,
+    double2* __restrict__ outp, long long ostride, int lc, int npair, int m, int tile,
+    int nvalid) {
+    constexpr int CH = anal_chunk(NF);
+    constexpr int SROWS = 2 * NF * kAnalChunk;   // (field, Re/Im, degree) rows per stage
+    static_assert(2 * NF * CH == 32, "one transpose row per lane");
     const int nwarps = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    double* bufRe = smem + warp * (2 * kAnalChunk * kAnalPad);
-    double* bufIm = bufRe + kAnalChunk * kAnalPad;
-    // two buffers of per-warp chunk sums, alternating between chunks
-    double* wsum = smem + nwarps * (2 * kAnalChunk * kAnalPad);   // [2][nwarps][32]
+    double* tb = smem + warp * (32 * kAnalPad);
+    // two buffers of per-warp stage sums, alternating between stages
+    double* wsum = smem + nwarps * (32 * kAnalPad);   // [2][nwarps][SROWS]
 
     const int p0 = tile * (blockDim.x * T) + threadIdx.x;
     double z[T];
@@ -256,107 +305,117 @@ __device__ __forceinline__ void anal_order(
     const long long o = packed_off(m, lc);
     const double2* __restrict__ rm = rec + o;
     const int nsteps = lc - m + 1;   // degrees l = m .. lc, s = l - m
-    const int nchunks = (nsteps + kAnalChunk - 1) / kAnalChunk;
-    auto load_chunk = [&](int c) {
+    const int nstages = (nsteps + kAnalChunk - 1) / kAnalChunk;
+    auto load_stage = [&](int c) {
         const int sidx = c * kAnalChunk + threadIdx.x;
         if (threadIdx.x < kAnalChunk && sidx < nsteps)
             cp_async16(&rstage[c & 1][threadIdx.x], &rm[sidx]);
         cp_async_commit();
     };
-    load_chunk(0);
+    load_stage(0);
+    if (nstages > 1) load_stage(1);
 
     const double start = pmm[m];
     // symmetric (l-m even) and antisymmetric (l-m odd) combinations
-    double gsR[T], gsI[T], gaR[T], gaI[T], q1[T], q2[T];
+    double gsR[T][NF], gsI[T][NF], gaR[T][NF], gaI[T][NF], q1[T], q2[T];
 #pragma unroll
     for (int t = 0; t < T; ++t) {
-        gsR[t] = gsI[t] = gaR[t] = gaI[t] = 0.0;
-        if (pv[t] < npair) {
-            const double r = rtab[(long long)m * npair + pv[t]];
-            if (r != 0.0) {
-                const double2 a = sp[((long long)pv[t] * (lc + 1) + m) * 2 + 0];
-                const double2 b = sp[((long long)pv[t] * (lc + 1) + m) * 2 + 1];
+        const double r = pv[t] < npair ? rtab[(long long)m * npair + pv[t]] : 0.0;
+#pragma unroll
+        for (int j = 0; j < NF; ++j) {
+            gsR[t][j] = gsI[t][j] = gaR[t][j] = gaI[t][j] = 0.0;
+            if (j < nvalid && r != 0.0) {
+                const double2* x = sp + j * sstride + ((long long)pv[t] * (lc + 1) + m) * 2;
+                const double2 a = x[0];
+                const double2 b = x[1];
                 const double aR = a.x * r, aI = a.y * r;
                 const double bR = b.x * r, bI = b.y * r;
-                gsR[t] = aR + bR; gsI[t] = aI + bI;
-                gaR[t] = aR - bR; gaI[t] = aI - bI;
+                gsR[t][j] = aR + bR; gsI[t][j] = aI + bI;
+                gaR[t][j] = aR - bR; gaI[t][j] = aI - bI;
             }
         }
-        q1[t] = start;
-        q2[t] = 0.0;
+        // the step s = 0 of the table (beta = -1) turns this into Q(0) = start
+        q1[t] = 0.0;
+        q2[t] = start;
     }
+    if (nstages > 1) cp_async_wait<1>(); else cp_async_wait<0>();
+    __syncthreads();
     int buf = 0;
-    for (int c = 0; c < nchunks; ++c) {
-        const int c0 = c * kAnalChunk;
-        const int cn = min(kAnalChunk, nsteps - c0);
-        if (c + 1 < nchunks) {
-            load_chunk(c + 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        __syncthreads();
-        const double2* wcoef = rstage[c & 1];
-        double accR, accI;
-        if (cn == kAnalChunk) {
-            // c0 is a multiple of the (even) chunk length: the parity of
-            // s = c0 + k is that of k, fixed by the unrolling
+    for (int sg = 0; sg < nstages; ++sg) {
+        const int s0 = sg * kAnalChunk;
+        const double2* stg = rstage[sg & 1];
+        double* ws = wsum + (buf * nwarps + warp) * SROWS;
+        // the stage starts at s0, a multiple of kRecSegment: the first step
+        // ends a recursion segment (D(0) = 1 for the first stage)
+#pragma unroll 1
+        for (int ci = 0; ci < NF; ++ci) {
+            const int c0 = s0 + ci * CH;
+            const int cn = min(CH, nsteps - c0);
+            if (cn <= 0) break;
+            const double2* wcoef = stg + ci * CH;
+            double accR[NF], accI[NF];
+            // parity of s = c0 + k is that of k (c0 even)
+            if (cn == CH) {
 #pragma unroll
-            for (int k = 0; k < kAnalChunk; ++k) {
-                if (k == 0 && c0 == 0) {
-                    accR = 0.0;
-                    accI = 0.0;
+                for (int k = 0; k < CH; ++k) {
+                    anal_step<T, NF>((k & 1) != 0, wcoef[k], z, q1, q2, gsR, gsI, gaR, gaI,
+                                     accR, accI);
+                    if (k == 0 && ci == 0) rec_rescale<T>(wcoef[0].y, q1, q2);
 #pragma unroll
-                    for (int t = 0; t < T; ++t) {
-                        accR = fma(q1[t], gsR[t], accR);
-                        accI = fma(q1[t], gsI[t], accI);
+                    for (int j = 0; j < NF; ++j) {
+                        tb[((2 * j + 0) * CH + k) * kAnalPad + lane] = accR[j];
+                        tb[((2 * j + 1) * CH + k) * kAnalPad + lane] = accI[j];
                     }
-                } else {
-                    anal_step<T>((k & 1) != 0, wcoef[k], z, q1, q2, gsR, gsI, gaR, gaI,
-                                 accR, accI);
                 }
-                bufRe[k * kAnalPad + lane] = accR;
-                bufIm[k * kAnalPad + lane] = accI;
-            }
-        } else {
-            for (int k = 0; k < cn; ++k) {
-                if (k == 0 && c0 == 0) {
-                    accR = 0.0;
-                    accI = 0.0;
+            } else {
+                for (int k = 0; k < cn; ++k) {
+                    anal_step<T, NF>((k & 1) != 0, wcoef[k], z, q1, q2, gsR, gsI, gaR, gaI,
+                                     accR, accI);
+                    if (k == 0 && ci == 0) rec_rescale<T>(wcoef[0].y, q1, q2);
 #pragma unroll
-                    for (int t = 0; t < T; ++t) {
-                        accR = fma(q1[t], gsR[t], accR);
-                        accI = fma(q1[t], gsI[t], accI);
+                    for (int j = 0; j < NF; ++j) {
+                        tb[((2 * j + 0) * CH + k) * kAnalPad + lane] = accR[j];
+                        tb[((2 * j + 1) * CH + k) * kAnalPad + lane] = accI[j];
                     }
-                } else {
-                    anal_step<T>((k & 1) != 0, wcoef[k], z, q1, q2, gsR, gsI, gaR, gaI,
-                                 accR, accI);
                 }
-                bufRe[k * kAnalPad + lane] = accR;
-                bufIm[k * kAnalPad + lane] = accI;
             }
-        }
-        __syncwarp();
-        // lane j < 16 sums the real parts of degree c0+j, lane j >= 16 the
-        // imaginary parts of degree c0+j-16, over the 32 lanes of the warp
-        {
-            const int row = lane & (kAnalChunk - 1);
-            const double* b = (lane < kAnalChunk ? bufRe : bufIm) + row * kAnalPad;
-            double sum = 0.0;
-            if (row < cn) {
-#pragma unroll 8
-                for (int i = 0; i < 32; ++i) sum += b[i];
+            __syncwarp();
+            // row = lane = (2*field + Re/Im)*CH + degree: sum over the 32
+            // lanes of the warp, four interleaved partial sums
+            {
+                const int k = lane % CH;
+                const double* b = tb + lane * kAnalPad;
+                double sum = 0.0;
+                if (k < cn) {
+                    double s4[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+                    for (int q = 0; q < 32; ++q) s4[q & 3] += b[q];
+                    sum = ((s4[0] + s4[1]) + (s4[2] + s4[3])) * wcoef[k].y;   // Q -> P sums
+                }
+                // stage row layout: (2*field + Re/Im)*kAnalChunk + degree in stage
+                ws[(lane / CH) * kAnalChunk + ci * CH + k] = sum;
             }
-            wsum[(buf * nwarps + warp) * 32 + lane] = sum;
+            __syncwarp();
         }
+        // stage sums of all warps are in wsum[buf]; the next stage's {beta, D}
+        // were issued a stage ahead
+        if (sg + 1 < nstages) cp_async_wait<0>();
         __syncthreads();
+        if (sg + 2 < nstages) load_stage(sg + 2);
         if (warp == 0) {
-            double sum = 0.0;
-            for (int w = 0; w < nwarps; ++w) sum += wsum[(buf * nwarps + w) * 32 + lane];
-            const int row = lane & (kAnalChunk - 1);
-            if (row < cn) {
-                double* dst = reinterpret_cast<double*>(outp + o + c0 + row);
-                dst[lane < kAnalChunk ? 0 : 1] = sum;
+            const int sn = min(kAnalChunk, nsteps - s0);
+#pragma unroll
+            for (int i = 0; i < SROWS / 32; ++i) {
+                const int r = lane + 32 * i;
+                const int k = r % kAnalChunk;
+                const int fc = r / kAnalChunk;   // 2*field + Re/Im
+                double sum = 0.0;
+                for (int w = 0; w < nwarps; ++w) sum += wsum[(buf * nwarps + w) * SROWS + r];
+                if (k < sn && (fc >> 1) < nvalid) {
+                    double* dst = reinterpret_cast<double*>(outp + (fc >> 1) * ostride + o +
+                                                            s0 + k);
+                    dst[fc & 1] = sum;
+                }
             }
         }
         buf ^= 1;

@@ -87,6 +87,28 @@ __global__ void k_rec_tables(double2* __restrict__ rec, int lc, int norm) {
     rec[packed_off(m, lc) + (l - m)] = make_double2(f1, f2);
 }
 
+// rescaled recursion table (legendre.cuh): from {ff1, ff2} per packed
+// (l, m), s = l - m, a = ff1, b = ff2:
+//   beta(s) = b(s) / (a(s) a(s-1))  (s >= 2; 0 for s <= 1),
+//   D(s)    = a(s0+1) * ... * a(s), s0 = kRecSegment * floor((s-1)/kRecSegment),
+//   D(0)    = 1, beta(0) = -1: from the state Q(-1) = 0, Q(-2) = start the
+//   step s = 0 yields Q(0) = start exactly, so the analysis runs one
+//   uniform step per degree from s = 0.
+__global__ void k_rec_scaled(const double2* __restrict__ ff, double2* __restrict__ out,
+                             int lc) {
+    const int m = blockIdx.y;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m + s > lc) return;
+    const double2* f = ff + packed_off(m, lc);
+    double beta = s == 0 ? -1.0 : 0.0, d = 1.0;
+    if (s >= 1) {
+        const int s0 = ((s - 1) / kRecSegment) * kRecSegment;
+        for (int i = s0 + 1; i <= s; ++i) d *= f[i].x;
+        if (s >= 2) beta = f[s].y / (f[s].x * f[s - 1].x);
+    }
+    out[packed_off(m, lc) + s] = make_double2(beta, d);
+}
+
 // rescale table: rtab[m*npair + p] = (1/scalef) * u_p^m by repeated
 // multiplication, as rescalem in MakeGridDH.f95:548-552; m = 0 is unscaled.
 __global__ void k_rtab(double* __restrict__ rtab, const double* __restrict__ u,
@@ -429,6 +451,7 @@ static int plan_finish(shtc_plan* P, const std::vector<double>& z,
     std::vector<double> pmm(lc + 1);
     host_pmm(lc, P->norm, P->csphase, pmm.data());
     double* d_u = nullptr;
+    double2* d_ff = nullptr;   // {ff1, ff2}, only needed to build d_rec
     if ((rc = dev_upload(&P->d_rec, (const double2*)nullptr, (size_t)P->nlm, st, &acc))) return rc;
     if ((rc = dev_upload(&P->d_pmm, pmm.data(), (size_t)lc + 1, st, &acc))) return rc;
     if ((rc = dev_upload(&P->d_rtab, (const double*)nullptr, (size_t)(lc + 1) * np, st, &acc))) return rc;
@@ -446,9 +469,14 @@ static int plan_finish(shtc_plan* P, const std::vector<double>& z,
         if ((rc = map_cuda(cudaStreamSynchronize(st)))) return rc;
     }
     if ((rc = dev_upload(&d_u, u.data(), (size_t)np, st, &acc))) return rc;
+    if ((rc = dev_upload(&d_ff, (const double2*)nullptr, (size_t)P->nlm, st, &acc))) {
+        cudaFree(d_u);
+        return rc;
+    }
     {
         dim3 g((lc + 1 + 127) / 128, lc + 1);
-        k_rec_tables<<<g, 128, 0, st>>>(P->d_rec, lc, P->norm);
+        k_rec_tables<<<g, 128, 0, st>>>(d_ff, lc, P->norm);
+        k_rec_scaled<<<g, 128, 0, st>>>(d_ff, P->d_rec, lc);
         k_rtab<<<(np + 127) / 128, 128, 0, st>>>(P->d_rtab, d_u, lc, np);
         k_ring_weights<<<(np + 127) / 128, 128, 0, st>>>(d_q, P->d_arowN, P->d_arowS,
                                                          P->d_wN, P->d_wS, np, P->kind);
@@ -457,7 +485,8 @@ static int plan_finish(shtc_plan* P, const std::vector<double>& z,
     // host vectors (z, u, rows, pmm) die on return: finish the copies
     cudaError_t e = cudaStreamSynchronize(st);
     cudaFree(d_u);
-    acc -= (size_t)np * sizeof(double);
+    cudaFree(d_ff);
+    acc -= (size_t)np * sizeof(double) + (size_t)P->nlm * sizeof(double2);
     if (rc) return rc;
     if (e != cudaSuccess) return SHTC_ECUDA;
     if ((rc = build_fft_plan(&P->fft, P->nlon, st))) return rc;

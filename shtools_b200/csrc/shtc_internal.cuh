@@ -21,6 +21,8 @@ namespace shtc {
 
 // The Holmes-Featherstone scale factor of the reference (MakeGridDH.f95:228).
 constexpr double kScalef = 1.0e-280;
+// degrees per segment of the rescaled Legendre recursion (legendre.cuh)
+constexpr int kRecSegment = 16;
 
 // Maximum FFT radix handled by the in-shared-memory Stockham passes; other
 // prime factors go through Bluestein's algorithm.
@@ -64,7 +66,7 @@ struct shtc_plan {
     int npair;         // ring pairs
     long long nlm;     // packed (l, m) count, (lc+1)(lc+2)/2
     // device tables (owned)
-    double2* d_rec;    // {ff1, ff2} per packed (l, m)
+    double2* d_rec;    // {beta, D} of the rescaled recursion per packed (l, m)
     double* d_pmm;     // sectoral start value per m
     double* d_rtab;    // rescale factor u^m / scalef per (m, pair)
     double* d_z;       // cos(colatitude) of the northern ring of each pair
