@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--workload", default="glq2047", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="use the default Legendre tile shapes instead of tuning "
+                         "each plan once before the warm-up (shtools_b200.autotune)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="target duration of the CPU baseline sample")
     return ap.parse_args()
@@ -644,27 +647,31 @@ def run_cuda(args, w, rank, world, local_rank):
     value = transforms / (total_ms * 1e-3)
 
     # ---- end-to-end through the public API with host buffers ---------------
-    g_host = torch.empty(tuple(g.shape), dtype=torch.float64).pin_memory()
-    b_host = torch.empty(tuple(back.shape), dtype=torch.float64).pin_memory()
-    e2e_steps = max(1, min(args.steps, 5))
+    # every step uploads its inputs (cilm and a grid) from pinned host memory,
+    # runs synthesis and analysis, and downloads both results; the steps are
+    # pipelined over three streams (shtools_b200.pipeline)
+    from shtools_b200.pipeline import pipelined
+    g_in = g.cpu().pin_memory()
+    outs = [(torch.empty(tuple(g.shape), dtype=torch.float64).pin_memory(),
+             torch.empty(tuple(back.shape), dtype=torch.float64).pin_memory())
+            for _ in range(2)]
+    e2e_steps = max(2, min(args.steps, 10))
+    fn = lambda x, gg: (synth(x), anal(gg))
+    pipelined(fn, [(c_host, g_in)] * 2, outs, device=dev)     # warm-up
     barrier()
     torch.cuda.synchronize(dev)
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
     a.record(st)
-    for i in range(e2e_steps):
-        xd = c_host.to(dev, non_blocking=True)          # H2D coefficients
-        gd = synth(xd)
-        g_host.copy_(gd, non_blocking=True)              # D2H grid
-        gd2 = g_host.to(dev, non_blocking=True)          # H2D grid
-        bd = anal(gd2)
-        b_host.copy_(bd, non_blocking=True)              # D2H coefficients
+    pipelined(fn, [(c_host, g_in)] * e2e_steps,
+              [outs[i % 2] for i in range(e2e_steps)], device=dev)
     b.record(st)
     torch.cuda.synchronize(dev)
     e2e_ms = max_over_ranks(a.elapsed_time(b), dev)
     e2e_value = 2.0 * F * e2e_steps * world / (e2e_ms * 1e-3)
-    h2d = c_host.numel() * 8 + g_host.numel() * 8
-    d2h = g_host.numel() * 8 + b_host.numel() * 8
+    e2e_ok = bool(torch.equal(outs[(e2e_steps - 1) % 2][1], back.cpu()))
+    h2d = c_host.numel() * 8 + g_in.numel() * 8
+    d2h = outs[0][0].numel() * 8 + outs[0][1].numel() * 8
 
     # ---- roofline of the dominant kernel ------------------------------------
     names = ["pack", "legendre_synth", "fft_c2r", "fft_r2c", "legendre_anal",
@@ -705,9 +712,10 @@ def run_cuda(args, w, rank, world, local_rank):
         "roundtrip_max_perdeg_err": rt_err,
         "e2e": {"value": e2e_value, "unit": "transforms/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "steps": e2e_steps,
-                "path": "torch API from pinned host buffers: H2D cilm, "
-                        "synthesis, D2H grid, H2D grid, analysis, D2H cilm"},
+                "steps": e2e_steps, "result_matches_device_run": e2e_ok,
+                "path": "public torch API on pinned host buffers: per step H2D cilm "
+                        "+ H2D grid, synthesis + analysis, D2H grid + D2H cilm; "
+                        "steps pipelined on 3 streams (shtools_b200.pipeline)"},
         "gpu_launches": int(sum(cnt)),
         "clocks": clk.summary(),
     }
@@ -748,6 +756,10 @@ def main():
                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(res))
         return 0
+    if not args.no_autotune:
+        # tile shapes from the project autotuner, tuned when a plan is created
+        # (before the warm-up, outside the timed region)
+        os.environ.setdefault("SHTC_AUTOTUNE", "1")
     if world > 1:
         import torch
         import datetime
@@ -770,6 +782,8 @@ def main():
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     if rank == 0:
+        res.setdefault("config", {})["tile_shapes"] = (
+            "default" if args.no_autotune else "autotuned per plan (shtools_b200.autotune)")
         print(json.dumps(res))
     return 0
 

@@ -45,8 +45,15 @@ struct BatchGroup {
 };
 
 constexpr int kBatchSynthNF = 4;
-constexpr int kBatchThreads = 128;        // ring pairs per tile (T = 1)
-constexpr int kBatchAnalWarps = 4;
+constexpr int kBatchThreads = 128;        // synthesis: ring pairs per tile (T = 1)
+// analysis: 2 warps x 4 ring pairs per lane = 256 pairs per tile, one tile
+// per order for lmax <= 511; per degree a lane then does 8 FP64 operations
+// against 2 shared-memory stores and loads, which keeps the transpose
+// reduction off the critical path
+constexpr int kBatchAnalWarps = 2;
+constexpr int kBatchAnalT = 4;
+constexpr int kBatchAnalNF = 1;
+constexpr int kBatchAnalPairs = 32 * kBatchAnalWarps * kBatchAnalT;
 
 // ---------------------------------------------------------------------------
 // kernels
@@ -137,7 +144,7 @@ k_batch_synth(const BatchGroup* __restrict__ G, const int4* __restrict__ items,
     }
 }
 
-// persistent analysis: item (g, m, tile, f)
+// persistent analysis: item (g, m, tile, f0), fields f0 .. f0+kBatchAnalNF-1
 __global__ void __launch_bounds__(32 * kBatchAnalWarps)
 k_batch_anal(const BatchGroup* __restrict__ G, const int4* __restrict__ items,
              int nitems, int* __restrict__ counter, double2* __restrict__ work) {
@@ -149,11 +156,13 @@ k_batch_anal(const BatchGroup* __restrict__ G, const int4* __restrict__ items,
         if (i >= nitems) return;
         const int4 w = items[i];
         const BatchGroup& g = G[w.x];
-        const int f = w.w;
-        anal_order<1, 1>(smem_anal, rstage, g.rec, g.pmm, g.rtab, g.z,
-                         work + g.spec_off + (long long)f * g.npair * (g.lc + 1) * 2, 0,
-                         work + g.pack_off + ((long long)w.z * g.nf + f) * g.nlm, 0, g.lc,
-                         g.npair, w.y, w.z, 1);
+        const int f0 = w.w;
+        const long long sstride = (long long)g.npair * (g.lc + 1) * 2;
+        anal_order<kBatchAnalT, kBatchAnalNF>(smem_anal, rstage, g.rec, g.pmm, g.rtab, g.z,
+                                    work + g.spec_off + f0 * sstride, sstride,
+                                    work + g.pack_off + ((long long)w.z * g.nf + f0) * g.nlm,
+                                    g.nlm, g.lc, g.npair, w.y, w.z,
+                                    min(kBatchAnalNF, g.nf - f0));
     }
 }
 
@@ -166,7 +175,7 @@ k_batch_c2r(const BatchGroup* __restrict__ G, const FftArgs* __restrict__ FA,
     const int4 j = jobs[blockIdx.x];
     const BatchGroup& g = G[j.x];
     const FftArgs F = FA[j.x];
-    fft_c2r_body<double>(F, smem_fft, j.z, j.y, work + g.spec_off, grid + g.grid_off,
+    fft_c2r_body<double>(F, F.tw, smem_fft, j.z, j.y, work + g.spec_off, grid + g.grid_off,
                  (long long)g.nlat * g.nlon, g.nlon, 1, g.rowN, g.rowS, nullptr,
                  nullptr, 1.0, g.lc, g.npair, 0);
 }
@@ -179,7 +188,7 @@ k_batch_r2c(const BatchGroup* __restrict__ G, const FftArgs* __restrict__ FA,
     const int4 j = jobs[blockIdx.x];
     const BatchGroup& g = G[j.x];
     const FftArgs F = FA[j.x];
-    fft_r2c_body<double>(F, smem_fft, j.z, j.y, grid + g.grid_off, (long long)g.nlat * g.nlon,
+    fft_r2c_body<double>(F, F.tw, smem_fft, j.z, j.y, grid + g.grid_off, (long long)g.nlat * g.nlon,
                  g.nlon, 1, work + g.spec_off, g.arowN, g.arowS, g.wN, g.wS,
                  g.inv_nlon, g.lc, g.npair, 0);
 }
@@ -263,7 +272,7 @@ extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
         g.lc = P->lc; g.npair = P->npair; g.nf = nf; g.norm = P->norm;
         g.nlat = P->nlat; g.nlon = P->nlon;
         g.fft_jobs = P->fft.mode == 0 ? P->npair : 2 * P->npair;
-        g.tiles = (P->npair + kBatchThreads - 1) / kBatchThreads;
+        g.tiles = (P->npair + kBatchAnalPairs - 1) / kBatchAnalPairs;   // analysis tiles
         g.inv_nlon = 1.0 / (double)P->nlon;
         g.nlm = P->nlm;
         g.cilm_off = coff;
@@ -276,21 +285,28 @@ extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
         spec += (long long)nf * P->npair * (P->lc + 1) * 2;
         B->h_groups.push_back(g);
         fa[gi] = fft_args(P->fft);
-        smem = std::max(smem, P->fft.smem);
+        smem = std::max(smem, P->fft.smem_data);   // twiddles stay in global memory
         threads = std::max(threads, P->fft.threads);
         // work items, with costs for longest-first ordering
         const int lc = P->lc;
         for (int m = 0; m <= lc; ++m) {
             pitems.push_back(make_int2(gi, m));
-            for (int t = 0; t < g.tiles; ++t) {
+            const int stiles = (P->npair + kBatchThreads - 1) / kBatchThreads;
+            for (int t = 0; t < stiles; ++t) {
                 const int pairs = std::min(kBatchThreads, P->npair - t * kBatchThreads);
                 for (int f0 = 0; f0 < nf; f0 += kBatchSynthNF) {
                     const int nv = std::min(kBatchSynthNF, nf - f0);
                     sc.push_back({(double)(lc - m + 1) * pairs * (4.0 + 2.0 * nv),
                                   make_int4(gi, m, t, f0)});
                 }
-                for (int f = 0; f < nf; ++f)
-                    ac.push_back({(double)(lc - m + 1) * pairs * 6.0, make_int4(gi, m, t, f)});
+            }
+            for (int t = 0; t < g.tiles; ++t) {
+                const int pairs = std::min(kBatchAnalPairs, P->npair - t * kBatchAnalPairs);
+                for (int f0 = 0; f0 < nf; f0 += kBatchAnalNF) {
+                    const int nv = std::min(kBatchAnalNF, nf - f0);
+                    ac.push_back({(double)(lc - m + 1) * pairs * (2.0 + 2.5 * nv),
+                                  make_int4(gi, m, t, f0)});
+                }
             }
         }
         for (int f = 0; f < nf; ++f)
@@ -327,7 +343,7 @@ extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
         cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, B->device);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_synth, kBatchThreads, 0);
         B->synth_ctas = sm * std::max(1, per);
-        const size_t asmem = anal_smem_bytes(kBatchAnalWarps, 1);
+        const size_t asmem = anal_smem_bytes(kBatchAnalWarps, kBatchAnalNF);
         cudaFuncSetAttribute(k_batch_anal, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)asmem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_anal,
@@ -420,7 +436,7 @@ extern "C" SHTC_API int shtc_batch_analysis(const shtc_batch* B, const double* g
     if ((rc = map_cuda(cudaGetLastError()))) return rc;
     if ((rc = map_cuda(cudaMemsetAsync(B->d_counter, 0, sizeof(int), st)))) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
-    k_batch_anal<<<B->anal_ctas, 32 * kBatchAnalWarps, anal_smem_bytes(kBatchAnalWarps, 1),
+    k_batch_anal<<<B->anal_ctas, 32 * kBatchAnalWarps, anal_smem_bytes(kBatchAnalWarps, kBatchAnalNF),
                    st>>>(B->d_groups, B->d_aitems, B->naitems, B->d_counter, w);
     stage_end(SHTC_STAGE_LEGENDRE_ANAL, st);
     if ((rc = map_cuda(cudaGetLastError()))) return rc;

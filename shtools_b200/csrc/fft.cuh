@@ -115,11 +115,12 @@ __device__ __forceinline__ void dft_small(double2* v) {
 }
 
 // One Stockham pass of radix R from x to y (ping-pong shared buffers).
+// tw: this pass's base twiddles, entry k < ns = exp(-2 pi i k/(ns R)); the
+// powers w^q, q >= 2, are formed by repeated multiplication.
 template <int R, int SIGN>
 __device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
                                          double2* __restrict__ y, int M, int ns,
                                          const double2* __restrict__ tw) {
-    // tw: this pass's twiddles, entry (q-1)*ns + k
     const int nr = M / R;
     for (int j = threadIdx.x; j < nr; j += blockDim.x) {
         const int k = j % ns;
@@ -127,8 +128,14 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = x[j + q * nr];
         if (k != 0) {
+            const double2 w = twv<SIGN>(tw, k);
+            double2 wq = w;
+            v[1] = cmul(v[1], w);
 #pragma unroll
-            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twv<SIGN>(tw, (q - 1) * ns + k));
+            for (int q = 2; q < R; ++q) {
+                wq = cmul(wq, w);
+                v[q] = cmul(v[q], wq);
+            }
         }
         dft_small<R, SIGN>(v);
         const int d = (j - k) * R + k;
@@ -137,9 +144,22 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
     }
 }
 
+// L2 prefetch of the 128-byte lines of [p, p + bytes), spread over the CTA;
+// every address issued lies inside the range's lines
+__device__ __forceinline__ void prefetch_l2_range(const void* p, size_t bytes) {
+    if (bytes == 0) return;
+    const uintptr_t b = (uintptr_t)p;
+    const uintptr_t e = b + bytes;
+    for (uintptr_t a = (b & ~(uintptr_t)127) + (uintptr_t)threadIdx.x * 128; a < e;
+         a += (uintptr_t)blockDim.x * 128) {
+        const size_t g = __cvta_generic_to_global((const void*)(a < b ? b : a));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(g));
+    }
+}
+
 // Runs the passes; the data starts in a, the result pointer is returned.
 template <int SIGN>
-__device__ double2* fft_run(double2* a, double2* b, int M, const int* fac,
+__device__ __forceinline__ double2* fft_run(double2* a, double2* b, int M, const int* fac,
                             int nfac, const double2* __restrict__ tw,
                             const int* tw_off) {
     int ns = 1;
@@ -167,7 +187,7 @@ __device__ double2* fft_run(double2* a, double2* b, int M, const int* fac,
 }
 
 struct FftArgs {
-    int n, mode, m, nfac, bluestein, mb;
+    int n, mode, m, nfac, bluestein, mb, ntw;
     int fac[kMaxFactors];
     int tw_off[kMaxFactors];
     const double2* tw;
@@ -177,11 +197,13 @@ struct FftArgs {
 };
 
 // Complex DFT of length F.m of buf with sign SIGN; buf and tmp each hold
-// F.mb (Bluestein) or F.m elements.  Returns the pointer holding the result.
+// F.mb (Bluestein) or F.m elements; tw: the plan's twiddles (F.tw, or a
+// copy in shared memory).  Returns the pointer holding the result.
 template <int SIGN>
-__device__ double2* fft_exec(const FftArgs& F, double2* buf, double2* tmp) {
+__device__ __forceinline__ double2* fft_exec(const FftArgs& F, const double2* tw, double2* buf,
+                             double2* tmp) {
     __syncthreads();
-    if (!F.bluestein) return fft_run<SIGN>(buf, tmp, F.m, F.fac, F.nfac, F.tw, F.tw_off);
+    if (!F.bluestein) return fft_run<SIGN>(buf, tmp, F.m, F.fac, F.nfac, tw, F.tw_off);
     // Bluestein: X_k = c_k sum_j (x_j c_j) conj(c_{k-j}), c_t = exp(-+ i pi t^2/m)
     const int m = F.m, mb = F.mb;
     for (int t = threadIdx.x; t < mb; t += blockDim.x) {
@@ -193,7 +215,7 @@ __device__ double2* fft_exec(const FftArgs& F, double2* buf, double2* tmp) {
             buf[t] = make_double2(0.0, 0.0);
         }
     }
-    double2* r = fft_run<-1>(buf, tmp, mb, F.fac, F.nfac, F.tw, F.tw_off);
+    double2* r = fft_run<-1>(buf, tmp, mb, F.fac, F.nfac, tw, F.tw_off);
     double2* o = (r == buf) ? tmp : buf;
     for (int t = threadIdx.x; t < mb; t += blockDim.x) {
         double2 kf;
@@ -205,7 +227,7 @@ __device__ double2* fft_exec(const FftArgs& F, double2* buf, double2* tmp) {
         }
         r[t] = cmul(r[t], kf);
     }
-    double2* r2 = fft_run<+1>(r, o, mb, F.fac, F.nfac, F.tw, F.tw_off);
+    double2* r2 = fft_run<+1>(r, o, mb, F.fac, F.nfac, tw, F.tw_off);
     const double inv = 1.0 / (double)mb;
     for (int t = threadIdx.x; t < m; t += blockDim.x) {
         double2 c = F.chirp[t];
@@ -224,7 +246,7 @@ __device__ double2* fft_exec(const FftArgs& F, double2* buf, double2* tmp) {
 // the ring weight when wN/wS are given (analysis adjoint).
 template <typename GT>
 __device__ __forceinline__ void fft_c2r_body(
-    const FftArgs& F, double2* smem_fft, int job, int f,
+    const FftArgs& F, const double2* tw, double2* smem_fft, int job, int f,
     const double2* __restrict__ spec, GT* __restrict__ grid, long long gf,
     long long grs, long long gcs, const int* __restrict__ rowN,
     const int* __restrict__ rowS, const double* __restrict__ wN,
@@ -252,7 +274,7 @@ __device__ __forceinline__ void fft_c2r_body(
             a[k] = make_double2(xn.x - xs.y, xn.y + xs.x);
             if (k > 0) a[n - k] = make_double2(xn.x + xs.y, -xn.y + xs.x);
         }
-        const double2* r = fft_exec<+1>(F, a, b);
+        const double2* r = fft_exec<+1>(F, tw, a, b);
         const double sN = wN ? wN[p] * wscale : 1.0;
         const double sS = wS ? wS[p] * wscale : 1.0;
         GT* gN = rN >= 0 ? grid + f * gf + rN * grs : nullptr;
@@ -289,7 +311,7 @@ __device__ __forceinline__ void fft_c2r_body(
             const double2 wb = cmul(w, B);
             a[k] = make_double2(A.x - wb.y, A.y + wb.x);
         }
-        const double2* r = fft_exec<+1>(F, a, b);
+        const double2* r = fft_exec<+1>(F, tw, a, b);
         const double sc = (h ? (wS ? wS[p] * wscale : 1.0) : (wN ? wN[p] * wscale : 1.0));
         GT* g = grid + f * gf + row * grs;
 #pragma unroll 4
@@ -307,7 +329,7 @@ __device__ __forceinline__ void fft_c2r_body(
 // fold_extend adds column n into column 0 (adjoint of the extend copy).
 template <typename GT>
 __device__ __forceinline__ void fft_r2c_body(
-    const FftArgs& F, double2* smem_fft, int job, int f,
+    const FftArgs& F, const double2* tw, double2* smem_fft, int job, int f,
     const GT* __restrict__ grid, long long gf, long long grs, long long gcs,
     double2* __restrict__ spec, const int* __restrict__ rowN,
     const int* __restrict__ rowS, const double* __restrict__ wN,
@@ -332,7 +354,7 @@ __device__ __forceinline__ void fft_r2c_body(
             }
             a[j] = make_double2(xn, xs);
         }
-        const double2* r = fft_exec<-1>(F, a, b);
+        const double2* r = fft_exec<-1>(F, tw, a, b);
         const double sN = wN ? wN[p] * wscale : wscale;
         const double sS = wS ? wS[p] * wscale : wscale;
         double2* X = spec + ((long long)f * npair + p) * (lc + 1) * 2;
@@ -364,7 +386,7 @@ __device__ __forceinline__ void fft_r2c_body(
             if (fold_extend && j == 0) x0 += (double)g[(long long)n * gcs];
             a[j] = make_double2(x0, x1);
         }
-        const double2* r = fft_exec<-1>(F, a, b);
+        const double2* r = fft_exec<-1>(F, tw, a, b);
         const double sc = h ? (wS ? wS[p] * wscale : wscale) : (wN ? wN[p] * wscale : wscale);
 #pragma unroll 4
         for (int k = threadIdx.x; k <= lc; k += blockDim.x) {
@@ -377,6 +399,34 @@ __device__ __forceinline__ void fft_r2c_body(
             const double xr = E.x + wo.x, xi = E.y + wo.y;
             X[2 * k] = make_double2(sc * xr, -(sc * xi));
         }
+    }
+}
+
+// L2 prefetch of the input of the c2r item (job, f): the pair's spectrum row
+__device__ __forceinline__ void fft_c2r_prefetch(int mode, int job, int f,
+                                                 const double2* spec, int lc, int npair) {
+    const int p = mode == 0 ? job : (job >> 1);
+    prefetch_l2_range(spec + ((long long)f * npair + p) * (lc + 1) * 2,
+                      (size_t)(lc + 1) * 2 * sizeof(double2));
+}
+
+// L2 prefetch of the input of the r2c item (job, f): its grid rows
+// (contiguous rows only)
+template <typename GT>
+__device__ __forceinline__ void fft_r2c_prefetch(int mode, int n, int job, int f,
+                                                 const GT* grid, long long gf, long long grs,
+                                                 long long gcs, const int* rowN,
+                                                 const int* rowS, int extra) {
+    if (gcs != 1) return;
+    const size_t bytes = (size_t)(n + extra) * sizeof(GT);
+    if (mode == 0) {
+        const int rN = rowN[job], rS = rowS[job];
+        if (rN >= 0) prefetch_l2_range(grid + f * gf + rN * grs, bytes);
+        if (rS >= 0) prefetch_l2_range(grid + f * gf + rS * grs, bytes);
+    } else {
+        const int p = job >> 1;
+        const int row = (job & 1) ? rowS[p] : rowN[p];
+        if (row >= 0) prefetch_l2_range(grid + f * gf + row * grs, bytes);
     }
 }
 

@@ -190,28 +190,56 @@ k_unpack_coef(const double2* __restrict__ partial, int ntiles, CT* __restrict__ 
 // per-plan FFT kernels: CTA = (job, field); job = ring pair (odd n) or
 // 2*pair + ring (even n)
 // ---------------------------------------------------------------------------
-template <typename GT>
-__global__ void __launch_bounds__(512)
-k_fft_c2r(FftArgs F, const double2* __restrict__ spec, GT* __restrict__ grid,
-          long long gf, long long grs, long long gcs, const int* __restrict__ rowN,
-          const int* __restrict__ rowS, const double* __restrict__ wN,
-          const double* __restrict__ wS, double wscale, int lc, int npair,
-          int extend_col) {
-    extern __shared__ double2 smem_fft[];
-    fft_c2r_body<GT>(F, smem_fft, blockIdx.x, blockIdx.y, spec, grid, gf, grs, gcs, rowN,
-                 rowS, wN, wS, wscale, lc, npair, extend_col);
+// Persistent FFT kernels: CTA b handles the items b, b + gridDim.x, ... of
+// the nitems = jobs * nfield (job, field) pairs; while one item's FFT runs,
+// the next item's input lines are prefetched into L2.  With tw_smem the
+// plan's twiddles are copied once per CTA behind the two data buffers.
+__device__ __forceinline__ const double2* fft_stage_twiddles(const FftArgs& F,
+                                                             double2* smem_fft,
+                                                             int tw_smem) {
+    if (!tw_smem) return F.tw;
+    const int len = F.bluestein ? F.mb : F.m;
+    double2* tws = smem_fft + 2 * len;
+    for (int i = threadIdx.x; i < F.ntw; i += blockDim.x) tws[i] = F.tw[i];
+    return tws;   // made visible by the barrier that opens fft_exec
 }
 
 template <typename GT>
 __global__ void __launch_bounds__(512)
-k_fft_r2c(FftArgs F, const GT* __restrict__ grid, long long gf, long long grs,
-          long long gcs, double2* __restrict__ spec, const int* __restrict__ rowN,
-          const int* __restrict__ rowS, const double* __restrict__ wN,
-          const double* __restrict__ wS, double wscale, int lc, int npair,
-          int fold_extend) {
+k_fft_c2r(FftArgs F, int tw_smem, int jobs, int nitems, const double2* __restrict__ spec,
+          GT* __restrict__ grid, long long gf, long long grs, long long gcs,
+          const int* __restrict__ rowN, const int* __restrict__ rowS,
+          const double* __restrict__ wN, const double* __restrict__ wS, double wscale,
+          int lc, int npair, int extend_col) {
     extern __shared__ double2 smem_fft[];
-    fft_r2c_body<GT>(F, smem_fft, blockIdx.x, blockIdx.y, grid, gf, grs, gcs, spec, rowN,
-                 rowS, wN, wS, wscale, lc, npair, fold_extend);
+    const double2* tw = fft_stage_twiddles(F, smem_fft, tw_smem);
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int nx = it + gridDim.x;
+        if (nx < nitems) fft_c2r_prefetch(F.mode, nx % jobs, nx / jobs, spec, lc, npair);
+        fft_c2r_body<GT>(F, tw, smem_fft, it % jobs, it / jobs, spec, grid, gf, grs, gcs,
+                         rowN, rowS, wN, wS, wscale, lc, npair, extend_col);
+        __syncthreads();
+    }
+}
+
+template <typename GT>
+__global__ void __launch_bounds__(512)
+k_fft_r2c(FftArgs F, int tw_smem, int jobs, int nitems, const GT* __restrict__ grid,
+          long long gf, long long grs, long long gcs, double2* __restrict__ spec,
+          const int* __restrict__ rowN, const int* __restrict__ rowS,
+          const double* __restrict__ wN, const double* __restrict__ wS, double wscale,
+          int lc, int npair, int fold_extend) {
+    extern __shared__ double2 smem_fft[];
+    const double2* tw = fft_stage_twiddles(F, smem_fft, tw_smem);
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int nx = it + gridDim.x;
+        if (nx < nitems)
+            fft_r2c_prefetch<GT>(F.mode, F.n, nx % jobs, nx / jobs, grid, gf, grs, gcs, rowN,
+                                 rowS, fold_extend);
+        fft_r2c_body<GT>(F, tw, smem_fft, it % jobs, it / jobs, grid, gf, grs, gcs, spec,
+                         rowN, rowS, wN, wS, wscale, lc, npair, fold_extend);
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -220,7 +248,7 @@ k_fft_r2c(FftArgs F, const GT* __restrict__ grid, long long gf, long long grs,
 FftArgs fft_args(const FftPlan& f) {
     FftArgs a;
     a.n = f.n; a.mode = f.mode; a.m = f.m; a.nfac = f.nfac;
-    a.bluestein = f.bluestein; a.mb = f.mb;
+    a.bluestein = f.bluestein; a.mb = f.mb; a.ntw = f.ntw;
     for (int i = 0; i < kMaxFactors; ++i) {
         a.fac[i] = i < f.nfac ? f.fac[i] : 0;
         a.tw_off[i] = i < f.nfac ? f.tw_off[i] : 0;
@@ -376,6 +404,21 @@ static int fft_smem_setup(const void* fn, const FftPlan& f) {
                                          (int)f.smem));
 }
 
+// persistent grid: as many CTAs as fit on the device at once, at most one
+// per item
+template <typename K>
+static int fft_grid(K kernel, const FftPlan& f, int nitems, int* blocks) {
+    int dev = 0, sms = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, f.threads,
+                                                                  f.smem);
+    if (e != cudaSuccess) return map_cuda(e);
+    const long long cap = (long long)(sms > 0 ? sms : 1) * (occ > 0 ? occ : 1);
+    *blocks = (int)(nitems < cap ? nitems : cap);
+    return SHTC_OK;
+}
+
 template <typename GT>
 static int launch_c2r_t(const shtc_plan* P, const double2* spec, GT* grid, long long gf,
                         long long grs, long long gcs, int nfield, int weighted,
@@ -384,18 +427,20 @@ static int launch_c2r_t(const shtc_plan* P, const double2* spec, GT* grid, long 
     int rc = fft_smem_setup((const void*)k_fft_c2r<GT>, f);
     if (rc) return rc;
     const int jobs = f.mode == 0 ? P->npair : 2 * P->npair;
-    dim3 g(jobs, nfield);
+    const int nitems = jobs * nfield;
+    int blocks = 0;
+    if ((rc = fft_grid(k_fft_c2r<GT>, f, nitems, &blocks))) return rc;
+    if (blocks == 0) return SHTC_OK;
     // synthesis uses the synthesis ring map (with the extend row and column);
     // the analysis adjoint uses the analysis ring map and ring weights
     if (weighted) {
-        k_fft_c2r<GT><<<g, f.threads, f.smem, st>>>(fft_args(f), spec, grid, gf, grs, gcs,
-                                                    P->d_arowN, P->d_arowS, P->d_wN,
-                                                    P->d_wS, 1.0 / (double)P->nlon, P->lc,
-                                                    P->npair, 0);
+        k_fft_c2r<GT><<<blocks, f.threads, f.smem, st>>>(
+            fft_args(f), f.tw_smem, jobs, nitems, spec, grid, gf, grs, gcs, P->d_arowN,
+            P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, 0);
     } else {
-        k_fft_c2r<GT><<<g, f.threads, f.smem, st>>>(fft_args(f), spec, grid, gf, grs, gcs,
-                                                    P->d_rowN, P->d_rowS, nullptr, nullptr,
-                                                    1.0, P->lc, P->npair, P->extend);
+        k_fft_c2r<GT><<<blocks, f.threads, f.smem, st>>>(
+            fft_args(f), f.tw_smem, jobs, nitems, spec, grid, gf, grs, gcs, P->d_rowN,
+            P->d_rowS, nullptr, nullptr, 1.0, P->lc, P->npair, P->extend);
     }
     return map_cuda(cudaGetLastError());
 }
@@ -417,19 +462,21 @@ static int launch_r2c_t(const shtc_plan* P, const GT* grid, long long gf, long l
     int rc = fft_smem_setup((const void*)k_fft_r2c<GT>, f);
     if (rc) return rc;
     const int jobs = f.mode == 0 ? P->npair : 2 * P->npair;
-    dim3 g(jobs, nfield);
+    const int nitems = jobs * nfield;
+    int blocks = 0;
+    if ((rc = fft_grid(k_fft_r2c<GT>, f, nitems, &blocks))) return rc;
+    if (blocks == 0) return SHTC_OK;
     if (weighted) {
         // analysis: fcoef = (w * Re) / nlong, the reference's order of operations
         // is reproduced up to one rounding by folding 1/nlong into the weight
-        k_fft_r2c<GT><<<g, f.threads, f.smem, st>>>(fft_args(f), grid, gf, grs, gcs, spec,
-                                                    P->d_arowN, P->d_arowS, P->d_wN,
-                                                    P->d_wS, 1.0 / (double)P->nlon, P->lc,
-                                                    P->npair, 0);
+        k_fft_r2c<GT><<<blocks, f.threads, f.smem, st>>>(
+            fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_arowN,
+            P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, 0);
     } else {
         // synthesis adjoint: plain (Re, -Im) of the rows of the cotangent
-        k_fft_r2c<GT><<<g, f.threads, f.smem, st>>>(fft_args(f), grid, gf, grs, gcs, spec,
-                                                    P->d_rowN, P->d_rowS, nullptr, nullptr,
-                                                    1.0, P->lc, P->npair, fold_extend);
+        k_fft_r2c<GT><<<blocks, f.threads, f.smem, st>>>(
+            fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_rowN,
+            P->d_rowS, nullptr, nullptr, 1.0, P->lc, P->npair, fold_extend);
     }
     return map_cuda(cudaGetLastError());
 }

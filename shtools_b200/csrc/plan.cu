@@ -230,27 +230,25 @@ static int factor_len(int n, int* fac) {
     return k;
 }
 
-// Twiddles of every Stockham pass, pass after pass: for the pass of radix R
-// applied after sub-transforms of size ns, entry (q-1)*ns + k holds
-// exp(-2 pi i k q / (ns R)), so that threads of consecutive k read
-// consecutive entries.
-static void pass_twiddles(int len, const int* fac, int nfac, std::vector<double2>& out,
-                          int* off) {
+// Base twiddles of every Stockham pass, pass after pass: for the pass of
+// radix R applied after sub-transforms of length ns, entry k < ns holds
+// w_k = exp(-2 pi i k / (ns R)); the butterfly forms w_k^q, q = 2..R-1, by
+// repeated complex multiplication (a few ulp for R <= 13).  Threads of
+// consecutive k read consecutive entries.
+static int pass_twiddles(const int* fac, int nfac, std::vector<double2>& out, int* off) {
     out.clear();
     const long double tp = 2.0L * 3.141592653589793238462643383279502884L;
     int ns = 1;
     for (int i = 0; i < nfac; ++i) {
         const int R = fac[i];
         off[i] = (int)out.size();
-        for (int q = 1; q < R; ++q)
-            for (int k = 0; k < ns; ++k) {
-                const long long t = ((long long)k * q) % ((long long)ns * R);
-                const long double a = tp * (long double)t / (long double)(ns * R);
-                out.push_back(make_double2((double)cosl(a), (double)(-sinl(a))));
-            }
+        for (int k = 0; k < ns; ++k) {
+            const long double a = tp * (long double)k / (long double)((long long)ns * R);
+            out.push_back(make_double2((double)cosl(a), (double)(-sinl(a))));
+        }
         ns *= R;
     }
-    (void)len;
+    return (int)out.size();
 }
 
 int build_fft_plan(FftPlan* f, int n, cudaStream_t st) {
@@ -300,7 +298,7 @@ int build_fft_plan(FftPlan* f, int n, cudaStream_t st) {
         }
     }
     if (nf > kMaxFactors) return SHTC_EUNSUP;
-    pass_twiddles(f->bluestein ? f->mb : f->m, fac, nf, tw, f->tw_off);
+    f->ntw = pass_twiddles(fac, nf, tw, f->tw_off);
     f->nfac = nf;
     for (int i = 0; i < nf; ++i) f->fac[i] = fac[i];
     if (f->mode == 1) {
@@ -312,12 +310,16 @@ int build_fft_plan(FftPlan* f, int n, cudaStream_t st) {
         }
     }
     const int len = f->bluestein ? f->mb : f->m;
-    // two shared buffers: Stockham passes ping-pong between them
-    f->smem = 2 * (size_t)len * sizeof(double2);
+    // two shared buffers: Stockham passes ping-pong between them; the
+    // per-plan kernels also keep the twiddles in shared memory when they fit
+    f->smem_data = 2 * (size_t)len * sizeof(double2);
     int maxsmem = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (maxsmem > 0 && f->smem > (size_t)maxsmem) return SHTC_EUNSUP;
+    if (maxsmem > 0 && f->smem_data > (size_t)maxsmem) return SHTC_EUNSUP;
+    const size_t with_tw = f->smem_data + (size_t)f->ntw * sizeof(double2);
+    f->tw_smem = (maxsmem > 0 && with_tw <= (size_t)maxsmem) ? 1 : 0;
+    f->smem = f->tw_smem ? with_tw : f->smem_data;
     f->threads = len > 2048 ? 512 : (len > 512 ? 256 : 128);
     auto up = [&](double2** d, const std::vector<double2>& h) -> int {
         if (h.empty()) { *d = nullptr; return SHTC_OK; }

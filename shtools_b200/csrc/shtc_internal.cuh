@@ -38,13 +38,18 @@ struct FftPlan {
     int fac[kMaxFactors];
     int bluestein;     // 1 if m has a prime factor > kMaxRadix
     int mb;            // Bluestein convolution length (power of two)
-    double2* d_tw;     // per-pass twiddles: pass i at tw_off[i], entry (q-1)*ns+k
-                       // = exp(-2 pi i k q / (ns R)), of the length-(mb or m) FFT
+    double2* d_tw;     // per-pass base twiddles: pass i (radix R after sub-transforms
+                       // of length ns) at tw_off[i], entry k < ns = exp(-2 pi i k/(ns R)),
+                       // of the length-(mb or m) FFT
     int tw_off[kMaxFactors];
+    int ntw;           // entries of d_tw (sum of ns over the passes)
     double2* d_twn;    // mode 1: exp(-2 pi i k / n), k < n/2
     double2* d_chirp;  // Bluestein: exp(-i pi t^2 / m), t < m
     double2* d_kern;   // Bluestein: FFT_mb of the conjugate chirp kernel
-    size_t smem;       // dynamic shared memory bytes per CTA
+    size_t smem_data;  // shared bytes of the two data buffers
+    size_t smem;       // dynamic shared memory bytes per CTA of the per-plan kernels:
+                       // smem_data, plus the twiddles when tw_smem
+    int tw_smem;       // per-plan kernels copy d_tw into shared memory
     int threads;       // CTA size
 };
 
