@@ -166,31 +166,61 @@ k_batch_anal(const BatchGroup* __restrict__ G, const int4* __restrict__ items,
     }
 }
 
-// FFT jobs: item (g, f, job); the group's FftArgs are read from memory
+// Persistent FFT kernels: items (g, f, job) are handed out through a global
+// counter, so CTAs stay busy across groups of different FFT lengths; the
+// group's FftArgs are read in place from global memory, and the input lines
+// of the CTA's next item are prefetched into L2 while the current FFT runs.
 __global__ void __launch_bounds__(512)
 k_batch_c2r(const BatchGroup* __restrict__ G, const FftArgs* __restrict__ FA,
-            const int4* __restrict__ jobs, const double2* __restrict__ work,
-            double* __restrict__ grid) {
+            const int4* __restrict__ jobs, int njobs, int* __restrict__ counter,
+            const double2* __restrict__ work, double* __restrict__ grid) {
     extern __shared__ double2 smem_fft[];
-    const int4 j = jobs[blockIdx.x];
-    const BatchGroup& g = G[j.x];
-    const FftArgs F = FA[j.x];
-    fft_c2r_body<double>(F, F.tw, smem_fft, j.z, j.y, work + g.spec_off, grid + g.grid_off,
-                 (long long)g.nlat * g.nlon, g.nlon, 1, g.rowN, g.rowS, nullptr,
-                 nullptr, 1.0, g.lc, g.npair, 0);
+    __shared__ int s_item;
+    int i = next_item(counter, &s_item);
+    while (i < njobs) {
+        const int nx = next_item(counter, &s_item);
+        if (nx < njobs) {
+            const int4 jn = jobs[nx];
+            const BatchGroup& gn = G[jn.x];
+            fft_c2r_prefetch(FA[jn.x].mode, jn.z, jn.y, work + gn.spec_off, gn.lc, gn.npair);
+        }
+        const int4 j = jobs[i];
+        const BatchGroup& g = G[j.x];
+        const FftArgs& F = FA[j.x];
+        fft_c2r_body<double>(F, F.tw, smem_fft, j.z, j.y, work + g.spec_off,
+                             grid + g.grid_off, (long long)g.nlat * g.nlon, g.nlon, 1,
+                             g.rowN, g.rowS, nullptr, nullptr, 1.0, g.lc, g.npair, 0);
+        __syncthreads();
+        i = nx;
+    }
 }
 
 __global__ void __launch_bounds__(512)
 k_batch_r2c(const BatchGroup* __restrict__ G, const FftArgs* __restrict__ FA,
-            const int4* __restrict__ jobs, const double* __restrict__ grid,
-            double2* __restrict__ work) {
+            const int4* __restrict__ jobs, int njobs, int* __restrict__ counter,
+            const double* __restrict__ grid, double2* __restrict__ work) {
     extern __shared__ double2 smem_fft[];
-    const int4 j = jobs[blockIdx.x];
-    const BatchGroup& g = G[j.x];
-    const FftArgs F = FA[j.x];
-    fft_r2c_body<double>(F, F.tw, smem_fft, j.z, j.y, grid + g.grid_off, (long long)g.nlat * g.nlon,
-                 g.nlon, 1, work + g.spec_off, g.arowN, g.arowS, g.wN, g.wS,
-                 g.inv_nlon, g.lc, g.npair, 0);
+    __shared__ int s_item;
+    int i = next_item(counter, &s_item);
+    while (i < njobs) {
+        const int nx = next_item(counter, &s_item);
+        if (nx < njobs) {
+            const int4 jn = jobs[nx];
+            const BatchGroup& gn = G[jn.x];
+            const FftArgs& Fn = FA[jn.x];
+            fft_r2c_prefetch<double>(Fn.mode, Fn.n, jn.z, jn.y, grid + gn.grid_off,
+                                     (long long)gn.nlat * gn.nlon, gn.nlon, 1, gn.arowN,
+                                     gn.arowS, 0);
+        }
+        const int4 j = jobs[i];
+        const BatchGroup& g = G[j.x];
+        const FftArgs& F = FA[j.x];
+        fft_r2c_body<double>(F, F.tw, smem_fft, j.z, j.y, grid + g.grid_off,
+                             (long long)g.nlat * g.nlon, g.nlon, 1, work + g.spec_off,
+                             g.arowN, g.arowS, g.wN, g.wS, g.inv_nlon, g.lc, g.npair, 0);
+        __syncthreads();
+        i = nx;
+    }
 }
 
 }  // namespace shtc
@@ -217,6 +247,7 @@ struct shtc_batch {
     int fft_threads = 128;
     int synth_ctas = 0;
     int anal_ctas = 0;
+    int fft_ctas = 0;
     long long cilm_total = 0;
     long long grid_total = 0;
 };
@@ -355,6 +386,12 @@ extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
             cudaFuncSetAttribute(k_batch_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)B->fft_smem);
         }
+        int pc = 0, pr = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pc, k_batch_c2r, B->fft_threads,
+                                                      B->fft_smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pr, k_batch_r2c, B->fft_threads,
+                                                      B->fft_smem);
+        B->fft_ctas = std::min(B->njobs, sm * std::max(1, std::min(pc, pr)));
         rc = map_cuda(cudaStreamSynchronize(st));
     }
     if (rc) {
@@ -416,8 +453,9 @@ extern "C" SHTC_API int shtc_batch_synthesis(const shtc_batch* B, const double* 
     stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
     if ((rc = map_cuda(cudaGetLastError()))) return rc;
     stage_begin(SHTC_STAGE_FFT_C2R, st);
-    k_batch_c2r<<<B->njobs, B->fft_threads, B->fft_smem, st>>>(B->d_groups, B->d_fft,
-                                                               B->d_jobs, w, grid);
+    if ((rc = map_cuda(cudaMemsetAsync(B->d_counter + 1, 0, sizeof(int), st)))) return rc;
+    k_batch_c2r<<<B->fft_ctas, B->fft_threads, B->fft_smem, st>>>(
+        B->d_groups, B->d_fft, B->d_jobs, B->njobs, B->d_counter + 1, w, grid);
     stage_end(SHTC_STAGE_FFT_C2R, st);
     return map_cuda(cudaGetLastError());
 }
@@ -430,8 +468,9 @@ extern "C" SHTC_API int shtc_batch_analysis(const shtc_batch* B, const double* g
     cudaStream_t st = (cudaStream_t)stream;
     double2* w = (double2*)work;
     stage_begin(SHTC_STAGE_FFT_R2C, st);
-    k_batch_r2c<<<B->njobs, B->fft_threads, B->fft_smem, st>>>(B->d_groups, B->d_fft,
-                                                               B->d_jobs, grid, w);
+    if ((rc = map_cuda(cudaMemsetAsync(B->d_counter + 1, 0, sizeof(int), st)))) return rc;
+    k_batch_r2c<<<B->fft_ctas, B->fft_threads, B->fft_smem, st>>>(
+        B->d_groups, B->d_fft, B->d_jobs, B->njobs, B->d_counter + 1, grid, w);
     stage_end(SHTC_STAGE_FFT_R2C, st);
     if ((rc = map_cuda(cudaGetLastError()))) return rc;
     if ((rc = map_cuda(cudaMemsetAsync(B->d_counter, 0, sizeof(int), st)))) return rc;
