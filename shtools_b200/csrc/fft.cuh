@@ -122,8 +122,10 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
                                          double2* __restrict__ y, int M, int ns,
                                          const double2* __restrict__ tw) {
     const int nr = M / R;
+    // k = j mod ns, updated incrementally as j advances by blockDim.x
+    const int kstep = (int)(blockDim.x % (unsigned)ns);
+    int k = (int)(threadIdx.x % (unsigned)ns);
     for (int j = threadIdx.x; j < nr; j += blockDim.x) {
-        const int k = j % ns;
         double2 v[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = x[j + q * nr];
@@ -141,6 +143,8 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
         const int d = (j - k) * R + k;
 #pragma unroll
         for (int q = 0; q < R; ++q) y[d + q * ns] = v[q];
+        k += kstep;
+        if (k >= ns) k -= ns;
     }
 }
 
@@ -222,7 +226,7 @@ __device__ __forceinline__ double2* fft_exec(const FftArgs& F, const double2* tw
         if (SIGN < 0) {
             kf = F.kern[t];
         } else {
-            kf = F.kern[(mb - t) & (mb - 1)];
+            kf = F.kern[t == 0 ? 0 : mb - t];
             kf.y = -kf.y;
         }
         r[t] = cmul(r[t], kf);

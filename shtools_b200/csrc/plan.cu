@@ -261,8 +261,15 @@ int build_fft_plan(FftPlan* f, int n, cudaStream_t st) {
     std::vector<double2> tw, twn, chirp, kern;
     if (nf < 0) {
         f->bluestein = 1;
-        int mb = 1;
-        while (mb < 2 * f->m - 1) mb <<= 1;
+        // convolution length: the smallest 7-smooth mb >= 2m - 1 (Stockham
+        // radices 2, 3, 4, 5, 7), on average ~30% below the next power of two
+        int mb = 2 * f->m - 1;
+        for (;; ++mb) {
+            int r = mb;
+            for (int p : {2, 3, 5, 7})
+                while (r % p == 0) r /= p;
+            if (r == 1) break;
+        }
         f->mb = mb;
         nf = factor_len(mb, fac);
         chirp.resize(f->m);

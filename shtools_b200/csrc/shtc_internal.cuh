@@ -37,7 +37,7 @@ struct FftPlan {
     int nfac;          // radices of the length-m (or Bluestein) FFT
     int fac[kMaxFactors];
     int bluestein;     // 1 if m has a prime factor > kMaxRadix
-    int mb;            // Bluestein convolution length (power of two)
+    int mb;            // Bluestein convolution length (7-smooth, >= 2m - 1)
     double2* d_tw;     // per-pass base twiddles: pass i (radix R after sub-transforms
                        // of length ns) at tw_off[i], entry k < ns = exp(-2 pi i k/(ns R)),
                        // of the length-(mb or m) FFT
