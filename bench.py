@@ -782,8 +782,11 @@ def main():
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     if rank == 0:
-        res.setdefault("config", {})["tile_shapes"] = (
-            "default" if args.no_autotune else "autotuned per plan (shtools_b200.autotune)")
+        if w["kind"] == "glq_batch":
+            res.setdefault("config", {})["tile_shapes"] = "fixed batched-kernel shapes"
+        else:
+            res.setdefault("config", {})["tile_shapes"] = (
+                "default" if args.no_autotune else "autotuned per plan (shtools_b200.autotune)")
         print(json.dumps(res))
     return 0
 

@@ -1,7 +1,7 @@
 // Device code of the longitude FFTs (c2r for synthesis, r2c for analysis),
 // shared by the per-plan kernels (kernels.cu) and the batched kernels
 // (batch.cu).  Stockham autosort passes ping-pong between two shared
-// buffers; radix 2, 3, 4, 5, 7, 11, 13 butterflies; Bluestein's algorithm
+// buffers; radix 2, 3, 4, 5, 7, 8, 11, 13 butterflies; Bluestein's algorithm
 // for lengths with other prime factors.  Conventions are those of FFTW's
 // unnormalised r2c / c2r (src/FFTW3.f95:212-271).
 #pragma once
@@ -56,10 +56,52 @@ __host__ __device__ constexpr double root_sin(int R, int u) {
             : u == 5 ? 0.6631226582407952 : 0.23931566428755777);
 }
 
-// radix-R DFT of v[] in place (R = 2, 4, or an odd prime <= 13)
+// radix-4 DFT of a, b, c, d in place (forward for SIGN < 0)
+template <int SIGN>
+__device__ __forceinline__ void dft4(double2& a, double2& b, double2& c, double2& d) {
+    const double2 s0 = make_double2(a.x + c.x, a.y + c.y);
+    const double2 d0 = make_double2(a.x - c.x, a.y - c.y);
+    const double2 s1 = make_double2(b.x + d.x, b.y + d.y);
+    const double2 d1 = make_double2(b.x - d.x, b.y - d.y);
+    // forward: multiply d1 by -i; backward: by +i
+    const double2 e = SIGN < 0 ? make_double2(d1.y, -d1.x) : make_double2(-d1.y, d1.x);
+    a = make_double2(s0.x + s1.x, s0.y + s1.y);
+    c = make_double2(s0.x - s1.x, s0.y - s1.y);
+    b = make_double2(d0.x + e.x, d0.y + e.y);
+    d = make_double2(d0.x - e.x, d0.y - e.y);
+}
+
+// radix-R DFT of v[] in place (R = 2, 4, 8, or an odd prime <= 13)
 template <int R, int SIGN>
 __device__ __forceinline__ void dft_small(double2* v) {
-    if (R == 2) {
+    if (R == 8) {
+        // two radix-4 DFTs of the even and odd samples, then
+        // X_k = E_k + w^k O_k, X_{k+4} = E_k - w^k O_k, w = exp(-+ 2 pi i / 8)
+        double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+        double2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+        dft4<SIGN>(e0, e1, e2, e3);
+        dft4<SIGN>(o0, o1, o2, o3);
+        const double h = 0.70710678118654752440;   // 1/sqrt(2)
+        // w^1 o1, w^2 o2, w^3 o3 with w = (1 -+ i)/sqrt(2)
+        double2 t1, t2, t3;
+        if (SIGN < 0) {
+            t1 = make_double2(h * (o1.x + o1.y), h * (o1.y - o1.x));
+            t2 = make_double2(o2.y, -o2.x);
+            t3 = make_double2(h * (o3.y - o3.x), -h * (o3.x + o3.y));
+        } else {
+            t1 = make_double2(h * (o1.x - o1.y), h * (o1.y + o1.x));
+            t2 = make_double2(-o2.y, o2.x);
+            t3 = make_double2(-h * (o3.x + o3.y), h * (o3.x - o3.y));
+        }
+        v[0] = make_double2(e0.x + o0.x, e0.y + o0.y);
+        v[4] = make_double2(e0.x - o0.x, e0.y - o0.y);
+        v[1] = make_double2(e1.x + t1.x, e1.y + t1.y);
+        v[5] = make_double2(e1.x - t1.x, e1.y - t1.y);
+        v[2] = make_double2(e2.x + t2.x, e2.y + t2.y);
+        v[6] = make_double2(e2.x - t2.x, e2.y - t2.y);
+        v[3] = make_double2(e3.x + t3.x, e3.y + t3.y);
+        v[7] = make_double2(e3.x - t3.x, e3.y - t3.y);
+    } else if (R == 2) {
         const double2 a = v[0], b = v[1];
         v[0] = make_double2(a.x + b.x, a.y + b.y);
         v[1] = make_double2(a.x - b.x, a.y - b.y);
@@ -175,6 +217,7 @@ __device__ __forceinline__ double2* fft_run(double2* a, double2* b, int M, const
             case 2: fft_pass<2, SIGN>(a, b, M, ns, t); break;
             case 3: fft_pass<3, SIGN>(a, b, M, ns, t); break;
             case 4: fft_pass<4, SIGN>(a, b, M, ns, t); break;
+            case 8: fft_pass<8, SIGN>(a, b, M, ns, t); break;
             case 5: fft_pass<5, SIGN>(a, b, M, ns, t); break;
             case 7: fft_pass<7, SIGN>(a, b, M, ns, t); break;
             case 11: fft_pass<11, SIGN>(a, b, M, ns, t); break;

@@ -217,6 +217,7 @@ __global__ void k_ring_weights(const double* __restrict__ q,
 // ---------------------------------------------------------------------------
 static int factor_len(int n, int* fac) {
     int k = 0;
+    while (n % 8 == 0) { fac[k++] = 8; n /= 8; }
     while (n % 4 == 0) { fac[k++] = 4; n /= 4; }
     while (n % 2 == 0) { fac[k++] = 2; n /= 2; }
     for (int p = 3; p <= n; p += 2) {
