@@ -57,6 +57,10 @@ def lib():
         L.orc_preglq_iter.argtypes = [ctypes.c_double, ctypes.c_double, _I,
                                       _D, _D, _I]
         L.orc_dhaj.argtypes = [_I, _D, _I]
+        L.orc_makegrid_dhc.argtypes = [_D, _D, _I, _I, _I, _I, _I, _I, _I]
+        L.orc_shexpand_dhc.argtypes = [_D, _I, _D, _I, _I, _I, _I, _I, _I]
+        L.orc_makegrid_glqc.argtypes = [_D, _D, _I, _I, _D, _I, _I, _I, _I]
+        L.orc_shexpand_glqc.argtypes = [_D, _I, _I, _D, _I, _D, _D, _I, _I, _I]
         L.orc_rec_tables.argtypes = [_I, _I, _D, _D]
         L.orc_fft_c2c.argtypes = [_I, _D, _D, _I]
         L.orc_fft_r2c.argtypes = [_I, _D, _D, _D]
@@ -253,5 +257,79 @@ def power_law_cilm(lmax, seed, beta=2.0):
     c *= np.sqrt((l + 1.0) ** (-beta) / (2 * l + 1.0))[None, :, None]
     mask = l[None, :, None] >= l[None, None, :]
     c = np.where(mask, c, 0.0)
+    c[1, :, 0] = 0.0
+    return c
+
+
+# --------------------------------------------------------------------------
+# Complex transforms (complex128 arrays; cilm[0] the order +m, cilm[1] -m)
+# --------------------------------------------------------------------------
+def _c128(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.complex128))
+
+
+def makegrid_dhc(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
+                 extend=0):
+    """MakeGridDHC (MakeGridDHC.f95:1).  Returns complex (n+extend, sampling*n+extend)."""
+    cilm = _c128(cilm)
+    lmax, lmax_calc = _lmaxes(cilm, lmax, lmax_calc)
+    n = 2 * lmax + 2
+    grid = np.zeros((n + int(extend), sampling * n + int(extend)), dtype=np.complex128)
+    _check(lib().orc_makegrid_dhc(_p(grid), _p(cilm), cilm.shape[1], lmax, int(norm),
+                                  int(sampling), int(csphase), lmax_calc, int(extend)))
+    return grid
+
+
+def shexpand_dhc(grid, norm=1, sampling=1, csphase=1, lmax_calc=None):
+    """SHExpandDHC (SHExpandDHC.f95:1).  Returns complex (2, lmax_calc+1, lmax_calc+1)."""
+    grid = _c128(grid)
+    n = grid.shape[0]
+    if lmax_calc is None:
+        lmax_calc = n // 2 - 1
+    cilm = np.zeros((2, lmax_calc + 1, lmax_calc + 1), dtype=np.complex128)
+    _check(lib().orc_shexpand_dhc(_p(cilm), lmax_calc + 1, _p(grid), n, grid.shape[1],
+                                  int(norm), int(sampling), int(csphase), int(lmax_calc)))
+    return cilm
+
+
+def makegrid_glqc(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
+                  extend=0):
+    """MakeGridGLQC (MakeGridGLQC.f95:1).  Returns complex (lmax+1, 2*lmax+1+extend)."""
+    cilm = _c128(cilm)
+    lmax, lmax_calc = _lmaxes(cilm, lmax, lmax_calc)
+    if zero is None:
+        zero, _ = shglq(lmax)
+    zero = _f64(zero)
+    grid = np.zeros((lmax + 1, 2 * lmax + 1 + int(extend)), dtype=np.complex128)
+    _check(lib().orc_makegrid_glqc(_p(grid), _p(cilm), cilm.shape[1], lmax, _p(zero),
+                                   int(norm), int(csphase), lmax_calc, int(extend)))
+    return grid
+
+
+def shexpand_glqc(grid, w=None, zero=None, norm=1, csphase=1, lmax_calc=None):
+    """SHExpandGLQC (SHExpandGLQC.f95:1).  Returns complex (2, lmax_calc+1, lmax_calc+1)."""
+    grid = _c128(grid)
+    lmax = grid.shape[0] - 1
+    if zero is None or w is None:
+        zero, w = shglq(lmax)
+    zero = _f64(zero)
+    w = _f64(w)
+    if lmax_calc is None:
+        lmax_calc = lmax
+    cilm = np.zeros((2, lmax_calc + 1, lmax_calc + 1), dtype=np.complex128)
+    _check(lib().orc_shexpand_glqc(_p(cilm), lmax_calc + 1, lmax, _p(grid), grid.shape[1],
+                                   _p(w), _p(zero), int(norm), int(csphase),
+                                   int(lmax_calc)))
+    return cilm
+
+
+def power_law_cilm_complex(L, seed, beta=2.0):
+    """Seeded complex coefficients (2, L+1, L+1) with per-degree power
+    S(l) = (l+1)^-beta; cilm[1, :, 0] (order -0) is zero."""
+    rng = np.random.default_rng(seed)
+    c = rng.standard_normal((2, L + 1, L + 1)) + 1j * rng.standard_normal((2, L + 1, L + 1))
+    l = np.arange(L + 1)
+    c *= np.sqrt((l + 1.0) ** -beta / (2 * (2 * l + 1.0)))[None, :, None]
+    c = np.where(l[:, None] >= l[None, :], c, 0.0)
     c[1, :, 0] = 0.0
     return c

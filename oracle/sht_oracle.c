@@ -20,6 +20,8 @@
  *   SHExpandGLQ ............. src/SHExpandGLQ.f95:98-691  (on-the-fly branch)
  *   PreGLQ .................. src/PreGLQ.f95:54-151
  *   DHaj .................... src/DHaj.f95:41-107
+ *   complex transforms ...... src/MakeGridDHC.f95, SHExpandDHC.f95,
+ *                             MakeGridGLQC.f95, SHExpandGLQC.f95
  *
  * FFTW (third-party, not vendored; environment.yml pins fftw>=3.3.8) is
  * replaced by the project-written FFT below: unnormalised DFTs with the
@@ -1101,6 +1103,535 @@ int orc_shexpand_glq_window(double *cilm, int cdim, int lmax, const double *grid
                             int pair_hi) {
     return shexpand_glq_impl(cilm, cdim, lmax, grid, ncols, w, zero, norm,
                              csphase, lmax_calc, pair_lo, pair_hi);
+}
+
+/* ======================================================================== */
+/*  Complex transforms                                                      */
+/*    MakeGridDHC  ........ src/MakeGridDHC.f95:100-643                      */
+/*    SHExpandDHC  ........ src/SHExpandDHC.f95:100-725                      */
+/*    MakeGridGLQC ........ src/MakeGridGLQC.f95 (on-the-fly branch)         */
+/*    SHExpandGLQC ........ src/SHExpandGLQC.f95 (on-the-fly branch)         */
+/*  cilm[k][l][m][re/im] (2, cdim, cdim) complex: k = 0 the order +m, k = 1  */
+/*  the order -m (Y*_lm = (-1)^m Y_l,-m); grids [i][j][re/im].  The tables  */
+/*  ff1/ff2 are those of the real transforms; the sectoral start omits the  */
+/*  real transforms' sqrt(2), and the norm-3 divisors omit their 1/2.       */
+/*  Longitude transforms are complex DFTs of length nlong (FFTW backward    */
+/*  for synthesis, forward for analysis, both unnormalised).                */
+/* ======================================================================== */
+
+#define CCR(k, l, m) cilm[((((size_t)(k) * cdim + (size_t)(l)) * cdim + (size_t)(m)) * 2)]
+#define CCI(k, l, m) cilm[((((size_t)(k) * cdim + (size_t)(l)) * cdim + (size_t)(m)) * 2) + 1]
+
+static double pmm_start_c(int norm) {
+    const double pi = acos(-1.0);
+    return norm == 4 ? SCALEF / sqrt(4.0 * pi) : SCALEF;   /* no sqr(2) */
+}
+
+/* pmm update of the sectoral recursion; returns pm2 (the m-th start value) */
+static double pmm_step(const rec_tab *t, int phase, int m, double *pmm) {
+    const double *sqr = t->sqr;
+    switch (t->norm) {
+        case 1: case 4:
+            *pmm = phase * *pmm * sqr[2 * m + 1] / sqr[2 * m];
+            return *pmm;
+        case 2:
+            *pmm = phase * *pmm * sqr[2 * m + 1] / sqr[2 * m];
+            return *pmm / sqr[2 * m + 1];
+        default:
+            *pmm = phase * *pmm * (double)(2 * m - 1);
+            return *pmm;
+    }
+}
+
+/* pmm of m = lc, times rescalem (the closing term of every latitude) */
+static double pmm_last(const rec_tab *t, int phase, double pmm, double rescalem) {
+    const double *sqr = t->sqr;
+    const int lc = t->lc;
+    switch (t->norm) {
+        case 1: case 4: return phase * pmm * sqr[2 * lc + 1] / sqr[2 * lc] * rescalem;
+        case 2: return phase * pmm / sqr[2 * lc] * rescalem;
+        default: return phase * pmm * (double)(2 * lc - 1) * rescalem;
+    }
+}
+
+static double msign(int m) { return (m % 2 == 0) ? 1.0 : -1.0; }
+
+/* Synthesis of one ring pair (MakeGridDHC.f95:530-620): coef (north) and
+ * coefs (south), complex arrays of length nlong, zero on entry. */
+static void synthc_ring(const rec_tab *t, const double *cilm, int cdim, int phase,
+                        double z, double u, int nlong, double *cr, double *ci,
+                        double *sr, double *si) {
+    const int lc = t->lc, d = lc + 1, norm = t->norm;
+    const double *ff1 = t->ff1, *ff2 = t->ff2;
+    double pm2, pm1, p, pmm, rescalem, tr, ti;
+
+    pm2 = p00(norm);
+    tr = CCR(0, 0, 0) * pm2; ti = CCI(0, 0, 0) * pm2;
+    cr[0] += tr; ci[0] += ti;
+    sr[0] += tr; si[0] += ti;
+
+    pm1 = ff1[(size_t)1 * d + 0] * z * pm2;
+    tr = CCR(0, 1, 0) * pm1; ti = CCI(0, 1, 0) * pm1;
+    cr[0] += tr; ci[0] += ti;
+    sr[0] -= tr; si[0] -= ti;
+
+    for (int l = 2; l <= lc; ++l) {
+        p = ff1[(size_t)l * d + 0] * z * pm1 - ff2[(size_t)l * d + 0] * pm2;
+        tr = CCR(0, l, 0) * p; ti = CCI(0, l, 0) * p;
+        cr[0] += tr; ci[0] += ti;
+        const double fs = (l % 2 == 0) ? 1.0 : -1.0;
+        sr[0] += tr * fs; si[0] += ti * fs;
+        pm2 = pm1;
+        pm1 = p;
+    }
+
+    pmm = pmm_start_c(norm);
+    rescalem = 1.0 / SCALEF;
+    for (int m = 1; m <= lc - 1; ++m) {
+        const int mn = nlong - m;            /* Fortran nlong-(m-1), 0-based */
+        rescalem = rescalem * u;
+        pm2 = pmm_step(t, phase, m, &pmm);
+
+        tr = CCR(0, m, m) * pm2; ti = CCI(0, m, m) * pm2;
+        cr[m] += tr; ci[m] += ti; sr[m] += tr; si[m] += ti;
+        tr = CCR(1, m, m) * pm2; ti = CCI(1, m, m) * pm2;
+        cr[mn] += tr; ci[mn] += ti; sr[mn] += tr; si[mn] += ti;
+
+        pm1 = z * ff1[(size_t)(m + 1) * d + m] * pm2;
+        tr = CCR(0, m + 1, m) * pm1; ti = CCI(0, m + 1, m) * pm1;
+        cr[m] += tr; ci[m] += ti; sr[m] -= tr; si[m] -= ti;
+        tr = CCR(1, m + 1, m) * pm1; ti = CCI(1, m + 1, m) * pm1;
+        cr[mn] += tr; ci[mn] += ti; sr[mn] -= tr; si[mn] -= ti;
+
+        for (int l = m + 2; l <= lc; ++l) {
+            p = z * ff1[(size_t)l * d + m] * pm1 - ff2[(size_t)l * d + m] * pm2;
+            pm2 = pm1;
+            pm1 = p;
+            const double fs = ((l - m) % 2 == 0) ? 1.0 : -1.0;
+            tr = CCR(0, l, m) * p; ti = CCI(0, l, m) * p;
+            cr[m] += tr; ci[m] += ti; sr[m] += tr * fs; si[m] += ti * fs;
+            tr = CCR(1, l, m) * p; ti = CCI(1, l, m) * p;
+            cr[mn] += tr; ci[mn] += ti; sr[mn] += tr * fs; si[mn] += ti * fs;
+        }
+        cr[m] = cr[m] * rescalem; ci[m] = ci[m] * rescalem;
+        sr[m] = sr[m] * rescalem; si[m] = si[m] * rescalem;
+        cr[mn] = cr[mn] * rescalem * msign(m); ci[mn] = ci[mn] * rescalem * msign(m);
+        sr[mn] = sr[mn] * rescalem * msign(m); si[mn] = si[mn] * rescalem * msign(m);
+    }
+
+    rescalem = rescalem * u;
+    pmm = pmm_last(t, phase, pmm, rescalem);
+    tr = CCR(0, lc, lc) * pmm; ti = CCI(0, lc, lc) * pmm;
+    cr[lc] += tr; ci[lc] += ti; sr[lc] += tr; si[lc] += ti;
+    tr = CCR(1, lc, lc) * pmm * msign(lc); ti = CCI(1, lc, lc) * pmm * msign(lc);
+    cr[nlong - lc] += tr; ci[nlong - lc] += ti;
+    sr[nlong - lc] += tr; si[nlong - lc] += ti;
+}
+
+/* Equator ring (MakeGridDHC.f95:424-497): z = 0, even l-m only */
+static void synthc_equator(const rec_tab *t, const double *cilm, int cdim, int phase,
+                           int nlong, double *cr, double *ci) {
+    const int lc = t->lc, d = lc + 1, norm = t->norm;
+    const double *ff2 = t->ff2;
+    double pm2, p, pmm, rescalem;
+
+    pm2 = p00(norm);
+    cr[0] += CCR(0, 0, 0) * pm2; ci[0] += CCI(0, 0, 0) * pm2;
+    for (int l = 2; l <= lc; l += 2) {
+        p = -ff2[(size_t)l * d + 0] * pm2;
+        pm2 = p;
+        cr[0] += CCR(0, l, 0) * p; ci[0] += CCI(0, l, 0) * p;
+    }
+    pmm = pmm_start_c(norm);
+    rescalem = 1.0 / SCALEF;
+    for (int m = 1; m <= lc - 1; ++m) {
+        const int mn = nlong - m;
+        pm2 = pmm_step(t, phase, m, &pmm);
+        cr[m] += CCR(0, m, m) * pm2; ci[m] += CCI(0, m, m) * pm2;
+        cr[mn] += CCR(1, m, m) * pm2; ci[mn] += CCI(1, m, m) * pm2;
+        for (int l = m + 2; l <= lc; l += 2) {
+            p = -ff2[(size_t)l * d + m] * pm2;
+            cr[m] += CCR(0, l, m) * p; ci[m] += CCI(0, l, m) * p;
+            cr[mn] += CCR(1, l, m) * p; ci[mn] += CCI(1, l, m) * p;
+            pm2 = p;
+        }
+        cr[m] = cr[m] * rescalem; ci[m] = ci[m] * rescalem;
+        cr[mn] = cr[mn] * rescalem * msign(m); ci[mn] = ci[mn] * rescalem * msign(m);
+    }
+    pmm = pmm_last(t, phase, pmm, rescalem);
+    cr[lc] += CCR(0, lc, lc) * pmm; ci[lc] += CCI(0, lc, lc) * pmm;
+    cr[nlong - lc] += CCR(1, lc, lc) * pmm * msign(lc);
+    ci[nlong - lc] += CCI(1, lc, lc) * pmm * msign(lc);
+}
+
+/* Analysis of one ring pair (SHExpandDHC.f95:552-658); f1/f2 are the
+ * weighted complex spectra of the north / south rings (length nlong),
+ * rescaled in place as in Fortran. */
+static void analc_ring(const rec_tab *t, double *cilm, int cdim, int phase, double z,
+                       double u, int nlong, double *f1r, double *f1i, double *f2r,
+                       double *f2i) {
+    const int lc = t->lc, d = lc + 1, norm = t->norm;
+    const double *ff1 = t->ff1, *ff2 = t->ff2;
+    double pm2, pm1, p, pmm, rescalem;
+    double a1r[2], a1i[2], a2r[2], a2i[2];   /* [0]: fsymsign -1, [1]: +1 */
+
+    pm2 = p00(norm);
+    CCR(0, 0, 0) += pm2 * (f1r[0] + f2r[0]);
+    CCI(0, 0, 0) += pm2 * (f1i[0] + f2i[0]);
+    if (lc == 0) return;
+    pm1 = ff1[(size_t)1 * d + 0] * z * pm2;
+    CCR(0, 1, 0) += pm1 * (f1r[0] - f2r[0]);
+    CCI(0, 1, 0) += pm1 * (f1i[0] - f2i[0]);
+    a1r[0] = f1r[0] - f2r[0]; a1i[0] = f1i[0] - f2i[0];
+    a1r[1] = f1r[0] + f2r[0]; a1i[1] = f1i[0] + f2i[0];
+    for (int l = 2; l <= lc; ++l) {
+        p = ff1[(size_t)l * d + 0] * z * pm1 - ff2[(size_t)l * d + 0] * pm2;
+        pm2 = pm1;
+        pm1 = p;
+        const int s = (l % 2 == 0) ? 1 : 0;
+        CCR(0, l, 0) += p * a1r[s];
+        CCI(0, l, 0) += p * a1i[s];
+    }
+    pmm = pmm_start_c(norm);
+    rescalem = 1.0 / SCALEF;
+    for (int m = 1; m <= lc - 1; ++m) {
+        const int mn = nlong - m;
+        rescalem = rescalem * u;
+        pm2 = pmm_step(t, phase, m, &pmm);
+        f1r[m] = f1r[m] * rescalem; f1i[m] = f1i[m] * rescalem;
+        f1r[mn] = f1r[mn] * rescalem * msign(m); f1i[mn] = f1i[mn] * rescalem * msign(m);
+        f2r[m] = f2r[m] * rescalem; f2i[m] = f2i[m] * rescalem;
+        f2r[mn] = f2r[mn] * rescalem * msign(m); f2i[mn] = f2i[mn] * rescalem * msign(m);
+
+        CCR(0, m, m) += pm2 * (f1r[m] + f2r[m]);
+        CCI(0, m, m) += pm2 * (f1i[m] + f2i[m]);
+        CCR(1, m, m) += pm2 * (f1r[mn] + f2r[mn]);
+        CCI(1, m, m) += pm2 * (f1i[mn] + f2i[mn]);
+
+        pm1 = z * ff1[(size_t)(m + 1) * d + m] * pm2;
+        CCR(0, m + 1, m) += pm1 * (f1r[m] - f2r[m]);
+        CCI(0, m + 1, m) += pm1 * (f1i[m] - f2i[m]);
+        CCR(1, m + 1, m) += pm1 * (f1r[mn] - f2r[mn]);
+        CCI(1, m + 1, m) += pm1 * (f1i[mn] - f2i[mn]);
+
+        a1r[0] = f1r[m] - f2r[m]; a1i[0] = f1i[m] - f2i[m];
+        a1r[1] = f1r[m] + f2r[m]; a1i[1] = f1i[m] + f2i[m];
+        a2r[0] = f1r[mn] - f2r[mn]; a2i[0] = f1i[mn] - f2i[mn];
+        a2r[1] = f1r[mn] + f2r[mn]; a2i[1] = f1i[mn] + f2i[mn];
+        for (int l = m + 2; l <= lc; ++l) {
+            p = z * ff1[(size_t)l * d + m] * pm1 - ff2[(size_t)l * d + m] * pm2;
+            pm2 = pm1;
+            pm1 = p;
+            const int s = ((l - m) % 2 == 0) ? 1 : 0;
+            CCR(0, l, m) += p * a1r[s]; CCI(0, l, m) += p * a1i[s];
+            CCR(1, l, m) += p * a2r[s]; CCI(1, l, m) += p * a2i[s];
+        }
+    }
+    rescalem = rescalem * u;
+    pmm = pmm_last(t, phase, pmm, rescalem);
+    CCR(0, lc, lc) += pmm * (f1r[lc] + f2r[lc]);
+    CCI(0, lc, lc) += pmm * (f1i[lc] + f2i[lc]);
+    CCR(1, lc, lc) += msign(lc) * pmm * (f1r[nlong - lc] + f2r[nlong - lc]);
+    CCI(1, lc, lc) += msign(lc) * pmm * (f1i[nlong - lc] + f2i[nlong - lc]);
+}
+
+/* Equator ring of the analysis (SHExpandDHC.f95:465-548) */
+static void analc_equator(const rec_tab *t, double *cilm, int cdim, int phase,
+                          int nlong, double *f1r, double *f1i) {
+    const int lc = t->lc, d = lc + 1, norm = t->norm;
+    const double *ff2 = t->ff2;
+    double pm2, p, pmm, rescalem;
+    pm2 = p00(norm);
+    CCR(0, 0, 0) += pm2 * f1r[0];
+    CCI(0, 0, 0) += pm2 * f1i[0];
+    if (lc == 0) return;
+    for (int l = 2; l <= lc; l += 2) {
+        p = -ff2[(size_t)l * d + 0] * pm2;
+        pm2 = p;
+        CCR(0, l, 0) += p * f1r[0];
+        CCI(0, l, 0) += p * f1i[0];
+    }
+    pmm = pmm_start_c(norm);
+    rescalem = 1.0 / SCALEF;
+    for (int m = 1; m <= lc - 1; ++m) {
+        const int mn = nlong - m;
+        pm2 = pmm_step(t, phase, m, &pmm);
+        f1r[m] = f1r[m] * rescalem; f1i[m] = f1i[m] * rescalem;
+        f1r[mn] = f1r[mn] * rescalem * msign(m); f1i[mn] = f1i[mn] * rescalem * msign(m);
+        CCR(0, m, m) += pm2 * f1r[m]; CCI(0, m, m) += pm2 * f1i[m];
+        CCR(1, m, m) += pm2 * f1r[mn]; CCI(1, m, m) += pm2 * f1i[mn];
+        for (int l = m + 2; l <= lc; l += 2) {
+            p = -ff2[(size_t)l * d + m] * pm2;
+            pm2 = p;
+            CCR(0, l, m) += p * f1r[m]; CCI(0, l, m) += p * f1i[m];
+            CCR(1, l, m) += p * f1r[mn]; CCI(1, l, m) += p * f1i[mn];
+        }
+    }
+    pmm = pmm_last(t, phase, pmm, rescalem);
+    CCR(0, lc, lc) += pmm * f1r[lc];
+    CCI(0, lc, lc) += pmm * f1i[lc];
+    CCR(1, lc, lc) += msign(lc) * pmm * f1r[nlong - lc];
+    CCI(1, lc, lc) += msign(lc) * pmm * f1i[nlong - lc];
+}
+
+/* Divide by the integral of Ylm Ylm* (SHExpandDHC.f95:689-723) */
+static void analc_normalise(double *cilm, int cdim, int lc, int norm) {
+    const double pi = acos(-1.0);
+    for (int l = 0; l <= lc; ++l) {
+        if (norm == 1 || norm == 2) {
+            for (int k = 0; k < 2; ++k)
+                for (int m = 0; m <= l; ++m) {
+                    if (norm == 1) {
+                        CCR(k, l, m) = CCR(k, l, m) / (4 * pi);
+                        CCI(k, l, m) = CCI(k, l, m) / (4 * pi);
+                    } else {
+                        CCR(k, l, m) = CCR(k, l, m) * (2 * l + 1) / (4 * pi);
+                        CCI(k, l, m) = CCI(k, l, m) * (2 * l + 1) / (4 * pi);
+                    }
+                }
+        } else if (norm == 3) {
+            double prod = 4 * pi / (double)(2 * l + 1);
+            CCR(0, l, 0) = CCR(0, l, 0) / prod;
+            CCI(0, l, 0) = CCI(0, l, 0) / prod;
+            for (int m = 1; m <= l - 1; ++m) {
+                prod = prod * (l + m) * (l - m + 1);
+                for (int k = 0; k < 2; ++k) {
+                    CCR(k, l, m) = CCR(k, l, m) / prod;
+                    CCI(k, l, m) = CCI(k, l, m) / prod;
+                }
+            }
+            if (l != 0)
+                for (int k = 0; k < 2; ++k) {
+                    CCR(k, l, l) = CCR(k, l, l) / (prod * 2 * l);
+                    CCI(k, l, l) = CCI(k, l, l) / (prod * 2 * l);
+                }
+        }
+    }
+}
+
+/* writes the backward DFT of (cr, ci) into grid row `row` (complex, ncols) */
+static void c2c_row(orc_fft *plan, int nlong, double *cr, double *ci, double *grid,
+                    int row, int ncols) {
+    orc_fft_exec(plan, cr, ci, +1);
+    for (int j = 0; j < nlong; ++j) {
+        grid[((size_t)row * ncols + j) * 2] = cr[j];
+        grid[((size_t)row * ncols + j) * 2 + 1] = ci[j];
+    }
+}
+
+int orc_makegrid_dhc(double *grid, const double *cilm, int cdim, int lmax, int norm,
+                     int sampling, int csphase, int lmax_calc, int extend) {
+    if (sampling != 1 && sampling != 2) return ORC_EBOUND;
+    if (extend != 0 && extend != 1) return ORC_EBOUND;
+    if (norm < 1 || norm > 4) return ORC_EBOUND;
+    if (csphase != 1 && csphase != -1) return ORC_EBOUND;
+    if (lmax_calc > lmax) return ORC_EBOUND;
+    const int n = 2 * lmax + 2;
+    const int nlong = sampling == 1 ? n : 2 * n;
+    const int nlat_out = n + extend, nlong_out = nlong + extend;
+    int lc = lmax_calc < 0 ? lmax : lmax_calc;
+    if (lc > cdim - 1) lc = cdim - 1;
+    const double pi = acos(-1.0);
+    if (lc == 0) {
+        const double pm2 = p00(norm);
+        for (int i = 0; i < nlat_out; ++i)
+            for (int j = 0; j < nlong_out; ++j) {
+                grid[((size_t)i * nlong_out + j) * 2] = CCR(0, 0, 0) * pm2;
+                grid[((size_t)i * nlong_out + j) * 2 + 1] = CCI(0, 0, 0) * pm2;
+            }
+        return ORC_OK;
+    }
+    rec_tab t;
+    if (rec_build(&t, lc, norm)) return ORC_EALLOC;
+    orc_fft *plan = fft_plan(nlong);
+    double *cr = malloc(sizeof(double) * (size_t)nlong), *ci = malloc(sizeof(double) * (size_t)nlong);
+    double *sr = malloc(sizeof(double) * (size_t)nlong), *si = malloc(sizeof(double) * (size_t)nlong);
+    const int i_eq = n / 2 + 1;   /* 1-based */
+    memset(cr, 0, sizeof(double) * (size_t)nlong); memset(ci, 0, sizeof(double) * (size_t)nlong);
+    synthc_equator(&t, cilm, cdim, csphase, nlong, cr, ci);
+    c2c_row(plan, nlong, cr, ci, grid, i_eq - 1, nlong_out);
+    for (int i = 1; i <= i_eq - 1; ++i) {
+        const int i_s = 2 * i_eq - i;
+        const double theta = pi * (double)(i - 1) / (double)n;
+        const double z = cos(theta);
+        const double u = sqrt((1.0 - z) * (1.0 + z));
+        memset(cr, 0, sizeof(double) * (size_t)nlong); memset(ci, 0, sizeof(double) * (size_t)nlong);
+        memset(sr, 0, sizeof(double) * (size_t)nlong); memset(si, 0, sizeof(double) * (size_t)nlong);
+        synthc_ring(&t, cilm, cdim, csphase, z, u, nlong, cr, ci, sr, si);
+        c2c_row(plan, nlong, cr, ci, grid, i - 1, nlong_out);
+        if (!(i == 1 && extend == 0)) c2c_row(plan, nlong, sr, si, grid, i_s - 1, nlong_out);
+    }
+    if (extend == 1)
+        for (int i = 0; i < nlat_out; ++i) {
+            grid[((size_t)i * nlong_out + nlong) * 2] = grid[((size_t)i * nlong_out) * 2];
+            grid[((size_t)i * nlong_out + nlong) * 2 + 1] = grid[((size_t)i * nlong_out) * 2 + 1];
+        }
+    free(cr); free(ci); free(sr); free(si);
+    fft_free(plan);
+    rec_free(&t);
+    return ORC_OK;
+}
+
+/* forward DFT of complex grid row `row` times scale: out = cc * s */
+static void row_spectrum(orc_fft *plan, const double *grid, int row, int ncols, int nlong,
+                         double *fr, double *fi) {
+    for (int j = 0; j < nlong; ++j) {
+        fr[j] = grid[((size_t)row * ncols + j) * 2];
+        fi[j] = grid[((size_t)row * ncols + j) * 2 + 1];
+    }
+    orc_fft_exec(plan, fr, fi, -1);
+}
+
+int orc_shexpand_dhc(double *cilm, int cdim, const double *grid, int n, int ncols,
+                     int norm, int sampling, int csphase, int lmax_calc) {
+    const int lmax = n / 2 - 1;
+    int lc = lmax_calc < 0 ? lmax : lmax_calc;
+    if (lc > lmax) return ORC_EBOUND;
+    if (sampling != 1 && sampling != 2) return ORC_EBOUND;
+    if (n % 2 != 0) return ORC_EBOUND;
+    if (cdim < lc + 1) return ORC_EDIM;
+    const int nlong = sampling == 1 ? n : 2 * n;
+    if (ncols < nlong) return ORC_EDIM;
+    if (csphase != 1 && csphase != -1) return ORC_EBOUND;
+    if (norm < 1 || norm > 4) return ORC_EBOUND;
+    const double pi = acos(-1.0);
+    memset(cilm, 0, sizeof(double) * 4 * (size_t)cdim * cdim);
+    double *aj = malloc(sizeof(double) * (size_t)n);
+    orc_dhaj(n, aj, 0);
+    for (int i = 0; i < n; ++i) aj[i] = aj[i] * sqrt(4.0 * pi);
+    rec_tab t;
+    if (rec_build(&t, lc, norm)) { free(aj); return ORC_EALLOC; }
+    orc_fft *plan = fft_plan(nlong);
+    double *f1r = malloc(sizeof(double) * (size_t)nlong), *f1i = malloc(sizeof(double) * (size_t)nlong);
+    double *f2r = malloc(sizeof(double) * (size_t)nlong), *f2i = malloc(sizeof(double) * (size_t)nlong);
+    const int i_eq = n / 2 + 1;
+    const double s2p = sqrt(2 * pi);
+    /* equator first (SHExpandDHC.f95:465) */
+    row_spectrum(plan, grid, i_eq - 1, ncols, nlong, f1r, f1i);
+    for (int k = 0; k < nlong; ++k) {
+        f1r[k] = f1r[k] * s2p * aj[i_eq - 1] / (double)nlong;
+        f1i[k] = f1i[k] * s2p * aj[i_eq - 1] / (double)nlong;
+    }
+    analc_equator(&t, cilm, cdim, csphase, nlong, f1r, f1i);
+    for (int i = 2; i <= i_eq - 1; ++i) {
+        const double theta = (i - 1) * pi / (double)n;
+        const double z = cos(theta);
+        const double u = sqrt((1.0 - z) * (1.0 + z));
+        const int i_s = 2 * i_eq - i;
+        row_spectrum(plan, grid, i - 1, ncols, nlong, f1r, f1i);
+        row_spectrum(plan, grid, i_s - 1, ncols, nlong, f2r, f2i);
+        for (int k = 0; k < nlong; ++k) {
+            f1r[k] = f1r[k] * s2p * aj[i - 1] / (double)nlong;
+            f1i[k] = f1i[k] * s2p * aj[i - 1] / (double)nlong;
+            f2r[k] = f2r[k] * s2p * aj[i_s - 1] / (double)nlong;
+            f2i[k] = f2i[k] * s2p * aj[i_s - 1] / (double)nlong;
+        }
+        analc_ring(&t, cilm, cdim, csphase, z, u, nlong, f1r, f1i, f2r, f2i);
+    }
+    analc_normalise(cilm, cdim, lc, norm);
+    free(aj); free(f1r); free(f1i); free(f2r); free(f2i);
+    fft_free(plan);
+    rec_free(&t);
+    return ORC_OK;
+}
+
+int orc_makegrid_glqc(double *grid, const double *cilm, int cdim, int lmax,
+                      const double *zero, int norm, int csphase, int lmax_calc,
+                      int extend) {
+    if (extend != 0 && extend != 1) return ORC_EBOUND;
+    if (!zero) return ORC_ECONV;
+    if (norm < 1 || norm > 4) return ORC_EBOUND;
+    if (csphase != 1 && csphase != -1) return ORC_EBOUND;
+    if (lmax_calc > lmax) return ORC_EBOUND;
+    const int nlong = 2 * lmax + 1, nlat = lmax + 1;
+    const int nlong_out = nlong + extend;
+    int lc = lmax_calc < 0 ? lmax : lmax_calc;
+    if (lc > cdim - 1) lc = cdim - 1;
+    if (lc == 0) {
+        const double pm2 = p00(norm);
+        for (int i = 0; i < nlat; ++i)
+            for (int j = 0; j < nlong_out; ++j) {
+                grid[((size_t)i * nlong_out + j) * 2] = CCR(0, 0, 0) * pm2;
+                grid[((size_t)i * nlong_out + j) * 2 + 1] = CCI(0, 0, 0) * pm2;
+            }
+        return ORC_OK;
+    }
+    rec_tab t;
+    if (rec_build(&t, lc, norm)) return ORC_EALLOC;
+    orc_fft *plan = fft_plan(nlong);
+    double *cr = malloc(sizeof(double) * (size_t)nlong), *ci = malloc(sizeof(double) * (size_t)nlong);
+    double *sr = malloc(sizeof(double) * (size_t)nlong), *si = malloc(sizeof(double) * (size_t)nlong);
+    for (int i = 1; i <= (nlat + 1) / 2; ++i) {
+        memset(cr, 0, sizeof(double) * (size_t)nlong); memset(ci, 0, sizeof(double) * (size_t)nlong);
+        memset(sr, 0, sizeof(double) * (size_t)nlong); memset(si, 0, sizeof(double) * (size_t)nlong);
+        if (i == (nlat + 1) / 2 && nlat % 2 != 0) {
+            synthc_equator(&t, cilm, cdim, csphase, nlong, cr, ci);
+            c2c_row(plan, nlong, cr, ci, grid, i - 1, nlong_out);
+        } else {
+            const double z = zero[i - 1];
+            const double u = sqrt((1.0 - z) * (1.0 + z));
+            const int i_s = nlat + 1 - i;
+            synthc_ring(&t, cilm, cdim, csphase, z, u, nlong, cr, ci, sr, si);
+            c2c_row(plan, nlong, cr, ci, grid, i - 1, nlong_out);
+            c2c_row(plan, nlong, sr, si, grid, i_s - 1, nlong_out);
+        }
+    }
+    if (extend == 1)
+        for (int i = 0; i < nlat; ++i) {
+            grid[((size_t)i * nlong_out + nlong) * 2] = grid[((size_t)i * nlong_out) * 2];
+            grid[((size_t)i * nlong_out + nlong) * 2 + 1] = grid[((size_t)i * nlong_out) * 2 + 1];
+        }
+    free(cr); free(ci); free(sr); free(si);
+    fft_free(plan);
+    rec_free(&t);
+    return ORC_OK;
+}
+
+int orc_shexpand_glqc(double *cilm, int cdim, int lmax, const double *grid, int ncols,
+                      const double *w, const double *zero, int norm, int csphase,
+                      int lmax_calc) {
+    int lc = lmax_calc < 0 ? lmax : lmax_calc;
+    if (lc > lmax) return ORC_EBOUND;
+    if (cdim < lc + 1) return ORC_EDIM;
+    if (ncols < 2 * lmax + 1) return ORC_EDIM;
+    if (!zero) return ORC_ECONV;
+    if (norm < 1 || norm > 4) return ORC_EBOUND;
+    if (csphase != 1 && csphase != -1) return ORC_EBOUND;
+    const int nlong = 2 * (lmax + 1) - 1, nlat = lmax + 1;
+    const double pi = acos(-1.0);
+    memset(cilm, 0, sizeof(double) * 4 * (size_t)cdim * cdim);
+    rec_tab t;
+    if (rec_build(&t, lc, norm)) return ORC_EALLOC;
+    orc_fft *plan = fft_plan(nlong);
+    double *f1r = malloc(sizeof(double) * (size_t)nlong), *f1i = malloc(sizeof(double) * (size_t)nlong);
+    double *f2r = malloc(sizeof(double) * (size_t)nlong), *f2i = malloc(sizeof(double) * (size_t)nlong);
+    for (int i = 1; i <= (nlat + 1) / 2; ++i) {
+        row_spectrum(plan, grid, i - 1, ncols, nlong, f1r, f1i);
+        for (int k = 0; k < nlong; ++k) {
+            const double s = 2 * w[i - 1] * pi;
+            f1r[k] = s * f1r[k] / (double)nlong;
+            f1i[k] = s * f1i[k] / (double)nlong;
+        }
+        if (i == (nlat + 1) / 2 && nlat % 2 != 0) {
+            analc_equator(&t, cilm, cdim, csphase, nlong, f1r, f1i);
+        } else {
+            const double z = zero[i - 1];
+            const double u = sqrt((1.0 - z) * (1.0 + z));
+            const int i_s = nlat + 1 - i;
+            row_spectrum(plan, grid, i_s - 1, ncols, nlong, f2r, f2i);
+            for (int k = 0; k < nlong; ++k) {
+                const double s = 2 * w[i_s - 1] * pi;
+                f2r[k] = s * f2r[k] / (double)nlong;
+                f2i[k] = s * f2i[k] / (double)nlong;
+            }
+            analc_ring(&t, cilm, cdim, csphase, z, u, nlong, f1r, f1i, f2r, f2i);
+        }
+    }
+    analc_normalise(cilm, cdim, lc, norm);
+    free(f1r); free(f1i); free(f2r); free(f2i);
+    fft_free(plan);
+    rec_free(&t);
+    return ORC_OK;
 }
 
 /* Number of host threads OpenMP would use (1 when built without OpenMP). */
