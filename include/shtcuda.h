@@ -77,11 +77,20 @@ SHTC_API int shtc_plan_create_glq(shtc_plan** plan, int lmax, const double* zero
                          const double* w, int lmax_calc, int norm, int csphase,
                          int extend, void* stream);
 
+/* Plans of the complex transforms (MakeGridDHC.f95:100-160,
+ * MakeGridGLQC.f95): same grids and arguments as above; the transforms on
+ * them are shtc_synthesis_c / shtc_analysis_c. */
+SHTC_API int shtc_plan_create_dhc(shtc_plan** plan, int lmax, int sampling, int lmax_calc,
+                                  int norm, int csphase, int extend, void* stream);
+SHTC_API int shtc_plan_create_glqc(shtc_plan** plan, int lmax, const double* zero,
+                                   const double* w, int lmax_calc, int norm, int csphase,
+                                   int extend, void* stream);
+
 SHTC_API int shtc_plan_destroy(shtc_plan* plan);
 
 /* info[0..15] = kind, lmax, lmax_comp, norm, csphase, sampling, extend,
  * nlat, nlon, nlat_out, nlon_out, npair, nlm, device_bytes, bluestein,
- * fft_mode */
+ * fft_mode (2 for the plans of the complex transforms) */
 SHTC_API int shtc_plan_info(const shtc_plan* plan, long long* info, int ninfo);
 
 /* Tile shapes of the Legendre kernels (no counterpart in the reference):
@@ -238,6 +247,27 @@ SHTC_API int shtc_timing_enable(int on);
 SHTC_API int shtc_timing_collect(double* ms, int* counts, int nstages);
 
 /* ------------------------------------------------------------------------ */
+/* Complex transforms on device buffers (plans from shtc_plan_create_dhc /  */
+/* _glqc).  cilm and grid hold interleaved complex doubles (the layout of   */
+/* double _Complex); strides are in complex elements.                       */
+/*   cilm: (f, k, l, m), k = 0 the order +m, k = 1 the order -m             */
+/*         (Y*_lm = (-1)^m Y_l,-m; cilm[k=1][l][0] is ignored / returned 0).*/
+/* The workspace is shtc_workspace_bytes(plan, nfield) of the complex plan. */
+/* ------------------------------------------------------------------------ */
+
+/* MakeGridDHC / MakeGridGLQC (src/MakeGridDHC.f95:1, src/MakeGridGLQC.f95:1) */
+SHTC_API int shtc_synthesis_c(const shtc_plan* plan, const void* cilm, long long csf,
+                              long long csk, long long csl, long long csm, int cilm_dim,
+                              void* grid, long long gsf, long long gsr, long long gsc,
+                              int nfield, void* work, size_t work_bytes, void* stream);
+
+/* SHExpandDHC / SHExpandGLQC (src/SHExpandDHC.f95:1, src/SHExpandGLQC.f95:1) */
+SHTC_API int shtc_analysis_c(const shtc_plan* plan, const void* grid, long long gsf,
+                             long long gsr, long long gsc, void* cilm, long long csf,
+                             long long csk, long long csl, long long csm, int cilm_dim,
+                             int nfield, void* work, size_t work_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Drop-ins of the reference C interface, include/shtools.h.  Host arrays,  */
 /* Fortran column-major: cilm(2, cilm_dim, cilm_dim), grid(d0, d1).  NULL  */
 /* optional arguments take the reference defaults.  The plx arguments of   */
@@ -256,6 +286,40 @@ SHTC_API void SHExpandDH(const double* grid, const int grid_d0, const int grid_d
                 const int n, double* cilm, const int cilm_dim, int* lmax,
                 const int* norm, const int* sampling, const int* csphase,
                 const int* lmax_calc, int* exitstatus);
+
+/* Complex drop-ins: complex arrays are passed as shtc_complex, which has
+ * the layout of C's double _Complex (interleaved re, im). */
+#ifdef __cplusplus
+typedef struct shtc_complex_s { double re, im; } shtc_complex;
+#else
+typedef double _Complex shtc_complex;
+#endif
+
+/* include/shtools.h:117-128 (src/SHExpandDHC.f95:1) */
+SHTC_API void SHExpandDHC(const shtc_complex* grid, const int grid_d0, const int grid_d1,
+                          const int n, shtc_complex* cilm, const int cilm_dim, int* lmax,
+                          const int* norm, const int* sampling, const int* csphase,
+                          const int* lmax_calc, int* exitstatus);
+
+/* include/shtools.h:129-141 (src/MakeGridDHC.f95:1) */
+SHTC_API void MakeGridDHC(shtc_complex* griddh, const int griddh_d0, const int griddh_d1,
+                          int* n, const shtc_complex* cilm, const int cilm_dim,
+                          const int lmax, const int* norm, const int* sampling,
+                          const int* csphase, const int* lmax_calc, const int* extend,
+                          int* exitstatus);
+
+/* include/shtools.h:174-184 (src/SHExpandGLQC.f95:1) */
+SHTC_API void SHExpandGLQC(shtc_complex* cilm, const int cilm_dim, const int lmax,
+                           const shtc_complex* gridglq, const double* w, const double* plx,
+                           const double* zero, const int* norm, const int* csphase,
+                           const int* lmax_calc, int* exitstatus);
+
+/* include/shtools.h:185-197 (src/MakeGridGLQC.f95:1) */
+SHTC_API void MakeGridGLQC(shtc_complex* gridglq, const int gridglq_d0,
+                           const int gridglq_d1, const shtc_complex* cilm,
+                           const int cilm_dim, const int lmax, const double* plx,
+                           const double* zero, const int* norm, const int* csphase,
+                           const int* lmax_calc, const int* extend, int* exitstatus);
 
 /* include/shtools.h:153-165 (src/MakeGridGLQ.f95:1) */
 SHTC_API void MakeGridGLQ(double* gridglq, const int gridglq_d0, const int gridglq_d1,

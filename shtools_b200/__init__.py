@@ -2,7 +2,8 @@
 
 GPU implementation of the SHTOOLS transforms MakeGridDH / SHExpandDH and
 MakeGridGLQ / SHExpandGLQ (every norm, csphase, sampling, lmax_calc and
-extend option), the quadrature routines PreGLQ / SHGLQ / DHaj, and their
+extend option), their complex counterparts MakeGridDHC / SHExpandDHC /
+MakeGridGLQC / SHExpandGLQC, the quadrature routines PreGLQ / SHGLQ / DHaj, and their
 adjoints for autograd.  The arithmetic runs in hand-written sm_100a kernels
 of libshtcuda (shtools_b200/csrc, C ABI in include/shtcuda.h); PyTorch
 provides device memory and streams.
@@ -15,10 +16,12 @@ provides device memory and streams.
     backend.register()                                # pyshtools 'cuda'
 """
 from .transforms import (MakeGridDH, SHExpandDH, MakeGridGLQ, SHExpandGLQ,
+                         MakeGridDHC, SHExpandDHC, MakeGridGLQC, SHExpandGLQC,
                          PreGLQ, SHGLQ, DHaj, Plan, get_plan,
                          clear_plan_cache, GRID_DH, GRID_GLQ)
 from ._lib import SHTCudaError
 
-__all__ = ["MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ", "PreGLQ",
+__all__ = ["MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ",
+           "MakeGridDHC", "SHExpandDHC", "MakeGridGLQC", "SHExpandGLQC", "PreGLQ",
            "SHGLQ", "DHaj", "Plan", "get_plan", "clear_plan_cache", "GRID_DH",
            "GRID_GLQ", "SHTCudaError"]

@@ -36,7 +36,9 @@ EXPORTS = (
     "shtc_batch_workspace_bytes", "shtc_batch_synthesis", "shtc_batch_analysis",
     "shtc_preglq",
     "shtc_dhaj", "MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ",
-    "SHGLQ", "PreGLQ", "DHaj",
+    "SHGLQ", "PreGLQ", "DHaj", "shtc_plan_create_dhc", "shtc_plan_create_glqc",
+    "shtc_synthesis_c", "shtc_analysis_c", "MakeGridDHC", "SHExpandDHC",
+    "MakeGridGLQC", "SHExpandGLQC",
 )
 
 
@@ -76,6 +78,11 @@ def _bind(L):
     L.shtc_analysis_ex.argtypes = [_P] + gridx + coefx + tail
     L.shtc_synthesis_adjoint_ex.argtypes = [_P] + gridx + coefx + tail
     L.shtc_analysis_adjoint_ex.argtypes = [_P] + coefx + gridx + tail
+    L.shtc_plan_create_dhc.argtypes = [ctypes.POINTER(_P), _I, _I, _I, _I, _I, _I, _P]
+    L.shtc_plan_create_glqc.argtypes = [ctypes.POINTER(_P), _I, _DP, _DP, _I, _I, _I,
+                                        _I, _P]
+    L.shtc_synthesis_c.argtypes = [_P] + coef + grid + tail
+    L.shtc_analysis_c.argtypes = [_P] + grid + coef + tail
     L.shtc_preglq.argtypes = [_D, _D, _I, _P, _P, _P]
     L.shtc_dhaj.argtypes = [_I, _P, _I, _P]
     L.MakeGridDH.argtypes = [_DP, _I, _I, _IP, _DP, _I, _I, _IP, _IP, _IP, _IP, _IP,
@@ -87,8 +94,14 @@ def _bind(L):
     L.SHGLQ.argtypes = [_I, _DP, _DP, _DP, _IP, _IP, _IP, _IP]
     L.PreGLQ.argtypes = [_D, _D, _I, _DP, _DP, _IP]
     L.DHaj.argtypes = [_I, _DP, _I, _IP, _IP]
+    # complex arrays as untyped pointers to interleaved (re, im) doubles
+    L.MakeGridDHC.argtypes = [_P, _I, _I, _IP, _P, _I, _I, _IP, _IP, _IP, _IP, _IP, _IP]
+    L.SHExpandDHC.argtypes = [_P, _I, _I, _I, _P, _I, _IP, _IP, _IP, _IP, _IP, _IP]
+    L.MakeGridGLQC.argtypes = [_P, _I, _I, _P, _I, _I, _DP, _DP, _IP, _IP, _IP, _IP, _IP]
+    L.SHExpandGLQC.argtypes = [_P, _I, _I, _P, _DP, _DP, _DP, _IP, _IP, _IP, _IP]
     for name in ("MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ", "SHGLQ",
-                 "PreGLQ", "DHaj"):
+                 "PreGLQ", "DHaj", "MakeGridDHC", "SHExpandDHC", "MakeGridGLQC",
+                 "SHExpandGLQC"):
         getattr(L, name).restype = None
     return L
 

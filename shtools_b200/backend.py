@@ -7,7 +7,7 @@ numpy arrays out, the arithmetic on the GPU.  After ``register()``,
 ``SHCoeffs.expand()`` and ``SHGrid.expand()`` run here unchanged
 (pyshtools/shclasses/shcoeffs.py:4343-4377, shgrid.py:2105, 3011).
 
-Only the real DH and GLQ transforms are implemented on the GPU.  The other
+The real and complex DH and GLQ transforms run on the GPU.  The other
 names that the backend injectors rebind (pyshtools/expand/__init__.py:91-111,
 pyshtools/rotate/__init__.py:18-21) are taken from the reference's own
 'shtools' backend when pyshtools is importable, so that switching backends
@@ -101,19 +101,48 @@ def _passthrough(name):
         f = _fallback(name)
         if f is None:
             raise NotImplementedError(
-                "%s is not part of the GPU transforms (real DH/GLQ only) and "
+                "%s is not part of the GPU transforms (DH/GLQ only) and "
                 "the reference 'shtools' backend is not importable" % name)
         return f(*args, **kwargs)
     fn.__name__ = name
     fn.__doc__ = ("Delegates to the reference 'shtools' backend: the GPU "
-                  "backend implements the real DH and GLQ transforms only.")
+                  "backend implements the DH and GLQ transforms only.")
     return fn
 
 
-MakeGridDHC = _passthrough("MakeGridDHC")
-SHExpandDHC = _passthrough("SHExpandDHC")
-MakeGridGLQC = _passthrough("MakeGridGLQC")
-SHExpandGLQC = _passthrough("SHExpandGLQC")
+def MakeGridDHC(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
+                extend=False):
+    """griddh = MakeGridDHC(cilm, [lmax, norm, sampling, csphase, lmax_calc,
+    extend]) -- see src/MakeGridDHC.f95:1 and ducc0_wrapper.py:552."""
+    return _np(_t.MakeGridDHC(np.asarray(cilm, dtype=np.complex128), lmax=lmax,
+                              norm=norm, sampling=sampling, csphase=csphase,
+                              lmax_calc=lmax_calc, extend=extend))
+
+
+def SHExpandDHC(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None):
+    """cilm = SHExpandDHC(griddh, [norm, sampling, csphase, lmax_calc]) -- see
+    src/SHExpandDHC.f95:1 and ducc0_wrapper.py:745."""
+    return _np(_t.SHExpandDHC(np.asarray(griddh, dtype=np.complex128), norm=norm,
+                              sampling=sampling, csphase=csphase, lmax_calc=lmax_calc))
+
+
+def MakeGridGLQC(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
+                 extend=False):
+    """gridglq = MakeGridGLQC(cilm, [zero, lmax, norm, csphase, lmax_calc,
+    extend]) -- see src/MakeGridGLQC.f95:1 and ducc0_wrapper.py:917."""
+    return _np(_t.MakeGridGLQC(np.asarray(cilm, dtype=np.complex128), zero=zero,
+                               lmax=lmax, norm=norm, csphase=csphase,
+                               lmax_calc=lmax_calc, extend=extend))
+
+
+def SHExpandGLQC(gridglq, w=None, zero=None, norm=1, csphase=1, lmax_calc=None):
+    """cilm = SHExpandGLQC(gridglq, [w, zero, norm, csphase, lmax_calc]) -- see
+    src/SHExpandGLQC.f95:1."""
+    return _np(_t.SHExpandGLQC(np.asarray(gridglq, dtype=np.complex128), w=w,
+                               zero=zero, norm=norm, csphase=csphase,
+                               lmax_calc=lmax_calc))
+
+
 MakeGradientDH = _passthrough("MakeGradientDH")
 SHRotateRealCoef = _passthrough("SHRotateRealCoef")
 

@@ -44,9 +44,11 @@ static size_t spec_region(const shtc_plan* P, int nfield) {
     return align256((size_t)nfield * P->npair * (P->lc + 1) * 2 * sizeof(double2));
 }
 
+// complex plans carry two internal fields (orders +m and -m) per field
 extern "C" size_t shtc_workspace_bytes(const shtc_plan* P, int nfield) {
     if (!P || nfield < 1) return 0;
-    return coef_region(P, nfield) + spec_region(P, nfield);
+    const int nf = P->cplx ? 2 * nfield : nfield;
+    return coef_region(P, nf) + spec_region(P, nf);
 }
 
 static int check_call(const shtc_plan* P, const void* a, const void* b,
@@ -65,6 +67,11 @@ static int check_dtypes(int a, int b) {
     return ok(a) && ok(b) ? SHTC_OK : SHTC_EBOUND;
 }
 
+// real entry points need a real plan, the complex ones a complex plan
+static int check_kind(const shtc_plan* P, int cplx) {
+    return P && P->cplx != cplx ? SHTC_EBOUND : SHTC_OK;
+}
+
 extern "C" int shtc_synthesis_ex(const shtc_plan* P, const void* cilm, int cdt,
                                  long long csf, long long csk, long long csl,
                                  long long csm, int cdim, void* grid, int gdt,
@@ -72,6 +79,7 @@ extern "C" int shtc_synthesis_ex(const shtc_plan* P, const void* cilm, int cdt,
                                  int nfield, void* work, size_t wb, void* stream) {
     int rc = check_call(P, cilm, grid, nfield, work, wb);
     if (rc) return rc;
+    if ((rc = check_kind(P, 0))) return rc;
     if ((rc = check_dtypes(cdt, gdt))) return rc;
     if (cdim < 1) return SHTC_EDIM;
     cudaStream_t st = (cudaStream_t)stream;
@@ -98,6 +106,7 @@ extern "C" int shtc_analysis_ex(const shtc_plan* P, const void* grid, int gdt,
                                 void* work, size_t wb, void* stream) {
     int rc = check_call(P, grid, cilm, nfield, work, wb);
     if (rc) return rc;
+    if ((rc = check_kind(P, 0))) return rc;
     if ((rc = check_dtypes(cdt, gdt))) return rc;
     if (cdim < P->lc + 1) return SHTC_EDIM;
     cudaStream_t st = (cudaStream_t)stream;
@@ -127,6 +136,7 @@ extern "C" int shtc_synthesis_adjoint_ex(const shtc_plan* P, const void* grid, i
                                          void* stream) {
     int rc = check_call(P, grid, cilm, nfield, work, wb);
     if (rc) return rc;
+    if ((rc = check_kind(P, 0))) return rc;
     if ((rc = check_dtypes(cdt, gdt))) return rc;
     if (cdim < 1) return SHTC_EDIM;
     cudaStream_t st = (cudaStream_t)stream;
@@ -155,6 +165,7 @@ extern "C" int shtc_analysis_adjoint_ex(const shtc_plan* P, const void* cilm, in
                                         int nfield, void* work, size_t wb, void* stream) {
     int rc = check_call(P, cilm, grid, nfield, work, wb);
     if (rc) return rc;
+    if ((rc = check_kind(P, 0))) return rc;
     if ((rc = check_dtypes(cdt, gdt))) return rc;
     if (cdim < 1) return SHTC_EDIM;
     cudaStream_t st = (cudaStream_t)stream;
@@ -209,17 +220,77 @@ extern "C" int shtc_analysis_adjoint(const shtc_plan* P, const double* cilm,
 }
 
 // ---------------------------------------------------------------------------
+// complex transforms: the Legendre stages run on 2 internal fields per field
+// (orders +m and -m, sharing one recursion), the longitude transforms are
+// complex DFTs
+// ---------------------------------------------------------------------------
+extern "C" int shtc_synthesis_c(const shtc_plan* P, const void* cilm, long long csf,
+                                long long csk, long long csl, long long csm, int cdim,
+                                void* grid, long long gsf, long long gsr, long long gsc,
+                                int nfield, void* work, size_t wb, void* stream) {
+    int rc = check_call(P, cilm, grid, nfield, work, wb);
+    if (rc) return rc;
+    if ((rc = check_kind(P, 1))) return rc;
+    if (cdim < 1) return SHTC_EDIM;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nf2 = 2 * nfield;
+    double2* packed = (double2*)work;
+    double2* spec = (double2*)((char*)work + coef_region(P, nf2));
+    stage_begin(SHTC_STAGE_PACK, st);
+    rc = launch_pack_coef_c(P, (const double2*)cilm, csf, csk, csl, csm, cdim, packed, nfield,
+                            st);
+    stage_end(SHTC_STAGE_PACK, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_LEGENDRE_SYNTH, st);
+    rc = launch_legendre_synth(P, packed, spec, nf2, st);
+    stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_FFT_C2R, st);
+    rc = launch_fft_c2c_synth(P, spec, (double2*)grid, gsf, gsr, gsc, nfield, st);
+    stage_end(SHTC_STAGE_FFT_C2R, st);
+    return rc;
+}
+
+extern "C" int shtc_analysis_c(const shtc_plan* P, const void* grid, long long gsf,
+                               long long gsr, long long gsc, void* cilm, long long csf,
+                               long long csk, long long csl, long long csm, int cdim,
+                               int nfield, void* work, size_t wb, void* stream) {
+    int rc = check_call(P, grid, cilm, nfield, work, wb);
+    if (rc) return rc;
+    if ((rc = check_kind(P, 1))) return rc;
+    if (cdim < P->lc + 1) return SHTC_EDIM;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nf2 = 2 * nfield;
+    double2* partial = (double2*)work;
+    double2* spec = (double2*)((char*)work + coef_region(P, nf2));
+    const int tiles = anal_tiles(P);
+    stage_begin(SHTC_STAGE_FFT_R2C, st);
+    rc = launch_fft_c2c_anal(P, (const double2*)grid, gsf, gsr, gsc, spec, nfield, st);
+    stage_end(SHTC_STAGE_FFT_R2C, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
+    rc = launch_legendre_anal(P, spec, partial, tiles, nf2, st);
+    stage_end(SHTC_STAGE_LEGENDRE_ANAL, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_UNPACK, st);
+    rc = launch_unpack_coef_c(P, partial, tiles, (double2*)cilm, csf, csk, csl, csm, cdim,
+                              nfield, st);
+    stage_end(SHTC_STAGE_UNPACK, st);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
 // host drop-ins of include/shtools.h
 // ---------------------------------------------------------------------------
 namespace {
 
 struct PlanKey {
-    int kind, lmax, lc, norm, csphase, sampling, extend, device;
+    int kind, lmax, lc, norm, csphase, sampling, extend, device, cplx;
     std::vector<double> zero;
     bool operator<(const PlanKey& o) const {
-        return std::tie(kind, lmax, lc, norm, csphase, sampling, extend, device, zero) <
+        return std::tie(kind, lmax, lc, norm, csphase, sampling, extend, device, cplx, zero) <
                std::tie(o.kind, o.lmax, o.lc, o.norm, o.csphase, o.sampling, o.extend,
-                        o.device, o.zero);
+                        o.device, o.cplx, o.zero);
     }
 };
 
@@ -230,10 +301,10 @@ std::map<PlanKey, shtc_plan*> g_plans;
 // life of the process, like the reference's saved tables.
 int cached_plan(int kind, int lmax, int lc, int norm, int csphase, int sampling,
                 int extend, const double* zero, const double* w, shtc_plan** out,
-                cudaStream_t st) {
+                cudaStream_t st, int cplx = 0) {
     PlanKey k;
     k.kind = kind; k.lmax = lmax; k.lc = lc; k.norm = norm; k.csphase = csphase;
-    k.sampling = sampling; k.extend = extend;
+    k.sampling = sampling; k.extend = extend; k.cplx = cplx;
     cudaGetDevice(&k.device);
     if (zero) k.zero.assign(zero, zero + lmax + 1);
     if (w) k.zero.insert(k.zero.end(), w, w + lmax + 1);
@@ -241,9 +312,13 @@ int cached_plan(int kind, int lmax, int lc, int norm, int csphase, int sampling,
     auto it = g_plans.find(k);
     if (it != g_plans.end()) { *out = it->second; return SHTC_OK; }
     shtc_plan* p = nullptr;
-    int rc = kind == SHTC_GRID_DH
-                 ? shtc_plan_create_dh(&p, lmax, sampling, lc, norm, csphase, extend, st)
-                 : shtc_plan_create_glq(&p, lmax, zero, w, lc, norm, csphase, extend, st);
+    int rc;
+    if (kind == SHTC_GRID_DH)
+        rc = cplx ? shtc_plan_create_dhc(&p, lmax, sampling, lc, norm, csphase, extend, st)
+                  : shtc_plan_create_dh(&p, lmax, sampling, lc, norm, csphase, extend, st);
+    else
+        rc = cplx ? shtc_plan_create_glqc(&p, lmax, zero, w, lc, norm, csphase, extend, st)
+                  : shtc_plan_create_glq(&p, lmax, zero, w, lc, norm, csphase, extend, st);
     if (rc) return rc;
     g_plans[k] = p;
     *out = p;
@@ -438,6 +513,167 @@ extern "C" void PreGLQ(const double x1, const double x2, const int n,
     rc = shtc_preglq(x1, x2, n, (double*)dz.p, (double*)dw.p, st);
     if (!rc) rc = map_cuda(cudaMemcpyAsync(zero, dz.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     if (!rc) rc = map_cuda(cudaMemcpyAsync(w, dw.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
+    set_status(exitstatus, rc);
+}
+
+// Complex drop-ins (include/shtools.h:117-141, 174-197): the same argument
+// handling as the real ones; arrays of interleaved complex doubles.
+extern "C" void MakeGridDHC(shtc_complex* griddh, const int d0, const int d1, int* n,
+                            const shtc_complex* cilm, const int cdim, const int lmax,
+                            const int* norm, const int* sampling, const int* csphase,
+                            const int* lmax_calc, const int* extend, int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    const int nn = 2 * lmax + 2;
+    if (n) *n = nn;
+    const int samp = opt(sampling, 1), ext = opt(extend, 0), nrm = opt(norm, 1),
+              cs = opt(csphase, 1);
+    if (samp != 1 && samp != 2) return set_status(exitstatus, SHTC_EBOUND);
+    if (ext != 0 && ext != 1) return set_status(exitstatus, SHTC_EBOUND);
+    const int nlat_out = nn + ext, nlon_out = samp * nn + ext;
+    if (d0 < nlat_out || d1 < nlon_out) return set_status(exitstatus, SHTC_EDIM);
+    if (nrm < 1 || nrm > 4) return set_status(exitstatus, SHTC_EBOUND);
+    if (cs != 1 && cs != -1) return set_status(exitstatus, SHTC_EBOUND);
+    int lc = lmax < cdim - 1 ? lmax : cdim - 1;
+    if (lmax_calc) {
+        if (*lmax_calc > lmax) return set_status(exitstatus, SHTC_EBOUND);
+        if (*lmax_calc < lc) lc = *lmax_calc;
+    }
+    if (lc < 0) return set_status(exitstatus, SHTC_EDIM);
+    cudaStream_t st = cudaStreamPerThread;
+    shtc_plan* P = nullptr;
+    int rc = cached_plan(SHTC_GRID_DH, lmax, lc, nrm, cs, samp, ext, nullptr, nullptr, &P, st,
+                         1);
+    if (rc) return set_status(exitstatus, rc);
+    DevBuf dc, dg, dw;
+    const size_t cb = sizeof(double2) * 2 * (size_t)cdim * cdim;
+    const size_t wb = shtc_workspace_bytes(P, 1);
+    if ((rc = dc.alloc(cb)) || (rc = dg.alloc(sizeof(double2) * (size_t)d0 * d1)) ||
+        (rc = dw.alloc(wb)))
+        return set_status(exitstatus, rc);
+    rc = map_cuda(cudaMemcpyAsync(dc.p, cilm, cb, cudaMemcpyHostToDevice, st));
+    if (!rc) rc = shtc_synthesis_c(P, dc.p, 0, 1, 2, 2LL * cdim, cdim, dg.p, 0, 1, d0, 1,
+                                   dw.p, wb, st);
+    if (!rc) rc = map_cuda(cudaMemcpy2DAsync(griddh, sizeof(double2) * d0, dg.p,
+                                             sizeof(double2) * d0, sizeof(double2) * nlat_out,
+                                             nlon_out, cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
+    set_status(exitstatus, rc);
+}
+
+extern "C" void SHExpandDHC(const shtc_complex* grid, const int d0, const int d1,
+                            const int n, shtc_complex* cilm, const int cdim, int* lmax,
+                            const int* norm, const int* sampling, const int* csphase,
+                            const int* lmax_calc, int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    const int L = n / 2 - 1;
+    if (lmax) *lmax = L;
+    int lc = L;
+    if (lmax_calc) {
+        if (*lmax_calc > L) return set_status(exitstatus, SHTC_EBOUND);
+        lc = *lmax_calc < L ? *lmax_calc : L;
+    }
+    const int samp = opt(sampling, 1), nrm = opt(norm, 1), cs = opt(csphase, 1);
+    if (samp != 1 && samp != 2) return set_status(exitstatus, SHTC_EBOUND);
+    if (n % 2 != 0) return set_status(exitstatus, SHTC_EBOUND);
+    if (cdim < lc + 1) return set_status(exitstatus, SHTC_EDIM);
+    if (d0 < n || d1 < samp * n) return set_status(exitstatus, SHTC_EDIM);
+    if (cs != 1 && cs != -1) return set_status(exitstatus, SHTC_EBOUND);
+    if (nrm < 1 || nrm > 4) return set_status(exitstatus, SHTC_EBOUND);
+    cudaStream_t st = cudaStreamPerThread;
+    shtc_plan* P = nullptr;
+    int rc = cached_plan(SHTC_GRID_DH, L, lc, nrm, cs, samp, 0, nullptr, nullptr, &P, st, 1);
+    if (rc) return set_status(exitstatus, rc);
+    DevBuf dc, dg, dw;
+    const size_t cb = sizeof(double2) * 2 * (size_t)cdim * cdim;
+    const size_t wb = shtc_workspace_bytes(P, 1);
+    if ((rc = dc.alloc(cb)) || (rc = dg.alloc(sizeof(double2) * (size_t)d0 * d1)) ||
+        (rc = dw.alloc(wb)))
+        return set_status(exitstatus, rc);
+    rc = map_cuda(cudaMemcpyAsync(dg.p, grid, sizeof(double2) * (size_t)d0 * d1,
+                                  cudaMemcpyHostToDevice, st));
+    if (!rc) rc = map_cuda(cudaMemsetAsync(dc.p, 0, cb, st));
+    if (!rc) rc = shtc_analysis_c(P, dg.p, 0, 1, d0, dc.p, 0, 1, 2, 2LL * cdim, cdim, 1,
+                                  dw.p, wb, st);
+    if (!rc) rc = map_cuda(cudaMemcpyAsync(cilm, dc.p, cb, cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
+    set_status(exitstatus, rc);
+}
+
+extern "C" void MakeGridGLQC(shtc_complex* gridglq, const int d0, const int d1,
+                             const shtc_complex* cilm, const int cdim, const int lmax,
+                             const double* plx, const double* zero, const int* norm,
+                             const int* csphase, const int* lmax_calc, const int* extend,
+                             int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    const int ext = opt(extend, 0), nrm = opt(norm, 1), cs = opt(csphase, 1);
+    if (ext != 0 && ext != 1) return set_status(exitstatus, SHTC_EBOUND);
+    const int nlat = lmax + 1, nlon_out = 2 * lmax + 1 + ext;
+    if (d1 < nlon_out || d0 < nlat) return set_status(exitstatus, SHTC_EDIM);
+    if (plx) return set_status(exitstatus, SHTC_EBOUND);
+    if (!zero) return set_status(exitstatus, SHTC_ENOZERO);
+    if (nrm < 1 || nrm > 4) return set_status(exitstatus, SHTC_EBOUND);
+    if (cs != 1 && cs != -1) return set_status(exitstatus, SHTC_EBOUND);
+    int lc = lmax < cdim - 1 ? lmax : cdim - 1;
+    if (lmax_calc) {
+        if (*lmax_calc > lmax) return set_status(exitstatus, SHTC_EBOUND);
+        if (*lmax_calc < lc) lc = *lmax_calc;
+    }
+    if (lc < 0) return set_status(exitstatus, SHTC_EDIM);
+    cudaStream_t st = cudaStreamPerThread;
+    shtc_plan* P = nullptr;
+    int rc = cached_plan(SHTC_GRID_GLQ, lmax, lc, nrm, cs, 1, ext, zero, nullptr, &P, st, 1);
+    if (rc) return set_status(exitstatus, rc);
+    DevBuf dc, dg, dw;
+    const size_t cb = sizeof(double2) * 2 * (size_t)cdim * cdim;
+    const size_t wb = shtc_workspace_bytes(P, 1);
+    if ((rc = dc.alloc(cb)) || (rc = dg.alloc(sizeof(double2) * (size_t)d0 * d1)) ||
+        (rc = dw.alloc(wb)))
+        return set_status(exitstatus, rc);
+    rc = map_cuda(cudaMemcpyAsync(dc.p, cilm, cb, cudaMemcpyHostToDevice, st));
+    if (!rc) rc = shtc_synthesis_c(P, dc.p, 0, 1, 2, 2LL * cdim, cdim, dg.p, 0, 1, d0, 1,
+                                   dw.p, wb, st);
+    if (!rc) rc = map_cuda(cudaMemcpy2DAsync(gridglq, sizeof(double2) * d0, dg.p,
+                                             sizeof(double2) * d0, sizeof(double2) * nlat,
+                                             nlon_out, cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
+    set_status(exitstatus, rc);
+}
+
+extern "C" void SHExpandGLQC(shtc_complex* cilm, const int cdim, const int lmax,
+                             const shtc_complex* gridglq, const double* w,
+                             const double* plx, const double* zero, const int* norm,
+                             const int* csphase, const int* lmax_calc, int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    int lc = lmax;
+    if (lmax_calc) {
+        if (*lmax_calc > lmax) return set_status(exitstatus, SHTC_EBOUND);
+        lc = *lmax_calc < lmax ? *lmax_calc : lmax;
+    }
+    if (cdim < lc + 1) return set_status(exitstatus, SHTC_EDIM);
+    if (!w) return set_status(exitstatus, SHTC_EDIM);
+    if (plx) return set_status(exitstatus, SHTC_EBOUND);
+    if (!zero) return set_status(exitstatus, SHTC_ENOZERO);
+    const int nrm = opt(norm, 1), cs = opt(csphase, 1);
+    if (nrm < 1 || nrm > 4) return set_status(exitstatus, SHTC_EBOUND);
+    if (cs != 1 && cs != -1) return set_status(exitstatus, SHTC_EBOUND);
+    const int nlat = lmax + 1, nlon = 2 * lmax + 1;
+    cudaStream_t st = cudaStreamPerThread;
+    shtc_plan* P = nullptr;
+    int rc = cached_plan(SHTC_GRID_GLQ, lmax, lc, nrm, cs, 1, 0, zero, w, &P, st, 1);
+    if (rc) return set_status(exitstatus, rc);
+    DevBuf dc, dg, dw;
+    const size_t cb = sizeof(double2) * 2 * (size_t)cdim * cdim;
+    const size_t wb = shtc_workspace_bytes(P, 1);
+    if ((rc = dc.alloc(cb)) || (rc = dg.alloc(sizeof(double2) * (size_t)nlat * nlon)) ||
+        (rc = dw.alloc(wb)))
+        return set_status(exitstatus, rc);
+    rc = map_cuda(cudaMemcpyAsync(dg.p, gridglq, sizeof(double2) * (size_t)nlat * nlon,
+                                  cudaMemcpyHostToDevice, st));
+    if (!rc) rc = map_cuda(cudaMemsetAsync(dc.p, 0, cb, st));
+    if (!rc) rc = shtc_analysis_c(P, dg.p, 0, 1, nlat, dc.p, 0, 1, 2, 2LL * cdim, cdim, 1,
+                                  dw.p, wb, st);
+    if (!rc) rc = map_cuda(cudaMemcpyAsync(cilm, dc.p, cb, cudaMemcpyDeviceToHost, st));
     if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
     set_status(exitstatus, rc);
 }

@@ -292,9 +292,9 @@ extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
     for (int gi = 0; gi < ngroup; ++gi) {
         const shtc_plan* P = plans[gi];
         const int nf = nfields[gi];
-        if (!P || nf < 1 || P->device != B->device || P->extend != 0) {
+        if (!P || nf < 1 || P->device != B->device || P->extend != 0 || P->cplx) {
             delete B;
-            return P && P->extend != 0 ? SHTC_EBOUND : SHTC_EHANDLE;
+            return P && (P->extend != 0 || P->cplx) ? SHTC_EBOUND : SHTC_EHANDLE;
         }
         BatchGroup g;
         g.rec = P->d_rec; g.pmm = P->d_pmm; g.rtab = P->d_rtab; g.z = P->d_z;

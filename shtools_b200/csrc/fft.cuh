@@ -449,6 +449,96 @@ __device__ __forceinline__ void fft_r2c_body(
     }
 }
 
+// ---------------------------------------------------------------------------
+// complex grids (MakeGridDHC / SHExpandDHC, MakeGridGLQC / SHExpandGLQC)
+// ---------------------------------------------------------------------------
+// Item (job, u): job = pair*2 + ring (0 north, 1 south), u the user field,
+// whose orders +m and -m are the internal fields 2u and 2u+1 of spec.
+//
+// Synthesis: the Legendre stage wrote spec = (a_m*h, -b_m*h), h = m ? 1/2 : 1,
+// the real c2r convention; undone exactly here.  Bin m takes the +m sums, bin
+// n-m the -m sums times (-1)^m (MakeGridDHC.f95:612-616); the ring is the
+// unnormalised backward DFT of length n.
+__device__ __forceinline__ void fft_c2c_synth_body(
+    const FftArgs& F, const double2* tw, double2* smem_fft, int job, int u,
+    const double2* __restrict__ spec, double2* __restrict__ grid, long long gf,
+    long long grs, long long gcs, const int* __restrict__ rowN,
+    const int* __restrict__ rowS, int lc, int npair, int extend_col) {
+    const int p = job >> 1;
+    const int h = job & 1;
+    const int row = h ? rowS[p] : rowN[p];
+    if (row < 0) return;
+    const int len = F.bluestein ? F.mb : F.m;
+    double2* a = smem_fft;
+    double2* b = smem_fft + len;
+    const int n = F.m;
+    const long long fstride = (long long)npair * (lc + 1) * 2;
+    const double2* Xp = spec + (2LL * u) * fstride + (long long)p * (lc + 1) * 2 + h;
+    const double2* Xn = Xp + fstride;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) a[k] = make_double2(0.0, 0.0);
+    __syncthreads();
+    for (int m = threadIdx.x; m <= lc; m += blockDim.x) {
+        const double2 v = Xp[2 * m];
+        if (m == 0) {
+            a[0] = make_double2(v.x, -v.y);
+        } else {
+            a[m] = make_double2(2.0 * v.x, -2.0 * v.y);
+            const double2 w = Xn[2 * m];
+            const double sg = (m & 1) ? -2.0 : 2.0;
+            a[n - m] = make_double2(sg * w.x, -sg * w.y);
+        }
+    }
+    const double2* r = fft_exec<+1>(F, tw, a, b);
+    double2* g = grid + u * gf + row * grs;
+#pragma unroll 4
+    for (int j = threadIdx.x; j < n; j += blockDim.x) g[j * gcs] = r[j];
+    if (extend_col && threadIdx.x == 0) g[(long long)n * gcs] = r[0];
+}
+
+// Analysis: the forward DFT of the ring times its weight w/n gives
+// fcoef (SHExpandDHC.f95:478); spec of field 2u takes fcoef(m), field 2u+1
+// fcoef(n-m) * (-1)^m (SHExpandDHC.f95:596-600), both as (Re, Im).
+__device__ __forceinline__ void fft_c2c_anal_body(
+    const FftArgs& F, const double2* tw, double2* smem_fft, int job, int u,
+    const double2* __restrict__ grid, long long gf, long long grs, long long gcs,
+    double2* __restrict__ spec, const int* __restrict__ rowN,
+    const int* __restrict__ rowS, const double* __restrict__ wN,
+    const double* __restrict__ wS, double wscale, int lc, int npair) {
+    const int p = job >> 1;
+    const int h = job & 1;
+    const int row = h ? rowS[p] : rowN[p];
+    const long long fstride = (long long)npair * (lc + 1) * 2;
+    double2* Xp = spec + (2LL * u) * fstride + (long long)p * (lc + 1) * 2 + h;
+    double2* Xn = Xp + fstride;
+    if (row < 0) {
+        for (int m = threadIdx.x; m <= lc; m += blockDim.x) {
+            Xp[2 * m] = make_double2(0.0, 0.0);
+            Xn[2 * m] = make_double2(0.0, 0.0);
+        }
+        return;
+    }
+    const int len = F.bluestein ? F.mb : F.m;
+    double2* a = smem_fft;
+    double2* b = smem_fft + len;
+    const int n = F.m;
+    const double2* g = grid + u * gf + row * grs;
+#pragma unroll 4
+    for (int j = threadIdx.x; j < n; j += blockDim.x) a[j] = g[j * gcs];
+    const double2* r = fft_exec<-1>(F, tw, a, b);
+    const double sc = (h ? wS[p] : wN[p]) * wscale;
+    for (int m = threadIdx.x; m <= lc; m += blockDim.x) {
+        const double2 zp = r[m];
+        Xp[2 * m] = make_double2(sc * zp.x, sc * zp.y);
+        if (m == 0) {
+            Xn[0] = make_double2(0.0, 0.0);
+        } else {
+            const double2 zn = r[n - m];
+            const double sg = (m & 1) ? -sc : sc;
+            Xn[2 * m] = make_double2(sg * zn.x, sg * zn.y);
+        }
+    }
+}
+
 // L2 prefetch of the input of the c2r item (job, f): the pair's spectrum row
 __device__ __forceinline__ void fft_c2r_prefetch(int mode, int job, int f,
                                                  const double2* spec, int lc, int npair) {

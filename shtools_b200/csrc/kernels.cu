@@ -491,4 +491,171 @@ int launch_fft_r2c(const shtc_plan* P, const void* grid, int dtype, long long gf
                                       weighted, fold_extend, st);
 }
 
+// ---------------------------------------------------------------------------
+// complex transforms (MakeGridDHC / SHExpandDHC, MakeGridGLQC / SHExpandGLQC)
+// ---------------------------------------------------------------------------
+// pack: complex cilm[u][k][l][m] (k = 0 the order +m, 1 the order -m) ->
+// packed [(l, m)][2u + k] = (Re, Im) * D(l - m); the -0 entry is ignored as in
+// the reference.  Same 32x32 shared-memory tiles as k_pack_coef; grid.z =
+// 2 * fields.
+__global__ void __launch_bounds__(kCoefTile * kCoefRows)
+k_pack_coef_c(const double2* __restrict__ cilm, long long sf, long long sk, long long sl,
+              long long sm, int cdim, double2* __restrict__ packed, int lc, int nfield2,
+              const double2* __restrict__ rec) {
+    __shared__ double2 tile[kCoefTile][kCoefTile + 1];   // [m - m0][l - l0]
+    const int l0 = blockIdx.x * kCoefTile, m0 = blockIdx.y * kCoefTile;
+    const int fk = blockIdx.z, u = fk >> 1, k = fk & 1;
+    if (m0 > l0 + kCoefTile - 1) return;
+    const int tx = threadIdx.x;
+    for (int j = threadIdx.y; j < kCoefTile; j += kCoefRows) {
+        const int l = l0 + j, m = m0 + tx;
+        double2 v = make_double2(0.0, 0.0);
+        if (m <= l && l <= lc && l < cdim && !(k == 1 && m == 0))
+            v = cilm[u * sf + k * sk + l * sl + m * sm];
+        tile[tx][j] = v;
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < kCoefTile; j += kCoefRows) {
+        const int m = m0 + j, l = l0 + tx;
+        if (m > l || l > lc) continue;
+        const long long idx = packed_off(m, lc) + (l - m);
+        const double2 v = tile[j][tx];
+        const double d = rec[idx].y;
+        packed[idx * nfield2 + fk] = make_double2(v.x * d, v.y * d);
+    }
+}
+
+// unpack: tile sums of the internal fields 2u + k -> complex cilm[u][k][l][m],
+// divided by the integral of Y_lm Y*_lm (SHExpandDHC.f95:689-723); the -0
+// entry is zero.
+__global__ void __launch_bounds__(kCoefTile * kCoefRows)
+k_unpack_coef_c(const double2* __restrict__ partial, int ntiles, double2* __restrict__ cilm,
+                long long sf, long long sk, long long sl, long long sm, int cdim, int lc,
+                long long nlm, int nfield2, int norm, const double* __restrict__ nrm3) {
+    const double pi = 3.141592653589793238462643383279502884;
+    __shared__ double2 tile[kCoefTile][kCoefTile + 1];   // [m - m0][l - l0]
+    const int l0 = blockIdx.x * kCoefTile, m0 = blockIdx.y * kCoefTile;
+    const int fk = blockIdx.z, u = fk >> 1, k = fk & 1;
+    const int tx = threadIdx.x;
+    for (int j = threadIdx.y; j < kCoefTile; j += kCoefRows) {
+        const int m = m0 + j, l = l0 + tx;
+        double c = 0.0, s = 0.0;
+        if (m <= l && l <= lc && l < cdim && !(k == 1 && m == 0)) {
+            const long long idx = packed_off(m, lc) + (l - m);
+            for (int t = 0; t < ntiles; ++t) {
+                const double2 v = partial[((long long)t * nfield2 + fk) * nlm + idx];
+                c += v.x;
+                s += v.y;
+            }
+            switch (norm) {
+                case 1:
+                    c = c / (4 * pi);
+                    s = s / (4 * pi);
+                    break;
+                case 2:
+                    c = c * (2 * l + 1) / (4 * pi);
+                    s = s * (2 * l + 1) / (4 * pi);
+                    break;
+                case 3:
+                    c = c / nrm3[idx];
+                    s = s / nrm3[idx];
+                    break;
+                default:
+                    break;
+            }
+        }
+        tile[j][tx] = make_double2(c, s);
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < kCoefTile; j += kCoefRows) {
+        const int l = l0 + j, m = m0 + tx;
+        if (l >= cdim || m >= cdim) continue;
+        cilm[u * sf + k * sk + l * sl + m * sm] = tile[tx][j];
+    }
+}
+
+// persistent complex-grid FFT kernels over (job, field) items, as k_fft_c2r
+__global__ void __launch_bounds__(512)
+k_fft_c2c_synth(FftArgs F, int tw_smem, int jobs, int nitems,
+                const double2* __restrict__ spec, double2* __restrict__ grid, long long gf,
+                long long grs, long long gcs, const int* __restrict__ rowN,
+                const int* __restrict__ rowS, int lc, int npair, int extend_col) {
+    extern __shared__ double2 smem_fft[];
+    const double2* tw = fft_stage_twiddles(F, smem_fft, tw_smem);
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        fft_c2c_synth_body(F, tw, smem_fft, it % jobs, it / jobs, spec, grid, gf, grs, gcs,
+                           rowN, rowS, lc, npair, extend_col);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(512)
+k_fft_c2c_anal(FftArgs F, int tw_smem, int jobs, int nitems,
+               const double2* __restrict__ grid, long long gf, long long grs, long long gcs,
+               double2* __restrict__ spec, const int* __restrict__ rowN,
+               const int* __restrict__ rowS, const double* __restrict__ wN,
+               const double* __restrict__ wS, double wscale, int lc, int npair) {
+    extern __shared__ double2 smem_fft[];
+    const double2* tw = fft_stage_twiddles(F, smem_fft, tw_smem);
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        fft_c2c_anal_body(F, tw, smem_fft, it % jobs, it / jobs, grid, gf, grs, gcs, spec,
+                          rowN, rowS, wN, wS, wscale, lc, npair);
+        __syncthreads();
+    }
+}
+
+int launch_pack_coef_c(const shtc_plan* P, const double2* cilm, long long sf, long long sk,
+                       long long sl, long long sm, int cdim, double2* packed, int nfield,
+                       cudaStream_t st) {
+    const int nt = (P->lc + kCoefTile) / kCoefTile;
+    const dim3 grid(nt, nt, 2 * nfield), block(kCoefTile, kCoefRows);
+    k_pack_coef_c<<<grid, block, 0, st>>>(cilm, sf, sk, sl, sm, cdim, packed, P->lc,
+                                          2 * nfield, P->d_rec);
+    return map_cuda(cudaGetLastError());
+}
+
+int launch_unpack_coef_c(const shtc_plan* P, const double2* partial, int ntiles,
+                         double2* cilm, long long sf, long long sk, long long sl,
+                         long long sm, int cdim, int nfield, cudaStream_t st) {
+    const int nt = (cdim + kCoefTile - 1) / kCoefTile;
+    const dim3 grid(nt, nt, 2 * nfield), block(kCoefTile, kCoefRows);
+    k_unpack_coef_c<<<grid, block, 0, st>>>(partial, ntiles, cilm, sf, sk, sl, sm, cdim,
+                                            P->lc, P->nlm, 2 * nfield, P->norm, P->d_nrm);
+    return map_cuda(cudaGetLastError());
+}
+
+int launch_fft_c2c_synth(const shtc_plan* P, const double2* spec, double2* grid,
+                         long long gf, long long grs, long long gcs, int nfield,
+                         cudaStream_t st) {
+    const FftPlan& f = P->fft;
+    int rc = fft_smem_setup((const void*)k_fft_c2c_synth, f);
+    if (rc) return rc;
+    const int jobs = 2 * P->npair;
+    const int nitems = jobs * nfield;
+    int blocks = 0;
+    if ((rc = fft_grid(k_fft_c2c_synth, f, nitems, &blocks))) return rc;
+    if (blocks == 0) return SHTC_OK;
+    k_fft_c2c_synth<<<blocks, f.threads, f.smem, st>>>(
+        fft_args(f), f.tw_smem, jobs, nitems, spec, grid, gf, grs, gcs, P->d_rowN,
+        P->d_rowS, P->lc, P->npair, P->extend);
+    return map_cuda(cudaGetLastError());
+}
+
+int launch_fft_c2c_anal(const shtc_plan* P, const double2* grid, long long gf,
+                        long long grs, long long gcs, double2* spec, int nfield,
+                        cudaStream_t st) {
+    const FftPlan& f = P->fft;
+    int rc = fft_smem_setup((const void*)k_fft_c2c_anal, f);
+    if (rc) return rc;
+    const int jobs = 2 * P->npair;
+    const int nitems = jobs * nfield;
+    int blocks = 0;
+    if ((rc = fft_grid(k_fft_c2c_anal, f, nitems, &blocks))) return rc;
+    if (blocks == 0) return SHTC_OK;
+    k_fft_c2c_anal<<<blocks, f.threads, f.smem, st>>>(
+        fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_arowN,
+        P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair);
+    return map_cuda(cudaGetLastError());
+}
+
 }  // namespace shtc

@@ -252,11 +252,11 @@ static int pass_twiddles(const int* fac, int nfac, std::vector<double2>& out, in
     return (int)out.size();
 }
 
-int build_fft_plan(FftPlan* f, int n, cudaStream_t st) {
+int build_fft_plan(FftPlan* f, int n, int cplx, cudaStream_t st) {
     memset(f, 0, sizeof(*f));
     f->n = n;
-    f->mode = (n % 2 == 0) ? 1 : 0;
-    f->m = f->mode ? n / 2 : n;
+    f->mode = cplx ? 2 : ((n % 2 == 0) ? 1 : 0);
+    f->m = f->mode == 1 ? n / 2 : n;
     int fac[kMaxFactors];
     int nf = factor_len(f->m, fac);
     std::vector<double2> tw, twn, chirp, kern;
@@ -377,15 +377,18 @@ static void plan_free_tables(shtc_plan* P) {
 // sectoral start values, replicating the running product of the reference
 // (MakeGridDH.f95:542-603): pm2 for m < lc, the final pmm (without the
 // rescale factor) for m = lc, and P00 for m = 0.
-static void host_pmm(int lc, int norm, int csphase, double* out) {
+// Complex transforms start the sectoral recursion without the real
+// harmonics' sqrt(2) (MakeGridDHC.f95:442-446).
+static void host_pmm(int lc, int norm, int csphase, int cplx, double* out) {
     const double pi = acos(-1.0);
     out[0] = norm == 4 ? 1.0 / sqrt(4.0 * pi) : 1.0;
     if (lc == 0) return;
     double pmm;
+    const double s2 = cplx ? 1.0 : sqrt(2.0);
     switch (norm) {
-        case 1: case 2: pmm = sqrt(2.0) * kScalef; break;
+        case 1: case 2: pmm = cplx ? kScalef : s2 * kScalef; break;
         case 3: pmm = kScalef; break;
-        default: pmm = sqrt(2.0) * kScalef / sqrt(4.0 * pi); break;
+        default: pmm = cplx ? kScalef / sqrt(4.0 * pi) : s2 * kScalef / sqrt(4.0 * pi); break;
     }
     for (int m = 1; m <= lc - 1; ++m) {
         switch (norm) {
@@ -416,14 +419,15 @@ static void host_pmm(int lc, int norm, int csphase, double* out) {
     }
 }
 
-// norm-3 divisors of SHExpandDH.f95:685-700 per packed (l, m)
-static void host_nrm3(int lc, std::vector<double>& out) {
+// norm-3 divisors of SHExpandDH.f95:685-700 per packed (l, m); the complex
+// transforms omit the halving for m >= 1 (SHExpandDHC.f95:708-720)
+static void host_nrm3(int lc, int cplx, std::vector<double>& out) {
     const double pi = acos(-1.0);
     out.assign((size_t)(lc + 1) * (lc + 2) / 2, 1.0);
     for (int l = 0; l <= lc; ++l) {
         double prod = 4 * pi / (double)(2 * l + 1);
         out[packed_off(0, lc) + l] = prod;
-        prod = prod / 2.0;
+        if (!cplx) prod = prod / 2.0;
         for (int m = 1; m <= l - 1; ++m) {
             prod = prod * (l + m) * (l - m + 1);
             out[packed_off(m, lc) + (l - m)] = prod;
@@ -459,7 +463,7 @@ static int plan_finish(shtc_plan* P, const std::vector<double>& z,
     P->nlm = (long long)(lc + 1) * (lc + 2) / 2;
     size_t acc = 0;
     std::vector<double> pmm(lc + 1);
-    host_pmm(lc, P->norm, P->csphase, pmm.data());
+    host_pmm(lc, P->norm, P->csphase, P->cplx, pmm.data());
     double* d_u = nullptr;
     double2* d_ff = nullptr;   // {ff1, ff2}, only needed to build d_rec
     if ((rc = dev_upload(&P->d_rec, (const double2*)nullptr, (size_t)P->nlm, st, &acc))) return rc;
@@ -474,7 +478,7 @@ static int plan_finish(shtc_plan* P, const std::vector<double>& z,
     if ((rc = dev_upload(&P->d_wS, (const double*)nullptr, (size_t)np, st, &acc))) return rc;
     if (P->norm == 3) {
         std::vector<double> n3;
-        host_nrm3(lc, n3);
+        host_nrm3(lc, P->cplx, n3);
         if ((rc = dev_upload(&P->d_nrm, n3.data(), n3.size(), st, &acc))) return rc;
         if ((rc = map_cuda(cudaStreamSynchronize(st)))) return rc;
     }
@@ -499,7 +503,7 @@ static int plan_finish(shtc_plan* P, const std::vector<double>& z,
     acc -= (size_t)np * sizeof(double) + (size_t)P->nlm * sizeof(double2);
     if (rc) return rc;
     if (e != cudaSuccess) return SHTC_ECUDA;
-    if ((rc = build_fft_plan(&P->fft, P->nlon, st))) return rc;
+    if ((rc = build_fft_plan(&P->fft, P->nlon, P->cplx, st))) return rc;
     size_t fb = 0;
     const int len = P->fft.bluestein ? P->fft.mb : P->fft.m;
     fb += (size_t)len * sizeof(double2);
@@ -510,9 +514,8 @@ static int plan_finish(shtc_plan* P, const std::vector<double>& z,
     return SHTC_OK;
 }
 
-extern "C" int shtc_plan_create_dh(shtc_plan** out, int lmax, int sampling,
-                                   int lmax_calc, int norm, int csphase,
-                                   int extend, void* stream) {
+static int create_dh(shtc_plan** out, int lmax, int sampling, int lmax_calc, int norm,
+                     int csphase, int extend, int cplx, void* stream) {
     if (!out) return SHTC_EHANDLE;
     *out = nullptr;
     if (lmax < 0) return SHTC_EBOUND;
@@ -526,6 +529,7 @@ extern "C" int shtc_plan_create_dh(shtc_plan** out, int lmax, int sampling,
     if (!P) return SHTC_EALLOC;
     memset(P, 0, sizeof(*P));
     P->kind = SHTC_GRID_DH;
+    P->cplx = cplx;
     P->lmax = lmax;
     P->lc = lmax_calc < 0 ? lmax : lmax_calc;
     P->norm = norm;
@@ -582,14 +586,24 @@ extern "C" int shtc_plan_create_dh(shtc_plan** out, int lmax, int sampling,
     return SHTC_OK;
 }
 
+extern "C" int shtc_plan_create_dh(shtc_plan** out, int lmax, int sampling,
+                                   int lmax_calc, int norm, int csphase,
+                                   int extend, void* stream) {
+    return create_dh(out, lmax, sampling, lmax_calc, norm, csphase, extend, 0, stream);
+}
+
+extern "C" int shtc_plan_create_dhc(shtc_plan** out, int lmax, int sampling,
+                                    int lmax_calc, int norm, int csphase,
+                                    int extend, void* stream) {
+    return create_dh(out, lmax, sampling, lmax_calc, norm, csphase, extend, 1, stream);
+}
+
 extern "C" int shtc_preglq(double x1, double x2, int n, double* zero, double* w,
                            void* stream);
 
-extern "C" int shtc_plan_create_glq(shtc_plan** out, int lmax,
-                                    const double* zero_host,
-                                    const double* w_host, int lmax_calc,
-                                    int norm, int csphase, int extend,
-                                    void* stream) {
+static int create_glq(shtc_plan** out, int lmax, const double* zero_host,
+                      const double* w_host, int lmax_calc, int norm, int csphase,
+                      int extend, int cplx, void* stream) {
     if (!out) return SHTC_EHANDLE;
     *out = nullptr;
     if (lmax < 0) return SHTC_EBOUND;
@@ -602,6 +616,7 @@ extern "C" int shtc_plan_create_glq(shtc_plan** out, int lmax,
     if (!P) return SHTC_EALLOC;
     memset(P, 0, sizeof(*P));
     P->kind = SHTC_GRID_GLQ;
+    P->cplx = cplx;
     P->lmax = lmax;
     P->lc = lmax_calc < 0 ? lmax : lmax_calc;
     P->norm = norm;
@@ -664,6 +679,24 @@ extern "C" int shtc_plan_create_glq(shtc_plan** out, int lmax,
     }
     *out = P;
     return SHTC_OK;
+}
+
+extern "C" int shtc_plan_create_glq(shtc_plan** out, int lmax,
+                                    const double* zero_host,
+                                    const double* w_host, int lmax_calc,
+                                    int norm, int csphase, int extend,
+                                    void* stream) {
+    return create_glq(out, lmax, zero_host, w_host, lmax_calc, norm, csphase, extend, 0,
+                      stream);
+}
+
+extern "C" int shtc_plan_create_glqc(shtc_plan** out, int lmax,
+                                     const double* zero_host,
+                                     const double* w_host, int lmax_calc,
+                                     int norm, int csphase, int extend,
+                                     void* stream) {
+    return create_glq(out, lmax, zero_host, w_host, lmax_calc, norm, csphase, extend, 1,
+                      stream);
 }
 
 extern "C" int shtc_plan_destroy(shtc_plan* P) {

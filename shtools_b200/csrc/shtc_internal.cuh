@@ -33,6 +33,7 @@ struct FftPlan {
     int n;             // real transform length (grid columns, nlong)
     int mode;          // 0: two rings in one complex length-n FFT (odd n)
                        // 1: one ring via a complex FFT of length n/2 (even n)
+                       // 2: complex grids, one ring per complex length-n FFT
     int m;             // complex FFT length executed in shared memory
     int nfac;          // radices of the length-m (or Bluestein) FFT
     int fac[kMaxFactors];
@@ -64,6 +65,8 @@ struct shtc_plan {
     int csphase;       // +1 / -1
     int sampling;      // DH: 1 or 2; GLQ: 1
     int extend;        // synthesis output has the extra column (and DH row)
+    int cplx;          // complex transforms (MakeGridDHC & co.): 2 internal fields
+                       // (orders +m and -m) per user field, c2c FFTs
     int nlat;          // rings of the grid without the extend row
     int nlon;          // longitudes without the extend column (FFT length)
     int nlat_out;      // synthesis output rows (with extend)
@@ -98,7 +101,7 @@ __host__ __device__ inline long long packed_off(int m, int lc) {
 }
 
 // plan.cu
-int build_fft_plan(FftPlan* f, int n, cudaStream_t stream);
+int build_fft_plan(FftPlan* f, int n, int cplx, cudaStream_t stream);
 void free_fft_plan(FftPlan* f);
 
 // kernels.cu launchers (return cudaGetLastError() mapped to SHTC codes)
@@ -122,6 +125,20 @@ int launch_unpack_coef(const shtc_plan* P, const double2* partial, int ntiles,
                        long long sm, int cdim, int nfield, int normalise,
                        cudaStream_t st);
 int anal_tiles(const shtc_plan* P);
+// complex plans: cilm (nfield, 2, cdim, cdim) and grids of interleaved complex
+// doubles, strides in complex elements; internal fields 2u (+m), 2u+1 (-m)
+int launch_pack_coef_c(const shtc_plan* P, const double2* cilm, long long sf, long long sk,
+                       long long sl, long long sm, int cdim, double2* packed, int nfield,
+                       cudaStream_t st);
+int launch_unpack_coef_c(const shtc_plan* P, const double2* partial, int ntiles,
+                         double2* cilm, long long sf, long long sk, long long sl,
+                         long long sm, int cdim, int nfield, cudaStream_t st);
+int launch_fft_c2c_synth(const shtc_plan* P, const double2* spec, double2* grid,
+                         long long gf, long long grs, long long gcs, int nfield,
+                         cudaStream_t st);
+int launch_fft_c2c_anal(const shtc_plan* P, const double2* grid, long long gf,
+                        long long grs, long long gcs, double2* spec, int nfield,
+                        cudaStream_t st);
 int map_cuda(cudaError_t e);
 
 // timing.cu: event brackets around kernel stages (SHTC_STAGE_* ids)

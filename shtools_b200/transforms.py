@@ -42,7 +42,7 @@ class Plan:
     """
 
     def __init__(self, kind, lmax, lmax_calc=None, norm=1, csphase=1,
-                 sampling=1, extend=0, zero=None, w=None, device=None):
+                 sampling=1, extend=0, zero=None, w=None, device=None, cplx=False):
         import ctypes
         self.lib = _lib.load()
         if device is None:
@@ -55,10 +55,11 @@ class Plan:
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             st = _stream_ptr(self.device)
+            self.cplx = bool(cplx)
             if kind == GRID_DH:
-                rc = self.lib.shtc_plan_create_dh(ctypes.byref(h), int(lmax),
-                                                  int(sampling), lc, int(norm),
-                                                  int(csphase), int(extend), st)
+                fn = self.lib.shtc_plan_create_dhc if cplx else self.lib.shtc_plan_create_dh
+                rc = fn(ctypes.byref(h), int(lmax), int(sampling), lc, int(norm),
+                        int(csphase), int(extend), st)
             else:
                 zp = wp = None
                 if zero is not None:
@@ -67,9 +68,10 @@ class Plan:
                 if w is not None:
                     self._w = np.ascontiguousarray(w, dtype=np.float64)
                     wp = self._w.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-                rc = self.lib.shtc_plan_create_glq(ctypes.byref(h), int(lmax), zp, wp,
-                                                   lc, int(norm), int(csphase),
-                                                   int(extend), st)
+                fn = self.lib.shtc_plan_create_glqc if cplx else \
+                    self.lib.shtc_plan_create_glq
+                rc = fn(ctypes.byref(h), int(lmax), zp, wp, lc, int(norm), int(csphase),
+                        int(extend), st)
         _lib.check(rc, "plan creation")
         self.handle = h
         info = (ctypes.c_longlong * 16)()
@@ -129,6 +131,35 @@ class Plan:
         self._run(self.lib.shtc_analysis_ex, grid, out, F, False)
         return out
 
+    # -- complex transforms (complex plans; complex128 tensors) ---------------
+    def _run_c(self, fn, src, dst, nfield, src_is_coef):
+        ws, nb = self.workspace(nfield)
+        with torch.cuda.device(self.device):
+            st = _stream_ptr(self.device)
+            c, g = (src, dst) if src_is_coef else (dst, src)
+            cargs = (ctypes_void(c.data_ptr()), c.stride(0), c.stride(1), c.stride(2),
+                     c.stride(3), c.shape[2])
+            gargs = (ctypes_void(g.data_ptr()), g.stride(0), g.stride(1), g.stride(2))
+            args = (cargs + gargs) if src_is_coef else (gargs + cargs)
+            rc = fn(self.handle, *args, int(nfield), ctypes_void(ws.data_ptr()), nb, st)
+        _lib.check(rc, fn.__name__)
+
+    def synthesis_c(self, cilm, out=None):
+        F = cilm.shape[0]
+        if out is None:
+            out = torch.empty((F, self.info["nlat_out"], self.info["nlon_out"]),
+                              dtype=torch.complex128, device=self.device)
+        self._run_c(self.lib.shtc_synthesis_c, cilm, out, F, True)
+        return out
+
+    def analysis_c(self, grid, cdim=None, out=None):
+        F = grid.shape[0]
+        cdim = self.lc + 1 if cdim is None else cdim
+        if out is None:
+            out = torch.empty((F, 2, cdim, cdim), dtype=torch.complex128, device=self.device)
+        self._run_c(self.lib.shtc_analysis_c, grid, out, F, False)
+        return out
+
     def synthesis_adjoint(self, grid, cdim, dtype=None):
         F = grid.shape[0]
         out = torch.empty((F, 2, cdim, cdim), dtype=dtype or grid.dtype,
@@ -152,7 +183,7 @@ _plans = {}
 
 
 def get_plan(kind, lmax, lmax_calc, norm, csphase, sampling=1, extend=0,
-             zero=None, w=None, device=None, tune=None):
+             zero=None, w=None, device=None, tune=None, cplx=False):
     """Cached Plan for the option set (thread-safe).  New plans are
     autotuned when ``tune`` is true or the environment sets SHTC_AUTOTUNE=1
     (shtools_b200.autotune)."""
@@ -164,12 +195,12 @@ def get_plan(kind, lmax, lmax_calc, norm, csphase, sampling=1, extend=0,
     zkey = None if zero is None else np.asarray(zero, dtype=np.float64).tobytes()
     wkey = None if w is None else np.asarray(w, dtype=np.float64).tobytes()
     key = (kind, int(lmax), int(lmax_calc), int(norm), int(csphase),
-           int(sampling), int(extend), dev.index, zkey, wkey)
+           int(sampling), int(extend), dev.index, zkey, wkey, bool(cplx))
     with _cache_lock:
         p = _plans.get(key)
         if p is None:
             p = Plan(kind, lmax, lmax_calc, norm, csphase, sampling, extend,
-                     zero, w, dev)
+                     zero, w, dev, cplx=cplx)
             _plans[key] = p
             if tune or (tune is None and os.environ.get("SHTC_AUTOTUNE") == "1"):
                 from . import autotune
@@ -411,6 +442,94 @@ def SHExpandGLQ(gridglq, w=None, zero=None, norm=1, csphase=1,
     plan = get_plan(GRID_GLQ, lmax, lc, norm, csphase, 1, 0, zero=z, w=wh,
                     device=grid.device)
     return _Analysis.apply(grid, plan, lc + 1, dtype)
+
+
+# ---------------------------------------------------------------------------
+# complex transforms (not differentiable)
+# ---------------------------------------------------------------------------
+def _as_cuda_c(t):
+    if isinstance(t, np.ndarray):
+        t = torch.from_numpy(np.asarray(t, dtype=np.complex128))
+    if not isinstance(t, torch.Tensor):
+        t = torch.as_tensor(np.asarray(t, dtype=np.complex128))
+    if not t.is_cuda:
+        t = t.to("cuda")
+    if t.dtype != torch.complex128:
+        t = t.to(torch.complex128)
+    return t
+
+
+def _synth_c(cilm, plan):
+    c, lead = _flat(cilm[..., :2, :, :], 3)
+    g = plan.synthesis_c(c)
+    return g.reshape(tuple(lead) + tuple(g.shape[1:]))
+
+
+def _anal_c(grid, plan, cdim):
+    g, lead = _flat(grid, 2)
+    c = plan.analysis_c(g[:, :plan.info["nlat"], :plan.info["nlon"]], cdim)
+    return c.reshape(tuple(lead) + tuple(c.shape[1:]))
+
+
+def MakeGridDHC(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
+                extend=False):
+    """Complex Driscoll-Healy synthesis on the GPU (src/MakeGridDHC.f95:1).
+
+    cilm: (..., 2, D, D) complex; cilm[..., 0, l, m] multiplies Y_lm and
+    cilm[..., 1, l, m] multiplies Y_l,-m (Y*_lm = (-1)^m Y_l,-m).  Returns the
+    complex grid (..., n+extend, sampling*n+extend).
+    """
+    _check_common(norm, csphase)
+    if sampling not in (1, 2):
+        raise ValueError("sampling must be 1 (n by n) or 2 (n by 2n); got %r"
+                         % (sampling,))
+    lmax, lc = _resolve_synth(np.shape(cilm), lmax, lmax_calc)
+    cilm = _as_cuda_c(cilm)
+    plan = get_plan(GRID_DH, lmax, lc, norm, csphase, sampling, int(bool(extend)),
+                    device=cilm.device, cplx=True)
+    return _synth_c(cilm, plan)
+
+
+def SHExpandDHC(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None):
+    """Complex Driscoll-Healy analysis on the GPU (src/SHExpandDHC.f95:1).
+    Returns (..., 2, lmax_calc+1, lmax_calc+1) complex128."""
+    _check_common(norm, csphase)
+    lmax, lc = _resolve_anal_dh(np.shape(griddh), sampling, lmax_calc)
+    grid = _as_cuda_c(griddh)
+    plan = get_plan(GRID_DH, lmax, lc, norm, csphase, sampling, 0, device=grid.device,
+                    cplx=True)
+    return _anal_c(grid, plan, lc + 1)
+
+
+def MakeGridGLQC(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
+                 extend=False):
+    """Complex Gauss-Legendre synthesis on the GPU (src/MakeGridGLQC.f95:1).
+    Returns (..., lmax+1, 2*lmax+1+extend) complex128."""
+    _check_common(norm, csphase)
+    lmax, lc = _resolve_synth(np.shape(cilm), lmax, lmax_calc)
+    z = None if zero is None else _host64(zero, lmax + 1, "zero")
+    cilm = _as_cuda_c(cilm)
+    plan = get_plan(GRID_GLQ, lmax, lc, norm, csphase, 1, int(bool(extend)), zero=z,
+                    device=cilm.device, cplx=True)
+    return _synth_c(cilm, plan)
+
+
+def SHExpandGLQC(gridglq, w=None, zero=None, norm=1, csphase=1, lmax_calc=None):
+    """Complex Gauss-Legendre analysis on the GPU (src/SHExpandGLQC.f95:1).
+    Returns (..., 2, lmax_calc+1, lmax_calc+1) complex128."""
+    _check_common(norm, csphase)
+    lmax, lc = _resolve_anal_glq(np.shape(gridglq), lmax_calc)
+    nlat = lmax + 1
+    z = None if zero is None else _host64(zero, nlat, "zero")
+    wh = None if w is None else _host64(w, nlat, "w")
+    grid = _as_cuda_c(gridglq)
+    if (z is None) != (wh is None):
+        zz, ww = SHGLQ(lmax, device=grid.device)
+        z = zz if z is None else z
+        wh = ww if wh is None else wh
+    plan = get_plan(GRID_GLQ, lmax, lc, norm, csphase, 1, 0, zero=z, w=wh,
+                    device=grid.device, cplx=True)
+    return _anal_c(grid, plan, lc + 1)
 
 
 def _host64(a, n, what):

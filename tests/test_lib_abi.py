@@ -24,7 +24,8 @@ def lib():
 def test_header_declares_the_reference_dropins():
     names = declared_functions()
     for ref in ("MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ",
-                "SHGLQ", "PreGLQ", "DHaj"):
+                "SHGLQ", "PreGLQ", "DHaj", "MakeGridDHC", "SHExpandDHC",
+                "MakeGridGLQC", "SHExpandGLQC"):
         assert ref in names
     assert len(names) >= 20
 
