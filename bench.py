@@ -44,6 +44,10 @@ WORKLOADS = {
     # config 3 shape: 8 DH fields, lmax 719, sampling 2
     "dh719x8": dict(kind="dh", lmax=719, nfield=8, sampling=2, beta=2.0,
                     seed=3000),
+    # complex DH (MakeGridDHC / SHExpandDHC), config 3 shape: 8 fields,
+    # lmax 719, sampling 2
+    "dhc719x8": dict(kind="dhc", lmax=719, nfield=8, sampling=2, beta=2.0,
+                     seed=3500),
     # config 1 shape: one DH field, lmax 255, sampling 2
     "dh255": dict(kind="dh", lmax=255, nfield=1, sampling=2, beta=2.0,
                   seed=1000),
@@ -95,9 +99,9 @@ def flops_per_transform(w, L=None):
     return 8.0 * (nlat / 2.0) * nlm
 
 
-def power_law(L, seed, beta):
-    from oracle.oracle import power_law_cilm  # same seeded recipe, numpy only
-    return power_law_cilm(L, seed, beta)
+def power_law(L, seed, beta, cplx=False):
+    from shtools_b200.synthetic import power_law_cilm, power_law_cilm_complex
+    return (power_law_cilm_complex if cplx else power_law_cilm)(L, seed, beta)
 
 
 # ---------------------------------------------------------------------------
@@ -588,10 +592,16 @@ def run_cuda(args, w, rank, world, local_rank):
     torch.cuda.set_device(dev)
     lib = _lib.load()
     L, F = w["lmax"], w["nfield"]
-    cil = np.stack([power_law(L, w["seed"] + i, w["beta"]) for i in range(F)])
+    cplx = w["kind"] == "dhc"
+    cil = np.stack([power_law(L, w["seed"] + i, w["beta"], cplx) for i in range(F)])
     c_host = torch.from_numpy(cil).pin_memory()
     c = c_host.to(dev)
-    if w["kind"] == "glq":
+    esize = 16 if cplx else 8
+    if cplx:
+        s = w["sampling"]
+        synth = lambda x: sht.MakeGridDHC(x, sampling=s)
+        anal = lambda g: sht.SHExpandDHC(g, sampling=s)
+    elif w["kind"] == "glq":
         zero_t, w_t = sht.PreGLQ(-1.0, 1.0, L + 1, device=dev)
         zero, wts = zero_t.cpu().numpy(), w_t.cpu().numpy()
         synth = lambda x: sht.MakeGridGLQ(x, zero=zero)
@@ -612,8 +622,8 @@ def run_cuda(args, w, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     # accuracy of the round trip (size-independent property, per degree)
     bb = back.cpu().numpy()
-    num = np.sqrt(((bb - cil) ** 2).sum(axis=(1, 3)))
-    den = np.sqrt((cil ** 2).sum(axis=(1, 3)))
+    num = np.sqrt((np.abs(bb - cil) ** 2).sum(axis=(1, 3)))
+    den = np.sqrt((np.abs(cil) ** 2).sum(axis=(1, 3)))
     rt_err = float((num / np.where(den > 0, den, 1)).max())
 
     peak = fp64_peak(torch, dev)
@@ -652,8 +662,8 @@ def run_cuda(args, w, rank, world, local_rank):
     # pipelined over three streams (shtools_b200.pipeline)
     from shtools_b200.pipeline import pipelined
     g_in = g.cpu().pin_memory()
-    outs = [(torch.empty(tuple(g.shape), dtype=torch.float64).pin_memory(),
-             torch.empty(tuple(back.shape), dtype=torch.float64).pin_memory())
+    outs = [(torch.empty(tuple(g.shape), dtype=g.dtype).pin_memory(),
+             torch.empty(tuple(back.shape), dtype=back.dtype).pin_memory())
             for _ in range(2)]
     e2e_steps = max(2, min(args.steps, 10))
     fn = lambda x, gg: (synth(x), anal(gg))
@@ -670,15 +680,16 @@ def run_cuda(args, w, rank, world, local_rank):
     e2e_ms = max_over_ranks(a.elapsed_time(b), dev)
     e2e_value = 2.0 * F * e2e_steps * world / (e2e_ms * 1e-3)
     e2e_ok = bool(torch.equal(outs[(e2e_steps - 1) % 2][1], back.cpu()))
-    h2d = c_host.numel() * 8 + g_in.numel() * 8
-    d2h = outs[0][0].numel() * 8 + outs[0][1].numel() * 8
+    h2d = c_host.numel() * esize + g_in.numel() * esize
+    d2h = outs[0][0].numel() * esize + outs[0][1].numel() * esize
 
     # ---- roofline of the dominant kernel ------------------------------------
     names = ["pack", "legendre_synth", "fft_c2r", "fft_r2c", "legendre_anal",
              "unpack"]
     dom = max((1, 4), key=lambda i: ms[i])
     per_launch_ms = ms[dom] / max(1, cnt[dom])
-    fl = flops_per_transform(w) * F
+    # complex fields: two coefficient sets (orders +m, -m) per field
+    fl = flops_per_transform(w) * F * (2 if cplx else 1)
     achieved = fl / (per_launch_ms * 1e-3) / 1e12
     traffic = load_traffic("%s_%s" % (names[dom], args.workload))
     stage = {names[i]: {"ms_per_launch": (ms[i] / cnt[i]) if cnt[i] else None,
@@ -695,7 +706,7 @@ def run_cuda(args, w, rank, world, local_rank):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "c128" if cplx else "f64",
         "data": "synthetic seeded power-law coefficients, S(l)=(l+1)^-%g" % w["beta"],
         "config": {"workload": args.workload, "kind": w["kind"], "lmax": L,
                    "fields_per_gpu": F, "sampling": w["sampling"],
@@ -771,7 +782,7 @@ def main():
         res = run_cuda_grad(args, w, rank, world, local_rank)
     else:
         res = run_cuda(args, w, rank, world, local_rank)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and w["kind"] != "dhc":
         one_step, sample, threads = cpu_sample(w, args.cpu_seconds / 2)
         v, dt = one_step()
         res["cpu_baseline"] = {"value": v, "unit": "transforms/s",
