@@ -56,8 +56,9 @@ def _save_cache(d):
 def plan_key(plan):
     i = plan.info
     name = torch.cuda.get_device_name(plan.device)
-    return "%s|kind%d|L%d|lc%d|s%d" % (name, i["kind"], i["lmax"], i["lmax_comp"],
-                                       i["sampling"])
+    return "%s|kind%d|L%d|lc%d|s%d%s" % (name, i["kind"], i["lmax"], i["lmax_comp"],
+                                         i["sampling"],
+                                         "|complex" if getattr(plan, "cplx", False) else "")
 
 
 def _time_stage(plan, fn, stage, reps):
@@ -102,23 +103,27 @@ def tune_plan(plan, reps=3, use_cache=True, verbose=False):
         i = plan.info
         lc = i["lmax_comp"]
         g = torch.Generator(device=plan.device).manual_seed(0)
-        c = torch.randn((1, 2, lc + 1, lc + 1), generator=g, dtype=torch.float64,
+        # complex plans are timed on complex fields (two coefficient sets each)
+        dt = torch.complex128 if getattr(plan, "cplx", False) else torch.float64
+        c = torch.randn((1, 2, lc + 1, lc + 1), generator=g, dtype=dt,
                         device=plan.device)
-        grid = torch.randn((1, i["nlat"], i["nlon"]), generator=g,
-                           dtype=torch.float64, device=plan.device)
+        grid = torch.randn((1, i["nlat"], i["nlon"]), generator=g, dtype=dt,
+                           device=plan.device)
+        synth = plan.synthesis_c if dt == torch.complex128 else plan.synthesis
+        anal = plan.analysis_c if dt == torch.complex128 else plan.analysis
         s_c, a_c = candidates(i["npair"])
         times = {}
         best_s, best_st = None, float("inf")
         for t in s_c:
             set_shape(plan, t, 0, 0)
-            ms = _time_stage(plan, lambda: plan.synthesis(c), STAGE_SYNTH, reps)
+            ms = _time_stage(plan, lambda: synth(c), STAGE_SYNTH, reps)
             times["synth_T%d" % t] = ms
             if ms < best_st:
                 best_s, best_st = t, ms
         best_a, best_at = None, float("inf")
         for t, w in a_c:
             set_shape(plan, 0, t, w)
-            ms = _time_stage(plan, lambda: plan.analysis(grid), STAGE_ANAL, reps)
+            ms = _time_stage(plan, lambda: anal(grid), STAGE_ANAL, reps)
             times["anal_T%d_W%d" % (t, w)] = ms
             if ms < best_at:
                 best_a, best_at = (t, w), ms
