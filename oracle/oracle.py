@@ -57,6 +57,7 @@ def lib():
         L.orc_preglq_iter.argtypes = [ctypes.c_double, ctypes.c_double, _I,
                                       _D, _D, _I]
         L.orc_dhaj.argtypes = [_I, _D, _I]
+        L.orc_makegradient_dh.argtypes = [_D, _D, _D, _I, _I, _I, _I, _I, ctypes.c_double]
         L.orc_makegrid_dhc.argtypes = [_D, _D, _I, _I, _I, _I, _I, _I, _I]
         L.orc_shexpand_dhc.argtypes = [_D, _I, _D, _I, _I, _I, _I, _I, _I]
         L.orc_makegrid_glqc.argtypes = [_D, _D, _I, _I, _D, _I, _I, _I, _I]
@@ -333,3 +334,16 @@ def power_law_cilm_complex(L, seed, beta=2.0):
     c = np.where(l[:, None] >= l[None, :], c, 0.0)
     c[1, :, 0] = 0.0
     return c
+
+
+def makegradient_dh(cilm, lmax=None, sampling=1, lmax_calc=None, extend=0, radius=1.0):
+    """MakeGradientDH (MakeGradientDH.f95:1).  Returns (theta, phi) grids."""
+    cilm = _f64(cilm)
+    lmax, lmax_calc = _lmaxes(cilm, lmax, lmax_calc)
+    n = 2 * lmax + 2
+    shape = (n + int(extend), sampling * n + int(extend))
+    th = np.zeros(shape)
+    ph = np.zeros(shape)
+    _check(lib().orc_makegradient_dh(_p(th), _p(ph), _p(cilm), cilm.shape[1], lmax,
+                                     int(sampling), lmax_calc, int(extend), float(radius)))
+    return th, ph

@@ -1634,6 +1634,166 @@ int orc_shexpand_glqc(double *cilm, int cdim, int lmax, const double *grid, int 
     return ORC_OK;
 }
 
+/* ======================================================================== */
+/*  MakeGradientDH (src/MakeGradientDH.f95:1-658): horizontal gradient of a  */
+/*  4-pi normalised real field (csphase 1) on a DH grid,                     */
+/*      theta = (1/r) dF/dtheta,  phi = 1/(r sin theta) dF/dphi,             */
+/*  dP/dz from (1-z^2) dP_l/dz = a_l P_(l-1) - l z P_l; zero at the poles.   */
+/*  theta, phi: (n+extend) x (nlong+extend) row-major.                       */
+/* ======================================================================== */
+
+/* one ring's m = 0..lc sums for the c2r (halved for m >= 1 by the caller):
+ * north (t, p) and south (ts, ps); rounding order of MakeGradientDH.f95:427-549 */
+static void grad_ring(const rec_tab *t, const double *cilm, int cdim, double z, double u,
+                      double *tr, double *ti, double *pr, double *pi_, double *tsr,
+                      double *tsi, double *psr, double *psi) {
+    const int lc = t->lc, d = lc + 1;
+    const double *sqr = t->sqr, *ff1 = t->ff1, *ff2 = t->ff2;
+    double pm2, pm1, p, pmm, rescalem, dpl, tempr, c_r, c_i;
+    double coeft0 = 0.0, coefts0 = 0.0;
+
+    pm2 = 1.0;
+    pm1 = 0.0;
+    if (lc != 0) {
+        pm1 = ff1[(size_t)1 * d + 0] * z;
+        dpl = ff1[(size_t)1 * d + 0];
+        tempr = CIL(0, 1, 0) * dpl;
+        coeft0 = coeft0 + tempr;
+        coefts0 = coefts0 + tempr;
+    }
+    for (int l = 2; l <= lc; ++l) {
+        p = ff1[(size_t)l * d + 0] * z * pm1 - ff2[(size_t)l * d + 0] * pm2;
+        dpl = l * (sqr[2 * l + 1] / sqr[2 * l - 1] * pm1 - z * p) / (u * u);
+        tempr = CIL(0, l, 0) * dpl;
+        coeft0 = coeft0 + tempr;
+        coefts0 = coefts0 - tempr * ((l % 2 == 0) ? 1.0 : -1.0);
+        pm2 = pm1;
+        pm1 = p;
+    }
+    tr[0] = coeft0; ti[0] = 0.0; tsr[0] = coefts0; tsi[0] = 0.0;
+    pr[0] = 0.0; pi_[0] = 0.0; psr[0] = 0.0; psi[0] = 0.0;
+
+    pmm = sqr[2] * SCALEF;   /* sqr(2) * scalef */
+    rescalem = 1.0 / SCALEF;
+    for (int m = 1; m <= lc - 1; ++m) {
+        double atr = 0, ati = 0, atsr = 0, atsi = 0, apr = 0, api = 0, apsr = 0, apsi = 0;
+        rescalem = rescalem * u;
+        pmm = pmm * sqr[2 * m + 1] / sqr[2 * m];
+        pm2 = pmm;
+        /* (m, m): tempc = cmplx(S, C) * pm2 * m */
+        c_r = CIL(1, m, m) * pm2 * m; c_i = CIL(0, m, m) * pm2 * m;
+        apr += c_r; api += c_i; apsr += c_r; apsi += c_i;
+        dpl = -m * z * pm2 / (u * u);
+        c_r = CIL(0, m, m) * dpl; c_i = -CIL(1, m, m) * dpl;
+        atr += c_r; ati += c_i; atsr -= c_r; atsi -= c_i;
+
+        pm1 = z * ff1[(size_t)(m + 1) * d + m] * pm2;
+        c_r = CIL(1, m + 1, m) * pm1 * m; c_i = CIL(0, m + 1, m) * pm1 * m;
+        apr += c_r; api += c_i; apsr -= c_r; apsi -= c_i;
+        dpl = (sqr[2 * m + 3] * pmm - z * (m + 1) * pm1) / (u * u);
+        c_r = CIL(0, m + 1, m) * dpl; c_i = -CIL(1, m + 1, m) * dpl;
+        atr += c_r; ati += c_i; atsr += c_r; atsi += c_i;
+
+        for (int l = m + 2; l <= lc; ++l) {
+            p = z * ff1[(size_t)l * d + m] * pm1 - ff2[(size_t)l * d + m] * pm2;
+            const double fs = ((l - m) % 2 == 0) ? 1.0 : -1.0;
+            c_r = CIL(1, l, m) * p * m; c_i = CIL(0, l, m) * p * m;
+            apr += c_r; api += c_i; apsr += c_r * fs; apsi += c_i * fs;
+            dpl = (sqr[2 * l + 1] * sqr[l - m] * sqr[l + m] / sqr[2 * l - 1] * pm1
+                   - z * l * p) / (u * u);
+            c_r = CIL(0, l, m) * dpl; c_i = -CIL(1, l, m) * dpl;
+            atr += c_r; ati += c_i; atsr -= c_r * fs; atsi -= c_i * fs;
+            pm2 = pm1;
+            pm1 = p;
+        }
+        tr[m] = atr * rescalem; ti[m] = ati * rescalem;
+        tsr[m] = atsr * rescalem; tsi[m] = atsi * rescalem;
+        pr[m] = apr * rescalem; pi_[m] = api * rescalem;
+        psr[m] = apsr * rescalem; psi[m] = apsi * rescalem;
+    }
+    if (lc != 0) {
+        rescalem = rescalem * u;
+        pmm = pmm * sqr[2 * lc + 1] / sqr[2 * lc] * rescalem;
+        c_r = CIL(1, lc, lc) * pmm * lc; c_i = CIL(0, lc, lc) * pmm * lc;
+        pr[lc] = c_r; pi_[lc] = c_i; psr[lc] = c_r; psi[lc] = c_i;
+        dpl = -lc * z * pmm / (u * u);
+        c_r = CIL(0, lc, lc) * dpl; c_i = -CIL(1, lc, lc) * dpl;
+        tr[lc] = c_r; ti[lc] = c_i; tsr[lc] = -c_r; tsi[lc] = -c_i;
+    }
+}
+
+/* c2r of m = 0..lc sums (m >= 1 halved, the rest zero) into row `row` times s */
+static void grad_row(orc_fft *plan, int nlong, int lc, const double *cr, const double *ci,
+                     double *wr, double *wi, double *row, double s, double sfac_div,
+                     double *out) {
+    const int nh = nlong / 2 + 1;
+    double *ar = malloc(sizeof(double) * (size_t)nh), *ai = malloc(sizeof(double) * (size_t)nh);
+    for (int k = 0; k < nh; ++k) { ar[k] = 0.0; ai[k] = 0.0; }
+    ar[0] = cr[0]; ai[0] = 0.0;
+    for (int m = 1; m <= lc && m < nh; ++m) { ar[m] = cr[m] / 2.0; ai[m] = ci[m] / 2.0; }
+    fft_c2r(plan, ar, ai, row, wr, wi);
+    for (int j = 0; j < nlong; ++j) out[j] = sfac_div != 0.0 ? row[j] / s / sfac_div : s * row[j];
+    free(ar); free(ai);
+}
+
+int orc_makegradient_dh(double *theta_g, double *phi_g, const double *cilm, int cdim,
+                        int lmax, int sampling, int lmax_calc, int extend, double radius) {
+    if (sampling != 1 && sampling != 2) return ORC_EBOUND;
+    if (extend != 0 && extend != 1) return ORC_EBOUND;
+    if (lmax_calc > lmax) return ORC_EBOUND;
+    const int n = 2 * lmax + 2;
+    const int nlong = sampling == 1 ? n : 2 * n;
+    const int nlong_out = nlong + extend, nlat_out = n + extend;
+    int lc = lmax_calc < 0 ? lmax : lmax_calc;
+    if (lc > cdim - 1) lc = cdim - 1;
+    const double pi = acos(-1.0);
+    const double r = radius;
+    rec_tab t;
+    if (rec_build(&t, lc, 1)) return ORC_EALLOC;
+    orc_fft *plan = fft_plan(nlong);
+    const int L2 = lc + 2;
+    double *b[8];
+    for (int k = 0; k < 8; ++k) b[k] = calloc((size_t)L2, sizeof(double));
+    double *wr = malloc(sizeof(double) * (size_t)nlong), *wi = malloc(sizeof(double) * (size_t)nlong);
+    double *row = malloc(sizeof(double) * (size_t)nlong);
+    const int i_eq = n / 2 + 1;
+    memset(theta_g, 0, sizeof(double) * (size_t)nlat_out * nlong_out);
+    memset(phi_g, 0, sizeof(double) * (size_t)nlat_out * nlong_out);
+    for (int i = 1; i <= i_eq; ++i) {
+        const double theta = i == i_eq ? pi / 2.0 : pi * (double)(i - 1) / (double)n;
+        const double z = i == i_eq ? 0.0 : cos(theta);
+        const double u = i == i_eq ? 1.0 : sqrt((1.0 - z) * (1.0 + z));
+        const int i_s = 2 * i_eq - i;
+        if (i == 1) continue;   /* undefined at the poles: zero rows */
+        for (int k = 0; k < 8; ++k) memset(b[k], 0, sizeof(double) * (size_t)L2);
+        grad_ring(&t, cilm, cdim, z, u, b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7]);
+        const double st = sin(theta);
+        /* theta = -sin(theta) * grid / r ; phi = grid / r / sin(theta) */
+        grad_row(plan, nlong, lc, b[0], b[1], wr, wi, row, -st, 0.0,
+                 &theta_g[(size_t)(i - 1) * nlong_out]);
+        for (int j = 0; j < nlong; ++j) theta_g[(size_t)(i - 1) * nlong_out + j] /= r;
+        grad_row(plan, nlong, lc, b[2], b[3], wr, wi, row, r, st,
+                 &phi_g[(size_t)(i - 1) * nlong_out]);
+        if (i != i_eq) {
+            grad_row(plan, nlong, lc, b[4], b[5], wr, wi, row, -st, 0.0,
+                     &theta_g[(size_t)(i_s - 1) * nlong_out]);
+            for (int j = 0; j < nlong; ++j) theta_g[(size_t)(i_s - 1) * nlong_out + j] /= r;
+            grad_row(plan, nlong, lc, b[6], b[7], wr, wi, row, r, st,
+                     &phi_g[(size_t)(i_s - 1) * nlong_out]);
+        }
+    }
+    if (extend == 1)
+        for (int i = 0; i < nlat_out; ++i) {
+            theta_g[(size_t)i * nlong_out + nlong] = theta_g[(size_t)i * nlong_out];
+            phi_g[(size_t)i * nlong_out + nlong] = phi_g[(size_t)i * nlong_out];
+        }
+    for (int k = 0; k < 8; ++k) free(b[k]);
+    free(wr); free(wi); free(row);
+    fft_free(plan);
+    rec_free(&t);
+    return ORC_OK;
+}
+
 /* Number of host threads OpenMP would use (1 when built without OpenMP). */
 int orc_max_threads(void) {
 #ifdef _OPENMP
