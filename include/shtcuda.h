@@ -267,6 +267,19 @@ SHTC_API int shtc_analysis_c(const shtc_plan* plan, const void* grid, long long 
                              long long csk, long long csl, long long csm, int cilm_dim,
                              int nfield, void* work, size_t work_bytes, void* stream);
 
+/* MakeGradientDH (src/MakeGradientDH.f95:1) on device buffers: the theta and
+ * phi components of the horizontal gradient, (1/r) dF/dtheta and
+ * 1/(r sin theta) dF/dphi, on the grids of a real DH plan created with
+ * norm 1 and csphase 1 (the reference's only normalisation); zero on the
+ * pole rows.  Strides as above; theta and phi share the grid strides.  The
+ * workspace is shtc_gradient_workspace_bytes(plan, nfield). */
+SHTC_API size_t shtc_gradient_workspace_bytes(const shtc_plan* plan, int nfield);
+SHTC_API int shtc_gradient_dh(const shtc_plan* plan, const double* cilm, long long csf,
+                              long long csk, long long csl, long long csm, int cilm_dim,
+                              double* theta, double* phi, long long gsf, long long gsr,
+                              long long gsc, double radius, int nfield, void* work,
+                              size_t work_bytes, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Drop-ins of the reference C interface, include/shtools.h.  Host arrays,  */
 /* Fortran column-major: cilm(2, cilm_dim, cilm_dim), grid(d0, d1).  NULL  */
@@ -320,6 +333,14 @@ SHTC_API void MakeGridGLQC(shtc_complex* gridglq, const int gridglq_d0,
                            const int cilm_dim, const int lmax, const double* plx,
                            const double* zero, const int* norm, const int* csphase,
                            const int* lmax_calc, const int* extend, int* exitstatus);
+
+/* src/cWrapper.f95:295-317, bind(c, name="MakeGradientDH") (src/MakeGradientDH.f95:1);
+ * theta and phi are (d0, d1) column-major */
+SHTC_API void MakeGradientDH(const double* cilm, const int cilm_dim, const int lmax,
+                             double* theta, double* phi, const int theta_d0,
+                             const int theta_d1, int* n, const int* sampling,
+                             const int* lmax_calc, const int* extend, const double* radius,
+                             int* exitstatus);
 
 /* include/shtools.h:153-165 (src/MakeGridGLQ.f95:1) */
 SHTC_API void MakeGridGLQ(double* gridglq, const int gridglq_d0, const int gridglq_d1,

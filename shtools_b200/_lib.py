@@ -38,7 +38,8 @@ EXPORTS = (
     "shtc_dhaj", "MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ",
     "SHGLQ", "PreGLQ", "DHaj", "shtc_plan_create_dhc", "shtc_plan_create_glqc",
     "shtc_synthesis_c", "shtc_analysis_c", "MakeGridDHC", "SHExpandDHC",
-    "MakeGridGLQC", "SHExpandGLQC",
+    "MakeGridGLQC", "SHExpandGLQC", "shtc_gradient_workspace_bytes",
+    "shtc_gradient_dh", "MakeGradientDH",
 )
 
 
@@ -83,6 +84,9 @@ def _bind(L):
                                         _I, _P]
     L.shtc_synthesis_c.argtypes = [_P] + coef + grid + tail
     L.shtc_analysis_c.argtypes = [_P] + grid + coef + tail
+    L.shtc_gradient_workspace_bytes.restype = _SZ
+    L.shtc_gradient_workspace_bytes.argtypes = [_P, _I]
+    L.shtc_gradient_dh.argtypes = [_P] + coef + [_P, _P, _LL, _LL, _LL, _D] + tail
     L.shtc_preglq.argtypes = [_D, _D, _I, _P, _P, _P]
     L.shtc_dhaj.argtypes = [_I, _P, _I, _P]
     L.MakeGridDH.argtypes = [_DP, _I, _I, _IP, _DP, _I, _I, _IP, _IP, _IP, _IP, _IP,
@@ -99,9 +103,11 @@ def _bind(L):
     L.SHExpandDHC.argtypes = [_P, _I, _I, _I, _P, _I, _IP, _IP, _IP, _IP, _IP, _IP]
     L.MakeGridGLQC.argtypes = [_P, _I, _I, _P, _I, _I, _DP, _DP, _IP, _IP, _IP, _IP, _IP]
     L.SHExpandGLQC.argtypes = [_P, _I, _I, _P, _DP, _DP, _DP, _IP, _IP, _IP, _IP]
+    L.MakeGradientDH.argtypes = [_DP, _I, _I, _DP, _DP, _I, _I, _IP, _IP, _IP, _IP, _DP,
+                                 _IP]
     for name in ("MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ", "SHGLQ",
                  "PreGLQ", "DHaj", "MakeGridDHC", "SHExpandDHC", "MakeGridGLQC",
-                 "SHExpandGLQC"):
+                 "SHExpandGLQC", "MakeGradientDH"):
         getattr(L, name).restype = None
     return L
 

@@ -143,7 +143,16 @@ def SHExpandGLQC(gridglq, w=None, zero=None, norm=1, csphase=1, lmax_calc=None):
                                lmax_calc=lmax_calc))
 
 
-MakeGradientDH = _passthrough("MakeGradientDH")
+def MakeGradientDH(cilm, lmax=None, sampling=1, lmax_calc=None, extend=False,
+                   radius=None):
+    """theta, phi = MakeGradientDH(cilm, [lmax, sampling, lmax_calc, extend,
+    radius]) -- see src/MakeGradientDH.f95:1 and ducc0_wrapper.py:1164."""
+    th, ph = _t.MakeGradientDH(np.asarray(cilm, dtype=np.float64), lmax=lmax,
+                               sampling=sampling, lmax_calc=lmax_calc, extend=extend,
+                               radius=radius)
+    return _np(th), _np(ph)
+
+
 SHRotateRealCoef = _passthrough("SHRotateRealCoef")
 
 

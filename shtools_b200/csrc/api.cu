@@ -280,6 +280,39 @@ extern "C" int shtc_analysis_c(const shtc_plan* P, const void* grid, long long g
 }
 
 // ---------------------------------------------------------------------------
+// MakeGradientDH: a real DH plan with norm 1 and csphase 1 (the reference's
+// only case); workspace = packed (3 nfield) | spectra (3 nfield) | (2 nfield)
+// ---------------------------------------------------------------------------
+extern "C" size_t shtc_gradient_workspace_bytes(const shtc_plan* P, int nfield) {
+    if (!P || nfield < 1) return 0;
+    return coef_region(P, 3 * nfield) + spec_region(P, 3 * nfield) +
+           spec_region(P, 2 * nfield);
+}
+
+extern "C" int shtc_gradient_dh(const shtc_plan* P, const double* cilm, long long csf,
+                                long long csk, long long csl, long long csm, int cdim,
+                                double* theta, double* phi, long long gsf, long long gsr,
+                                long long gsc, double radius, int nfield, void* work,
+                                size_t wb, void* stream) {
+    if (!P || !cilm || !theta || !phi) return SHTC_EHANDLE;
+    if (nfield < 1) return SHTC_EBOUND;
+    if (P->kind != SHTC_GRID_DH || P->cplx || P->norm != 1 || P->csphase != 1)
+        return SHTC_EBOUND;
+    if (!(radius > 0.0) && !(radius < 0.0)) return SHTC_EBOUND;
+    if (cdim < 1) return SHTC_EDIM;
+    if (!work || wb < shtc_gradient_workspace_bytes(P, nfield)) return SHTC_EWORK;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != P->device) return SHTC_EHANDLE;
+    char* w = (char*)work;
+    double2* packed = (double2*)w;
+    double2* spec = (double2*)(w + coef_region(P, 3 * nfield));
+    double2* spec2 = (double2*)(w + coef_region(P, 3 * nfield) + spec_region(P, 3 * nfield));
+    return launch_gradient_dh(P, cilm, csf, csk, csl, csm, cdim, theta, phi, gsf, gsr, gsc,
+                              radius, nfield, packed, spec, spec2, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
 // host drop-ins of include/shtools.h
 // ---------------------------------------------------------------------------
 namespace {
@@ -674,6 +707,50 @@ extern "C" void SHExpandGLQC(shtc_complex* cilm, const int cdim, const int lmax,
     if (!rc) rc = shtc_analysis_c(P, dg.p, 0, 1, nlat, dc.p, 0, 1, 2, 2LL * cdim, cdim, 1,
                                   dw.p, wb, st);
     if (!rc) rc = map_cuda(cudaMemcpyAsync(cilm, dc.p, cb, cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
+    set_status(exitstatus, rc);
+}
+
+// src/cWrapper.f95:295-317 (src/MakeGradientDH.f95:1)
+extern "C" void MakeGradientDH(const double* cilm, const int cdim, const int lmax,
+                               double* theta, double* phi, const int d0, const int d1,
+                               int* n, const int* sampling, const int* lmax_calc,
+                               const int* extend, const double* radius, int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    const int nn = 2 * lmax + 2;
+    if (n) *n = nn;
+    const int samp = opt(sampling, 1), ext = opt(extend, 0);
+    const double r = radius ? *radius : 1.0;
+    if (samp != 1 && samp != 2) return set_status(exitstatus, SHTC_EBOUND);
+    if (ext != 0 && ext != 1) return set_status(exitstatus, SHTC_EBOUND);
+    const int nlat_out = nn + ext, nlon_out = samp * nn + ext;
+    if (d0 < nlat_out || d1 < nlon_out) return set_status(exitstatus, SHTC_EDIM);
+    int lc = lmax < cdim - 1 ? lmax : cdim - 1;
+    if (lmax_calc) {
+        if (*lmax_calc > lmax) return set_status(exitstatus, SHTC_EBOUND);
+        if (*lmax_calc < lc) lc = *lmax_calc;
+    }
+    if (lc < 0) return set_status(exitstatus, SHTC_EDIM);
+    cudaStream_t st = cudaStreamPerThread;
+    shtc_plan* P = nullptr;
+    int rc = cached_plan(SHTC_GRID_DH, lmax, lc, 1, 1, samp, ext, nullptr, nullptr, &P, st);
+    if (rc) return set_status(exitstatus, rc);
+    DevBuf dc, dt, dp, dw;
+    const size_t wb = shtc_gradient_workspace_bytes(P, 1);
+    const size_t gb = sizeof(double) * (size_t)d0 * d1;
+    if ((rc = dc.alloc(sizeof(double) * 2 * (size_t)cdim * cdim)) || (rc = dt.alloc(gb)) ||
+        (rc = dp.alloc(gb)) || (rc = dw.alloc(wb)))
+        return set_status(exitstatus, rc);
+    rc = map_cuda(cudaMemcpyAsync(dc.p, cilm, sizeof(double) * 2 * (size_t)cdim * cdim,
+                                  cudaMemcpyHostToDevice, st));
+    if (!rc) rc = shtc_gradient_dh(P, (const double*)dc.p, 0, 1, 2, 2LL * cdim, cdim,
+                                   (double*)dt.p, (double*)dp.p, 0, 1, d0, r, 1, dw.p, wb, st);
+    if (!rc) rc = map_cuda(cudaMemcpy2DAsync(theta, sizeof(double) * d0, dt.p,
+                                             sizeof(double) * d0, sizeof(double) * nlat_out,
+                                             nlon_out, cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaMemcpy2DAsync(phi, sizeof(double) * d0, dp.p,
+                                             sizeof(double) * d0, sizeof(double) * nlat_out,
+                                             nlon_out, cudaMemcpyDeviceToHost, st));
     if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
     set_status(exitstatus, rc);
 }

@@ -658,4 +658,109 @@ int launch_fft_c2c_anal(const shtc_plan* P, const double2* grid, long long gf,
     return map_cuda(cudaGetLastError());
 }
 
+// ---------------------------------------------------------------------------
+// MakeGradientDH (src/MakeGradientDH.f95): horizontal gradient on a DH grid.
+// With (1 - z^2) dP_l/dz = a_l P_(l-1) - l z P_l, a_l = sqrt((2l+1)(l-m)(l+m)/(2l-1)),
+// the theta sums are (S1 - z S2)/u^2 with S1 = sum_l c_(l+1) a_(l+1) P_l and
+// S2 = sum_l l c_l P_l, and the phi sums are i m S0 with S0 = sum_l c_l P_l:
+// three ordinary Legendre sums per field (internal fields 3u, 3u+1, 3u+2),
+// evaluated by the synthesis kernels in one recursion pass.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double grad_a(int l, int m) {
+    // sqr(2l+1) * sqr(l-m) * sqr(l+m) / sqr(2l-1), MakeGradientDH.f95:487
+    return sqrt((double)(2 * l + 1)) * sqrt((double)(l - m)) * sqrt((double)(l + m)) /
+           sqrt((double)(2 * l - 1));
+}
+
+__global__ void k_pack_grad(const double* __restrict__ cilm, long long sf, long long sk,
+                            long long sl, long long sm, int cdim,
+                            double2* __restrict__ packed, int lc, int nfield,
+                            const double2* __restrict__ rec) {
+    const int m = blockIdx.y;
+    const int l = m + blockIdx.x * blockDim.x + threadIdx.x;
+    const int u = blockIdx.z;
+    if (l > lc) return;
+    const long long idx = packed_off(m, lc) + (l - m);
+    const double* b = cilm + u * sf;
+    double c = 0.0, s = 0.0, c1 = 0.0, s1 = 0.0;
+    if (l < cdim) {
+        c = b[l * sl + m * sm];
+        s = m == 0 ? 0.0 : b[sk + l * sl + m * sm];
+    }
+    if (l + 1 <= lc && l + 1 < cdim) {
+        const double a = grad_a(l + 1, m);
+        c1 = b[(l + 1) * sl + m * sm] * a;
+        s1 = m == 0 ? 0.0 : b[sk + (l + 1) * sl + m * sm] * a;
+    }
+    const double d = rec[idx].y;
+    double2* o = packed + idx * (3LL * nfield) + 3 * u;
+    o[0] = make_double2(c * d, s * d);
+    o[1] = make_double2(c1 * d, s1 * d);
+    o[2] = make_double2((double)l * c * d, (double)l * s * d);
+}
+
+// spec fields 3u..3u+2 -> c2r inputs of the theta (field u) and phi (field
+// nfield + u) grids, with the per-ring factors -sin(theta)/(r u^2) and
+// 1/(r sin(theta)) (MakeGradientDH.f95:539, 548); zero on the pole rows.
+__global__ void k_grad_combine(const double2* __restrict__ spec, double2* __restrict__ out,
+                               const double* __restrict__ zp, int npair, int lc, int nlat,
+                               int nfield, double inv_r) {
+    const long long per = (long long)npair * (lc + 1) * 2;   // one field
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int u = blockIdx.y;
+    if (i >= per) return;
+    const int h = (int)(i & 1);
+    const int m = (int)((i >> 1) % (lc + 1));
+    const int p = (int)((i >> 1) / (lc + 1));
+    const double2 x0 = spec[(3LL * u + 0) * per + i];
+    const double2 x1 = spec[(3LL * u + 1) * per + i];
+    const double2 x2 = spec[(3LL * u + 2) * per + i];
+    double2 t = make_double2(0.0, 0.0), f = make_double2(0.0, 0.0);
+    if (p > 0) {
+        const double z = h ? -zp[p] : zp[p];
+        const double uu = sqrt((1.0 - z) * (1.0 + z));
+        const double st = 2 * p == nlat ? 1.0 : sinpi((double)p / (double)nlat);
+        const double ct = -st * inv_r / (uu * uu);
+        t = make_double2(ct * (x1.x - z * x2.x), ct * (x1.y - z * x2.y));
+        const double cp = (double)m * inv_r / st;
+        f = make_double2(-cp * x0.y, cp * x0.x);
+    }
+    out[(long long)u * per + i] = t;
+    out[((long long)nfield + u) * per + i] = f;
+}
+
+int launch_gradient_dh(const shtc_plan* P, const double* cilm, long long sf, long long sk,
+                       long long sl, long long sm, int cdim, double* theta, double* phi,
+                       long long gf, long long grs, long long gcs, double radius,
+                       int nfield, double2* packed, double2* spec, double2* spec2,
+                       cudaStream_t st) {
+    const int lc = P->lc;
+    stage_begin(SHTC_STAGE_PACK, st);
+    {
+        dim3 grid((lc + 1 + 127) / 128, lc + 1, nfield);
+        k_pack_grad<<<grid, 128, 0, st>>>(cilm, sf, sk, sl, sm, cdim, packed, lc, nfield,
+                                          P->d_rec);
+    }
+    stage_end(SHTC_STAGE_PACK, st);
+    int rc = map_cuda(cudaGetLastError());
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_LEGENDRE_SYNTH, st);
+    rc = launch_legendre_synth(P, packed, spec, 3 * nfield, st);
+    stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_FFT_C2R, st);
+    {
+        const long long per = (long long)P->npair * (lc + 1) * 2;
+        dim3 grid((unsigned)((per + 255) / 256), nfield);
+        k_grad_combine<<<grid, 256, 0, st>>>(spec, spec2, P->d_z, P->npair, lc, P->nlat,
+                                             nfield, 1.0 / radius);
+        rc = map_cuda(cudaGetLastError());
+        if (!rc) rc = launch_fft_c2r(P, spec2, theta, SHTC_F64, gf, grs, gcs, nfield, 0, st);
+        if (!rc) rc = launch_fft_c2r(P, spec2 + (long long)nfield * per, phi, SHTC_F64, gf,
+                                     grs, gcs, nfield, 0, st);
+    }
+    stage_end(SHTC_STAGE_FFT_C2R, st);
+    return rc;
+}
+
 }  // namespace shtc

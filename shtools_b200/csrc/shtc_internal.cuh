@@ -136,6 +136,12 @@ int launch_unpack_coef_c(const shtc_plan* P, const double2* partial, int ntiles,
 int launch_fft_c2c_synth(const shtc_plan* P, const double2* spec, double2* grid,
                          long long gf, long long grs, long long gcs, int nfield,
                          cudaStream_t st);
+// MakeGradientDH: workspace = packed (3 nfield) | spec (3 nfield) | spec2 (2 nfield)
+int launch_gradient_dh(const shtc_plan* P, const double* cilm, long long sf, long long sk,
+                       long long sl, long long sm, int cdim, double* theta, double* phi,
+                       long long gf, long long grs, long long gcs, double radius,
+                       int nfield, double2* packed, double2* spec, double2* spec2,
+                       cudaStream_t st);
 int launch_fft_c2c_anal(const shtc_plan* P, const double2* grid, long long gf,
                         long long grs, long long gcs, double2* spec, int nfield,
                         cudaStream_t st);

@@ -532,6 +532,42 @@ def SHExpandGLQC(gridglq, w=None, zero=None, norm=1, csphase=1, lmax_calc=None):
     return _anal_c(grid, plan, lc + 1)
 
 
+def MakeGradientDH(cilm, lmax=None, sampling=1, lmax_calc=None, extend=False,
+                   radius=None):
+    """Horizontal gradient of a real field on a Driscoll-Healy grid, on the
+    GPU (src/MakeGradientDH.f95:1): returns (theta, phi) with
+    theta = (1/r) dF/dtheta and phi = 1/(r sin theta) dF/dphi, zero on the
+    pole rows.  cilm: (..., 2, D, D), 4-pi normalised without the
+    Condon-Shortley phase (the reference's only convention).  Not
+    differentiable."""
+    if sampling not in (1, 2):
+        raise ValueError("sampling must be 1 (n by n) or 2 (n by 2n); got %r"
+                         % (sampling,))
+    lmax, lc = _resolve_synth(np.shape(cilm), lmax, lmax_calc)
+    r = 1.0 if radius is None else float(radius)
+    if r == 0.0 or r != r:
+        raise ValueError("radius must be a nonzero number; got %r" % (radius,))
+    c = _as_cuda(cilm, "cilm").to(torch.float64)
+    plan = get_plan(GRID_DH, lmax, lc, 1, 1, sampling, int(bool(extend)), device=c.device)
+    cf, lead = _flat(c[..., :2, :, :], 3)
+    F = cf.shape[0]
+    shape = (F, plan.info["nlat_out"], plan.info["nlon_out"])
+    th = torch.empty(shape, dtype=torch.float64, device=c.device)
+    ph = torch.empty(shape, dtype=torch.float64, device=c.device)
+    lib = plan.lib
+    nb = int(lib.shtc_gradient_workspace_bytes(plan.handle, F))
+    ws = torch.empty(max(nb, 8), dtype=torch.uint8, device=c.device)
+    with torch.cuda.device(c.device):
+        rc = lib.shtc_gradient_dh(plan.handle, ctypes_void(cf.data_ptr()), cf.stride(0),
+                                  cf.stride(1), cf.stride(2), cf.stride(3), cf.shape[2],
+                                  ctypes_void(th.data_ptr()), ctypes_void(ph.data_ptr()),
+                                  th.stride(0), th.stride(1), th.stride(2), r, F,
+                                  ctypes_void(ws.data_ptr()), nb, _stream_ptr(c.device))
+    _lib.check(rc, "shtc_gradient_dh")
+    out = tuple(lead) + shape[1:]
+    return th.reshape(out), ph.reshape(out)
+
+
 def _host64(a, n, what):
     if isinstance(a, torch.Tensor):
         a = a.detach().cpu().numpy()

@@ -69,7 +69,7 @@ def test_backend_module_surface():
     # names outside the GPU transforms delegate to the reference backend,
     # which is not importable here
     with pytest.raises(NotImplementedError):
-        backend.MakeGradientDH(np.zeros((2, 3, 3)))
+        backend.SHRotateRealCoef(np.zeros((2, 3, 3)), np.zeros(3), np.zeros((4, 4, 4)))
 
 
 def test_backend_register_into_registry():
