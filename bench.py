@@ -48,6 +48,9 @@ WORKLOADS = {
     # lmax 719, sampling 2
     "dhc719x8": dict(kind="dhc", lmax=719, nfield=8, sampling=2, beta=2.0,
                      seed=3500),
+    # MakeGradientDH, config 3 shape: 8 fields, lmax 719, sampling 2
+    "gradient719x8": dict(kind="gradient", lmax=719, nfield=8, sampling=2, beta=2.0,
+                          seed=3700),
     # config 1 shape: one DH field, lmax 255, sampling 2
     "dh255": dict(kind="dh", lmax=255, nfield=1, sampling=2, beta=2.0,
                   seed=1000),
@@ -582,6 +585,99 @@ def run_cuda_grad(args, w, rank, world, local_rank):
     }
 
 
+def run_cuda_gradient(args, w, rank, world, local_rank):
+    """MakeGradientDH of every field per step (one transform per field, two
+    output grids), through the public torch API."""
+    import numpy as np
+    import torch
+    import shtools_b200 as sht
+    from shtools_b200 import _lib
+    from shtools_b200.pipeline import pipelined
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    L, F, s_ = w["lmax"], w["nfield"], w["sampling"]
+    c_host = torch.from_numpy(np.stack([power_law(L, w["seed"] + i, w["beta"])
+                                        for i in range(F)])).pin_memory()
+    c = c_host.to(dev)
+    st = torch.cuda.current_stream(dev)
+    step = lambda x: sht.MakeGradientDH(x, sampling=s_)
+    for _ in range(args.warmup):
+        th, ph = step(c)
+    torch.cuda.synchronize(dev)
+    # size-independent check: the phi component of a zonal field (m = 0) is 0
+    zonal = c.clone()
+    zonal[:, :, :, 1:] = 0.0
+    zero_phi = float(step(zonal)[1].abs().max().item())
+    peak = fp64_peak(torch, dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    torch.cuda.synchronize(dev)
+    lib.shtc_timing_enable(1)
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            evs[i][0].record(st)
+            step(c)
+            evs[i][1].record(st)
+        torch.cuda.synchronize(dev)
+    lib.shtc_timing_enable(0)
+    import ctypes
+    ms = (ctypes.c_double * 6)()
+    cnt = (ctypes.c_int * 6)()
+    lib.shtc_timing_collect(ms, cnt, 6)
+    total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), dev)
+    value = 1.0 * F * args.steps * world / (total_ms * 1e-3)
+    # end to end: host coefficients in, both host grids out, pipelined
+    outs = [(torch.empty(tuple(th.shape), dtype=th.dtype).pin_memory(),
+             torch.empty(tuple(ph.shape), dtype=ph.dtype).pin_memory()) for _ in range(2)]
+    e2e_steps = max(2, min(args.steps, 10))
+    pipelined(step, [(c_host,)] * 2, outs, device=dev)
+    torch.cuda.synchronize(dev)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    pipelined(step, [(c_host,)] * e2e_steps, [outs[i % 2] for i in range(e2e_steps)],
+              device=dev)
+    b.record(st)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(a.elapsed_time(b), dev)
+    names = ["pack", "legendre_synth", "fft_c2r", "fft_r2c", "legendre_anal", "unpack"]
+    per_launch_ms = ms[1] / max(1, cnt[1])
+    fl = 3.0 * flops_per_transform(w) * F        # three Legendre sums per field
+    achieved = fl / (per_launch_ms * 1e-3) / 1e12
+    return {
+        "metric": METRIC, "value": value, "unit": "transforms/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic seeded power-law coefficients, S(l)=(l+1)^-%g" % w["beta"],
+        "config": {"workload": args.workload, "kind": "dh gradient", "lmax": L,
+                   "fields_per_gpu": F, "sampling": s_, "precision": "fp64",
+                   "step": "MakeGradientDH of every field (theta and phi grids)",
+                   "l2": "flushed between steps (256 MiB write, outside step events)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "roofline": {"kernel": "legendre_synth", "bound": "fp64", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None,
+                     "peak_source": "measured FP64 FMA probe, this run",
+                     "flops_per_launch": fl, "traffic": None},
+        "stages": {names[i]: {"ms_per_launch": (ms[i] / cnt[i]) if cnt[i] else None,
+                              "launches": cnt[i]} for i in range(6)},
+        "zonal_field_max_abs_phi": zero_phi,
+        "e2e": {"value": 1.0 * F * e2e_steps * world / (e2e_ms * 1e-3),
+                "unit": "transforms/s", "steps": e2e_steps,
+                "h2d_bytes_per_step": c_host.numel() * 8,
+                "d2h_bytes_per_step": (outs[0][0].numel() + outs[0][1].numel()) * 8,
+                "path": "public torch API on pinned host buffers, pipelined on 3 streams"},
+        # the FFT stage holds 3 launches (combination, theta c2r, phi c2r)
+        "gpu_launches": int(sum(cnt)) + 2 * int(cnt[2]),
+        "clocks": clk.summary(),
+    }
+
+
 def run_cuda(args, w, rank, world, local_rank):
     import numpy as np
     import torch
@@ -780,9 +876,12 @@ def main():
         res = run_cuda_batch(args, w, rank, world, local_rank)
     elif w["kind"] == "dh_grad":
         res = run_cuda_grad(args, w, rank, world, local_rank)
+    elif w["kind"] == "gradient":
+        res = run_cuda_gradient(args, w, rank, world, local_rank)
     else:
         res = run_cuda(args, w, rank, world, local_rank)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and w["kind"] != "dhc":
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and \
+            w["kind"] not in ("dhc", "gradient"):
         one_step, sample, threads = cpu_sample(w, args.cpu_seconds / 2)
         v, dt = one_step()
         res["cpu_baseline"] = {"value": v, "unit": "transforms/s",
