@@ -158,7 +158,7 @@ __device__ __forceinline__ void dft_small(double2* v) {
 
 // One Stockham pass of radix R from x to y (ping-pong shared buffers).
 // tw: this pass's base twiddles, entry k < ns = exp(-2 pi i k/(ns R)); the
-// powers w^q, q >= 2, are formed by repeated multiplication.
+// powers w^q, q >= 2, are formed by multiplication.
 template <int R, int SIGN>
 __device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
                                          double2* __restrict__ y, int M, int ns,
@@ -172,14 +172,14 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = x[j + q * nr];
         if (k != 0) {
-            const double2 w = twv<SIGN>(tw, k);
-            double2 wq = w;
-            v[1] = cmul(v[1], w);
+            // w^q = w^(q/2) * w^(q - q/2): a product tree of depth log2(R)
+            // instead of a chain of R-2 dependent multiplications
+            double2 wp[R];
+            wp[1] = twv<SIGN>(tw, k);
 #pragma unroll
-            for (int q = 2; q < R; ++q) {
-                wq = cmul(wq, w);
-                v[q] = cmul(v[q], wq);
-            }
+            for (int q = 2; q < R; ++q) wp[q] = cmul(wp[q / 2], wp[q - q / 2]);
+#pragma unroll
+            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], wp[q]);
         }
         dft_small<R, SIGN>(v);
         const int d = (j - k) * R + k;
