@@ -280,6 +280,21 @@ SHTC_API int shtc_gradient_dh(const shtc_plan* plan, const double* cilm, long lo
                               long long gsc, double radius, int nfield, void* work,
                               size_t work_bytes, void* stream);
 
+/* SHMultiply (src/SHMultiply.f95:1) on device buffers: the product of fields
+ * of degrees lmax1 and lmax2, expanded to lmax1 + lmax2, through the GLQ grid
+ * of a plan created with shtc_plan_create_glq for lmax = lmax1 + lmax2
+ * (extend 0, lmax_calc = lmax).  cilm1/cilm2 are read up to their own
+ * degree; cilmout has cilm_dim_out >= lmax1 + lmax2 + 1.  Workspace:
+ * shtc_multiply_workspace_bytes(plan, nfield). */
+SHTC_API size_t shtc_multiply_workspace_bytes(const shtc_plan* plan, int nfield);
+SHTC_API int shtc_multiply(const shtc_plan* plan, const double* cilm1, long long c1sf,
+                           long long c1sk, long long c1sl, long long c1sm, int lmax1,
+                           const double* cilm2, long long c2sf, long long c2sk,
+                           long long c2sl, long long c2sm, int lmax2, double* cilmout,
+                           long long csf, long long csk, long long csl, long long csm,
+                           int cilm_dim_out, int nfield, void* work, size_t work_bytes,
+                           void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Drop-ins of the reference C interface, include/shtools.h.  Host arrays,  */
 /* Fortran column-major: cilm(2, cilm_dim, cilm_dim), grid(d0, d1).  NULL  */
@@ -341,6 +356,12 @@ SHTC_API void MakeGradientDH(const double* cilm, const int cilm_dim, const int l
                              const int theta_d1, int* n, const int* sampling,
                              const int* lmax_calc, const int* extend, const double* radius,
                              int* exitstatus);
+
+/* include/shtools.h:254-265 (src/SHMultiply.f95:1); precomp is ignored */
+SHTC_API void SHMultiply(double* cilmout, const int cilmout_dim, const double* cilm1,
+                         const int cilm1_dim, const int lmax1, const double* cilm2,
+                         const int cilm2_dim, const int lmax2, const int* precomp,
+                         const int* norm, const int* csphase, int* exitstatus);
 
 /* include/shtools.h:153-165 (src/MakeGridGLQ.f95:1) */
 SHTC_API void MakeGridGLQ(double* gridglq, const int gridglq_d0, const int gridglq_d1,

@@ -58,6 +58,7 @@ def lib():
                                       _D, _D, _I]
         L.orc_dhaj.argtypes = [_I, _D, _I]
         L.orc_makegradient_dh.argtypes = [_D, _D, _D, _I, _I, _I, _I, _I, ctypes.c_double]
+        L.orc_shmultiply.argtypes = [_D, _I, _D, _I, _I, _D, _I, _I, _I, _I]
         L.orc_makegrid_dhc.argtypes = [_D, _D, _I, _I, _I, _I, _I, _I, _I]
         L.orc_shexpand_dhc.argtypes = [_D, _I, _D, _I, _I, _I, _I, _I, _I]
         L.orc_makegrid_glqc.argtypes = [_D, _D, _I, _I, _D, _I, _I, _I, _I]
@@ -347,3 +348,16 @@ def makegradient_dh(cilm, lmax=None, sampling=1, lmax_calc=None, extend=0, radiu
     _check(lib().orc_makegradient_dh(_p(th), _p(ph), _p(cilm), cilm.shape[1], lmax,
                                      int(sampling), lmax_calc, int(extend), float(radius)))
     return th, ph
+
+
+def shmultiply(cilm1, cilm2, lmax1=None, lmax2=None, norm=1, csphase=1):
+    """SHMultiply (SHMultiply.f95:1).  Returns (2, lmax1+lmax2+1, lmax1+lmax2+1)."""
+    c1 = _f64(cilm1)
+    c2 = _f64(cilm2)
+    lmax1 = c1.shape[1] - 1 if lmax1 is None else int(lmax1)
+    lmax2 = c2.shape[1] - 1 if lmax2 is None else int(lmax2)
+    lo = lmax1 + lmax2
+    out = np.zeros((2, lo + 1, lo + 1))
+    _check(lib().orc_shmultiply(_p(out), lo + 1, _p(c1), c1.shape[1], lmax1, _p(c2),
+                                c2.shape[1], lmax2, int(norm), int(csphase)))
+    return out

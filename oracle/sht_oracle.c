@@ -1794,6 +1794,44 @@ int orc_makegradient_dh(double *theta_g, double *phi_g, const double *cilm, int 
     return ORC_OK;
 }
 
+/* ======================================================================== */
+/*  SHMultiply (src/SHMultiply.f95:1-375): the product of two fields of      */
+/*  degrees lmax1 and lmax2 expanded to lmax1 + lmax2 through a GLQ grid of */
+/*  that degree: MakeGridGLQ of both, pointwise product, SHExpandGLQ.       */
+/*  cilm arrays are (2, dim, dim); cilmout must have dim >= lmax1+lmax2+1.  */
+/* ======================================================================== */
+int orc_shmultiply(double *cout, int cdout, const double *c1, int cd1, int lmax1,
+                   const double *c2, int cd2, int lmax2, int norm, int csphase) {
+    if (cd1 < lmax1 + 1 || cd2 < lmax2 + 1 || cdout < lmax1 + lmax2 + 1) return ORC_EDIM;
+    const int lo = lmax1 + lmax2;
+    const int nlat = lo + 1, nlong = 2 * lo + 1;
+    double *zero = malloc(sizeof(double) * (size_t)nlat), *w = malloc(sizeof(double) * (size_t)nlat);
+    int rc = orc_preglq(-1.0, 1.0, nlat, zero, w);
+    /* the fields restricted to their degrees (cilm1(1:2,1:lmax1+1,1:lmax1+1)) */
+    double *a1 = calloc((size_t)2 * (lmax1 + 1) * (lmax1 + 1), sizeof(double));
+    double *a2 = calloc((size_t)2 * (lmax2 + 1) * (lmax2 + 1), sizeof(double));
+    for (int k = 0; k < 2; ++k)
+        for (int l = 0; l <= lmax1; ++l)
+            for (int m = 0; m <= lmax1; ++m)
+                a1[((size_t)k * (lmax1 + 1) + l) * (lmax1 + 1) + m] =
+                    c1[((size_t)k * cd1 + l) * cd1 + m];
+    for (int k = 0; k < 2; ++k)
+        for (int l = 0; l <= lmax2; ++l)
+            for (int m = 0; m <= lmax2; ++m)
+                a2[((size_t)k * (lmax2 + 1) + l) * (lmax2 + 1) + m] =
+                    c2[((size_t)k * cd2 + l) * cd2 + m];
+    double *g1 = malloc(sizeof(double) * (size_t)nlat * nlong);
+    double *g2 = malloc(sizeof(double) * (size_t)nlat * nlong);
+    if (!rc) rc = orc_makegrid_glq(g1, a1, lmax1 + 1, lo, zero, norm, csphase, -1, 0);
+    if (!rc) rc = orc_makegrid_glq(g2, a2, lmax2 + 1, lo, zero, norm, csphase, -1, 0);
+    if (!rc) {
+        for (size_t i = 0; i < (size_t)nlat * nlong; ++i) g1[i] = g1[i] * g2[i];
+        rc = orc_shexpand_glq(cout, cdout, lo, g1, nlong, w, zero, norm, csphase, lo);
+    }
+    free(zero); free(w); free(a1); free(a2); free(g1); free(g2);
+    return rc;
+}
+
 /* Number of host threads OpenMP would use (1 when built without OpenMP). */
 int orc_max_threads(void) {
 #ifdef _OPENMP

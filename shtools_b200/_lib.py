@@ -39,7 +39,8 @@ EXPORTS = (
     "SHGLQ", "PreGLQ", "DHaj", "shtc_plan_create_dhc", "shtc_plan_create_glqc",
     "shtc_synthesis_c", "shtc_analysis_c", "MakeGridDHC", "SHExpandDHC",
     "MakeGridGLQC", "SHExpandGLQC", "shtc_gradient_workspace_bytes",
-    "shtc_gradient_dh", "MakeGradientDH",
+    "shtc_gradient_dh", "MakeGradientDH", "shtc_multiply_workspace_bytes",
+    "shtc_multiply", "SHMultiply",
 )
 
 
@@ -87,6 +88,10 @@ def _bind(L):
     L.shtc_gradient_workspace_bytes.restype = _SZ
     L.shtc_gradient_workspace_bytes.argtypes = [_P, _I]
     L.shtc_gradient_dh.argtypes = [_P] + coef + [_P, _P, _LL, _LL, _LL, _D] + tail
+    L.shtc_multiply_workspace_bytes.restype = _SZ
+    L.shtc_multiply_workspace_bytes.argtypes = [_P, _I]
+    L.shtc_multiply.argtypes = ([_P, _P, _LL, _LL, _LL, _LL, _I, _P, _LL, _LL, _LL, _LL, _I]
+                                + coef + tail)
     L.shtc_preglq.argtypes = [_D, _D, _I, _P, _P, _P]
     L.shtc_dhaj.argtypes = [_I, _P, _I, _P]
     L.MakeGridDH.argtypes = [_DP, _I, _I, _IP, _DP, _I, _I, _IP, _IP, _IP, _IP, _IP,
@@ -105,7 +110,8 @@ def _bind(L):
     L.SHExpandGLQC.argtypes = [_P, _I, _I, _P, _DP, _DP, _DP, _IP, _IP, _IP, _IP]
     L.MakeGradientDH.argtypes = [_DP, _I, _I, _DP, _DP, _I, _I, _IP, _IP, _IP, _IP, _DP,
                                  _IP]
-    for name in ("MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ", "SHGLQ",
+    L.SHMultiply.argtypes = [_DP, _I, _DP, _I, _I, _DP, _I, _I, _IP, _IP, _IP, _IP]
+    for name in ("SHMultiply", "MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ", "SHGLQ",
                  "PreGLQ", "DHaj", "MakeGridDHC", "SHExpandDHC", "MakeGridGLQC",
                  "SHExpandGLQC", "MakeGradientDH"):
         getattr(L, name).restype = None

@@ -313,6 +313,76 @@ extern "C" int shtc_gradient_dh(const shtc_plan* P, const double* cilm, long lon
 }
 
 // ---------------------------------------------------------------------------
+// SHMultiply: both fields synthesised on the GLQ grid of the plan (degree
+// lmax1 + lmax2), the analysis FFT reads the two grids and transforms their
+// pointwise product.  Workspace: packed / partial sums (2 nfield) | spectra
+// (2 nfield) | grids (2 nfield x nlat x nlon doubles).
+// ---------------------------------------------------------------------------
+static size_t grid_region(const shtc_plan* P, int nfield) {
+    return align256((size_t)nfield * P->nlat * P->nlon * sizeof(double));
+}
+
+extern "C" size_t shtc_multiply_workspace_bytes(const shtc_plan* P, int nfield) {
+    if (!P || nfield < 1) return 0;
+    return coef_region(P, 2 * nfield) + spec_region(P, 2 * nfield) +
+           grid_region(P, 2 * nfield);
+}
+
+extern "C" int shtc_multiply(const shtc_plan* P, const double* cilm1, long long c1sf,
+                             long long c1sk, long long c1sl, long long c1sm, int lmax1,
+                             const double* cilm2, long long c2sf, long long c2sk,
+                             long long c2sl, long long c2sm, int lmax2, double* cilmout,
+                             long long csf, long long csk, long long csl, long long csm,
+                             int cdim_out, int nfield, void* work, size_t wb, void* stream) {
+    if (!P || !cilm1 || !cilm2 || !cilmout) return SHTC_EHANDLE;
+    if (nfield < 1 || lmax1 < 0 || lmax2 < 0) return SHTC_EBOUND;
+    if (P->kind != SHTC_GRID_GLQ || P->cplx || P->extend || P->lmax != lmax1 + lmax2 ||
+        P->lc != P->lmax)
+        return SHTC_EBOUND;
+    if (cdim_out < P->lmax + 1) return SHTC_EDIM;
+    if (!work || wb < shtc_multiply_workspace_bytes(P, nfield)) return SHTC_EWORK;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != P->device) return SHTC_EHANDLE;
+    cudaStream_t st = (cudaStream_t)stream;
+    char* w = (char*)work;
+    double2* packed = (double2*)w;
+    double2* spec = (double2*)(w + coef_region(P, 2 * nfield));
+    double* grids = (double*)(w + coef_region(P, 2 * nfield) + spec_region(P, 2 * nfield));
+    const long long gf = (long long)P->nlat * P->nlon;
+    const int tiles = anal_tiles(P);
+    stage_begin(SHTC_STAGE_PACK, st);
+    int rc = launch_pack_coef(P, cilm1, SHTC_F64, c1sf, c1sk, c1sl, c1sm, lmax1 + 1, packed,
+                              nfield, 0, st, 2 * nfield, 0);
+    if (!rc) rc = launch_pack_coef(P, cilm2, SHTC_F64, c2sf, c2sk, c2sl, c2sm, lmax2 + 1,
+                                   packed, nfield, 0, st, 2 * nfield, nfield);
+    stage_end(SHTC_STAGE_PACK, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_LEGENDRE_SYNTH, st);
+    rc = launch_legendre_synth(P, packed, spec, 2 * nfield, st);
+    stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_FFT_C2R, st);
+    rc = launch_fft_c2r(P, spec, grids, SHTC_F64, gf, P->nlon, 1, 2 * nfield, 0, st);
+    stage_end(SHTC_STAGE_FFT_C2R, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_FFT_R2C, st);
+    rc = launch_fft_r2c_product(P, grids, grids + (long long)nfield * gf, gf, P->nlon, 1, spec,
+                                nfield, st);
+    stage_end(SHTC_STAGE_FFT_R2C, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
+    rc = launch_legendre_anal(P, spec, packed, tiles, nfield, st);
+    stage_end(SHTC_STAGE_LEGENDRE_ANAL, st);
+    if (rc) return rc;
+    stage_begin(SHTC_STAGE_UNPACK, st);
+    rc = launch_unpack_coef(P, packed, tiles, cilmout, SHTC_F64, csf, csk, csl, csm, cdim_out,
+                            nfield, 1, st);
+    stage_end(SHTC_STAGE_UNPACK, st);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
 // host drop-ins of include/shtools.h
 // ---------------------------------------------------------------------------
 namespace {
@@ -751,6 +821,46 @@ extern "C" void MakeGradientDH(const double* cilm, const int cdim, const int lma
     if (!rc) rc = map_cuda(cudaMemcpy2DAsync(phi, sizeof(double) * d0, dp.p,
                                              sizeof(double) * d0, sizeof(double) * nlat_out,
                                              nlon_out, cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
+    set_status(exitstatus, rc);
+}
+
+// include/shtools.h:254-265 (src/SHMultiply.f95:1); precomp is accepted and
+// ignored (it selects the reference's precomputed Legendre tables)
+extern "C" void SHMultiply(double* cilmout, const int cdout, const double* cilm1,
+                           const int cd1, const int lmax1, const double* cilm2,
+                           const int cd2, const int lmax2, const int* precomp,
+                           const int* norm, const int* csphase, int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    (void)precomp;
+    if (lmax1 < 0 || lmax2 < 0) return set_status(exitstatus, SHTC_EBOUND);
+    if (cd1 < lmax1 + 1 || cd2 < lmax2 + 1 || cdout < lmax1 + lmax2 + 1)
+        return set_status(exitstatus, SHTC_EDIM);
+    const int nrm = opt(norm, 1), cs = opt(csphase, 1);
+    if (nrm < 1 || nrm > 4) return set_status(exitstatus, SHTC_EBOUND);
+    if (cs != 1 && cs != -1) return set_status(exitstatus, SHTC_EBOUND);
+    const int lo = lmax1 + lmax2;
+    cudaStream_t st = cudaStreamPerThread;
+    shtc_plan* P = nullptr;
+    int rc = cached_plan(SHTC_GRID_GLQ, lo, lo, nrm, cs, 1, 0, nullptr, nullptr, &P, st);
+    if (rc) return set_status(exitstatus, rc);
+    DevBuf d1, d2, dout, dw;
+    const size_t wb = shtc_multiply_workspace_bytes(P, 1);
+    const size_t b1 = sizeof(double) * 2 * (size_t)cd1 * cd1;
+    const size_t b2 = sizeof(double) * 2 * (size_t)cd2 * cd2;
+    const size_t bo = sizeof(double) * 2 * (size_t)cdout * cdout;
+    if ((rc = d1.alloc(b1)) || (rc = d2.alloc(b2)) || (rc = dout.alloc(bo)) ||
+        (rc = dw.alloc(wb)))
+        return set_status(exitstatus, rc);
+    rc = map_cuda(cudaMemcpyAsync(d1.p, cilm1, b1, cudaMemcpyHostToDevice, st));
+    if (!rc) rc = map_cuda(cudaMemcpyAsync(d2.p, cilm2, b2, cudaMemcpyHostToDevice, st));
+    if (!rc) rc = map_cuda(cudaMemsetAsync(dout.p, 0, bo, st));
+    // Fortran column-major (2, dim, dim): k stride 1, l stride 2, m stride 2 dim
+    if (!rc) rc = shtc_multiply(P, (const double*)d1.p, 0, 1, 2, 2LL * cd1, lmax1,
+                                (const double*)d2.p, 0, 1, 2, 2LL * cd2, lmax2,
+                                (double*)dout.p, 0, 1, 2, 2LL * cdout, cdout, 1, dw.p, wb,
+                                st);
+    if (!rc) rc = map_cuda(cudaMemcpyAsync(cilmout, dout.p, bo, cudaMemcpyDeviceToHost, st));
     if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
     set_status(exitstatus, rc);
 }

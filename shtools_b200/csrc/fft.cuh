@@ -375,13 +375,15 @@ __device__ __forceinline__ void fft_c2r_body(
 // (times wscale) as (Re, -Im), the reference's fcoef (SHExpandGLQ.f95:535-547).
 // fold_extend adds column n into column 0 (adjoint of the extend copy).
 template <typename GT>
+// grid2 (nullable): the transform of the pointwise product grid * grid2
+// (SHMultiply); the product is formed as each sample is loaded.
 __device__ __forceinline__ void fft_r2c_body(
     const FftArgs& F, const double2* tw, double2* smem_fft, int job, int f,
     const GT* __restrict__ grid, long long gf, long long grs, long long gcs,
     double2* __restrict__ spec, const int* __restrict__ rowN,
     const int* __restrict__ rowS, const double* __restrict__ wN,
     const double* __restrict__ wS, double wscale, int lc, int npair,
-    int fold_extend) {
+    int fold_extend, const GT* __restrict__ grid2 = nullptr) {
     const int len = F.bluestein ? F.mb : F.m;
     double2* a = smem_fft;
     double2* b = smem_fft + len;
@@ -398,6 +400,10 @@ __device__ __forceinline__ void fft_r2c_body(
             if (fold_extend && j == 0) {
                 if (gN) xn += (double)gN[(long long)n * gcs];
                 if (gS) xs += (double)gS[(long long)n * gcs];
+            }
+            if (grid2) {
+                if (gN) xn = xn * (double)(grid2 + f * gf + rN * grs)[j * gcs];
+                if (gS) xs = xs * (double)(grid2 + f * gf + rS * grs)[j * gcs];
             }
             a[j] = make_double2(xn, xs);
         }
@@ -429,8 +435,13 @@ __device__ __forceinline__ void fft_r2c_body(
 #pragma unroll 4
         for (int j = threadIdx.x; j < M; j += blockDim.x) {
             double x0 = (double)g[(2LL * j) * gcs];
-            const double x1 = (double)g[(2LL * j + 1) * gcs];
+            double x1 = (double)g[(2LL * j + 1) * gcs];
             if (fold_extend && j == 0) x0 += (double)g[(long long)n * gcs];
+            if (grid2) {
+                const GT* g2 = grid2 + f * gf + row * grs;
+                x0 = x0 * (double)g2[(2LL * j) * gcs];
+                x1 = x1 * (double)g2[(2LL * j + 1) * gcs];
+            }
             a[j] = make_double2(x0, x1);
         }
         const double2* r = fft_exec<-1>(F, tw, a, b);

@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(kCoefTile * kCoefRows)
 k_pack_coef(const CT* __restrict__ cilm, long long sf, long long sk, long long sl,
             long long sm, int cdim, double2* __restrict__ packed, int lc, int nfield,
             int norm, const double* __restrict__ nrm3, int scale_mode,
-            const double2* __restrict__ rec) {
+            const double2* __restrict__ rec, int f_off) {
     __shared__ double2 tile[kCoefTile][kCoefTile + 1];   // [m - m0][l - l0]
     const int l0 = blockIdx.x * kCoefTile, m0 = blockIdx.y * kCoefTile;
     const int f = blockIdx.z;
@@ -86,7 +86,7 @@ k_pack_coef(const CT* __restrict__ cilm, long long sf, long long sk, long long s
         }
         // D(l - m) of the rescaled recursion (legendre.cuh)
         const double d = rec[idx].y;
-        packed[idx * nfield + f] = make_double2(v.x * d, v.y * d);
+        packed[idx * nfield + f_off + f] = make_double2(v.x * d, v.y * d);
     }
 }
 
@@ -259,7 +259,7 @@ k_fft_r2c(FftArgs F, int tw_smem, int jobs, int nitems, const GT* __restrict__ g
           long long gf, long long grs, long long gcs, double2* __restrict__ spec,
           const int* __restrict__ rowN, const int* __restrict__ rowS,
           const double* __restrict__ wN, const double* __restrict__ wS, double wscale,
-          int lc, int npair, int fold_extend) {
+          int lc, int npair, int fold_extend, const GT* __restrict__ grid2) {
     extern __shared__ double2 smem_fft[];
     const double2* tw = fft_stage_twiddles(F, smem_fft, tw_smem);
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -268,7 +268,7 @@ k_fft_r2c(FftArgs F, int tw_smem, int jobs, int nitems, const GT* __restrict__ g
             fft_r2c_prefetch<GT>(F.mode, F.n, nx % jobs, nx / jobs, grid, gf, grs, gcs, rowN,
                                  rowS, fold_extend);
         fft_r2c_body<GT>(F, tw, smem_fft, it % jobs, it / jobs, grid, gf, grs, gcs, spec,
-                         rowN, rowS, wN, wS, wscale, lc, npair, fold_extend);
+                         rowN, rowS, wN, wS, wscale, lc, npair, fold_extend, grid2);
         __syncthreads();
     }
 }
@@ -291,18 +291,21 @@ FftArgs fft_args(const FftPlan& f) {
 int launch_pack_coef(const shtc_plan* P, const void* cilm, int dtype, long long sf,
                      long long sk, long long sl, long long sm, int cdim,
                      double2* packed, int nfield, int scale_mode,
-                     cudaStream_t st) {
+                     cudaStream_t st, int nfield_total, int f_off) {
+    // fields f_off .. f_off+nfield-1 of a packed array of nfield_total fields
+    // (nfield_total = 0: nfield, f_off = 0)
+    const int ntot = nfield_total > 0 ? nfield_total : nfield;
     const int lc = P->lc;
     const int nt = (lc + kCoefTile) / kCoefTile;
     const dim3 grid(nt, nt, nfield), block(kCoefTile, kCoefRows);
     if (dtype == SHTC_F32)
         k_pack_coef<float><<<grid, block, 0, st>>>((const float*)cilm, sf, sk, sl, sm, cdim,
-                                                 packed, lc, nfield, P->norm, P->d_nrm,
-                                                 scale_mode, P->d_rec);
+                                                 packed, lc, ntot, P->norm, P->d_nrm,
+                                                 scale_mode, P->d_rec, f_off);
     else
         k_pack_coef<double><<<grid, block, 0, st>>>((const double*)cilm, sf, sk, sl, sm, cdim,
-                                                  packed, lc, nfield, P->norm, P->d_nrm,
-                                                  scale_mode, P->d_rec);
+                                                  packed, lc, ntot, P->norm, P->d_nrm,
+                                                  scale_mode, P->d_rec, f_off);
     return map_cuda(cudaGetLastError());
 }
 
@@ -498,7 +501,7 @@ int launch_fft_c2r(const shtc_plan* P, const double2* spec, void* grid, int dtyp
 template <typename GT>
 static int launch_r2c_t(const shtc_plan* P, const GT* grid, long long gf, long long grs,
                         long long gcs, double2* spec, int nfield, int weighted,
-                        int fold_extend, cudaStream_t st) {
+                        int fold_extend, cudaStream_t st, const GT* grid2 = nullptr) {
     const FftPlan& f = P->fft;
     int rc = fft_smem_setup((const void*)k_fft_r2c<GT>, f);
     if (rc) return rc;
@@ -512,14 +515,22 @@ static int launch_r2c_t(const shtc_plan* P, const GT* grid, long long gf, long l
         // is reproduced up to one rounding by folding 1/nlong into the weight
         k_fft_r2c<GT><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_arowN,
-            P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, 0);
+            P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, 0,
+            grid2);
     } else {
         // synthesis adjoint: plain (Re, -Im) of the rows of the cotangent
         k_fft_r2c<GT><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_rowN,
-            P->d_rowS, nullptr, nullptr, 1.0, P->lc, P->npair, fold_extend);
+            P->d_rowS, nullptr, nullptr, 1.0, P->lc, P->npair, fold_extend, grid2);
     }
     return map_cuda(cudaGetLastError());
+}
+
+// analysis r2c of the pointwise products grid * grid2 (float64 grids)
+int launch_fft_r2c_product(const shtc_plan* P, const double* grid, const double* grid2,
+                           long long gf, long long grs, long long gcs, double2* spec,
+                           int nfield, cudaStream_t st) {
+    return launch_r2c_t<double>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st, grid2);
 }
 
 int launch_fft_r2c(const shtc_plan* P, const void* grid, int dtype, long long gf,

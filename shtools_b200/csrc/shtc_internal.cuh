@@ -108,7 +108,10 @@ void free_fft_plan(FftPlan* f);
 int launch_pack_coef(const shtc_plan* P, const void* cilm, int dtype, long long sf,
                      long long sk, long long sl, long long sm, int cdim,
                      double2* packed, int nfield, int scale_mode,
-                     cudaStream_t st);
+                     cudaStream_t st, int nfield_total = 0, int f_off = 0);
+int launch_fft_r2c_product(const shtc_plan* P, const double* grid, const double* grid2,
+                           long long gf, long long grs, long long gcs, double2* spec,
+                           int nfield, cudaStream_t st);
 int launch_legendre_synth(const shtc_plan* P, const double2* packed,
                           double2* spec, int nfield, cudaStream_t st);
 int launch_fft_c2r(const shtc_plan* P, const double2* spec, void* grid, int dtype,

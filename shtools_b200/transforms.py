@@ -568,6 +568,48 @@ def MakeGradientDH(cilm, lmax=None, sampling=1, lmax_calc=None, extend=False,
     return th.reshape(out), ph.reshape(out)
 
 
+def SHMultiply(cilm1, cilm2, lmax1=None, lmax2=None, precomp=None, norm=1, csphase=1):
+    """Spherical-harmonic expansion of the product of two fields, on the GPU
+    (src/SHMultiply.f95:1): both fields are synthesised on the Gauss-Legendre
+    grid of degree lmax1 + lmax2, multiplied pointwise, and expanded to that
+    degree.  cilm1, cilm2: (..., 2, D, D) with equal leading shapes.  Returns
+    (..., 2, lmax1+lmax2+1, lmax1+lmax2+1).  precomp is accepted and ignored
+    (it selects the reference's precomputed Legendre tables).  Not
+    differentiable."""
+    _check_common(norm, csphase)
+    c1 = _as_cuda(cilm1, "cilm1").to(torch.float64)
+    c2 = _as_cuda(cilm2, "cilm2").to(torch.float64)
+    for c in (c1, c2):
+        if c.dim() < 3 or c.shape[-3] < 2 or c.shape[-1] != c.shape[-2]:
+            raise ValueError("cilm must be dimensioned as (..., 2, lmax+1, lmax+1); got %s"
+                             % (tuple(c.shape),))
+    L1 = c1.shape[-1] - 1 if lmax1 is None else int(lmax1)
+    L2 = c2.shape[-1] - 1 if lmax2 is None else int(lmax2)
+    if L1 < 0 or L2 < 0 or L1 > c1.shape[-1] - 1 or L2 > c2.shape[-1] - 1:
+        raise ValueError("lmax1/lmax2 must lie within the dimensions of cilm1/cilm2")
+    if c1.shape[:-3] != c2.shape[:-3]:
+        raise ValueError("cilm1 and cilm2 must have the same leading dimensions")
+    lo = L1 + L2
+    plan = get_plan(GRID_GLQ, lo, lo, norm, csphase, 1, 0, device=c1.device)
+    f1, lead = _flat(c1[..., :2, :, :], 3)
+    f2, _ = _flat(c2[..., :2, :, :], 3)
+    F = f1.shape[0]
+    out = torch.zeros((F, 2, lo + 1, lo + 1), dtype=torch.float64, device=c1.device)
+    lib = plan.lib
+    nb = int(lib.shtc_multiply_workspace_bytes(plan.handle, F))
+    ws = torch.empty(max(nb, 8), dtype=torch.uint8, device=c1.device)
+    with torch.cuda.device(c1.device):
+        rc = lib.shtc_multiply(plan.handle, ctypes_void(f1.data_ptr()), f1.stride(0),
+                               f1.stride(1), f1.stride(2), f1.stride(3), L1,
+                               ctypes_void(f2.data_ptr()), f2.stride(0), f2.stride(1),
+                               f2.stride(2), f2.stride(3), L2, ctypes_void(out.data_ptr()),
+                               out.stride(0), out.stride(1), out.stride(2), out.stride(3),
+                               lo + 1, F, ctypes_void(ws.data_ptr()), nb,
+                               _stream_ptr(c1.device))
+    _lib.check(rc, "shtc_multiply")
+    return out.reshape(tuple(lead) + tuple(out.shape[1:]))
+
+
 def _host64(a, n, what):
     if isinstance(a, torch.Tensor):
         a = a.detach().cpu().numpy()
