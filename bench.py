@@ -51,6 +51,10 @@ WORKLOADS = {
     # MakeGradientDH, config 3 shape: 8 fields, lmax 719, sampling 2
     "gradient719x8": dict(kind="gradient", lmax=719, nfield=8, sampling=2, beta=2.0,
                           seed=3700),
+    # SHMultiply: one pair of fields of lmax 1024 and 1023 into lmax 2047 (the
+    # GLQ grid of the headline configuration, 2048 x 4095)
+    "multiply1024": dict(kind="multiply", lmax=1024, lmax2=1023, nfield=1, sampling=1,
+                         beta=2.0, seed=2100),
     # config 1 shape: one DH field, lmax 255, sampling 2
     "dh255": dict(kind="dh", lmax=255, nfield=1, sampling=2, beta=2.0,
                   seed=1000),
@@ -89,17 +93,25 @@ def batch_lmaxes(w):
     return [int(x) for x in rng.integers(w["lmin"], w["lmax"] + 1, w["nfield"])]
 
 
-def flops_per_transform(w, L=None):
-    """Algorithmic FP64 flops of the Legendre stage of one transform: per
-    ring pair and (l, m), 4 for the three-term recursion and 4 for the two
-    multiply-adds of the contraction (F_rec + F_contr with 2*nlat*N_lm each)."""
+def legendre_flops(w, nsums, L=None):
+    """Algorithmic FP64 flops of one Legendre-stage launch that evaluates
+    `nsums` coefficient sets on one grid: per ring pair and (l, m), 4 for the
+    three-term recursion, once per grid, and 4 for the two multiply-adds of
+    each contraction (F_rec + nsums * F_contr, each 2*nlat*N_lm).  One field
+    is 8 flops per (pair, l, m)."""
     if w["kind"] == "glq_batch" and L is None:
-        return sum(flops_per_transform(dict(w, kind="glq"), l) for l in batch_lmaxes(w)) \
-            / w["nfield"]
+        from collections import Counter
+        cnt = Counter(batch_lmaxes(w))
+        return sum(legendre_flops(dict(w, kind="glq"), n, l) for l, n in cnt.items())
     L = w["lmax"] if L is None else L
     nlm = (L + 1) * (L + 2) // 2
     nlat = L + 1 if w["kind"] in ("glq", "glq_batch") else 2 * L + 2
-    return 8.0 * (nlat / 2.0) * nlm
+    return 4.0 * (nlat / 2.0) * nlm * (1 + nsums)
+
+
+def flops_per_transform(w, L=None):
+    """Legendre-stage flops of one single-field transform (8 per pair and (l, m))."""
+    return legendre_flops(dict(w, kind="glq" if w["kind"] == "glq_batch" else w["kind"]), 1, L)
 
 
 def power_law(L, seed, beta, cplx=False):
@@ -443,7 +455,7 @@ def run_cuda_batch(args, w, rank, world, local_rank):
     names = ["pack", "legendre_synth", "fft_c2r", "fft_r2c", "legendre_anal", "unpack"]
     dom = max((1, 4), key=lambda i: ms[i])
     per_launch_ms = ms[dom] / max(1, cnt[dom])
-    fl = flops_per_transform(w) * F
+    fl = legendre_flops(w, None)
     achieved = fl / (per_launch_ms * 1e-3) / 1e12
     # end to end: host coefficients in, host coefficients out
     c_host = c.cpu().pin_memory()
@@ -558,7 +570,7 @@ def run_cuda_grad(args, w, rank, world, local_rank):
     names = ["pack", "legendre_synth", "fft_c2r", "fft_r2c", "legendre_anal", "unpack"]
     dom = max((1, 4), key=lambda i: ms[i])
     per_launch_ms = ms[dom] / max(1, cnt[dom])
-    fl = flops_per_transform(w) * F
+    fl = legendre_flops(w, F)
     achieved = fl / (per_launch_ms * 1e-3) / 1e12
     return {
         "metric": METRIC, "value": value, "unit": "transforms/s", "n_gpus": world,
@@ -646,7 +658,7 @@ def run_cuda_gradient(args, w, rank, world, local_rank):
     e2e_ms = max_over_ranks(a.elapsed_time(b), dev)
     names = ["pack", "legendre_synth", "fft_c2r", "fft_r2c", "legendre_anal", "unpack"]
     per_launch_ms = ms[1] / max(1, cnt[1])
-    fl = 3.0 * flops_per_transform(w) * F        # three Legendre sums per field
+    fl = legendre_flops(w, 3 * F)        # three Legendre sums per field, one recursion
     achieved = fl / (per_launch_ms * 1e-3) / 1e12
     return {
         "metric": METRIC, "value": value, "unit": "transforms/s", "n_gpus": world,
@@ -674,6 +686,107 @@ def run_cuda_gradient(args, w, rank, world, local_rank):
                 "path": "public torch API on pinned host buffers, pipelined on 3 streams"},
         # the FFT stage holds 3 launches (combination, theta c2r, phi c2r)
         "gpu_launches": int(sum(cnt)) + 2 * int(cnt[2]),
+        "clocks": clk.summary(),
+    }
+
+
+def run_cuda_multiply(args, w, rank, world, local_rank):
+    """SHMultiply of pairs of fields of degree lmax into degree 2*lmax (two
+    GLQ syntheses and one analysis per product), through the public torch
+    API."""
+    import numpy as np
+    import torch
+    import shtools_b200 as sht
+    from shtools_b200 import _lib
+    from shtools_b200.pipeline import pipelined
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    L, L2, F = w["lmax"], w["lmax2"], w["nfield"]
+    c1h = torch.from_numpy(np.stack([power_law(L, w["seed"] + i, w["beta"])
+                                     for i in range(F)])).pin_memory()
+    c2h = torch.from_numpy(np.stack([power_law(L2, w["seed"] + 100 + i, w["beta"])
+                                     for i in range(F)])).pin_memory()
+    c1, c2 = c1h.to(dev), c2h.to(dev)
+    st = torch.cuda.current_stream(dev)
+    step = lambda a, b: sht.SHMultiply(a, b)
+    for _ in range(args.warmup):
+        out = step(c1, c2)
+    torch.cuda.synchronize(dev)
+    # size-independent check: multiplying by the constant field 1 is the identity
+    one = torch.zeros((F, 2, 1, 1), dtype=torch.float64, device=dev)
+    one[:, 0, 0, 0] = 1.0
+    ident = step(c1, one)
+    ident_err = float((ident[..., :L + 1, :L + 1] - c1).abs().max().item() /
+                      c1.abs().max().item())
+    peak = fp64_peak(torch, dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    torch.cuda.synchronize(dev)
+    lib.shtc_timing_enable(1)
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            evs[i][0].record(st)
+            step(c1, c2)
+            evs[i][1].record(st)
+        torch.cuda.synchronize(dev)
+    lib.shtc_timing_enable(0)
+    import ctypes
+    ms = (ctypes.c_double * 6)()
+    cnt = (ctypes.c_int * 6)()
+    lib.shtc_timing_collect(ms, cnt, 6)
+    total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), dev)
+    value = 3.0 * F * args.steps * world / (total_ms * 1e-3)
+    outs = [(torch.empty(tuple(out.shape), dtype=out.dtype).pin_memory(),) for _ in range(2)]
+    e2e_steps = max(2, min(args.steps, 10))
+    pipelined(step, [(c1h, c2h)] * 2, outs, device=dev)
+    torch.cuda.synchronize(dev)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    pipelined(step, [(c1h, c2h)] * e2e_steps, [outs[i % 2] for i in range(e2e_steps)],
+              device=dev)
+    b.record(st)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(a.elapsed_time(b), dev)
+    names = ["pack", "legendre_synth", "fft_c2r", "fft_r2c", "legendre_anal", "unpack"]
+    wl = dict(w, kind="glq", lmax=L + L2)
+    dom = max((1, 4), key=lambda i: ms[i])
+    per_launch_ms = ms[dom] / max(1, cnt[dom])
+    fl = legendre_flops(wl, F * (2 if dom == 1 else 1))
+    achieved = fl / (per_launch_ms * 1e-3) / 1e12
+    return {
+        "metric": METRIC, "value": value, "unit": "transforms/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic seeded power-law coefficients, S(l)=(l+1)^-%g" % w["beta"],
+        "config": {"workload": args.workload, "kind": "SHMultiply (GLQ)",
+                   "lmax_in": [L, L2], "lmax_out": L + L2, "pairs_per_gpu": F,
+                   "precision": "fp64",
+                   "step": "SHMultiply of every pair: 2 syntheses + 1 analysis "
+                           "(counted as 3 transforms)",
+                   "l2": "flushed between steps (256 MiB write, outside step events)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "products_per_s": F * args.steps * world / (total_ms * 1e-3),
+        "roofline": {"kernel": names[dom], "bound": "fp64", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None,
+                     "peak_source": "measured FP64 FMA probe, this run",
+                     "flops_per_launch": fl, "traffic": None},
+        "stages": {names[i]: {"ms_per_launch": (ms[i] / cnt[i]) if cnt[i] else None,
+                              "launches": cnt[i]} for i in range(6)},
+        "multiply_by_one_max_rel_err": ident_err,
+        "e2e": {"value": 3.0 * F * e2e_steps * world / (e2e_ms * 1e-3),
+                "unit": "transforms/s", "steps": e2e_steps,
+                "h2d_bytes_per_step": (c1h.numel() + c2h.numel()) * 8,
+                "d2h_bytes_per_step": outs[0][0].numel() * 8,
+                "path": "public torch API on pinned host buffers, pipelined on 3 streams"},
+        # the pack stage holds 2 launches (one per input field set)
+        "gpu_launches": int(sum(cnt)) + int(cnt[0]),
         "clocks": clk.summary(),
     }
 
@@ -785,7 +898,7 @@ def run_cuda(args, w, rank, world, local_rank):
     dom = max((1, 4), key=lambda i: ms[i])
     per_launch_ms = ms[dom] / max(1, cnt[dom])
     # complex fields: two coefficient sets (orders +m, -m) per field
-    fl = flops_per_transform(w) * F * (2 if cplx else 1)
+    fl = legendre_flops(w, F * (2 if cplx else 1))
     achieved = fl / (per_launch_ms * 1e-3) / 1e12
     traffic = load_traffic("%s_%s" % (names[dom], args.workload))
     stage = {names[i]: {"ms_per_launch": (ms[i] / cnt[i]) if cnt[i] else None,
@@ -878,10 +991,12 @@ def main():
         res = run_cuda_grad(args, w, rank, world, local_rank)
     elif w["kind"] == "gradient":
         res = run_cuda_gradient(args, w, rank, world, local_rank)
+    elif w["kind"] == "multiply":
+        res = run_cuda_multiply(args, w, rank, world, local_rank)
     else:
         res = run_cuda(args, w, rank, world, local_rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and \
-            w["kind"] not in ("dhc", "gradient"):
+            w["kind"] not in ("dhc", "gradient", "multiply"):
         one_step, sample, threads = cpu_sample(w, args.cpu_seconds / 2)
         v, dt = one_step()
         res["cpu_baseline"] = {"value": v, "unit": "transforms/s",
