@@ -44,11 +44,19 @@ static size_t spec_region(const shtc_plan* P, int nfield) {
     return align256((size_t)nfield * P->npair * (P->lc + 1) * 2 * sizeof(double2));
 }
 
+// longitude FFTs too long for shared memory use a scratch behind the other
+// regions (fft_scratch_bytes, zero otherwise)
+static size_t fft_region(const shtc_plan* P) { return align256(fft_scratch_bytes(P)); }
+
+static double2* fft_scratch(const shtc_plan* P, void* work, size_t offset) {
+    return P->fft.gmem ? (double2*)((char*)work + offset) : nullptr;
+}
+
 // complex plans carry two internal fields (orders +m and -m) per field
 extern "C" size_t shtc_workspace_bytes(const shtc_plan* P, int nfield) {
     if (!P || nfield < 1) return 0;
     const int nf = P->cplx ? 2 * nfield : nfield;
-    return coef_region(P, nf) + spec_region(P, nf);
+    return coef_region(P, nf) + spec_region(P, nf) + fft_region(P);
 }
 
 static int check_call(const shtc_plan* P, const void* a, const void* b,
@@ -85,6 +93,7 @@ extern "C" int shtc_synthesis_ex(const shtc_plan* P, const void* cilm, int cdt,
     cudaStream_t st = (cudaStream_t)stream;
     double2* packed = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
+    double2* fbuf = fft_scratch(P, work, coef_region(P, nfield) + spec_region(P, nfield));
     stage_begin(SHTC_STAGE_PACK, st);
     rc = launch_pack_coef(P, cilm, cdt, csf, csk, csl, csm, cdim, packed, nfield, 0, st);
     stage_end(SHTC_STAGE_PACK, st);
@@ -94,7 +103,7 @@ extern "C" int shtc_synthesis_ex(const shtc_plan* P, const void* cilm, int cdt,
     stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_FFT_C2R, st);
-    rc = launch_fft_c2r(P, spec, grid, gdt, gsf, gsr, gsc, nfield, 0, st);
+    rc = launch_fft_c2r(P, spec, grid, gdt, gsf, gsr, gsc, nfield, 0, st, fbuf);
     stage_end(SHTC_STAGE_FFT_C2R, st);
     return rc;
 }
@@ -112,9 +121,10 @@ extern "C" int shtc_analysis_ex(const shtc_plan* P, const void* grid, int gdt,
     cudaStream_t st = (cudaStream_t)stream;
     double2* partial = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
+    double2* fbuf = fft_scratch(P, work, coef_region(P, nfield) + spec_region(P, nfield));
     const int tiles = anal_tiles(P);
     stage_begin(SHTC_STAGE_FFT_R2C, st);
-    rc = launch_fft_r2c(P, grid, gdt, gsf, gsr, gsc, spec, nfield, 1, 0, st);
+    rc = launch_fft_r2c(P, grid, gdt, gsf, gsr, gsc, spec, nfield, 1, 0, st, fbuf);
     stage_end(SHTC_STAGE_FFT_R2C, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
@@ -142,9 +152,10 @@ extern "C" int shtc_synthesis_adjoint_ex(const shtc_plan* P, const void* grid, i
     cudaStream_t st = (cudaStream_t)stream;
     double2* partial = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
+    double2* fbuf = fft_scratch(P, work, coef_region(P, nfield) + spec_region(P, nfield));
     const int tiles = anal_tiles(P);
     stage_begin(SHTC_STAGE_FFT_R2C, st);
-    rc = launch_fft_r2c(P, grid, gdt, gsf, gsr, gsc, spec, nfield, 0, P->extend, st);
+    rc = launch_fft_r2c(P, grid, gdt, gsf, gsr, gsc, spec, nfield, 0, P->extend, st, fbuf);
     stage_end(SHTC_STAGE_FFT_R2C, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
@@ -171,6 +182,7 @@ extern "C" int shtc_analysis_adjoint_ex(const shtc_plan* P, const void* cilm, in
     cudaStream_t st = (cudaStream_t)stream;
     double2* packed = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
+    double2* fbuf = fft_scratch(P, work, coef_region(P, nfield) + spec_region(P, nfield));
     stage_begin(SHTC_STAGE_PACK, st);
     rc = launch_pack_coef(P, cilm, cdt, csf, csk, csl, csm, cdim, packed, nfield, 1, st);
     stage_end(SHTC_STAGE_PACK, st);
@@ -180,7 +192,7 @@ extern "C" int shtc_analysis_adjoint_ex(const shtc_plan* P, const void* cilm, in
     stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_FFT_C2R, st);
-    rc = launch_fft_c2r(P, spec, grid, gdt, gsf, gsr, gsc, nfield, 1, st);
+    rc = launch_fft_c2r(P, spec, grid, gdt, gsf, gsr, gsc, nfield, 1, st, fbuf);
     stage_end(SHTC_STAGE_FFT_C2R, st);
     return rc;
 }
@@ -236,6 +248,7 @@ extern "C" int shtc_synthesis_c(const shtc_plan* P, const void* cilm, long long 
     const int nf2 = 2 * nfield;
     double2* packed = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nf2));
+    double2* fbuf = fft_scratch(P, work, coef_region(P, nf2) + spec_region(P, nf2));
     stage_begin(SHTC_STAGE_PACK, st);
     rc = launch_pack_coef_c(P, (const double2*)cilm, csf, csk, csl, csm, cdim, packed, nfield,
                             st);
@@ -246,7 +259,7 @@ extern "C" int shtc_synthesis_c(const shtc_plan* P, const void* cilm, long long 
     stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_FFT_C2R, st);
-    rc = launch_fft_c2c_synth(P, spec, (double2*)grid, gsf, gsr, gsc, nfield, st);
+    rc = launch_fft_c2c_synth(P, spec, (double2*)grid, gsf, gsr, gsc, nfield, st, fbuf);
     stage_end(SHTC_STAGE_FFT_C2R, st);
     return rc;
 }
@@ -263,9 +276,10 @@ extern "C" int shtc_analysis_c(const shtc_plan* P, const void* grid, long long g
     const int nf2 = 2 * nfield;
     double2* partial = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nf2));
+    double2* fbuf = fft_scratch(P, work, coef_region(P, nf2) + spec_region(P, nf2));
     const int tiles = anal_tiles(P);
     stage_begin(SHTC_STAGE_FFT_R2C, st);
-    rc = launch_fft_c2c_anal(P, (const double2*)grid, gsf, gsr, gsc, spec, nfield, st);
+    rc = launch_fft_c2c_anal(P, (const double2*)grid, gsf, gsr, gsc, spec, nfield, st, fbuf);
     stage_end(SHTC_STAGE_FFT_R2C, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
@@ -286,7 +300,7 @@ extern "C" int shtc_analysis_c(const shtc_plan* P, const void* grid, long long g
 extern "C" size_t shtc_gradient_workspace_bytes(const shtc_plan* P, int nfield) {
     if (!P || nfield < 1) return 0;
     return coef_region(P, 3 * nfield) + spec_region(P, 3 * nfield) +
-           spec_region(P, 2 * nfield);
+           spec_region(P, 2 * nfield) + fft_region(P);
 }
 
 extern "C" int shtc_gradient_dh(const shtc_plan* P, const double* cilm, long long csf,
@@ -307,9 +321,11 @@ extern "C" int shtc_gradient_dh(const shtc_plan* P, const double* cilm, long lon
     char* w = (char*)work;
     double2* packed = (double2*)w;
     double2* spec = (double2*)(w + coef_region(P, 3 * nfield));
-    double2* spec2 = (double2*)(w + coef_region(P, 3 * nfield) + spec_region(P, 3 * nfield));
+    const size_t o2 = coef_region(P, 3 * nfield) + spec_region(P, 3 * nfield);
+    double2* spec2 = (double2*)(w + o2);
+    double2* fbuf = fft_scratch(P, work, o2 + spec_region(P, 2 * nfield));
     return launch_gradient_dh(P, cilm, csf, csk, csl, csm, cdim, theta, phi, gsf, gsr, gsc,
-                              radius, nfield, packed, spec, spec2, (cudaStream_t)stream);
+                              radius, nfield, packed, spec, spec2, (cudaStream_t)stream, fbuf);
 }
 
 // ---------------------------------------------------------------------------
@@ -325,7 +341,7 @@ static size_t grid_region(const shtc_plan* P, int nfield) {
 extern "C" size_t shtc_multiply_workspace_bytes(const shtc_plan* P, int nfield) {
     if (!P || nfield < 1) return 0;
     return coef_region(P, 2 * nfield) + spec_region(P, 2 * nfield) +
-           grid_region(P, 2 * nfield);
+           grid_region(P, 2 * nfield) + fft_region(P);
 }
 
 extern "C" int shtc_multiply(const shtc_plan* P, const double* cilm1, long long c1sf,
@@ -349,6 +365,9 @@ extern "C" int shtc_multiply(const shtc_plan* P, const double* cilm1, long long 
     double2* packed = (double2*)w;
     double2* spec = (double2*)(w + coef_region(P, 2 * nfield));
     double* grids = (double*)(w + coef_region(P, 2 * nfield) + spec_region(P, 2 * nfield));
+    double2* fbuf = fft_scratch(P, work, coef_region(P, 2 * nfield) +
+                                             spec_region(P, 2 * nfield) +
+                                             grid_region(P, 2 * nfield));
     const long long gf = (long long)P->nlat * P->nlon;
     const int tiles = anal_tiles(P);
     stage_begin(SHTC_STAGE_PACK, st);
@@ -363,12 +382,12 @@ extern "C" int shtc_multiply(const shtc_plan* P, const double* cilm1, long long 
     stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_FFT_C2R, st);
-    rc = launch_fft_c2r(P, spec, grids, SHTC_F64, gf, P->nlon, 1, 2 * nfield, 0, st);
+    rc = launch_fft_c2r(P, spec, grids, SHTC_F64, gf, P->nlon, 1, 2 * nfield, 0, st, fbuf);
     stage_end(SHTC_STAGE_FFT_C2R, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_FFT_R2C, st);
     rc = launch_fft_r2c_product(P, grids, grids + (long long)nfield * gf, gf, P->nlon, 1, spec,
-                                nfield, st);
+                                nfield, st, fbuf);
     stage_end(SHTC_STAGE_FFT_R2C, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);

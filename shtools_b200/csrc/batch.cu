@@ -296,6 +296,10 @@ extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
             delete B;
             return P && (P->extend != 0 || P->cplx) ? SHTC_EBOUND : SHTC_EHANDLE;
         }
+        if (P->fft.gmem) {   // batched FFTs keep every ring in shared memory
+            delete B;
+            return SHTC_EUNSUP;
+        }
         BatchGroup g;
         g.rec = P->d_rec; g.pmm = P->d_pmm; g.rtab = P->d_rtab; g.z = P->d_z;
         g.rowN = P->d_rowN; g.rowS = P->d_rowS; g.arowN = P->d_arowN;

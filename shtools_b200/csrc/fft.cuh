@@ -1,8 +1,10 @@
 // Device code of the longitude FFTs (c2r for synthesis, r2c for analysis),
 // shared by the per-plan kernels (kernels.cu) and the batched kernels
 // (batch.cu).  Stockham autosort passes ping-pong between two shared
-// buffers; radix 2, 3, 4, 5, 7, 8, 11, 13 butterflies; Bluestein's algorithm
-// for lengths with other prime factors.  Conventions are those of FFTW's
+// buffers (per-plan kernels whose buffers exceed shared memory keep them in
+// a per-CTA global scratch instead, L2-resident, with the same barriers);
+// radix 2, 3, 4, 5, 7, 8, 11, 13 butterflies; Bluestein's algorithm for
+// lengths with other prime factors.  Conventions are those of FFTW's
 // unnormalised r2c / c2r (src/FFTW3.f95:212-271).
 #pragma once
 
@@ -234,7 +236,7 @@ __device__ __forceinline__ double2* fft_run(double2* a, double2* b, int M, const
 }
 
 struct FftArgs {
-    int n, mode, m, nfac, bluestein, mb, ntw;
+    int n, mode, m, nfac, bluestein, mb, ntw, gmem;
     int fac[kMaxFactors];
     int tw_off[kMaxFactors];
     const double2* tw;

@@ -230,9 +230,19 @@ __device__ __forceinline__ const double2* fft_stage_twiddles(const FftArgs& F,
                                                              int tw_smem) {
     if (!tw_smem) return F.tw;
     const int len = F.bluestein ? F.mb : F.m;
-    double2* tws = smem_fft + 2 * len;
+    // behind the two data buffers, or at the start when those are global
+    double2* tws = F.gmem ? smem_fft : smem_fft + 2 * len;
     for (int i = threadIdx.x; i < F.ntw; i += blockDim.x) tws[i] = F.tw[i];
     return tws;   // made visible by the barrier that opens fft_exec
+}
+
+// the CTA's two data buffers: shared memory, or its slice of the global
+// scratch (F.gmem); __syncthreads orders the passes in either
+__device__ __forceinline__ double2* fft_buffers(const FftArgs& F, double2* smem_fft,
+                                                double2* gbuf) {
+    if (!F.gmem) return smem_fft;
+    const int len = F.bluestein ? F.mb : F.m;
+    return gbuf + (size_t)blockIdx.x * 2 * len;
 }
 
 template <typename GT>
@@ -241,13 +251,14 @@ k_fft_c2r(FftArgs F, int tw_smem, int jobs, int nitems, const double2* __restric
           GT* __restrict__ grid, long long gf, long long grs, long long gcs,
           const int* __restrict__ rowN, const int* __restrict__ rowS,
           const double* __restrict__ wN, const double* __restrict__ wS, double wscale,
-          int lc, int npair, int extend_col) {
+          int lc, int npair, int extend_col, double2* __restrict__ gbuf) {
     extern __shared__ double2 smem_fft[];
     const double2* tw = fft_stage_twiddles(F, smem_fft, tw_smem);
+    double2* bufs = fft_buffers(F, smem_fft, gbuf);
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int nx = it + gridDim.x;
         if (nx < nitems) fft_c2r_prefetch(F.mode, nx % jobs, nx / jobs, spec, lc, npair);
-        fft_c2r_body<GT>(F, tw, smem_fft, it % jobs, it / jobs, spec, grid, gf, grs, gcs,
+        fft_c2r_body<GT>(F, tw, bufs, it % jobs, it / jobs, spec, grid, gf, grs, gcs,
                          rowN, rowS, wN, wS, wscale, lc, npair, extend_col);
         __syncthreads();
     }
@@ -259,15 +270,16 @@ k_fft_r2c(FftArgs F, int tw_smem, int jobs, int nitems, const GT* __restrict__ g
           long long gf, long long grs, long long gcs, double2* __restrict__ spec,
           const int* __restrict__ rowN, const int* __restrict__ rowS,
           const double* __restrict__ wN, const double* __restrict__ wS, double wscale,
-          int lc, int npair, int fold_extend, const GT* __restrict__ grid2) {
+          int lc, int npair, int fold_extend, const GT* __restrict__ grid2, double2* __restrict__ gbuf) {
     extern __shared__ double2 smem_fft[];
     const double2* tw = fft_stage_twiddles(F, smem_fft, tw_smem);
+    double2* bufs = fft_buffers(F, smem_fft, gbuf);
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int nx = it + gridDim.x;
         if (nx < nitems)
             fft_r2c_prefetch<GT>(F.mode, F.n, nx % jobs, nx / jobs, grid, gf, grs, gcs, rowN,
                                  rowS, fold_extend);
-        fft_r2c_body<GT>(F, tw, smem_fft, it % jobs, it / jobs, grid, gf, grs, gcs, spec,
+        fft_r2c_body<GT>(F, tw, bufs, it % jobs, it / jobs, grid, gf, grs, gcs, spec,
                          rowN, rowS, wN, wS, wscale, lc, npair, fold_extend, grid2);
         __syncthreads();
     }
@@ -279,7 +291,7 @@ k_fft_r2c(FftArgs F, int tw_smem, int jobs, int nitems, const GT* __restrict__ g
 FftArgs fft_args(const FftPlan& f) {
     FftArgs a;
     a.n = f.n; a.mode = f.mode; a.m = f.m; a.nfac = f.nfac;
-    a.bluestein = f.bluestein; a.mb = f.mb; a.ntw = f.ntw;
+    a.bluestein = f.bluestein; a.mb = f.mb; a.ntw = f.ntw; a.gmem = f.gmem;
     for (int i = 0; i < kMaxFactors; ++i) {
         a.fac[i] = i < f.nfac ? f.fac[i] : 0;
         a.tw_off[i] = i < f.nfac ? f.tw_off[i] : 0;
@@ -458,16 +470,25 @@ static int fft_grid(K kernel, const FftPlan& f, int nitems, int* blocks) {
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, f.threads,
                                                                   f.smem);
     if (e != cudaSuccess) return map_cuda(e);
-    const long long cap = (long long)(sms > 0 ? sms : 1) * (occ > 0 ? occ : 1);
+    long long cap = (long long)(sms > 0 ? sms : 1) * (occ > 0 ? occ : 1);
+    if (f.gmem && cap > f.gmem_ctas) cap = f.gmem_ctas;   // one scratch slice per CTA
     *blocks = (int)(nitems < cap ? nitems : cap);
     return SHTC_OK;
+}
+
+size_t fft_scratch_bytes(const shtc_plan* P) {
+    const FftPlan& f = P->fft;
+    if (!f.gmem) return 0;
+    const size_t len = (size_t)(f.bluestein ? f.mb : f.m);
+    return (size_t)f.gmem_ctas * 2 * len * sizeof(double2);
 }
 
 template <typename GT>
 static int launch_c2r_t(const shtc_plan* P, const double2* spec, GT* grid, long long gf,
                         long long grs, long long gcs, int nfield, int weighted,
-                        cudaStream_t st) {
+                        cudaStream_t st, double2* gbuf) {
     const FftPlan& f = P->fft;
+    if (f.gmem && !gbuf) return SHTC_EWORK;
     int rc = fft_smem_setup((const void*)k_fft_c2r<GT>, f);
     if (rc) return rc;
     const int jobs = f.mode == 0 ? P->npair : 2 * P->npair;
@@ -480,29 +501,31 @@ static int launch_c2r_t(const shtc_plan* P, const double2* spec, GT* grid, long 
     if (weighted) {
         k_fft_c2r<GT><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, spec, grid, gf, grs, gcs, P->d_arowN,
-            P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, 0);
+            P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, 0, gbuf);
     } else {
         k_fft_c2r<GT><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, spec, grid, gf, grs, gcs, P->d_rowN,
-            P->d_rowS, nullptr, nullptr, 1.0, P->lc, P->npair, P->extend);
+            P->d_rowS, nullptr, nullptr, 1.0, P->lc, P->npair, P->extend, gbuf);
     }
     return map_cuda(cudaGetLastError());
 }
 
 int launch_fft_c2r(const shtc_plan* P, const double2* spec, void* grid, int dtype,
                    long long gf, long long grs, long long gcs, int nfield,
-                   int weighted, cudaStream_t st) {
+                   int weighted, cudaStream_t st, double2* gbuf) {
     return dtype == SHTC_F32
-               ? launch_c2r_t<float>(P, spec, (float*)grid, gf, grs, gcs, nfield, weighted, st)
+               ? launch_c2r_t<float>(P, spec, (float*)grid, gf, grs, gcs, nfield, weighted, st,
+                                     gbuf)
                : launch_c2r_t<double>(P, spec, (double*)grid, gf, grs, gcs, nfield, weighted,
-                                      st);
+                                      st, gbuf);
 }
 
 template <typename GT>
 static int launch_r2c_t(const shtc_plan* P, const GT* grid, long long gf, long long grs,
                         long long gcs, double2* spec, int nfield, int weighted,
-                        int fold_extend, cudaStream_t st, const GT* grid2 = nullptr) {
+                        int fold_extend, cudaStream_t st, const GT* grid2, double2* gbuf) {
     const FftPlan& f = P->fft;
+    if (f.gmem && !gbuf) return SHTC_EWORK;
     int rc = fft_smem_setup((const void*)k_fft_r2c<GT>, f);
     if (rc) return rc;
     const int jobs = f.mode == 0 ? P->npair : 2 * P->npair;
@@ -516,12 +539,12 @@ static int launch_r2c_t(const shtc_plan* P, const GT* grid, long long gf, long l
         k_fft_r2c<GT><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_arowN,
             P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, 0,
-            grid2);
+            grid2, gbuf);
     } else {
         // synthesis adjoint: plain (Re, -Im) of the rows of the cotangent
         k_fft_r2c<GT><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_rowN,
-            P->d_rowS, nullptr, nullptr, 1.0, P->lc, P->npair, fold_extend, grid2);
+            P->d_rowS, nullptr, nullptr, 1.0, P->lc, P->npair, fold_extend, grid2, gbuf);
     }
     return map_cuda(cudaGetLastError());
 }
@@ -529,18 +552,18 @@ static int launch_r2c_t(const shtc_plan* P, const GT* grid, long long gf, long l
 // analysis r2c of the pointwise products grid * grid2 (float64 grids)
 int launch_fft_r2c_product(const shtc_plan* P, const double* grid, const double* grid2,
                            long long gf, long long grs, long long gcs, double2* spec,
-                           int nfield, cudaStream_t st) {
-    return launch_r2c_t<double>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st, grid2);
+                           int nfield, cudaStream_t st, double2* gbuf) {
+    return launch_r2c_t<double>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st, grid2, gbuf);
 }
 
 int launch_fft_r2c(const shtc_plan* P, const void* grid, int dtype, long long gf,
                    long long grs, long long gcs, double2* spec, int nfield,
-                   int weighted, int fold_extend, cudaStream_t st) {
+                   int weighted, int fold_extend, cudaStream_t st, double2* gbuf) {
     return dtype == SHTC_F32
                ? launch_r2c_t<float>(P, (const float*)grid, gf, grs, gcs, spec, nfield,
-                                     weighted, fold_extend, st)
+                                     weighted, fold_extend, st, nullptr, gbuf)
                : launch_r2c_t<double>(P, (const double*)grid, gf, grs, gcs, spec, nfield,
-                                      weighted, fold_extend, st);
+                                      weighted, fold_extend, st, nullptr, gbuf);
 }
 
 // ---------------------------------------------------------------------------
@@ -631,11 +654,12 @@ __global__ void __launch_bounds__(512)
 k_fft_c2c_synth(FftArgs F, int tw_smem, int jobs, int nitems,
                 const double2* __restrict__ spec, double2* __restrict__ grid, long long gf,
                 long long grs, long long gcs, const int* __restrict__ rowN,
-                const int* __restrict__ rowS, int lc, int npair, int extend_col) {
+                const int* __restrict__ rowS, int lc, int npair, int extend_col, double2* __restrict__ gbuf) {
     extern __shared__ double2 smem_fft[];
     const double2* tw = fft_stage_twiddles(F, smem_fft, tw_smem);
+    double2* bufs = fft_buffers(F, smem_fft, gbuf);
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-        fft_c2c_synth_body(F, tw, smem_fft, it % jobs, it / jobs, spec, grid, gf, grs, gcs,
+        fft_c2c_synth_body(F, tw, bufs, it % jobs, it / jobs, spec, grid, gf, grs, gcs,
                            rowN, rowS, lc, npair, extend_col);
         __syncthreads();
     }
@@ -646,11 +670,12 @@ k_fft_c2c_anal(FftArgs F, int tw_smem, int jobs, int nitems,
                const double2* __restrict__ grid, long long gf, long long grs, long long gcs,
                double2* __restrict__ spec, const int* __restrict__ rowN,
                const int* __restrict__ rowS, const double* __restrict__ wN,
-               const double* __restrict__ wS, double wscale, int lc, int npair) {
+               const double* __restrict__ wS, double wscale, int lc, int npair, double2* __restrict__ gbuf) {
     extern __shared__ double2 smem_fft[];
     const double2* tw = fft_stage_twiddles(F, smem_fft, tw_smem);
+    double2* bufs = fft_buffers(F, smem_fft, gbuf);
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-        fft_c2c_anal_body(F, tw, smem_fft, it % jobs, it / jobs, grid, gf, grs, gcs, spec,
+        fft_c2c_anal_body(F, tw, bufs, it % jobs, it / jobs, grid, gf, grs, gcs, spec,
                           rowN, rowS, wN, wS, wscale, lc, npair);
         __syncthreads();
     }
@@ -678,8 +703,9 @@ int launch_unpack_coef_c(const shtc_plan* P, const double2* partial, int ntiles,
 
 int launch_fft_c2c_synth(const shtc_plan* P, const double2* spec, double2* grid,
                          long long gf, long long grs, long long gcs, int nfield,
-                         cudaStream_t st) {
+                         cudaStream_t st, double2* gbuf) {
     const FftPlan& f = P->fft;
+    if (f.gmem && !gbuf) return SHTC_EWORK;
     int rc = fft_smem_setup((const void*)k_fft_c2c_synth, f);
     if (rc) return rc;
     const int jobs = 2 * P->npair;
@@ -689,14 +715,15 @@ int launch_fft_c2c_synth(const shtc_plan* P, const double2* spec, double2* grid,
     if (blocks == 0) return SHTC_OK;
     k_fft_c2c_synth<<<blocks, f.threads, f.smem, st>>>(
         fft_args(f), f.tw_smem, jobs, nitems, spec, grid, gf, grs, gcs, P->d_rowN,
-        P->d_rowS, P->lc, P->npair, P->extend);
+        P->d_rowS, P->lc, P->npair, P->extend, gbuf);
     return map_cuda(cudaGetLastError());
 }
 
 int launch_fft_c2c_anal(const shtc_plan* P, const double2* grid, long long gf,
                         long long grs, long long gcs, double2* spec, int nfield,
-                        cudaStream_t st) {
+                        cudaStream_t st, double2* gbuf) {
     const FftPlan& f = P->fft;
+    if (f.gmem && !gbuf) return SHTC_EWORK;
     int rc = fft_smem_setup((const void*)k_fft_c2c_anal, f);
     if (rc) return rc;
     const int jobs = 2 * P->npair;
@@ -706,7 +733,7 @@ int launch_fft_c2c_anal(const shtc_plan* P, const double2* grid, long long gf,
     if (blocks == 0) return SHTC_OK;
     k_fft_c2c_anal<<<blocks, f.threads, f.smem, st>>>(
         fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_arowN,
-        P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair);
+        P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, gbuf);
     return map_cuda(cudaGetLastError());
 }
 
@@ -785,7 +812,7 @@ int launch_gradient_dh(const shtc_plan* P, const double* cilm, long long sf, lon
                        long long sl, long long sm, int cdim, double* theta, double* phi,
                        long long gf, long long grs, long long gcs, double radius,
                        int nfield, double2* packed, double2* spec, double2* spec2,
-                       cudaStream_t st) {
+                       cudaStream_t st, double2* gbuf) {
     const int lc = P->lc;
     stage_begin(SHTC_STAGE_PACK, st);
     {
@@ -807,9 +834,10 @@ int launch_gradient_dh(const shtc_plan* P, const double* cilm, long long sf, lon
         k_grad_combine<<<grid, 256, 0, st>>>(spec, spec2, P->d_z, P->npair, lc, P->nlat,
                                              nfield, 1.0 / radius);
         rc = map_cuda(cudaGetLastError());
-        if (!rc) rc = launch_fft_c2r(P, spec2, theta, SHTC_F64, gf, grs, gcs, nfield, 0, st);
+        if (!rc) rc = launch_fft_c2r(P, spec2, theta, SHTC_F64, gf, grs, gcs, nfield, 0, st,
+                                     gbuf);
         if (!rc) rc = launch_fft_c2r(P, spec2 + (long long)nfield * per, phi, SHTC_F64, gf,
-                                     grs, gcs, nfield, 0, st);
+                                     grs, gcs, nfield, 0, st, gbuf);
     }
     stage_end(SHTC_STAGE_FFT_C2R, st);
     return rc;

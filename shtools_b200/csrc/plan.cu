@@ -324,11 +324,23 @@ int build_fft_plan(FftPlan* f, int n, int cplx, cudaStream_t st) {
     int maxsmem = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (maxsmem > 0 && f->smem_data > (size_t)maxsmem) return SHTC_EUNSUP;
-    const size_t with_tw = f->smem_data + (size_t)f->ntw * sizeof(double2);
-    f->tw_smem = (maxsmem > 0 && with_tw <= (size_t)maxsmem) ? 1 : 0;
-    f->smem = f->tw_smem ? with_tw : f->smem_data;
     f->threads = len > 2048 ? 512 : (len > 512 ? 256 : 128);
+    if (maxsmem > 0 && f->smem_data > (size_t)maxsmem) {
+        // too long for shared memory: the data buffers go to a global scratch
+        // (one pair per persistent CTA, L2-resident), the twiddles stay in
+        // shared memory when they fit
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        f->gmem = 1;
+        f->gmem_ctas = sms > 0 ? sms : 1;
+        const size_t tb = (size_t)f->ntw * sizeof(double2);
+        f->tw_smem = tb <= (size_t)maxsmem ? 1 : 0;
+        f->smem = f->tw_smem ? tb : 0;
+    } else {
+        const size_t with_tw = f->smem_data + (size_t)f->ntw * sizeof(double2);
+        f->tw_smem = (maxsmem > 0 && with_tw <= (size_t)maxsmem) ? 1 : 0;
+        f->smem = f->tw_smem ? with_tw : f->smem_data;
+    }
     auto up = [&](double2** d, const std::vector<double2>& h) -> int {
         if (h.empty()) { *d = nullptr; return SHTC_OK; }
         if (cudaMalloc((void**)d, h.size() * sizeof(double2)) != cudaSuccess) return SHTC_EALLOC;

@@ -51,6 +51,10 @@ struct FftPlan {
     size_t smem;       // dynamic shared memory bytes per CTA of the per-plan kernels:
                        // smem_data, plus the twiddles when tw_smem
     int tw_smem;       // per-plan kernels copy d_tw into shared memory
+    int gmem;          // 1: the two data buffers exceed shared memory and live in
+                       // a global scratch of gmem_ctas x 2 x len points (caller's
+                       // workspace); the passes then run through L2
+    int gmem_ctas;     // persistent CTAs of the global-buffer kernels
     int threads;       // CTA size
 };
 
@@ -111,15 +115,19 @@ int launch_pack_coef(const shtc_plan* P, const void* cilm, int dtype, long long 
                      cudaStream_t st, int nfield_total = 0, int f_off = 0);
 int launch_fft_r2c_product(const shtc_plan* P, const double* grid, const double* grid2,
                            long long gf, long long grs, long long gcs, double2* spec,
-                           int nfield, cudaStream_t st);
+                           int nfield, cudaStream_t st, double2* gbuf = nullptr);
 int launch_legendre_synth(const shtc_plan* P, const double2* packed,
                           double2* spec, int nfield, cudaStream_t st);
+// gbuf: the FFT scratch of the workspace (fft_scratch_bytes), needed when
+// P->fft.gmem
 int launch_fft_c2r(const shtc_plan* P, const double2* spec, void* grid, int dtype,
                    long long gf, long long grs, long long gcs, int nfield,
-                   int weighted, cudaStream_t st);
+                   int weighted, cudaStream_t st, double2* gbuf = nullptr);
 int launch_fft_r2c(const shtc_plan* P, const void* grid, int dtype, long long gf,
                    long long grs, long long gcs, double2* spec, int nfield,
-                   int weighted, int fold_extend, cudaStream_t st);
+                   int weighted, int fold_extend, cudaStream_t st,
+                   double2* gbuf = nullptr);
+size_t fft_scratch_bytes(const shtc_plan* P);
 int launch_legendre_anal(const shtc_plan* P, const double2* spec,
                          double2* partial, int ntiles_out, int nfield,
                          cudaStream_t st);
@@ -138,16 +146,16 @@ int launch_unpack_coef_c(const shtc_plan* P, const double2* partial, int ntiles,
                          long long sm, int cdim, int nfield, cudaStream_t st);
 int launch_fft_c2c_synth(const shtc_plan* P, const double2* spec, double2* grid,
                          long long gf, long long grs, long long gcs, int nfield,
-                         cudaStream_t st);
+                         cudaStream_t st, double2* gbuf = nullptr);
 // MakeGradientDH: workspace = packed (3 nfield) | spec (3 nfield) | spec2 (2 nfield)
 int launch_gradient_dh(const shtc_plan* P, const double* cilm, long long sf, long long sk,
                        long long sl, long long sm, int cdim, double* theta, double* phi,
                        long long gf, long long grs, long long gcs, double radius,
                        int nfield, double2* packed, double2* spec, double2* spec2,
-                       cudaStream_t st);
+                       cudaStream_t st, double2* gbuf = nullptr);
 int launch_fft_c2c_anal(const shtc_plan* P, const double2* grid, long long gf,
                         long long grs, long long gcs, double2* spec, int nfield,
-                        cudaStream_t st);
+                        cudaStream_t st, double2* gbuf = nullptr);
 int map_cuda(cudaError_t e);
 
 // timing.cu: event brackets around kernel stages (SHTC_STAGE_* ids)
