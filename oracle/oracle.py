@@ -59,6 +59,11 @@ def lib():
         L.orc_dhaj.argtypes = [_I, _D, _I]
         L.orc_makegradient_dh.argtypes = [_D, _D, _D, _I, _I, _I, _I, _I, ctypes.c_double]
         L.orc_shmultiply.argtypes = [_D, _I, _D, _I, _I, _D, _I, _I, _I, _I]
+        _F = ctypes.c_double
+        L.orc_makegravgrid_dh.argtypes = [_D, _D, _D, _D, _D, _D, _I, _I, _F, _F, _F, _F,
+                                          _I, _I, _I, _F, _I, _F, _I]
+        L.orc_normal_gravity.argtypes = [_F, _F, _F, _F, _F]
+        L.orc_normal_gravity.restype = _F
         L.orc_makegrid_dhc.argtypes = [_D, _D, _I, _I, _I, _I, _I, _I, _I]
         L.orc_shexpand_dhc.argtypes = [_D, _I, _D, _I, _I, _I, _I, _I, _I]
         L.orc_makegrid_glqc.argtypes = [_D, _D, _I, _I, _D, _I, _I, _I, _I]
@@ -348,6 +353,34 @@ def makegradient_dh(cilm, lmax=None, sampling=1, lmax_calc=None, extend=0, radiu
     _check(lib().orc_makegradient_dh(_p(th), _p(ph), _p(cilm), cilm.shape[1], lmax,
                                      int(sampling), lmax_calc, int(extend), float(radius)))
     return th, ph
+
+
+def normal_gravity(geocentric_lat, gm, omega, a, b):
+    """NormalGravity (NormalGravity.f95:1): latitude in degrees."""
+    return lib().orc_normal_gravity(float(geocentric_lat), float(gm), float(omega),
+                                    float(a), float(b))
+
+
+def makegravgrid_dh(cilm, gm, r0, lmax=None, a=None, f=0.0, sampling=2, lmax_calc=None,
+                    omega=None, normal_gravity=0, normal_gravity_gm=None, extend=0,
+                    pot=True):
+    """MakeGravGridDH (MakeGravGridDH.f95:1).  omega=None is the Fortran's
+    absent OMEGA (no rotation terms).  Returns (rad, theta, phi, total, pot),
+    pot None when not requested."""
+    cilm = _f64(cilm)
+    lmax, lmax_calc = _lmaxes(cilm, lmax, lmax_calc)
+    n = 2 * lmax + 2
+    shape = (n + int(extend), sampling * n + int(extend))
+    g = [np.zeros(shape) for _ in range(5 if pot else 4)]
+    a = r0 if a is None else a
+    ngm = gm if normal_gravity_gm is None else normal_gravity_gm
+    _check(lib().orc_makegravgrid_dh(_p(g[0]), _p(g[1]), _p(g[2]), _p(g[3]),
+                                     _p(g[4]) if pot else None, _p(cilm), cilm.shape[1],
+                                     lmax, float(gm), float(r0), float(a), float(f),
+                                     int(sampling), lmax_calc, int(omega is not None),
+                                     0.0 if omega is None else float(omega),
+                                     int(normal_gravity), float(ngm), int(extend)))
+    return (g[0], g[1], g[2], g[3], g[4] if pot else None)
 
 
 def shmultiply(cilm1, cilm2, lmax1=None, lmax2=None, norm=1, csphase=1):

@@ -1832,6 +1832,351 @@ int orc_shmultiply(double *cout, int cdout, const double *c1, int cd1, int lmax1
     return rc;
 }
 
+/* ======================================================================== */
+/*  NormalGravity (src/NormalGravity.f95): normal gravity on a rotating     */
+/*  flattened ellipsoid (Somigliana), at geocentric latitude in degrees.     */
+/* ======================================================================== */
+double orc_normal_gravity(double geocentric_lat, double gm, double omega, double a,
+                          double b) {
+    const double pi = acos(-1.0);
+    if (a == b && omega == 0.0) return gm / (a * a);
+    if (a == b) {
+        const double c = cos(geocentric_lat * pi / 180.0);
+        const double g = gm * gm / ((a * a) * (a * a))
+                         + a * (omega * omega) * (c * c) * (a * (omega * omega)
+                                                            - 2.0 * gm / (a * a));
+        return sqrt(g);
+    }
+    const double m = (omega * omega) * (a * a) * b / gm;
+    const double bigE = sqrt(a * a - b * b);       /* linear eccentricity */
+    const double ep = bigE / b;                    /* second eccentricity */
+    const double be = b / bigE;
+    const double q0 = 0.50 * ((1.0 + 3.0 * (be * be)) * atan(bigE / b) - 3.0 * b / bigE);
+    const double q0p = 3.0 * (1.0 + (be * be)) * (1.0 - b / bigE * atan(bigE / b)) - 1.0;
+    const double ga = gm / (a * b) * (1.0 - m - m * ep * q0p / 6.0 / q0);
+    const double gb = gm / (a * a) * (1.0 + m * ep * q0p / 3.0 / q0);
+    const double ab = a / b;
+    const double gl = atan((ab * ab) * tan(geocentric_lat * pi / 180.0));
+    const double cg = cos(gl), sg = sin(gl);
+    double ng = a * ga * (cg * cg) + b * gb * (sg * sg);
+    return ng / sqrt((a * a) * (cg * cg) + (b * b) * (sg * sg));
+}
+
+/* ======================================================================== */
+/*  MakeGravGridDH (src/MakeGravGridDH.f95:1-1069): gravity vector          */
+/*  (radial positive up, theta, phi), its magnitude and the potential on a  */
+/*  DH grid over a flattened ellipsoid of semi-major axis a and flattening  */
+/*  f.  V = GM/r sum_l (r0/r)^l sum_m C_lm Y_lm (4pi, no Condon-Shortley);  */
+/*  r on ring i is the ellipsoid radius r_ex at the ring's geocentric        */
+/*  latitude, applied through prefactor(l) = (r0/r_ex)^l.                   */
+/* ======================================================================== */
+
+/* accumulators of one ring: 8 complex sums over m = 0..lc (north and south
+ * of rad, pot, theta, phi) */
+enum { GR = 0, GRS, GU, GUS, GT, GTS, GP, GPS, GNSUM };
+
+/* one ring's sums, rounding order of MakeGravGridDH.f95:657-877 (the
+ * equator block, 383-585, is this with z = 0, u = 1) */
+static void grav_ring(const rec_tab *t, const double *cilm, int cdim, double z, double u,
+                      const double *pref, int calcu, double **sr, double **si) {
+    const int lc = t->lc, d = lc + 1;
+    const double *sqr = t->sqr, *ff1 = t->ff1, *ff2 = t->ff2;
+    const double uu = u * u;
+    const int deriv = u != 0.0;   /* theta/phi sums are not used on the poles */
+    double pm2, pm1, p, pmm, rescalem, dpl, tempr;
+    double r0 = 0.0, rs0 = 0.0, u0 = 0.0, us0 = 0.0, t0 = 0.0, ts0 = 0.0;
+
+    pm2 = 1.0;
+    pm1 = 0.0;
+    tempr = -CIL(0, 0, 0) * pm2;
+    r0 = r0 + tempr; rs0 = rs0 + tempr;
+    if (calcu) { tempr = CIL(0, 0, 0) * pm2; u0 = u0 + tempr; us0 = us0 + tempr; }
+    if (lc != 0) {
+        pm1 = ff1[(size_t)1 * d + 0] * z;
+        tempr = CIL(0, 1, 0) * pm1 * (-2.0) * pref[1];
+        r0 = r0 + tempr; rs0 = rs0 - tempr;
+        if (calcu) { tempr = CIL(0, 1, 0) * pm1 * pref[1]; u0 = u0 + tempr; us0 = us0 - tempr; }
+        dpl = ff1[(size_t)1 * d + 0];
+        tempr = CIL(0, 1, 0) * dpl * pref[1];
+        t0 = t0 + tempr; ts0 = ts0 + tempr;
+    }
+    for (int l = 2; l <= lc; ++l) {
+        const double fs = (l % 2 == 0) ? 1.0 : -1.0;
+        p = ff1[(size_t)l * d + 0] * z * pm1 - ff2[(size_t)l * d + 0] * pm2;
+        tempr = CIL(0, l, 0) * p * (double)(-(l + 1)) * pref[l];
+        r0 = r0 + tempr; rs0 = rs0 + tempr * fs;
+        if (calcu) {
+            tempr = CIL(0, l, 0) * p * pref[l];
+            u0 = u0 + tempr; us0 = us0 + tempr * fs;
+        }
+        if (deriv) {
+            dpl = l * (sqr[2 * l + 1] / sqr[2 * l - 1] * pm1 - z * p) / uu;
+            tempr = CIL(0, l, 0) * dpl * pref[l];
+            t0 = t0 + tempr; ts0 = ts0 - tempr * fs;
+        }
+        pm2 = pm1;
+        pm1 = p;
+    }
+    sr[GR][0] = r0; sr[GRS][0] = rs0; sr[GU][0] = u0; sr[GUS][0] = us0;
+    sr[GT][0] = t0; sr[GTS][0] = ts0; sr[GP][0] = 0.0; sr[GPS][0] = 0.0;
+    for (int k = 0; k < GNSUM; ++k) si[k][0] = 0.0;
+
+    pmm = sqr[2] * SCALEF;
+    rescalem = 1.0 / SCALEF;
+    for (int m = 1; m <= lc - 1; ++m) {
+        double ar[GNSUM] = {0}, ai[GNSUM] = {0};
+        double cr, ci;
+        rescalem = rescalem * u;
+        pmm = pmm * sqr[2 * m + 1] / sqr[2 * m];
+        pm2 = pmm;
+        /* (m, m), fsymsign = 1 */
+        cr = CIL(0, m, m) * pm2 * (double)(-m - 1) * pref[m];
+        ci = -CIL(1, m, m) * pm2 * (double)(-m - 1) * pref[m];
+        ar[GR] += cr; ai[GR] += ci; ar[GRS] += cr; ai[GRS] += ci;
+        if (calcu) {
+            cr = CIL(0, m, m) * pm2 * pref[m]; ci = -CIL(1, m, m) * pm2 * pref[m];
+            ar[GU] += cr; ai[GU] += ci; ar[GUS] += cr; ai[GUS] += ci;
+        }
+        cr = CIL(1, m, m) * pm2 * pref[m] * m; ci = CIL(0, m, m) * pm2 * pref[m] * m;
+        ar[GP] += cr; ai[GP] += ci; ar[GPS] += cr; ai[GPS] += ci;
+        if (deriv) {
+            dpl = -m * z * pm2 / uu;
+            cr = CIL(0, m, m) * dpl * pref[m]; ci = -CIL(1, m, m) * dpl * pref[m];
+            ar[GT] += cr; ai[GT] += ci; ar[GTS] -= cr; ai[GTS] -= ci;
+        }
+        /* (m+1, m), fsymsign = -1 */
+        pm1 = z * ff1[(size_t)(m + 1) * d + m] * pm2;
+        cr = CIL(0, m + 1, m) * pm1 * (double)(-m - 2) * pref[m + 1];
+        ci = -CIL(1, m + 1, m) * pm1 * (double)(-m - 2) * pref[m + 1];
+        ar[GR] += cr; ai[GR] += ci; ar[GRS] -= cr; ai[GRS] -= ci;
+        if (calcu) {
+            cr = CIL(0, m + 1, m) * pm1 * pref[m + 1];
+            ci = -CIL(1, m + 1, m) * pm1 * pref[m + 1];
+            ar[GU] += cr; ai[GU] += ci; ar[GUS] -= cr; ai[GUS] -= ci;
+        }
+        cr = CIL(1, m + 1, m) * pm1 * pref[m + 1] * m;
+        ci = CIL(0, m + 1, m) * pm1 * pref[m + 1] * m;
+        ar[GP] += cr; ai[GP] += ci; ar[GPS] -= cr; ai[GPS] -= ci;
+        if (deriv) {
+            dpl = (sqr[2 * m + 3] * pmm - z * (m + 1) * pm1) / uu;
+            cr = CIL(0, m + 1, m) * dpl * pref[m + 1];
+            ci = -CIL(1, m + 1, m) * dpl * pref[m + 1];
+            ar[GT] += cr; ai[GT] += ci; ar[GTS] += cr; ai[GTS] += ci;
+        }
+        for (int l = m + 2; l <= lc; ++l) {
+            const double fs = ((l - m) % 2 == 0) ? 1.0 : -1.0;
+            p = z * ff1[(size_t)l * d + m] * pm1 - ff2[(size_t)l * d + m] * pm2;
+            cr = CIL(0, l, m) * p * (double)(-(l + 1)) * pref[l];
+            ci = -CIL(1, l, m) * p * (double)(-(l + 1)) * pref[l];
+            ar[GR] += cr; ai[GR] += ci; ar[GRS] += cr * fs; ai[GRS] += ci * fs;
+            if (calcu) {
+                cr = CIL(0, l, m) * p * pref[l]; ci = -CIL(1, l, m) * p * pref[l];
+                ar[GU] += cr; ai[GU] += ci; ar[GUS] += cr * fs; ai[GUS] += ci * fs;
+            }
+            cr = CIL(1, l, m) * p * pref[l] * m; ci = CIL(0, l, m) * p * pref[l] * m;
+            ar[GP] += cr; ai[GP] += ci; ar[GPS] += cr * fs; ai[GPS] += ci * fs;
+            if (deriv) {
+                dpl = (sqr[2 * l + 1] * sqr[l - m] * sqr[l + m] / sqr[2 * l - 1] * pm1
+                       - z * l * p) / uu;
+                cr = CIL(0, l, m) * dpl * pref[l]; ci = -CIL(1, l, m) * dpl * pref[l];
+                ar[GT] += cr; ai[GT] += ci; ar[GTS] -= cr * fs; ai[GTS] -= ci * fs;
+            }
+            pm2 = pm1;
+            pm1 = p;
+        }
+        for (int k = 0; k < GNSUM; ++k) {
+            sr[k][m] = ar[k] * rescalem;
+            si[k][m] = ai[k] * rescalem;
+        }
+    }
+    if (lc != 0) {
+        double cr, ci;
+        for (int k = 0; k < GNSUM; ++k) { sr[k][lc] = 0.0; si[k][lc] = 0.0; }
+        rescalem = rescalem * u;
+        pmm = pmm * sqr[2 * lc + 1] / sqr[2 * lc] * rescalem;
+        cr = CIL(0, lc, lc) * pmm * (double)(-lc - 1) * pref[lc];
+        ci = -CIL(1, lc, lc) * pmm * (double)(-lc - 1) * pref[lc];
+        sr[GR][lc] = cr; si[GR][lc] = ci; sr[GRS][lc] = cr; si[GRS][lc] = ci;
+        if (calcu) {
+            cr = CIL(0, lc, lc) * pmm * pref[lc]; ci = -CIL(1, lc, lc) * pmm * pref[lc];
+            sr[GU][lc] = cr; si[GU][lc] = ci; sr[GUS][lc] = cr; si[GUS][lc] = ci;
+        }
+        cr = CIL(1, lc, lc) * pmm * pref[lc] * lc; ci = CIL(0, lc, lc) * pmm * pref[lc] * lc;
+        sr[GP][lc] = cr; si[GP][lc] = ci; sr[GPS][lc] = cr; si[GPS][lc] = ci;
+        if (deriv) {
+            dpl = -lc * z * pmm / uu;
+            cr = CIL(0, lc, lc) * dpl * pref[lc]; ci = -CIL(1, lc, lc) * dpl * pref[lc];
+            sr[GT][lc] = cr; si[GT][lc] = ci; sr[GTS][lc] = -cr; si[GTS][lc] = -ci;
+        }
+    }
+}
+
+/* c2r of the m = 0..lc sums (m >= 1 halved, the rest, Nyquist included,
+ * zero) into row[0..nlong-1] */
+static void grav_c2r(orc_fft *plan, int nlong, int lc, const double *cr, const double *ci,
+                     double *wr, double *wi, double *row) {
+    const int nh = nlong / 2 + 1;
+    double *ar = calloc((size_t)nh, sizeof(double)), *ai = calloc((size_t)nh, sizeof(double));
+    ar[0] = cr[0];
+    for (int m = 1; m <= lc && m < nh; ++m) { ar[m] = cr[m] / 2.0; ai[m] = ci[m] / 2.0; }
+    fft_c2r(plan, ar, ai, row, wr, wi);
+    free(ar); free(ai);
+}
+
+/* rad, theta, phi, total: (n+extend) x (nlong+extend) row-major; pot may be
+ * NULL.  has_omega = 0 is the reference's absent OMEGA (no rotation terms).
+ * Returns the reference's exit status (5: normal gravity without omega). */
+int orc_makegravgrid_dh(double *rad, double *theta_g, double *phi_g, double *total,
+                        double *pot, const double *cilm, int cdim, int lmax, double gm,
+                        double r0, double a, double f, int sampling, int lmax_calc,
+                        int has_omega, double omega, int normal_gravity,
+                        double normal_gravity_gm, int extend) {
+    if (cdim < 1) return ORC_EDIM;
+    if (sampling != 1 && sampling != 2) return ORC_EBOUND;
+    if (extend != 0 && extend != 1) return ORC_EBOUND;
+    if (normal_gravity != 0 && normal_gravity != 1) return ORC_EBOUND;
+    if (normal_gravity == 1 && !has_omega) return 5;
+    if (lmax_calc > lmax) return ORC_EBOUND;
+    const int n = 2 * lmax + 2;
+    const int nlong = sampling == 1 ? n : 2 * n;
+    const int nlong_out = nlong + extend, nlat_out = n + extend;
+    int lc = lmax_calc < 0 ? lmax : lmax_calc;
+    if (lc > cdim - 1) lc = cdim - 1;
+    if (lc > lmax) lc = lmax;
+    const int calcu = pot != NULL;
+    const double pi = acos(-1.0);
+    rec_tab t;
+    if (rec_build(&t, lc, 1)) return ORC_EALLOC;
+    orc_fft *plan = fft_plan(nlong);
+    const int L2 = lc + 2;
+    double *sr[GNSUM], *si[GNSUM];
+    for (int k = 0; k < GNSUM; ++k) {
+        sr[k] = calloc((size_t)L2, sizeof(double));
+        si[k] = calloc((size_t)L2, sizeof(double));
+    }
+    double *pref = calloc((size_t)L2, sizeof(double));
+    double *wr = malloc(sizeof(double) * (size_t)nlong), *wi = malloc(sizeof(double) * (size_t)nlong);
+    double *row = malloc(sizeof(double) * (size_t)nlong);
+    const size_t gsz = (size_t)nlat_out * nlong_out;
+    memset(rad, 0, sizeof(double) * gsz);
+    memset(theta_g, 0, sizeof(double) * gsz);
+    memset(phi_g, 0, sizeof(double) * gsz);
+    memset(total, 0, sizeof(double) * gsz);
+    if (calcu) memset(pot, 0, sizeof(double) * gsz);
+    const int i_eq = n / 2 + 1;
+    for (int i = 1; i <= i_eq; ++i) {
+        const int eq = i == i_eq;
+        const double theta = eq ? pi / 2.0 : pi * (double)(i - 1) / (double)n;
+        const double z = eq ? 0.0 : cos(theta);
+        const double u = eq ? 1.0 : sqrt((1.0 - z) * (1.0 + z));
+        const int i_s = 2 * i_eq - i;
+        double r_ex;
+        if (eq) {
+            r_ex = a;
+        } else if (i == 1) {
+            r_ex = a * (1.0 - f);
+        } else {
+            const double lat = pi / 2.0 - theta;
+            const double cl = cos(lat), sl = sin(lat);
+            r_ex = cl * cl + sl * sl / ((1.0 - f) * (1.0 - f));
+            r_ex = a * sqrt(1.0 / r_ex);
+        }
+        if (lc != 0) {
+            pref[1] = r0 / r_ex;
+            for (int l = 2; l <= lc; ++l) pref[l] = pref[l - 1] * r0 / r_ex;
+        }
+        grav_ring(&t, cilm, cdim, z, u, pref, calcu, sr, si);
+        const double st = sin(theta);
+        const double r2 = r_ex * r_ex;
+        /* north ring (or the equator) */
+        double *o;
+        o = &rad[(size_t)(i - 1) * nlong_out];
+        grav_c2r(plan, nlong, lc, sr[GR], si[GR], wr, wi, row);
+        for (int j = 0; j < nlong; ++j) o[j] = row[j] * gm / r2;
+        if (calcu) {
+            o = &pot[(size_t)(i - 1) * nlong_out];
+            grav_c2r(plan, nlong, lc, sr[GU], si[GU], wr, wi, row);
+            for (int j = 0; j < nlong; ++j) o[j] = row[j] * gm / r_ex;
+        }
+        if (i != 1) {
+            o = &theta_g[(size_t)(i - 1) * nlong_out];
+            grav_c2r(plan, nlong, lc, sr[GT], si[GT], wr, wi, row);
+            for (int j = 0; j < nlong; ++j) o[j] = -st * row[j] * gm / r2;
+            o = &phi_g[(size_t)(i - 1) * nlong_out];
+            grav_c2r(plan, nlong, lc, sr[GP], si[GP], wr, wi, row);
+            for (int j = 0; j < nlong; ++j) o[j] = row[j] * (gm / r2) / st;
+        }
+        /* south ring; the south pole only with extend */
+        if (!eq && !(i == 1 && extend == 0)) {
+            o = &rad[(size_t)(i_s - 1) * nlong_out];
+            grav_c2r(plan, nlong, lc, sr[GRS], si[GRS], wr, wi, row);
+            for (int j = 0; j < nlong; ++j) o[j] = row[j] * gm / r2;
+            if (calcu) {
+                o = &pot[(size_t)(i_s - 1) * nlong_out];
+                grav_c2r(plan, nlong, lc, sr[GUS], si[GUS], wr, wi, row);
+                for (int j = 0; j < nlong; ++j) o[j] = row[j] * gm / r_ex;
+            }
+            if (i != 1) {
+                o = &theta_g[(size_t)(i_s - 1) * nlong_out];
+                grav_c2r(plan, nlong, lc, sr[GTS], si[GTS], wr, wi, row);
+                for (int j = 0; j < nlong; ++j) o[j] = -st * row[j] * gm / r2;
+                o = &phi_g[(size_t)(i_s - 1) * nlong_out];
+                grav_c2r(plan, nlong, lc, sr[GPS], si[GPS], wr, wi, row);
+                for (int j = 0; j < nlong; ++j) o[j] = row[j] * (gm / r2) / st;
+            }
+        }
+    }
+    /* rotation (MakeGravGridDH.f95:987-1013) */
+    if (has_omega) {
+        for (int i = 1; i <= nlat_out; ++i) {
+            const double theta = pi * (double)(i - 1) / (double)n;
+            const double lat = pi / 2.0 - theta;
+            const double tl = tan(lat);
+            double r_ex = (1.0 + tl * tl) / (1.0 + tl * tl / ((1.0 - f) * (1.0 - f)));
+            r_ex = a * sqrt(r_ex);
+            const double st = sin(theta), ct = cos(theta);
+            const double so = st * omega;
+            const double rr = r_ex * (so * so);
+            const double tt = st * ct * r_ex * (omega * omega);
+            const double ro = r_ex * st * omega;
+            const double pp = 0.50 * (ro * ro);
+            for (int j = 0; j < nlong; ++j) {
+                rad[(size_t)(i - 1) * nlong_out + j] += rr;
+                theta_g[(size_t)(i - 1) * nlong_out + j] += tt;
+                if (calcu) pot[(size_t)(i - 1) * nlong_out + j] += pp;
+            }
+        }
+    }
+    for (int i = 0; i < nlat_out; ++i)
+        for (int j = 0; j < nlong; ++j) {
+            const size_t k = (size_t)i * nlong_out + j;
+            total[k] = sqrt(rad[k] * rad[k] + phi_g[k] * phi_g[k] + theta_g[k] * theta_g[k]);
+        }
+    if (normal_gravity == 1) {
+        const double b = a * (1.0 - f);
+        for (int i = 1; i <= nlat_out; ++i) {
+            const double theta = pi * (double)(i - 1) / (double)n;
+            const double lat = (pi / 2.0 - theta) * 180.0 / pi;
+            const double ng = orc_normal_gravity(lat, normal_gravity_gm, omega, a, b);
+            for (int j = 0; j < nlong; ++j) total[(size_t)(i - 1) * nlong_out + j] -= ng;
+        }
+    }
+    if (extend == 1)
+        for (int i = 0; i < nlat_out; ++i) {
+            const size_t k = (size_t)i * nlong_out;
+            rad[k + nlong] = rad[k];
+            theta_g[k + nlong] = theta_g[k];
+            phi_g[k + nlong] = phi_g[k];
+            total[k + nlong] = total[k];
+            if (calcu) pot[k + nlong] = pot[k];
+        }
+    for (int k = 0; k < GNSUM; ++k) { free(sr[k]); free(si[k]); }
+    free(pref); free(wr); free(wi); free(row);
+    fft_free(plan);
+    rec_free(&t);
+    return ORC_OK;
+}
+
 /* Number of host threads OpenMP would use (1 when built without OpenMP). */
 int orc_max_threads(void) {
 #ifdef _OPENMP

@@ -36,7 +36,7 @@ extern "C" const char* shtc_status_string(int s) {
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 static size_t coef_region(const shtc_plan* P, int nfield) {
-    const int tiles = anal_tiles(P);
+    const int tiles = anal_tiles(P, nfield);
     return align256((size_t)P->nlm * nfield * sizeof(double2) * (tiles > 1 ? tiles : 1));
 }
 
@@ -122,7 +122,7 @@ extern "C" int shtc_analysis_ex(const shtc_plan* P, const void* grid, int gdt,
     double2* partial = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
     double2* fbuf = fft_scratch(P, work, coef_region(P, nfield) + spec_region(P, nfield));
-    const int tiles = anal_tiles(P);
+    const int tiles = anal_tiles(P, nfield);
     stage_begin(SHTC_STAGE_FFT_R2C, st);
     rc = launch_fft_r2c(P, grid, gdt, gsf, gsr, gsc, spec, nfield, 1, 0, st, fbuf);
     stage_end(SHTC_STAGE_FFT_R2C, st);
@@ -153,7 +153,7 @@ extern "C" int shtc_synthesis_adjoint_ex(const shtc_plan* P, const void* grid, i
     double2* partial = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
     double2* fbuf = fft_scratch(P, work, coef_region(P, nfield) + spec_region(P, nfield));
-    const int tiles = anal_tiles(P);
+    const int tiles = anal_tiles(P, nfield);
     stage_begin(SHTC_STAGE_FFT_R2C, st);
     rc = launch_fft_r2c(P, grid, gdt, gsf, gsr, gsc, spec, nfield, 0, P->extend, st, fbuf);
     stage_end(SHTC_STAGE_FFT_R2C, st);
@@ -277,7 +277,7 @@ extern "C" int shtc_analysis_c(const shtc_plan* P, const void* grid, long long g
     double2* partial = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nf2));
     double2* fbuf = fft_scratch(P, work, coef_region(P, nf2) + spec_region(P, nf2));
-    const int tiles = anal_tiles(P);
+    const int tiles = anal_tiles(P, nf2);
     stage_begin(SHTC_STAGE_FFT_R2C, st);
     rc = launch_fft_c2c_anal(P, (const double2*)grid, gsf, gsr, gsc, spec, nfield, st, fbuf);
     stage_end(SHTC_STAGE_FFT_R2C, st);
@@ -369,7 +369,7 @@ extern "C" int shtc_multiply(const shtc_plan* P, const double* cilm1, long long 
                                              spec_region(P, 2 * nfield) +
                                              grid_region(P, 2 * nfield));
     const long long gf = (long long)P->nlat * P->nlon;
-    const int tiles = anal_tiles(P);
+    const int tiles = anal_tiles(P, nfield);
     stage_begin(SHTC_STAGE_PACK, st);
     int rc = launch_pack_coef(P, cilm1, SHTC_F64, c1sf, c1sk, c1sl, c1sm, lmax1 + 1, packed,
                               nfield, 0, st, 2 * nfield, 0);

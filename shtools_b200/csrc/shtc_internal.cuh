@@ -135,7 +135,7 @@ int launch_unpack_coef(const shtc_plan* P, const double2* partial, int ntiles,
                        void* cilm, int dtype, long long sf, long long sk, long long sl,
                        long long sm, int cdim, int nfield, int normalise,
                        cudaStream_t st);
-int anal_tiles(const shtc_plan* P);
+int anal_tiles(const shtc_plan* P, int nfield);
 // complex plans: cilm (nfield, 2, cdim, cdim) and grids of interleaved complex
 // doubles, strides in complex elements; internal fields 2u (+m), 2u+1 (-m)
 int launch_pack_coef_c(const shtc_plan* P, const double2* cilm, long long sf, long long sk,
