@@ -280,6 +280,24 @@ SHTC_API int shtc_gradient_dh(const shtc_plan* plan, const double* cilm, long lo
                               long long gsc, double radius, int nfield, void* work,
                               size_t work_bytes, void* stream);
 
+/* MakeGravGridDH (src/MakeGravGridDH.f95:1) on device buffers: the gravity
+ * vector of the potential V = GM/r sum_l (r0/r)^l C_lm Y_lm on a flattened
+ * ellipsoid (semi-major axis a, flattening f): rad (positive up), theta,
+ * phi, the magnitude total and, when pot is not NULL, the potential.
+ * has_omega = 0 is the reference's absent OMEGA (no centrifugal terms);
+ * normal_gravity = 1 removes the normal gravity of GM normal_gravity_gm
+ * from total (needs has_omega).  A real DH plan with norm 1 and csphase 1;
+ * the five grids share the strides; workspace
+ * shtc_gravity_workspace_bytes(plan, nfield). */
+SHTC_API size_t shtc_gravity_workspace_bytes(const shtc_plan* plan, int nfield);
+SHTC_API int shtc_gravity_dh(const shtc_plan* plan, const double* cilm, long long csf,
+                             long long csk, long long csl, long long csm, int cilm_dim,
+                             double gm, double r0, double a, double f, int has_omega,
+                             double omega, int normal_gravity, double normal_gravity_gm,
+                             double* rad, double* theta, double* phi, double* total,
+                             double* pot, long long gsf, long long gsr, long long gsc,
+                             int nfield, void* work, size_t work_bytes, void* stream);
+
 /* SHMultiply (src/SHMultiply.f95:1) on device buffers: the product of fields
  * of degrees lmax1 and lmax2, expanded to lmax1 + lmax2, through the GLQ grid
  * of a plan created with shtc_plan_create_glq for lmax = lmax1 + lmax2
@@ -356,6 +374,22 @@ SHTC_API void MakeGradientDH(const double* cilm, const int cilm_dim, const int l
                              const int theta_d1, int* n, const int* sampling,
                              const int* lmax_calc, const int* extend, const double* radius,
                              int* exitstatus);
+
+/* include/shtools.h:726-746, src/cWrapper.f95:1484-1514 (src/MakeGravGridDH.f95:1);
+ * rad, theta, phi, total and pot (NULL: not computed) are (nlat, nlon)
+ * column-major; the normal gravity uses gm.  exitstatus 5: normal_gravity
+ * 1 without omega, as the reference. */
+SHTC_API void MakeGravGridDH(const double* cilm, const int cilm_dim, const int lmax,
+                             const double gm, const double r0, const double a,
+                             const double f, double* rad, const int nlon, const int nlat,
+                             double* theta, double* phi, double* total, int* n,
+                             const int* sampling, const int* lmax_calc, const double* omega,
+                             const int* normal_gravity, double* pot, const int* extend,
+                             int* exitstatus);
+
+/* include/shtools.h:952-956 (src/NormalGravity.f95:1); host arithmetic */
+SHTC_API double NormalGravity(const double geocentric_lat, const double gm,
+                              const double omega, const double a, const double b);
 
 /* include/shtools.h:254-265 (src/SHMultiply.f95:1); precomp is ignored */
 SHTC_API void SHMultiply(double* cilmout, const int cilmout_dim, const double* cilm1,

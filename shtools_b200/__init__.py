@@ -17,13 +17,13 @@ provides device memory and streams.
 """
 from .transforms import (MakeGridDH, SHExpandDH, MakeGridGLQ, SHExpandGLQ,
                          MakeGridDHC, SHExpandDHC, MakeGridGLQC, SHExpandGLQC,
-                         MakeGradientDH, SHMultiply,
+                         MakeGradientDH, MakeGravGridDH, NormalGravity, SHMultiply,
                          PreGLQ, SHGLQ, DHaj, Plan, get_plan,
                          clear_plan_cache, GRID_DH, GRID_GLQ)
 from ._lib import SHTCudaError
 
 __all__ = ["MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ",
            "MakeGridDHC", "SHExpandDHC", "MakeGridGLQC", "SHExpandGLQC",
-           "MakeGradientDH", "SHMultiply", "PreGLQ",
+           "MakeGradientDH", "MakeGravGridDH", "NormalGravity", "SHMultiply", "PreGLQ",
            "SHGLQ", "DHaj", "Plan", "get_plan", "clear_plan_cache", "GRID_DH",
            "GRID_GLQ", "SHTCudaError"]

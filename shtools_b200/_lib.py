@@ -39,8 +39,9 @@ EXPORTS = (
     "SHGLQ", "PreGLQ", "DHaj", "shtc_plan_create_dhc", "shtc_plan_create_glqc",
     "shtc_synthesis_c", "shtc_analysis_c", "MakeGridDHC", "SHExpandDHC",
     "MakeGridGLQC", "SHExpandGLQC", "shtc_gradient_workspace_bytes",
-    "shtc_gradient_dh", "MakeGradientDH", "shtc_multiply_workspace_bytes",
-    "shtc_multiply", "SHMultiply",
+    "shtc_gradient_dh", "MakeGradientDH", "shtc_gravity_workspace_bytes",
+    "shtc_gravity_dh", "shtc_multiply_workspace_bytes", "shtc_multiply",
+    "MakeGravGridDH", "NormalGravity", "SHMultiply",
 )
 
 
@@ -88,6 +89,10 @@ def _bind(L):
     L.shtc_gradient_workspace_bytes.restype = _SZ
     L.shtc_gradient_workspace_bytes.argtypes = [_P, _I]
     L.shtc_gradient_dh.argtypes = [_P] + coef + [_P, _P, _LL, _LL, _LL, _D] + tail
+    L.shtc_gravity_workspace_bytes.restype = _SZ
+    L.shtc_gravity_workspace_bytes.argtypes = [_P, _I]
+    L.shtc_gravity_dh.argtypes = ([_P] + coef + [_D, _D, _D, _D, _I, _D, _I, _D,
+                                                 _P, _P, _P, _P, _P, _LL, _LL, _LL] + tail)
     L.shtc_multiply_workspace_bytes.restype = _SZ
     L.shtc_multiply_workspace_bytes.argtypes = [_P, _I]
     L.shtc_multiply.argtypes = ([_P, _P, _LL, _LL, _LL, _LL, _I, _P, _LL, _LL, _LL, _LL, _I]
@@ -111,9 +116,13 @@ def _bind(L):
     L.MakeGradientDH.argtypes = [_DP, _I, _I, _DP, _DP, _I, _I, _IP, _IP, _IP, _IP, _DP,
                                  _IP]
     L.SHMultiply.argtypes = [_DP, _I, _DP, _I, _I, _DP, _I, _I, _IP, _IP, _IP, _IP]
+    L.MakeGravGridDH.argtypes = [_DP, _I, _I, _D, _D, _D, _D, _DP, _I, _I, _DP, _DP, _DP,
+                                 _IP, _IP, _IP, _DP, _IP, _DP, _IP, _IP]
+    L.NormalGravity.argtypes = [_D, _D, _D, _D, _D]
+    L.NormalGravity.restype = _D
     for name in ("SHMultiply", "MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ", "SHGLQ",
                  "PreGLQ", "DHaj", "MakeGridDHC", "SHExpandDHC", "MakeGridGLQC",
-                 "SHExpandGLQC", "MakeGradientDH"):
+                 "SHExpandGLQC", "MakeGradientDH", "MakeGravGridDH"):
         getattr(L, name).restype = None
     return L
 

@@ -21,8 +21,8 @@ from . import transforms as _t
 
 __all__ = ["MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ", "SHGLQ",
            "MakeGridDHC", "SHExpandDHC", "MakeGridGLQC", "SHExpandGLQC",
-           "MakeGradientDH", "SHRotateRealCoef", "available", "register",
-           "set_nthreads"]
+           "MakeGradientDH", "MakeGravGridDH", "NormalGravity", "SHRotateRealCoef",
+           "available", "register", "set_nthreads"]
 
 
 def available():
@@ -151,6 +151,25 @@ def MakeGradientDH(cilm, lmax=None, sampling=1, lmax_calc=None, extend=False,
                                sampling=sampling, lmax_calc=lmax_calc, extend=extend,
                                radius=radius)
     return _np(th), _np(ph)
+
+
+def MakeGravGridDH(cilm, gm, r0, lmax=None, a=None, f=0.0, sampling=2, lmax_calc=None,
+                   omega=0.0, normal_gravity=1, normal_gravity_gm=None, extend=0):
+    """rad, theta, phi, total, pot = MakeGravGridDH(cilm, gm, r0, [lmax, a, f,
+    sampling, lmax_calc, omega, normal_gravity, normal_gravity_gm, extend])
+    -- the signature of pyshtools.gravmag.MakeGravGridDH
+    (src/pyshtools.pyf:1440-1477, src/MakeGravGridDH.f95:1)."""
+    g = _t.MakeGravGridDH(np.asarray(cilm, dtype=np.float64), gm, r0, lmax=lmax, a=a, f=f,
+                          sampling=sampling, lmax_calc=lmax_calc, omega=omega,
+                          normal_gravity=normal_gravity,
+                          normal_gravity_gm=normal_gravity_gm, extend=extend)
+    return tuple(_np(x) for x in g)
+
+
+def NormalGravity(geocentric_lat, gm, omega, a, b):
+    """value = NormalGravity(geocentric_lat, gm, omega, a, b) -- see
+    src/NormalGravity.f95:1."""
+    return _t.NormalGravity(geocentric_lat, gm, omega, a, b)
 
 
 SHRotateRealCoef = _passthrough("SHRotateRealCoef")

@@ -329,6 +329,54 @@ extern "C" int shtc_gradient_dh(const shtc_plan* P, const double* cilm, long lon
 }
 
 // ---------------------------------------------------------------------------
+// MakeGravGridDH: a real DH plan with norm 1 and csphase 1; workspace =
+// packed (3 nfield) | spectra (3 nfield) | (4 nfield) | ring and row tables
+// ---------------------------------------------------------------------------
+extern "C" size_t shtc_gravity_workspace_bytes(const shtc_plan* P, int nfield) {
+    if (!P || nfield < 1) return 0;
+    return coef_region(P, 3 * nfield) + spec_region(P, 3 * nfield) +
+           spec_region(P, 4 * nfield) + align256(grav_table_bytes(P)) + fft_region(P);
+}
+
+extern "C" int shtc_gravity_dh(const shtc_plan* P, const double* cilm, long long csf,
+                               long long csk, long long csl, long long csm, int cdim,
+                               double gm, double r0, double a, double f, int has_omega,
+                               double omega, int normal_gravity, double normal_gravity_gm,
+                               double* rad, double* theta, double* phi, double* total,
+                               double* pot, long long gsf, long long gsr, long long gsc,
+                               int nfield, void* work, size_t wb, void* stream) {
+    if (!P || !cilm || !rad || !theta || !phi || !total) return SHTC_EHANDLE;
+    if (nfield < 1) return SHTC_EBOUND;
+    if (P->kind != SHTC_GRID_DH || P->cplx || P->norm != 1 || P->csphase != 1)
+        return SHTC_EBOUND;
+    if (normal_gravity != 0 && normal_gravity != 1) return SHTC_EBOUND;
+    if (normal_gravity == 1 && !has_omega) return SHTC_EBOUND;
+    if (cdim < 1) return SHTC_EDIM;
+    if (!work || wb < shtc_gravity_workspace_bytes(P, nfield)) return SHTC_EWORK;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != P->device) return SHTC_EHANDLE;
+    GravParams g;
+    g.gm = gm; g.r0 = r0; g.a = a; g.f = f; g.omega = has_omega ? omega : 0.0;
+    g.ng_gm = normal_gravity_gm; g.has_omega = has_omega ? 1 : 0;
+    g.normal_gravity = normal_gravity;
+    char* w = (char*)work;
+    size_t o = 0;
+    double2* packed = (double2*)(w + o);
+    o += coef_region(P, 3 * nfield);
+    double2* spec = (double2*)(w + o);
+    o += spec_region(P, 3 * nfield);
+    double2* spec2 = (double2*)(w + o);
+    o += spec_region(P, 4 * nfield);
+    double* tab = (double*)(w + o);
+    o += align256(grav_table_bytes(P));
+    double2* fbuf = fft_scratch(P, work, o);
+    return launch_gravity_dh(P, cilm, csf, csk, csl, csm, cdim, g, rad, theta, phi, total,
+                             pot, gsf, gsr, gsc, nfield, packed, spec, spec2, tab,
+                             (cudaStream_t)stream, fbuf);
+}
+
+// ---------------------------------------------------------------------------
 // SHMultiply: both fields synthesised on the GLQ grid of the plan (degree
 // lmax1 + lmax2), the analysis FFT reads the two grids and transforms their
 // pointwise product.  Workspace: packed / partial sums (2 nfield) | spectra
@@ -840,6 +888,59 @@ extern "C" void MakeGradientDH(const double* cilm, const int cdim, const int lma
     if (!rc) rc = map_cuda(cudaMemcpy2DAsync(phi, sizeof(double) * d0, dp.p,
                                              sizeof(double) * d0, sizeof(double) * nlat_out,
                                              nlon_out, cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
+    set_status(exitstatus, rc);
+}
+
+// include/shtools.h:726-746 via src/cWrapper.f95:1484-1514 (src/MakeGravGridDH.f95:1)
+extern "C" void MakeGravGridDH(const double* cilm, const int cdim, const int lmax,
+                               const double gm, const double r0, const double a,
+                               const double f, double* rad, const int nlon, const int nlat,
+                               double* theta, double* phi, double* total, int* n,
+                               const int* sampling, const int* lmax_calc, const double* omega,
+                               const int* normal_gravity, double* pot, const int* extend,
+                               int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    const int nn = 2 * lmax + 2;
+    if (n) *n = nn;
+    const int samp = opt(sampling, 1), ext = opt(extend, 0), ng = opt(normal_gravity, 0);
+    if (samp != 1 && samp != 2) return set_status(exitstatus, SHTC_EBOUND);
+    if (ext != 0 && ext != 1) return set_status(exitstatus, SHTC_EBOUND);
+    if (cdim < 1) return set_status(exitstatus, SHTC_EDIM);
+    const int nlat_out = nn + ext, nlon_out = samp * nn + ext;
+    if (nlat < nlat_out || nlon < nlon_out) return set_status(exitstatus, SHTC_EDIM);
+    if (ng != 0 && ng != 1) return set_status(exitstatus, SHTC_EBOUND);
+    if (ng == 1 && !omega) return set_status(exitstatus, 5);   // MakeGravGridDH.f95:244-252
+    int lc = lmax < cdim - 1 ? lmax : cdim - 1;
+    if (lmax_calc) {
+        if (*lmax_calc > lmax) return set_status(exitstatus, SHTC_EBOUND);
+        if (*lmax_calc < lc) lc = *lmax_calc;
+    }
+    if (lc < 0) return set_status(exitstatus, SHTC_EDIM);
+    cudaStream_t st = cudaStreamPerThread;
+    shtc_plan* P = nullptr;
+    int rc = cached_plan(SHTC_GRID_DH, lmax, lc, 1, 1, samp, ext, nullptr, nullptr, &P, st);
+    if (rc) return set_status(exitstatus, rc);
+    DevBuf dc, dg, dw;
+    const size_t wb = shtc_gravity_workspace_bytes(P, 1);
+    const size_t gb = sizeof(double) * (size_t)nlat * nlon;
+    const int ngrid = pot ? 5 : 4;
+    if ((rc = dc.alloc(sizeof(double) * 2 * (size_t)cdim * cdim)) ||
+        (rc = dg.alloc(gb * ngrid)) || (rc = dw.alloc(wb)))
+        return set_status(exitstatus, rc);
+    double* d[5];
+    for (int k = 0; k < 5; ++k) d[k] = k < ngrid ? (double*)((char*)dg.p + gb * k) : nullptr;
+    rc = map_cuda(cudaMemcpyAsync(dc.p, cilm, sizeof(double) * 2 * (size_t)cdim * cdim,
+                                  cudaMemcpyHostToDevice, st));
+    // grids (nlat, nlon) column-major: row stride 1, column stride nlat
+    if (!rc) rc = shtc_gravity_dh(P, (const double*)dc.p, 0, 1, 2, 2LL * cdim, cdim, gm, r0, a,
+                                  f, omega ? 1 : 0, omega ? *omega : 0.0, ng, gm, d[0], d[1],
+                                  d[2], d[3], d[4], 0, 1, nlat, 1, dw.p, wb, st);
+    double* host[5] = {rad, theta, phi, total, pot};
+    for (int k = 0; k < ngrid && !rc; ++k)
+        rc = map_cuda(cudaMemcpy2DAsync(host[k], sizeof(double) * nlat, d[k],
+                                        sizeof(double) * nlat, sizeof(double) * nlat_out,
+                                        nlon_out, cudaMemcpyDeviceToHost, st));
     if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
     set_status(exitstatus, rc);
 }

@@ -816,6 +816,16 @@ __global__ void k_grad_combine(const double2* __restrict__ spec, double2* __rest
     out[((long long)nfield + u) * per + i] = f;
 }
 
+int launch_pack_grad(const shtc_plan* P, const double* cilm, long long sf, long long sk,
+                     long long sl, long long sm, int cdim, double2* packed, int nfield,
+                     cudaStream_t st) {
+    const int lc = P->lc;
+    dim3 grid((lc + 1 + 127) / 128, lc + 1, nfield);
+    k_pack_grad<<<grid, 128, 0, st>>>(cilm, sf, sk, sl, sm, cdim, packed, lc, nfield,
+                                      P->d_rec);
+    return map_cuda(cudaGetLastError());
+}
+
 int launch_gradient_dh(const shtc_plan* P, const double* cilm, long long sf, long long sk,
                        long long sl, long long sm, int cdim, double* theta, double* phi,
                        long long gf, long long grs, long long gcs, double radius,
@@ -823,13 +833,8 @@ int launch_gradient_dh(const shtc_plan* P, const double* cilm, long long sf, lon
                        cudaStream_t st, double2* gbuf) {
     const int lc = P->lc;
     stage_begin(SHTC_STAGE_PACK, st);
-    {
-        dim3 grid((lc + 1 + 127) / 128, lc + 1, nfield);
-        k_pack_grad<<<grid, 128, 0, st>>>(cilm, sf, sk, sl, sm, cdim, packed, lc, nfield,
-                                          P->d_rec);
-    }
+    int rc = launch_pack_grad(P, cilm, sf, sk, sl, sm, cdim, packed, nfield, st);
     stage_end(SHTC_STAGE_PACK, st);
-    int rc = map_cuda(cudaGetLastError());
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_SYNTH, st);
     rc = launch_legendre_synth(P, packed, spec, 3 * nfield, st);

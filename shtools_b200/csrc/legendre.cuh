@@ -66,16 +66,23 @@ __device__ __forceinline__ void cp_async_wait() {
 // ---------------------------------------------------------------------------
 // synthesis
 // ---------------------------------------------------------------------------
-template <int T, int NF>
+// RAD: the contraction uses q^s Q(s) for a per-ring factor q (the radial
+// factor (r0/r)^l of a potential): qs[] holds q^s and advances by qstep[]
+template <int T, int NF, bool RAD = false>
 __device__ __forceinline__ void synth_step(bool odd, double2 f, const double2* c,
-                                           const double* z, double* q1, double* q2,
-                                           double (*eR)[NF], double (*eI)[NF],
-                                           double (*oR)[NF], double (*oI)[NF]) {
+                                           const double* z, double* qs, const double* qstep,
+                                           double* q1, double* q2, double (*eR)[NF],
+                                           double (*eI)[NF], double (*oR)[NF],
+                                           double (*oI)[NF]) {
 #pragma unroll
     for (int t = 0; t < T; ++t) {
-        const double p = rec_step(z[t], f, q1[t], q2[t]);
+        double p = rec_step(z[t], f, q1[t], q2[t]);
         q2[t] = q1[t];
         q1[t] = p;
+        if constexpr (RAD) {
+            p *= qs[t];
+            qs[t] *= qstep[t];
+        }
 #pragma unroll
         for (int j = 0; j < NF; ++j) {
             if (odd) {
@@ -106,22 +113,45 @@ struct SynthStage {
 //   spec: [field][pair][m][ring] c2r inputs (a_m - i b_m) * (m ? 1/2 : 1),
 //         a_m = sum_l C_lm P_lm, b_m = sum_l S_lm P_lm (MakeGridDH.f95:566-612)
 // Ends with a barrier: the shared stage can be reused by the next item.
-template <int T, int NF>
+// RAD: sums of c_l q^l P_lm for a per-pair factor q, radq[p] = {q, log q}:
+// the recursion is the plain one (z exact); each term is multiplied by q^s,
+// s = l - m, taken at the first degree of every recursion segment from
+// qtab[p * nseg + k] = q^(16k + 1) (accurate powers) and advanced by q
+// within the segment; the epilogue multiplies by q^m = exp(m log q).  A
+// q^s built by repeated multiplication alone would carry s times the
+// rounding of q, and folding q into z and beta would perturb z itself.
+template <int T, int NF, bool RAD = false>
 __device__ __forceinline__ void synth_order(
     SynthStage<NF>& sm, const double2* __restrict__ rec,
     const double* __restrict__ pmm, const double* __restrict__ rtab,
     const double* __restrict__ zp, const double2* __restrict__ coef,
     double2* __restrict__ spec, int lc, int npair, int nfield, int m, int tile,
-    int f0, int nvalid) {
+    int f0, int nvalid, const double2* __restrict__ radq = nullptr,
+    const double* __restrict__ qtab = nullptr, int nseg = 0) {
     constexpr int R = 1 + NF;                       // 16-byte items per degree
     const int p0 = tile * (blockDim.x * T) + threadIdx.x;
-    double z[T];
+    double z[T], qs[T], qstep[T], lq[T];
     int pv[T];
 #pragma unroll
     for (int t = 0; t < T; ++t) {
         pv[t] = p0 + t * blockDim.x;
         z[t] = pv[t] < npair ? zp[pv[t]] : 0.0;
+        qs[t] = 1.0;
+        if constexpr (RAD) {
+            const double2 rq = pv[t] < npair ? radq[pv[t]] : make_double2(1.0, 0.0);
+            qstep[t] = rq.x;
+            lq[t] = rq.y;
+        } else {
+            qstep[t] = 1.0;
+            lq[t] = 0.0;
+        }
     }
+    // q^s at the first step of segment seg (RAD)
+    auto seg_power = [&](int seg) {
+#pragma unroll
+        for (int t = 0; t < T; ++t)
+            qs[t] = pv[t] < npair ? qtab[(long long)pv[t] * nseg + seg] : 1.0;
+    };
     const long long o = packed_off(m, lc);
     const double2* __restrict__ rm = rec + o;
     const double2* __restrict__ cm = coef + o * nfield + f0;
@@ -174,15 +204,23 @@ __device__ __forceinline__ void synth_order(
         if (cn == kSynthChunk) {
 #pragma unroll
             for (int k = 0; k < kSynthChunk; ++k) {
-                synth_step<T, NF>((k & 1) == 0, st[k * R], &st[k * R + 1], z, q1, q2,
-                                  eR, eI, oR, oI);
+                if constexpr (RAD) {
+                    if ((k & (kRecSegment - 1)) == 0)
+                        seg_power((c * kSynthChunk + k) / kRecSegment);
+                }
+                synth_step<T, NF, RAD>((k & 1) == 0, st[k * R], &st[k * R + 1], z, qs,
+                                       qstep, q1, q2, eR, eI, oR, oI);
                 if ((k & (kRecSegment - 1)) == kRecSegment - 1)
                     rec_rescale<T>(st[k * R].y, q1, q2);
             }
         } else {
             for (int k = 0; k < cn; ++k) {
-                synth_step<T, NF>((k & 1) == 0, st[k * R], &st[k * R + 1], z, q1, q2,
-                                  eR, eI, oR, oI);
+                if constexpr (RAD) {
+                    if ((k & (kRecSegment - 1)) == 0)
+                        seg_power((c * kSynthChunk + k) / kRecSegment);
+                }
+                synth_step<T, NF, RAD>((k & 1) == 0, st[k * R], &st[k * R + 1], z, qs,
+                                       qstep, q1, q2, eR, eI, oR, oI);
                 if ((k & (kRecSegment - 1)) == kRecSegment - 1)
                     rec_rescale<T>(st[k * R].y, q1, q2);
             }
@@ -194,7 +232,8 @@ __device__ __forceinline__ void synth_order(
 #pragma unroll
     for (int t = 0; t < T; ++t) {
         if (pv[t] >= npair) continue;
-        const double r = rtab[(long long)m * npair + pv[t]];
+        double r = rtab[(long long)m * npair + pv[t]];
+        if constexpr (RAD) r *= exp((double)m * lq[t]);
 #pragma unroll
         for (int j = 0; j < NF; ++j) {
             if (j >= nvalid) continue;

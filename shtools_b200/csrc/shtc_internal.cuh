@@ -153,6 +153,26 @@ int launch_gradient_dh(const shtc_plan* P, const double* cilm, long long sf, lon
                        long long gf, long long grs, long long gcs, double radius,
                        int nfield, double2* packed, double2* spec, double2* spec2,
                        cudaStream_t st, double2* gbuf = nullptr);
+// MakeGravGridDH (grav.cu): the three sums of a field packed as for the
+// gradient (c, c_(l+1) a_(l+1), l c); workspace = packed (3 nfield) | spec
+// (3 nfield) | spec2 (4 nfield) | tables (grav_table_bytes)
+int launch_pack_grad(const shtc_plan* P, const double* cilm, long long sf, long long sk,
+                     long long sl, long long sm, int cdim, double2* packed, int nfield,
+                     cudaStream_t st);
+struct GravParams {
+    double gm, r0, a, f, omega, ng_gm;
+    int has_omega;        // the reference's OMEGA present (rotation terms)
+    int normal_gravity;   // 1: total minus the normal gravity
+};
+size_t grav_table_bytes(const shtc_plan* P);
+int launch_gravity_dh(const shtc_plan* P, const double* cilm, long long sf, long long sk,
+                      long long sl, long long sm, int cdim, const GravParams& g,
+                      double* rad, double* theta, double* phi, double* total, double* pot,
+                      long long gf, long long grs, long long gcs, int nfield,
+                      double2* packed, double2* spec, double2* spec2, double* tab,
+                      cudaStream_t st, double2* gbuf);
+__host__ __device__ double normal_gravity(double geocentric_lat, double gm, double omega,
+                                          double a, double b);
 int launch_fft_c2c_anal(const shtc_plan* P, const double2* grid, long long gf,
                         long long grs, long long gcs, double2* spec, int nfield,
                         cudaStream_t st, double2* gbuf = nullptr);

@@ -568,6 +568,59 @@ def MakeGradientDH(cilm, lmax=None, sampling=1, lmax_calc=None, extend=False,
     return th.reshape(out), ph.reshape(out)
 
 
+def MakeGravGridDH(cilm, gm, r0, lmax=None, a=None, f=0.0, sampling=2, lmax_calc=None,
+                   omega=0.0, normal_gravity=1, normal_gravity_gm=None, extend=False):
+    """Gravity on a flattened ellipsoid, on the GPU (src/MakeGravGridDH.f95:1,
+    defaults of src/pyshtools.pyf:1440-1477): returns (rad, theta, phi,
+    total, pot) DH grids of the gravity vector of V = GM/r sum_l (r0/r)^l
+    C_lm Y_lm on the ellipsoid of semi-major axis a (default r0) and
+    flattening f (rad positive up; theta and phi zero on the poles), its
+    magnitude (minus the normal gravity when normal_gravity is 1, the
+    gravity disturbance) and the potential.  omega: rotation rate, adding
+    the centrifugal terms (None: the Fortran's absent OMEGA).  cilm:
+    (..., 2, D, D), 4-pi normalised without the Condon-Shortley phase.  Not
+    differentiable."""
+    if sampling not in (1, 2):
+        raise ValueError("sampling must be 1 (n by n) or 2 (n by 2n); got %r"
+                         % (sampling,))
+    if normal_gravity not in (0, 1):
+        raise ValueError("normal_gravity must be 0 or 1; got %r" % (normal_gravity,))
+    if normal_gravity == 1 and omega is None:
+        raise ValueError("omega must be specified when removing the normal gravity")
+    lmax, lc = _resolve_synth(np.shape(cilm), lmax, lmax_calc)
+    a = float(r0) if a is None else float(a)
+    ngm = float(gm) if normal_gravity_gm is None else float(normal_gravity_gm)
+    c = _as_cuda(cilm, "cilm").to(torch.float64)
+    plan = get_plan(GRID_DH, lmax, lc, 1, 1, sampling, int(bool(extend)), device=c.device)
+    cf, lead = _flat(c[..., :2, :, :], 3)
+    F = cf.shape[0]
+    shape = (F, plan.info["nlat_out"], plan.info["nlon_out"])
+    out = torch.empty((5,) + shape, dtype=torch.float64, device=c.device)
+    g = [out[k] for k in range(5)]
+    lib = plan.lib
+    nb = int(lib.shtc_gravity_workspace_bytes(plan.handle, F))
+    ws = torch.empty(max(nb, 8), dtype=torch.uint8, device=c.device)
+    with torch.cuda.device(c.device):
+        rc = lib.shtc_gravity_dh(plan.handle, ctypes_void(cf.data_ptr()), cf.stride(0),
+                                 cf.stride(1), cf.stride(2), cf.stride(3), cf.shape[2],
+                                 float(gm), float(r0), a, float(f), int(omega is not None),
+                                 0.0 if omega is None else float(omega), int(normal_gravity),
+                                 ngm, *[ctypes_void(t.data_ptr()) for t in g],
+                                 g[0].stride(0), g[0].stride(1), g[0].stride(2), F,
+                                 ctypes_void(ws.data_ptr()), nb, _stream_ptr(c.device))
+    _lib.check(rc, "shtc_gravity_dh")
+    shp = tuple(lead) + shape[1:]
+    return tuple(t.reshape(shp) for t in g)
+
+
+def NormalGravity(geocentric_lat, gm, omega, a, b):
+    """Normal gravity of a rotating ellipsoid at a geocentric latitude in
+    degrees (src/NormalGravity.f95:1), through the C ABI's host
+    implementation."""
+    return float(_lib.load().NormalGravity(float(geocentric_lat), float(gm), float(omega),
+                                           float(a), float(b)))
+
+
 def SHMultiply(cilm1, cilm2, lmax1=None, lmax2=None, precomp=None, norm=1, csphase=1):
     """Spherical-harmonic expansion of the product of two fields, on the GPU
     (src/SHMultiply.f95:1): both fields are synthesised on the Gauss-Legendre
