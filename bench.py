@@ -51,6 +51,10 @@ WORKLOADS = {
     # MakeGradientDH, config 3 shape: 8 fields, lmax 719, sampling 2
     "gradient719x8": dict(kind="gradient", lmax=719, nfield=8, sampling=2, beta=2.0,
                           seed=3700),
+    # MakeGravGridDH, config 3 shape: 8 fields, lmax 719, sampling 2, on a
+    # rotating ellipsoid with the normal gravity removed
+    "gravity719x8": dict(kind="gravity", lmax=719, nfield=8, sampling=2, beta=2.0,
+                         seed=3800),
     # SHMultiply: one pair of fields of lmax 1024 and 1023 into lmax 2047 (the
     # GLQ grid of the headline configuration, 2048 x 4095)
     "multiply1024": dict(kind="multiply", lmax=1024, lmax2=1023, nfield=1, sampling=1,
@@ -597,9 +601,15 @@ def run_cuda_grad(args, w, rank, world, local_rank):
     }
 
 
+# MakeGravGridDH workload parameters: Mars-like GM, reference radius,
+# ellipsoid and rotation; total is the gravity disturbance
+GRAV = dict(gm=4.2828372e13, r0=3396000.0, a=3395428.0, f=0.00589, omega=7.088218e-5)
+
+
 def run_cuda_gradient(args, w, rank, world, local_rank):
-    """MakeGradientDH of every field per step (one transform per field, two
-    output grids), through the public torch API."""
+    """MakeGradientDH (one transform per field, theta and phi grids) or
+    MakeGravGridDH (one transform per field, rad, theta, phi, total and pot
+    grids) of every field per step, through the public torch API."""
     import numpy as np
     import torch
     import shtools_b200 as sht
@@ -610,18 +620,26 @@ def run_cuda_gradient(args, w, rank, world, local_rank):
     torch.cuda.set_device(dev)
     lib = _lib.load()
     L, F, s_ = w["lmax"], w["nfield"], w["sampling"]
-    c_host = torch.from_numpy(np.stack([power_law(L, w["seed"] + i, w["beta"])
-                                        for i in range(F)])).pin_memory()
+    grav = w["kind"] == "gravity"
+    cs = np.stack([power_law(L, w["seed"] + i, w["beta"]) for i in range(F)])
+    if grav:
+        cs *= 1e-3
+        cs[:, 0, 0, 0] = 1.0
+        g = GRAV
+        step = lambda x: sht.MakeGravGridDH(x, g["gm"], g["r0"], a=g["a"], f=g["f"],
+                                            sampling=s_, omega=g["omega"], normal_gravity=1)
+    else:
+        step = lambda x: sht.MakeGradientDH(x, sampling=s_)
+    c_host = torch.from_numpy(cs).pin_memory()
     c = c_host.to(dev)
     st = torch.cuda.current_stream(dev)
-    step = lambda x: sht.MakeGradientDH(x, sampling=s_)
     for _ in range(args.warmup):
-        th, ph = step(c)
+        outs0 = step(c)
     torch.cuda.synchronize(dev)
     # size-independent check: the phi component of a zonal field (m = 0) is 0
     zonal = c.clone()
     zonal[:, :, :, 1:] = 0.0
-    zero_phi = float(step(zonal)[1].abs().max().item())
+    zero_phi = float(step(zonal)[2 if grav else 1].abs().max().item())
     peak = fp64_peak(torch, dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -642,9 +660,9 @@ def run_cuda_gradient(args, w, rank, world, local_rank):
     lib.shtc_timing_collect(ms, cnt, 6)
     total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), dev)
     value = 1.0 * F * args.steps * world / (total_ms * 1e-3)
-    # end to end: host coefficients in, both host grids out, pipelined
-    outs = [(torch.empty(tuple(th.shape), dtype=th.dtype).pin_memory(),
-             torch.empty(tuple(ph.shape), dtype=ph.dtype).pin_memory()) for _ in range(2)]
+    # end to end: host coefficients in, every host grid out, pipelined
+    outs = [tuple(torch.empty(tuple(o.shape), dtype=o.dtype).pin_memory() for o in outs0)
+            for _ in range(2)]
     e2e_steps = max(2, min(args.steps, 10))
     pipelined(step, [(c_host,)] * 2, outs, device=dev)
     torch.cuda.synchronize(dev)
@@ -660,34 +678,48 @@ def run_cuda_gradient(args, w, rank, world, local_rank):
     per_launch_ms = ms[1] / max(1, cnt[1])
     fl = legendre_flops(w, 3 * F)        # three Legendre sums per field, one recursion
     achieved = fl / (per_launch_ms * 1e-3) / 1e12
-    return {
+    if grav:
+        kind, what = "dh gravity", ("MakeGravGridDH of every field (rad, theta, phi, "
+                                    "total and pot grids; ellipsoid, rotation, "
+                                    "normal gravity removed)")
+        # pack stage: ring tables, powers, pack; FFT stage: combination, 4 c2r,
+        # centrifugal / normal-gravity pass
+        launches = 3 * int(cnt[0]) + int(cnt[1]) + 6 * int(cnt[2])
+        # the radial factor adds 2 multiplies per (pair, l, m) to the recursion
+        fl_note = "recursion + 3 contractions per (pair, l, m); q^l factor not counted"
+    else:
+        kind, what = "dh gradient", "MakeGradientDH of every field (theta and phi grids)"
+        # the FFT stage holds 3 launches (combination, theta c2r, phi c2r)
+        launches = int(sum(cnt)) + 2 * int(cnt[2])
+        fl_note = "recursion + 3 contractions per (pair, l, m)"
+    res = {
         "metric": METRIC, "value": value, "unit": "transforms/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic seeded power-law coefficients, S(l)=(l+1)^-%g" % w["beta"],
-        "config": {"workload": args.workload, "kind": "dh gradient", "lmax": L,
+        "config": {"workload": args.workload, "kind": kind, "lmax": L,
                    "fields_per_gpu": F, "sampling": s_, "precision": "fp64",
-                   "step": "MakeGradientDH of every field (theta and phi grids)",
+                   "step": what,
                    "l2": "flushed between steps (256 MiB write, outside step events)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "roofline": {"kernel": "legendre_synth", "bound": "fp64", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None,
                      "peak_source": "measured FP64 FMA probe, this run",
-                     "flops_per_launch": fl, "traffic": None},
+                     "flops_per_launch": fl, "flops_note": fl_note, "traffic": None},
         "stages": {names[i]: {"ms_per_launch": (ms[i] / cnt[i]) if cnt[i] else None,
                               "launches": cnt[i]} for i in range(6)},
         "zonal_field_max_abs_phi": zero_phi,
         "e2e": {"value": 1.0 * F * e2e_steps * world / (e2e_ms * 1e-3),
                 "unit": "transforms/s", "steps": e2e_steps,
                 "h2d_bytes_per_step": c_host.numel() * 8,
-                "d2h_bytes_per_step": (outs[0][0].numel() + outs[0][1].numel()) * 8,
+                "d2h_bytes_per_step": sum(o.numel() for o in outs[0]) * 8,
                 "path": "public torch API on pinned host buffers, pipelined on 3 streams"},
-        # the FFT stage holds 3 launches (combination, theta c2r, phi c2r)
-        "gpu_launches": int(sum(cnt)) + 2 * int(cnt[2]),
+        "gpu_launches": launches,
         "clocks": clk.summary(),
     }
+    return res
 
 
 def run_cuda_multiply(args, w, rank, world, local_rank):
@@ -989,14 +1021,14 @@ def main():
         res = run_cuda_batch(args, w, rank, world, local_rank)
     elif w["kind"] == "dh_grad":
         res = run_cuda_grad(args, w, rank, world, local_rank)
-    elif w["kind"] == "gradient":
+    elif w["kind"] in ("gradient", "gravity"):
         res = run_cuda_gradient(args, w, rank, world, local_rank)
     elif w["kind"] == "multiply":
         res = run_cuda_multiply(args, w, rank, world, local_rank)
     else:
         res = run_cuda(args, w, rank, world, local_rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and \
-            w["kind"] not in ("dhc", "gradient", "multiply"):
+            w["kind"] not in ("dhc", "gradient", "gravity", "multiply"):
         one_step, sample, threads = cpu_sample(w, args.cpu_seconds / 2)
         v, dt = one_step()
         res["cpu_baseline"] = {"value": v, "unit": "transforms/s",

@@ -158,11 +158,17 @@ def MakeGravGridDH(cilm, gm, r0, lmax=None, a=None, f=0.0, sampling=2, lmax_calc
     """rad, theta, phi, total, pot = MakeGravGridDH(cilm, gm, r0, [lmax, a, f,
     sampling, lmax_calc, omega, normal_gravity, normal_gravity_gm, extend])
     -- the signature of pyshtools.gravmag.MakeGravGridDH
-    (src/pyshtools.pyf:1440-1477, src/MakeGravGridDH.f95:1)."""
-    g = _t.MakeGravGridDH(np.asarray(cilm, dtype=np.float64), gm, r0, lmax=lmax, a=a, f=f,
-                          sampling=sampling, lmax_calc=lmax_calc, omega=omega,
-                          normal_gravity=normal_gravity,
-                          normal_gravity_gm=normal_gravity_gm, extend=extend)
+    (src/pyshtools.pyf:1440-1477, src/MakeGravGridDH.f95:1).  As through f2py,
+    None for an optional argument takes its default (omega 0.0, f 0.0,
+    sampling 2, normal_gravity 1, extend 0), as SHGravCoeffs.expand() relies
+    on (pyshtools/shclasses/shgravcoeffs.py:2574)."""
+    g = _t.MakeGravGridDH(np.asarray(cilm, dtype=np.float64), gm, r0, lmax=lmax, a=a,
+                          f=0.0 if f is None else f,
+                          sampling=2 if sampling is None else sampling,
+                          lmax_calc=lmax_calc, omega=0.0 if omega is None else omega,
+                          normal_gravity=1 if normal_gravity is None else normal_gravity,
+                          normal_gravity_gm=normal_gravity_gm,
+                          extend=0 if extend is None else extend)
     return tuple(_np(x) for x in g)
 
 

@@ -89,6 +89,11 @@ def test_grav_default_arguments(cuda, oracle):
     refb = oracle.makegravgrid_dh(c, MARS["gm"], MARS["r0"], f=MARS["f"], omega=MARS["omega"],
                                   normal_gravity=1, normal_gravity_gm=MARS["gm"] * 1.01)
     check(gb, refb)
+    # f2py semantics of the backend: None takes the default (omega 0.0)
+    gn = backend.MakeGravGridDH(c, MARS["gm"], MARS["r0"], omega=None, normal_gravity=0,
+                                f=None, sampling=None)
+    refn = oracle.makegravgrid_dh(c, MARS["gm"], MARS["r0"], sampling=2, omega=0.0)
+    check(gn, refn)
 
 
 def test_normal_gravity_matches_oracle(cuda, oracle):
