@@ -9,6 +9,9 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <type_traits>
 
 #include "shtc_internal.cuh"
 
@@ -206,7 +209,9 @@ __device__ __forceinline__ void prefetch_l2_range(const void* p, size_t bytes) {
 }
 
 // Runs the passes; the data starts in a, the result pointer is returned.
-template <int SIGN>
+// MAXR: the largest radix compiled in (8: plans whose factors are all <= 8,
+// which need far fewer registers than the radix-11/13 butterflies).
+template <int SIGN, int MAXR = 13>
 __device__ __forceinline__ double2* fft_run(double2* a, double2* b, int M, const int* fac,
                             int nfac, const double2* __restrict__ tw,
                             const int* tw_off) {
@@ -222,8 +227,12 @@ __device__ __forceinline__ double2* fft_run(double2* a, double2* b, int M, const
             case 8: fft_pass<8, SIGN>(a, b, M, ns, t); break;
             case 5: fft_pass<5, SIGN>(a, b, M, ns, t); break;
             case 7: fft_pass<7, SIGN>(a, b, M, ns, t); break;
-            case 11: fft_pass<11, SIGN>(a, b, M, ns, t); break;
-            case 13: fft_pass<13, SIGN>(a, b, M, ns, t); break;
+            case 11:
+                if constexpr (MAXR >= 11) fft_pass<11, SIGN>(a, b, M, ns, t);
+                break;
+            case 13:
+                if constexpr (MAXR >= 13) fft_pass<13, SIGN>(a, b, M, ns, t);
+                break;
             default: break;
         }
         ns *= r;
@@ -248,11 +257,11 @@ struct FftArgs {
 // Complex DFT of length F.m of buf with sign SIGN; buf and tmp each hold
 // F.mb (Bluestein) or F.m elements; tw: the plan's twiddles (F.tw, or a
 // copy in shared memory).  Returns the pointer holding the result.
-template <int SIGN>
+template <int SIGN, int MAXR = 13>
 __device__ __forceinline__ double2* fft_exec(const FftArgs& F, const double2* tw, double2* buf,
                              double2* tmp) {
     __syncthreads();
-    if (!F.bluestein) return fft_run<SIGN>(buf, tmp, F.m, F.fac, F.nfac, tw, F.tw_off);
+    if (!F.bluestein) return fft_run<SIGN, MAXR>(buf, tmp, F.m, F.fac, F.nfac, tw, F.tw_off);
     // Bluestein: X_k = c_k sum_j (x_j c_j) conj(c_{k-j}), c_t = exp(-+ i pi t^2/m)
     const int m = F.m, mb = F.mb;
     for (int t = threadIdx.x; t < mb; t += blockDim.x) {
@@ -264,7 +273,7 @@ __device__ __forceinline__ double2* fft_exec(const FftArgs& F, const double2* tw
             buf[t] = make_double2(0.0, 0.0);
         }
     }
-    double2* r = fft_run<-1>(buf, tmp, mb, F.fac, F.nfac, tw, F.tw_off);
+    double2* r = fft_run<-1, MAXR>(buf, tmp, mb, F.fac, F.nfac, tw, F.tw_off);
     double2* o = (r == buf) ? tmp : buf;
     for (int t = threadIdx.x; t < mb; t += blockDim.x) {
         double2 kf;
@@ -276,7 +285,7 @@ __device__ __forceinline__ double2* fft_exec(const FftArgs& F, const double2* tw
         }
         r[t] = cmul(r[t], kf);
     }
-    double2* r2 = fft_run<+1>(r, o, mb, F.fac, F.nfac, tw, F.tw_off);
+    double2* r2 = fft_run<+1, MAXR>(r, o, mb, F.fac, F.nfac, tw, F.tw_off);
     const double inv = 1.0 / (double)mb;
     for (int t = threadIdx.x; t < m; t += blockDim.x) {
         double2 c = F.chirp[t];
@@ -293,7 +302,7 @@ __device__ __forceinline__ double2* fft_exec(const FftArgs& F, const double2* tw
 // (even n): CTA = (pair*2 + ring, field), the ring is computed by a complex
 // length-n/2 inverse DFT and the even/odd split.  Output rows are scaled by
 // the ring weight when wN/wS are given (analysis adjoint).
-template <typename GT>
+template <typename GT, int MAXR = 13>
 __device__ __forceinline__ void fft_c2r_body(
     const FftArgs& F, const double2* tw, double2* smem_fft, int job, int f,
     const double2* __restrict__ spec, GT* __restrict__ grid, long long gf,
@@ -323,7 +332,7 @@ __device__ __forceinline__ void fft_c2r_body(
             a[k] = make_double2(xn.x - xs.y, xn.y + xs.x);
             if (k > 0) a[n - k] = make_double2(xn.x + xs.y, -xn.y + xs.x);
         }
-        const double2* r = fft_exec<+1>(F, tw, a, b);
+        const double2* r = fft_exec<+1, MAXR>(F, tw, a, b);
         const double sN = wN ? wN[p] * wscale : 1.0;
         const double sS = wS ? wS[p] * wscale : 1.0;
         GT* gN = rN >= 0 ? grid + f * gf + rN * grs : nullptr;
@@ -360,14 +369,28 @@ __device__ __forceinline__ void fft_c2r_body(
             const double2 wb = cmul(w, B);
             a[k] = make_double2(A.x - wb.y, A.y + wb.x);
         }
-        const double2* r = fft_exec<+1>(F, tw, a, b);
+        const double2* r = fft_exec<+1, MAXR>(F, tw, a, b);
         const double sc = (h ? (wS ? wS[p] * wscale : 1.0) : (wN ? wN[p] * wscale : 1.0));
         GT* g = grid + f * gf + row * grs;
+        if (gcs == 1 && ((uintptr_t)g & (2 * sizeof(GT) - 1)) == 0) {
+            // contiguous, aligned row: one vector store per sample pair
+            using GT2 = typename std::conditional<sizeof(GT) == 8, double2, float2>::type;
+            GT2* g2 = reinterpret_cast<GT2*>(g);
 #pragma unroll 4
-        for (int j = threadIdx.x; j < M; j += blockDim.x) {
-            const double2 v = r[j];
-            g[(2LL * j) * gcs] = (GT)(v.x * sc);
-            g[(2LL * j + 1) * gcs] = (GT)(v.y * sc);
+            for (int j = threadIdx.x; j < M; j += blockDim.x) {
+                const double2 v = r[j];
+                GT2 o;
+                o.x = (GT)(v.x * sc);
+                o.y = (GT)(v.y * sc);
+                g2[j] = o;
+            }
+        } else {
+#pragma unroll 4
+            for (int j = threadIdx.x; j < M; j += blockDim.x) {
+                const double2 v = r[j];
+                g[(2LL * j) * gcs] = (GT)(v.x * sc);
+                g[(2LL * j + 1) * gcs] = (GT)(v.y * sc);
+            }
         }
         if (extend_col && threadIdx.x == 0) g[(long long)n * gcs] = (GT)(r[0].x * sc);
     }
@@ -376,9 +399,9 @@ __device__ __forceinline__ void fft_c2r_body(
 // r2c: grid rows -> spec (m = 0..lc), each multiplied by the ring weight
 // (times wscale) as (Re, -Im), the reference's fcoef (SHExpandGLQ.f95:535-547).
 // fold_extend adds column n into column 0 (adjoint of the extend copy).
-template <typename GT>
 // grid2 (nullable): the transform of the pointwise product grid * grid2
 // (SHMultiply); the product is formed as each sample is loaded.
+template <typename GT, int MAXR = 13>
 __device__ __forceinline__ void fft_r2c_body(
     const FftArgs& F, const double2* tw, double2* smem_fft, int job, int f,
     const GT* __restrict__ grid, long long gf, long long grs, long long gcs,
@@ -409,7 +432,7 @@ __device__ __forceinline__ void fft_r2c_body(
             }
             a[j] = make_double2(xn, xs);
         }
-        const double2* r = fft_exec<-1>(F, tw, a, b);
+        const double2* r = fft_exec<-1, MAXR>(F, tw, a, b);
         const double sN = wN ? wN[p] * wscale : wscale;
         const double sS = wS ? wS[p] * wscale : wscale;
         double2* X = spec + ((long long)f * npair + p) * (lc + 1) * 2;
@@ -434,10 +457,19 @@ __device__ __forceinline__ void fft_r2c_body(
         }
         const int M = F.m;
         const GT* g = grid + f * gf + row * grs;
+        using GT2 = typename std::conditional<sizeof(GT) == 8, double2, float2>::type;
+        const bool vec = gcs == 1 && ((uintptr_t)g & (2 * sizeof(GT) - 1)) == 0;
 #pragma unroll 4
         for (int j = threadIdx.x; j < M; j += blockDim.x) {
-            double x0 = (double)g[(2LL * j) * gcs];
-            double x1 = (double)g[(2LL * j + 1) * gcs];
+            double x0, x1;
+            if (vec) {
+                const GT2 v = reinterpret_cast<const GT2*>(g)[j];
+                x0 = (double)v.x;
+                x1 = (double)v.y;
+            } else {
+                x0 = (double)g[(2LL * j) * gcs];
+                x1 = (double)g[(2LL * j + 1) * gcs];
+            }
             if (fold_extend && j == 0) x0 += (double)g[(long long)n * gcs];
             if (grid2) {
                 const GT* g2 = grid2 + f * gf + row * grs;
@@ -446,7 +478,7 @@ __device__ __forceinline__ void fft_r2c_body(
             }
             a[j] = make_double2(x0, x1);
         }
-        const double2* r = fft_exec<-1>(F, tw, a, b);
+        const double2* r = fft_exec<-1, MAXR>(F, tw, a, b);
         const double sc = h ? (wS ? wS[p] * wscale : wscale) : (wN ? wN[p] * wscale : wscale);
 #pragma unroll 4
         for (int k = threadIdx.x; k <= lc; k += blockDim.x) {
@@ -472,6 +504,7 @@ __device__ __forceinline__ void fft_r2c_body(
 // the real c2r convention; undone exactly here.  Bin m takes the +m sums, bin
 // n-m the -m sums times (-1)^m (MakeGridDHC.f95:612-616); the ring is the
 // unnormalised backward DFT of length n.
+template <int MAXR = 13>
 __device__ __forceinline__ void fft_c2c_synth_body(
     const FftArgs& F, const double2* tw, double2* smem_fft, int job, int u,
     const double2* __restrict__ spec, double2* __restrict__ grid, long long gf,
@@ -501,7 +534,7 @@ __device__ __forceinline__ void fft_c2c_synth_body(
             a[n - m] = make_double2(sg * w.x, -sg * w.y);
         }
     }
-    const double2* r = fft_exec<+1>(F, tw, a, b);
+    const double2* r = fft_exec<+1, MAXR>(F, tw, a, b);
     double2* g = grid + u * gf + row * grs;
 #pragma unroll 4
     for (int j = threadIdx.x; j < n; j += blockDim.x) g[j * gcs] = r[j];
@@ -511,6 +544,7 @@ __device__ __forceinline__ void fft_c2c_synth_body(
 // Analysis: the forward DFT of the ring times its weight w/n gives
 // fcoef (SHExpandDHC.f95:478); spec of field 2u takes fcoef(m), field 2u+1
 // fcoef(n-m) * (-1)^m (SHExpandDHC.f95:596-600), both as (Re, Im).
+template <int MAXR = 13>
 __device__ __forceinline__ void fft_c2c_anal_body(
     const FftArgs& F, const double2* tw, double2* smem_fft, int job, int u,
     const double2* __restrict__ grid, long long gf, long long grs, long long gcs,
@@ -537,7 +571,7 @@ __device__ __forceinline__ void fft_c2c_anal_body(
     const double2* g = grid + u * gf + row * grs;
 #pragma unroll 4
     for (int j = threadIdx.x; j < n; j += blockDim.x) a[j] = g[j * gcs];
-    const double2* r = fft_exec<-1>(F, tw, a, b);
+    const double2* r = fft_exec<-1, MAXR>(F, tw, a, b);
     const double sc = (h ? wS[p] : wN[p]) * wscale;
     for (int m = threadIdx.x; m <= lc; m += blockDim.x) {
         const double2 zp = r[m];

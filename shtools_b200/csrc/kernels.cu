@@ -245,8 +245,10 @@ __device__ __forceinline__ double2* fft_buffers(const FftArgs& F, double2* smem_
     return gbuf + (size_t)blockIdx.x * 2 * len;
 }
 
-template <typename GT>
-__global__ void __launch_bounds__(512)
+// MAXR = 8: plans whose radices are all <= 8, built for <= 64 registers
+// (four 256-thread CTAs per SM); MAXR = 13 carries the radix-11/13 passes
+template <typename GT, int MAXR>
+__global__ void __launch_bounds__(512, MAXR <= 8 ? 2 : 1)
 k_fft_c2r(FftArgs F, int tw_smem, int jobs, int nitems, const double2* __restrict__ spec,
           GT* __restrict__ grid, long long gf, long long grs, long long gcs,
           const int* __restrict__ rowN, const int* __restrict__ rowS,
@@ -258,14 +260,14 @@ k_fft_c2r(FftArgs F, int tw_smem, int jobs, int nitems, const double2* __restric
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int nx = it + gridDim.x;
         if (nx < nitems) fft_c2r_prefetch(F.mode, nx % jobs, nx / jobs, spec, lc, npair);
-        fft_c2r_body<GT>(F, tw, bufs, it % jobs, it / jobs, spec, grid, gf, grs, gcs,
+        fft_c2r_body<GT, MAXR>(F, tw, bufs, it % jobs, it / jobs, spec, grid, gf, grs, gcs,
                          rowN, rowS, wN, wS, wscale, lc, npair, extend_col);
         __syncthreads();
     }
 }
 
-template <typename GT>
-__global__ void __launch_bounds__(512)
+template <typename GT, int MAXR>
+__global__ void __launch_bounds__(512, MAXR <= 8 ? 2 : 1)
 k_fft_r2c(FftArgs F, int tw_smem, int jobs, int nitems, const GT* __restrict__ grid,
           long long gf, long long grs, long long gcs, double2* __restrict__ spec,
           const int* __restrict__ rowN, const int* __restrict__ rowS,
@@ -279,7 +281,7 @@ k_fft_r2c(FftArgs F, int tw_smem, int jobs, int nitems, const GT* __restrict__ g
         if (nx < nitems)
             fft_r2c_prefetch<GT>(F.mode, F.n, nx % jobs, nx / jobs, grid, gf, grs, gcs, rowN,
                                  rowS, fold_extend);
-        fft_r2c_body<GT>(F, tw, bufs, it % jobs, it / jobs, grid, gf, grs, gcs, spec,
+        fft_r2c_body<GT, MAXR>(F, tw, bufs, it % jobs, it / jobs, grid, gf, grs, gcs, spec,
                          rowN, rowS, wN, wS, wscale, lc, npair, fold_extend, grid2);
         __syncthreads();
     }
@@ -463,9 +465,26 @@ int launch_unpack_coef(const shtc_plan* P, const double2* partial, int ntiles,
     return map_cuda(cudaGetLastError());
 }
 
+// the FFT kernels live on shared memory: ask for the largest carveout so
+// that the resident CTAs are limited by registers, not by the L1 split
 static int fft_smem_setup(const void* fn, const FftPlan& f) {
-    return map_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)f.smem));
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)f.smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    return map_cuda(e);
+}
+
+// the register-capped build pays off when every radix of the plan
+// (Bluestein: of its convolution length) is <= 8 and shared memory leaves
+// room for more than one CTA per SM (at lmax 2799, 179 KB per CTA, the cap
+// only costs spills: 2-3% slower on B200)
+static bool fft_lean(const FftPlan& f) {
+    if (f.smem > 100 * 1024) return false;
+    for (int i = 0; i < f.nfac; ++i)
+        if (f.fac[i] > 8) return false;
+    return true;
 }
 
 // persistent grid: as many CTAs as fit on the device at once, at most one
@@ -491,27 +510,27 @@ size_t fft_scratch_bytes(const shtc_plan* P) {
     return (size_t)f.gmem_ctas * 2 * len * sizeof(double2);
 }
 
-template <typename GT>
+template <typename GT, int MAXR>
 static int launch_c2r_t(const shtc_plan* P, const double2* spec, GT* grid, long long gf,
                         long long grs, long long gcs, int nfield, int weighted,
                         cudaStream_t st, double2* gbuf) {
     const FftPlan& f = P->fft;
     if (f.gmem && !gbuf) return SHTC_EWORK;
-    int rc = fft_smem_setup((const void*)k_fft_c2r<GT>, f);
+    int rc = fft_smem_setup((const void*)k_fft_c2r<GT, MAXR>, f);
     if (rc) return rc;
     const int jobs = f.mode == 0 ? P->npair : 2 * P->npair;
     const int nitems = jobs * nfield;
     int blocks = 0;
-    if ((rc = fft_grid(k_fft_c2r<GT>, f, nitems, &blocks))) return rc;
+    if ((rc = fft_grid(k_fft_c2r<GT, MAXR>, f, nitems, &blocks))) return rc;
     if (blocks == 0) return SHTC_OK;
     // synthesis uses the synthesis ring map (with the extend row and column);
     // the analysis adjoint uses the analysis ring map and ring weights
     if (weighted) {
-        k_fft_c2r<GT><<<blocks, f.threads, f.smem, st>>>(
+        k_fft_c2r<GT, MAXR><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, spec, grid, gf, grs, gcs, P->d_arowN,
             P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, 0, gbuf);
     } else {
-        k_fft_c2r<GT><<<blocks, f.threads, f.smem, st>>>(
+        k_fft_c2r<GT, MAXR><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, spec, grid, gf, grs, gcs, P->d_rowN,
             P->d_rowS, nullptr, nullptr, 1.0, P->lc, P->npair, P->extend, gbuf);
     }
@@ -521,36 +540,42 @@ static int launch_c2r_t(const shtc_plan* P, const double2* spec, GT* grid, long 
 int launch_fft_c2r(const shtc_plan* P, const double2* spec, void* grid, int dtype,
                    long long gf, long long grs, long long gcs, int nfield,
                    int weighted, cudaStream_t st, double2* gbuf) {
+    if (fft_lean(P->fft))
+        return dtype == SHTC_F32
+                   ? launch_c2r_t<float, 8>(P, spec, (float*)grid, gf, grs, gcs, nfield,
+                                            weighted, st, gbuf)
+                   : launch_c2r_t<double, 8>(P, spec, (double*)grid, gf, grs, gcs, nfield,
+                                             weighted, st, gbuf);
     return dtype == SHTC_F32
-               ? launch_c2r_t<float>(P, spec, (float*)grid, gf, grs, gcs, nfield, weighted, st,
-                                     gbuf)
-               : launch_c2r_t<double>(P, spec, (double*)grid, gf, grs, gcs, nfield, weighted,
-                                      st, gbuf);
+               ? launch_c2r_t<float, 13>(P, spec, (float*)grid, gf, grs, gcs, nfield, weighted,
+                                         st, gbuf)
+               : launch_c2r_t<double, 13>(P, spec, (double*)grid, gf, grs, gcs, nfield,
+                                          weighted, st, gbuf);
 }
 
-template <typename GT>
+template <typename GT, int MAXR>
 static int launch_r2c_t(const shtc_plan* P, const GT* grid, long long gf, long long grs,
                         long long gcs, double2* spec, int nfield, int weighted,
                         int fold_extend, cudaStream_t st, const GT* grid2, double2* gbuf) {
     const FftPlan& f = P->fft;
     if (f.gmem && !gbuf) return SHTC_EWORK;
-    int rc = fft_smem_setup((const void*)k_fft_r2c<GT>, f);
+    int rc = fft_smem_setup((const void*)k_fft_r2c<GT, MAXR>, f);
     if (rc) return rc;
     const int jobs = f.mode == 0 ? P->npair : 2 * P->npair;
     const int nitems = jobs * nfield;
     int blocks = 0;
-    if ((rc = fft_grid(k_fft_r2c<GT>, f, nitems, &blocks))) return rc;
+    if ((rc = fft_grid(k_fft_r2c<GT, MAXR>, f, nitems, &blocks))) return rc;
     if (blocks == 0) return SHTC_OK;
     if (weighted) {
         // analysis: fcoef = (w * Re) / nlong, the reference's order of operations
         // is reproduced up to one rounding by folding 1/nlong into the weight
-        k_fft_r2c<GT><<<blocks, f.threads, f.smem, st>>>(
+        k_fft_r2c<GT, MAXR><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_arowN,
             P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, 0,
             grid2, gbuf);
     } else {
         // synthesis adjoint: plain (Re, -Im) of the rows of the cotangent
-        k_fft_r2c<GT><<<blocks, f.threads, f.smem, st>>>(
+        k_fft_r2c<GT, MAXR><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_rowN,
             P->d_rowS, nullptr, nullptr, 1.0, P->lc, P->npair, fold_extend, grid2, gbuf);
     }
@@ -561,17 +586,27 @@ static int launch_r2c_t(const shtc_plan* P, const GT* grid, long long gf, long l
 int launch_fft_r2c_product(const shtc_plan* P, const double* grid, const double* grid2,
                            long long gf, long long grs, long long gcs, double2* spec,
                            int nfield, cudaStream_t st, double2* gbuf) {
-    return launch_r2c_t<double>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st, grid2, gbuf);
+    return fft_lean(P->fft)
+               ? launch_r2c_t<double, 8>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st, grid2,
+                                         gbuf)
+               : launch_r2c_t<double, 13>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st, grid2,
+                                          gbuf);
 }
 
 int launch_fft_r2c(const shtc_plan* P, const void* grid, int dtype, long long gf,
                    long long grs, long long gcs, double2* spec, int nfield,
                    int weighted, int fold_extend, cudaStream_t st, double2* gbuf) {
+    if (fft_lean(P->fft))
+        return dtype == SHTC_F32
+                   ? launch_r2c_t<float, 8>(P, (const float*)grid, gf, grs, gcs, spec, nfield,
+                                            weighted, fold_extend, st, nullptr, gbuf)
+                   : launch_r2c_t<double, 8>(P, (const double*)grid, gf, grs, gcs, spec,
+                                             nfield, weighted, fold_extend, st, nullptr, gbuf);
     return dtype == SHTC_F32
-               ? launch_r2c_t<float>(P, (const float*)grid, gf, grs, gcs, spec, nfield,
-                                     weighted, fold_extend, st, nullptr, gbuf)
-               : launch_r2c_t<double>(P, (const double*)grid, gf, grs, gcs, spec, nfield,
-                                      weighted, fold_extend, st, nullptr, gbuf);
+               ? launch_r2c_t<float, 13>(P, (const float*)grid, gf, grs, gcs, spec, nfield,
+                                         weighted, fold_extend, st, nullptr, gbuf)
+               : launch_r2c_t<double, 13>(P, (const double*)grid, gf, grs, gcs, spec, nfield,
+                                          weighted, fold_extend, st, nullptr, gbuf);
 }
 
 // ---------------------------------------------------------------------------
@@ -658,7 +693,8 @@ k_unpack_coef_c(const double2* __restrict__ partial, int ntiles, double2* __rest
 }
 
 // persistent complex-grid FFT kernels over (job, field) items, as k_fft_c2r
-__global__ void __launch_bounds__(512)
+template <int MAXR>
+__global__ void __launch_bounds__(512, MAXR <= 8 ? 2 : 1)
 k_fft_c2c_synth(FftArgs F, int tw_smem, int jobs, int nitems,
                 const double2* __restrict__ spec, double2* __restrict__ grid, long long gf,
                 long long grs, long long gcs, const int* __restrict__ rowN,
@@ -667,13 +703,14 @@ k_fft_c2c_synth(FftArgs F, int tw_smem, int jobs, int nitems,
     const double2* tw = fft_stage_twiddles(F, smem_fft, tw_smem);
     double2* bufs = fft_buffers(F, smem_fft, gbuf);
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-        fft_c2c_synth_body(F, tw, bufs, it % jobs, it / jobs, spec, grid, gf, grs, gcs,
+        fft_c2c_synth_body<MAXR>(F, tw, bufs, it % jobs, it / jobs, spec, grid, gf, grs, gcs,
                            rowN, rowS, lc, npair, extend_col);
         __syncthreads();
     }
 }
 
-__global__ void __launch_bounds__(512)
+template <int MAXR>
+__global__ void __launch_bounds__(512, MAXR <= 8 ? 2 : 1)
 k_fft_c2c_anal(FftArgs F, int tw_smem, int jobs, int nitems,
                const double2* __restrict__ grid, long long gf, long long grs, long long gcs,
                double2* __restrict__ spec, const int* __restrict__ rowN,
@@ -683,7 +720,7 @@ k_fft_c2c_anal(FftArgs F, int tw_smem, int jobs, int nitems,
     const double2* tw = fft_stage_twiddles(F, smem_fft, tw_smem);
     double2* bufs = fft_buffers(F, smem_fft, gbuf);
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-        fft_c2c_anal_body(F, tw, bufs, it % jobs, it / jobs, grid, gf, grs, gcs, spec,
+        fft_c2c_anal_body<MAXR>(F, tw, bufs, it % jobs, it / jobs, grid, gf, grs, gcs, spec,
                           rowN, rowS, wN, wS, wscale, lc, npair);
         __syncthreads();
     }
@@ -709,40 +746,58 @@ int launch_unpack_coef_c(const shtc_plan* P, const double2* partial, int ntiles,
     return map_cuda(cudaGetLastError());
 }
 
-int launch_fft_c2c_synth(const shtc_plan* P, const double2* spec, double2* grid,
-                         long long gf, long long grs, long long gcs, int nfield,
-                         cudaStream_t st, double2* gbuf) {
+template <int MAXR>
+static int launch_c2c_synth_t(const shtc_plan* P, const double2* spec, double2* grid,
+                              long long gf, long long grs, long long gcs, int nfield,
+                              cudaStream_t st, double2* gbuf) {
     const FftPlan& f = P->fft;
     if (f.gmem && !gbuf) return SHTC_EWORK;
-    int rc = fft_smem_setup((const void*)k_fft_c2c_synth, f);
+    int rc = fft_smem_setup((const void*)k_fft_c2c_synth<MAXR>, f);
     if (rc) return rc;
     const int jobs = 2 * P->npair;
     const int nitems = jobs * nfield;
     int blocks = 0;
-    if ((rc = fft_grid(k_fft_c2c_synth, f, nitems, &blocks))) return rc;
+    if ((rc = fft_grid(k_fft_c2c_synth<MAXR>, f, nitems, &blocks))) return rc;
     if (blocks == 0) return SHTC_OK;
-    k_fft_c2c_synth<<<blocks, f.threads, f.smem, st>>>(
+    k_fft_c2c_synth<MAXR><<<blocks, f.threads, f.smem, st>>>(
         fft_args(f), f.tw_smem, jobs, nitems, spec, grid, gf, grs, gcs, P->d_rowN,
         P->d_rowS, P->lc, P->npair, P->extend, gbuf);
     return map_cuda(cudaGetLastError());
 }
 
-int launch_fft_c2c_anal(const shtc_plan* P, const double2* grid, long long gf,
-                        long long grs, long long gcs, double2* spec, int nfield,
-                        cudaStream_t st, double2* gbuf) {
+template <int MAXR>
+static int launch_c2c_anal_t(const shtc_plan* P, const double2* grid, long long gf,
+                             long long grs, long long gcs, double2* spec, int nfield,
+                             cudaStream_t st, double2* gbuf) {
     const FftPlan& f = P->fft;
     if (f.gmem && !gbuf) return SHTC_EWORK;
-    int rc = fft_smem_setup((const void*)k_fft_c2c_anal, f);
+    int rc = fft_smem_setup((const void*)k_fft_c2c_anal<MAXR>, f);
     if (rc) return rc;
     const int jobs = 2 * P->npair;
     const int nitems = jobs * nfield;
     int blocks = 0;
-    if ((rc = fft_grid(k_fft_c2c_anal, f, nitems, &blocks))) return rc;
+    if ((rc = fft_grid(k_fft_c2c_anal<MAXR>, f, nitems, &blocks))) return rc;
     if (blocks == 0) return SHTC_OK;
-    k_fft_c2c_anal<<<blocks, f.threads, f.smem, st>>>(
+    k_fft_c2c_anal<MAXR><<<blocks, f.threads, f.smem, st>>>(
         fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_arowN,
         P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, gbuf);
     return map_cuda(cudaGetLastError());
+}
+
+int launch_fft_c2c_synth(const shtc_plan* P, const double2* spec, double2* grid,
+                         long long gf, long long grs, long long gcs, int nfield,
+                         cudaStream_t st, double2* gbuf) {
+    return fft_lean(P->fft)
+               ? launch_c2c_synth_t<8>(P, spec, grid, gf, grs, gcs, nfield, st, gbuf)
+               : launch_c2c_synth_t<13>(P, spec, grid, gf, grs, gcs, nfield, st, gbuf);
+}
+
+int launch_fft_c2c_anal(const shtc_plan* P, const double2* grid, long long gf,
+                        long long grs, long long gcs, double2* spec, int nfield,
+                        cudaStream_t st, double2* gbuf) {
+    return fft_lean(P->fft)
+               ? launch_c2c_anal_t<8>(P, grid, gf, grs, gcs, spec, nfield, st, gbuf)
+               : launch_c2c_anal_t<13>(P, grid, gf, grs, gcs, spec, nfield, st, gbuf);
 }
 
 // ---------------------------------------------------------------------------
