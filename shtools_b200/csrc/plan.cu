@@ -215,19 +215,27 @@ __global__ void k_ring_weights(const double* __restrict__ q,
 // ---------------------------------------------------------------------------
 // FFT plan
 // ---------------------------------------------------------------------------
+// Pass order: the odd radices first, then 8, 4, 2.  A Stockham pass writes
+// y[(j - k) R + k + q ns], k = j mod ns: with ns = 1 consecutive threads
+// write R elements apart, an R-way shared-memory bank conflict for R = 8
+// (16-byte elements, 8 threads per 128-byte wavefront) but none for odd R;
+// with ns >= 3 the writes of consecutive threads are contiguous runs.
 static int factor_len(int n, int* fac) {
     int k = 0;
-    while (n % 8 == 0) { fac[k++] = 8; n /= 8; }
-    while (n % 4 == 0) { fac[k++] = 4; n /= 4; }
-    while (n % 2 == 0) { fac[k++] = 2; n /= 2; }
-    for (int p = 3; p <= n; p += 2) {
-        while (n % p == 0) {
+    int m = n;
+    int p2 = 0;
+    while (m % 2 == 0) { m /= 2; ++p2; }
+    for (int p = 3; p <= m; p += 2) {
+        while (m % p == 0) {
             if (p > kMaxRadix || (p != 3 && p != 5 && p != 7 && p != 11 && p != 13))
                 return -1;
             fac[k++] = p;
-            n /= p;
+            m /= p;
         }
     }
+    while (p2 >= 3) { fac[k++] = 8; p2 -= 3; }
+    if (p2 == 2) fac[k++] = 4;
+    if (p2 == 1) fac[k++] = 2;
     return k;
 }
 
