@@ -118,6 +118,35 @@ def flops_per_transform(w, L=None):
     return legendre_flops(dict(w, kind="glq" if w["kind"] == "glq_batch" else w["kind"]), 1, L)
 
 
+def fft_classes(lmaxes):
+    """Number of FFT kernel classes a GLQ batch launches per FFT stage: the
+    ring length (n = 2 lmax + 1, or its Bluestein length, the smallest
+    7-smooth number >= 2n - 1, when n has a prime factor above 13) decides
+    between radices <= 8 and a factor 11 or 13, and between 128-thread CTAs
+    (length <= 512) and larger ones."""
+    def smooth7(x):
+        for p in (2, 3, 5, 7):
+            while x % p == 0:
+                x //= p
+        return x == 1
+    classes = set()
+    for L in set(lmaxes):
+        n, odd, r = 2 * L + 1, [], 2 * L + 1
+        for p in (3, 5, 7, 11, 13):
+            while r % p == 0:
+                r //= p
+                odd.append(p)
+        if r == 1:
+            length, full = n, any(p > 8 for p in odd)
+        else:
+            length = 2 * n - 1
+            while not smooth7(length):
+                length += 1
+            full = False
+        classes.add((full, length > 512))
+    return len(classes)
+
+
 def power_law(L, seed, beta, cplx=False):
     from shtools_b200.synthetic import power_law_cilm, power_law_cilm_complex
     return (power_law_cilm_complex if cplx else power_law_cilm)(L, seed, beta)
@@ -506,7 +535,9 @@ def run_cuda_batch(args, w, rank, world, local_rank):
                 "h2d_bytes_per_step": c_host.numel() * 8 + g_host.numel() * 8,
                 "d2h_bytes_per_step": g_host.numel() * 8 + b_host.numel() * 8,
                 "path": "batch graphs from pinned host buffers"},
-        "gpu_launches": int(sum(cnt)) // 2 * args.steps,
+        # per step: pack, Legendre and unpack launches, and each FFT stage one
+        # launch per FFT class present (radices <= 8 / with 11 or 13)
+        "gpu_launches": (int(sum(cnt)) // 2 + 2 * (fft_classes(lm) - 1)) * args.steps,
         "clocks": clk.summary(),
     }
 

@@ -170,7 +170,14 @@ k_batch_anal(const BatchGroup* __restrict__ G, const int4* __restrict__ items,
 // counter, so CTAs stay busy across groups of different FFT lengths; the
 // group's FftArgs are read in place from global memory, and the input lines
 // of the CTA's next item are prefetched into L2 while the current FFT runs.
-__global__ void __launch_bounds__(512)
+// The jobs are split into classes, one persistent launch each: groups whose
+// radices are all <= 8 (every Bluestein length among them) run in a
+// register-capped build (MAXR = 8, more CTAs per SM), the others (factors 11
+// or 13) in the full build; within each, rings of up to 512 points run in
+// 128-thread CTAs with their own (small) shared memory, longer ones in
+// 256- or 512-thread CTAs.
+template <int MAXR>
+__global__ void __launch_bounds__(512, MAXR <= 8 ? 2 : 1)
 k_batch_c2r(const BatchGroup* __restrict__ G, const FftArgs* __restrict__ FA,
             const int4* __restrict__ jobs, int njobs, int* __restrict__ counter,
             const double2* __restrict__ work, double* __restrict__ grid) {
@@ -187,7 +194,7 @@ k_batch_c2r(const BatchGroup* __restrict__ G, const FftArgs* __restrict__ FA,
         const int4 j = jobs[i];
         const BatchGroup& g = G[j.x];
         const FftArgs& F = FA[j.x];
-        fft_c2r_body<double>(F, F.tw, smem_fft, j.z, j.y, work + g.spec_off,
+        fft_c2r_body<double, MAXR>(F, F.tw, smem_fft, j.z, j.y, work + g.spec_off,
                              grid + g.grid_off, (long long)g.nlat * g.nlon, g.nlon, 1,
                              g.rowN, g.rowS, nullptr, nullptr, 1.0, g.lc, g.npair, 0);
         __syncthreads();
@@ -195,7 +202,8 @@ k_batch_c2r(const BatchGroup* __restrict__ G, const FftArgs* __restrict__ FA,
     }
 }
 
-__global__ void __launch_bounds__(512)
+template <int MAXR>
+__global__ void __launch_bounds__(512, MAXR <= 8 ? 2 : 1)
 k_batch_r2c(const BatchGroup* __restrict__ G, const FftArgs* __restrict__ FA,
             const int4* __restrict__ jobs, int njobs, int* __restrict__ counter,
             const double* __restrict__ grid, double2* __restrict__ work) {
@@ -215,7 +223,7 @@ k_batch_r2c(const BatchGroup* __restrict__ G, const FftArgs* __restrict__ FA,
         const int4 j = jobs[i];
         const BatchGroup& g = G[j.x];
         const FftArgs& F = FA[j.x];
-        fft_r2c_body<double>(F, F.tw, smem_fft, j.z, j.y, grid + g.grid_off,
+        fft_r2c_body<double, MAXR>(F, F.tw, smem_fft, j.z, j.y, grid + g.grid_off,
                              (long long)g.nlat * g.nlon, g.nlon, 1, work + g.spec_off,
                              g.arowN, g.arowS, g.wN, g.wS, g.inv_nlon, g.lc, g.npair, 0);
         __syncthreads();
@@ -239,15 +247,18 @@ struct shtc_batch {
     int nsitems = 0;
     int4* d_aitems = nullptr;
     int naitems = 0;
-    int4* d_jobs = nullptr;
-    int njobs = 0;
-    int* d_counter = nullptr;
+    // FFT job classes (fft_class): 2 * (a radix above 8) + (more than 128
+    // threads); classes 0, 1 run the register-capped kernels
+    static constexpr int kClasses = 4;
+    int4* d_jobs[kClasses] = {};
+    int njobs[kClasses] = {};
+    int* d_counter = nullptr;   // [0] Legendre items, [1 + c] FFT jobs of class c
     size_t work_bytes = 0;
-    size_t fft_smem = 0;
-    int fft_threads = 128;
+    size_t fft_smem[kClasses] = {};
+    int fft_threads[kClasses] = {128, 128, 128, 128};
     int synth_ctas = 0;
     int anal_ctas = 0;
-    int fft_ctas = 0;
+    int fft_ctas[kClasses] = {};
     long long cilm_total = 0;
     long long grid_total = 0;
 };
@@ -258,8 +269,24 @@ static void batch_free(shtc_batch* B) {
     cudaFree(B->d_pitems);
     cudaFree(B->d_sitems);
     cudaFree(B->d_aitems);
-    cudaFree(B->d_jobs);
+    for (int c = 0; c < shtc_batch::kClasses; ++c) cudaFree(B->d_jobs[c]);
     cudaFree(B->d_counter);
+}
+
+// persistent CTAs of one FFT class: shared-memory size and carveout set on
+// both kernels, as many CTAs as fit on every SM, at most one per job
+template <typename KC, typename KR>
+static int fft_class_ctas(KC kc, KR kr, int sm, int njobs, int threads, size_t smem) {
+    if (njobs == 0) return 0;
+    for (const void* fn : {(const void*)kc, (const void*)kr}) {
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+    }
+    int pc = 0, pr = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pc, kc, threads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pr, kr, threads, smem);
+    return std::min(njobs, sm * std::max(1, std::min(pc, pr)));
 }
 
 template <typename Tp>
@@ -283,12 +310,13 @@ extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
     B->ngroup = ngroup;
     std::vector<FftArgs> fa(ngroup);
     long long pack = 0, spec = 0, coff = 0, goff = 0;
-    size_t smem = 0;
-    int threads = 128;
+    constexpr int NC = shtc_batch::kClasses;
+    size_t smem[NC] = {};
+    int threads[NC] = {128, 128, 128, 128};
     struct Cost { double c; int4 it; };
     std::vector<Cost> sc, ac;
     std::vector<int2> pitems;
-    std::vector<int4> jobs;
+    std::vector<int4> jobs[NC];
     for (int gi = 0; gi < ngroup; ++gi) {
         const shtc_plan* P = plans[gi];
         const int nf = nfields[gi];
@@ -320,8 +348,11 @@ extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
         spec += (long long)nf * P->npair * (P->lc + 1) * 2;
         B->h_groups.push_back(g);
         fa[gi] = fft_args(P->fft);
-        smem = std::max(smem, P->fft.smem_data);   // twiddles stay in global memory
-        threads = std::max(threads, P->fft.threads);
+        int cls = P->fft.threads > 128 ? 1 : 0;
+        for (int i = 0; i < P->fft.nfac; ++i)
+            if (P->fft.fac[i] > 8) cls = 2 + (cls & 1);
+        smem[cls] = std::max(smem[cls], P->fft.smem_data);   // twiddles stay in global memory
+        threads[cls] = std::max(threads[cls], P->fft.threads);
         // work items, with costs for longest-first ordering
         const int lc = P->lc;
         for (int m = 0; m <= lc; ++m) {
@@ -345,7 +376,7 @@ extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
             }
         }
         for (int f = 0; f < nf; ++f)
-            for (int j = 0; j < g.fft_jobs; ++j) jobs.push_back(make_int4(gi, f, j, 0));
+            for (int j = 0; j < g.fft_jobs; ++j) jobs[cls].push_back(make_int4(gi, f, j, 0));
     }
     // the spectra follow all packed-coefficient regions in the workspace
     for (BatchGroup& g : B->h_groups) g.spec_off += pack;
@@ -358,9 +389,11 @@ extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
     B->npitems = (int)pitems.size();
     B->nsitems = (int)si.size();
     B->naitems = (int)ai.size();
-    B->njobs = (int)jobs.size();
-    B->fft_smem = smem;
-    B->fft_threads = threads;
+    for (int c = 0; c < NC; ++c) {
+        B->njobs[c] = (int)jobs[c].size();
+        B->fft_smem[c] = smem[c];
+        B->fft_threads[c] = threads[c];
+    }
     B->cilm_total = coff;
     B->grid_total = goff;
     B->work_bytes = (size_t)(pack + spec) * sizeof(double2);
@@ -370,8 +403,8 @@ extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
     if (!rc) rc = upload(&B->d_pitems, pitems, st);
     if (!rc) rc = upload(&B->d_sitems, si, st);
     if (!rc) rc = upload(&B->d_aitems, ai, st);
-    if (!rc) rc = upload(&B->d_jobs, jobs, st);
-    if (!rc && cudaMalloc((void**)&B->d_counter, 2 * sizeof(int)) != cudaSuccess)
+    for (int c = 0; c < NC && !rc; ++c) rc = upload(&B->d_jobs[c], jobs[c], st);
+    if (!rc && cudaMalloc((void**)&B->d_counter, (1 + NC) * sizeof(int)) != cudaSuccess)
         rc = SHTC_EALLOC;
     if (!rc) {
         int sm = 0, per = 0;
@@ -384,18 +417,13 @@ extern "C" SHTC_API int shtc_batch_create(shtc_batch** out, int ngroup,
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_anal,
                                                       32 * kBatchAnalWarps, asmem);
         B->anal_ctas = sm * std::max(1, per);
-        if (B->fft_smem > 48 * 1024) {
-            cudaFuncSetAttribute(k_batch_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)B->fft_smem);
-            cudaFuncSetAttribute(k_batch_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)B->fft_smem);
-        }
-        int pc = 0, pr = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pc, k_batch_c2r, B->fft_threads,
-                                                      B->fft_smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pr, k_batch_r2c, B->fft_threads,
-                                                      B->fft_smem);
-        B->fft_ctas = std::min(B->njobs, sm * std::max(1, std::min(pc, pr)));
+        for (int c = 0; c < NC; ++c)
+            B->fft_ctas[c] = c < 2 ? fft_class_ctas(k_batch_c2r<8>, k_batch_r2c<8>, sm,
+                                                    B->njobs[c], B->fft_threads[c],
+                                                    B->fft_smem[c])
+                                   : fft_class_ctas(k_batch_c2r<13>, k_batch_r2c<13>, sm,
+                                                    B->njobs[c], B->fft_threads[c],
+                                                    B->fft_smem[c]);
         rc = map_cuda(cudaStreamSynchronize(st));
     }
     if (rc) {
@@ -457,9 +485,20 @@ extern "C" SHTC_API int shtc_batch_synthesis(const shtc_batch* B, const double* 
     stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
     if ((rc = map_cuda(cudaGetLastError()))) return rc;
     stage_begin(SHTC_STAGE_FFT_C2R, st);
-    if ((rc = map_cuda(cudaMemsetAsync(B->d_counter + 1, 0, sizeof(int), st)))) return rc;
-    k_batch_c2r<<<B->fft_ctas, B->fft_threads, B->fft_smem, st>>>(
-        B->d_groups, B->d_fft, B->d_jobs, B->njobs, B->d_counter + 1, w, grid);
+    if ((rc = map_cuda(cudaMemsetAsync(B->d_counter + 1, 0,
+                                       shtc_batch::kClasses * sizeof(int), st))))
+        return rc;
+    for (int c = 0; c < shtc_batch::kClasses; ++c) {
+        if (!B->njobs[c]) continue;
+        if (c < 2)
+            k_batch_c2r<8><<<B->fft_ctas[c], B->fft_threads[c], B->fft_smem[c], st>>>(
+                B->d_groups, B->d_fft, B->d_jobs[c], B->njobs[c], B->d_counter + 1 + c, w,
+                grid);
+        else
+            k_batch_c2r<13><<<B->fft_ctas[c], B->fft_threads[c], B->fft_smem[c], st>>>(
+                B->d_groups, B->d_fft, B->d_jobs[c], B->njobs[c], B->d_counter + 1 + c, w,
+                grid);
+    }
     stage_end(SHTC_STAGE_FFT_C2R, st);
     return map_cuda(cudaGetLastError());
 }
@@ -472,9 +511,20 @@ extern "C" SHTC_API int shtc_batch_analysis(const shtc_batch* B, const double* g
     cudaStream_t st = (cudaStream_t)stream;
     double2* w = (double2*)work;
     stage_begin(SHTC_STAGE_FFT_R2C, st);
-    if ((rc = map_cuda(cudaMemsetAsync(B->d_counter + 1, 0, sizeof(int), st)))) return rc;
-    k_batch_r2c<<<B->fft_ctas, B->fft_threads, B->fft_smem, st>>>(
-        B->d_groups, B->d_fft, B->d_jobs, B->njobs, B->d_counter + 1, grid, w);
+    if ((rc = map_cuda(cudaMemsetAsync(B->d_counter + 1, 0,
+                                       shtc_batch::kClasses * sizeof(int), st))))
+        return rc;
+    for (int c = 0; c < shtc_batch::kClasses; ++c) {
+        if (!B->njobs[c]) continue;
+        if (c < 2)
+            k_batch_r2c<8><<<B->fft_ctas[c], B->fft_threads[c], B->fft_smem[c], st>>>(
+                B->d_groups, B->d_fft, B->d_jobs[c], B->njobs[c], B->d_counter + 1 + c, grid,
+                w);
+        else
+            k_batch_r2c<13><<<B->fft_ctas[c], B->fft_threads[c], B->fft_smem[c], st>>>(
+                B->d_groups, B->d_fft, B->d_jobs[c], B->njobs[c], B->d_counter + 1 + c, grid,
+                w);
+    }
     stage_end(SHTC_STAGE_FFT_R2C, st);
     if ((rc = map_cuda(cudaGetLastError()))) return rc;
     if ((rc = map_cuda(cudaMemsetAsync(B->d_counter, 0, sizeof(int), st)))) return rc;
