@@ -713,8 +713,8 @@ def run_cuda_gradient(args, w, rank, world, local_rank):
         kind, what = "dh gravity", ("MakeGravGridDH of every field (rad, theta, phi, "
                                     "total and pot grids; ellipsoid, rotation, "
                                     "normal gravity removed)")
-        # pack stage: ring tables, powers, pack; FFT stage: combination, 4 c2r,
-        # centrifugal / normal-gravity pass
+        # pack stage: ring tables, powers, pack; FFT stage: combination (with
+        # the centrifugal terms), 4 c2r, magnitude / normal-gravity pass
         launches = 3 * int(cnt[0]) + int(cnt[1]) + 6 * int(cnt[2])
         # the radial factor adds 2 multiplies per (pair, l, m) to the recursion
         fl_note = "recursion + 3 contractions per (pair, l, m); q^l factor not counted"

@@ -1,9 +1,10 @@
 """Autotuner of the Legendre-kernel tile shapes.
 
 For a plan, times the single-field synthesis kernel for each choice of ring
-pairs per thread (1, 2, 4, 8) and the analysis kernel for each (pairs per
-thread, warps per CTA) pair, on random inputs of the plan's real size, with
-the library's per-stage CUDA-event timing, and keeps the fastest.  Results
+pairs per thread (1, 2, 4, 8) and the analysis kernel with its unpack for
+each (pairs per thread, warps per CTA) pair, on random inputs of the plan's
+real size, with the library's per-stage CUDA-event timing, and keeps the
+fastest.  Results
 are cached in a JSON file keyed by GPU model and plan geometry:
 ``$SHTC_TUNE_CACHE`` or ``~/.cache/shtools_b200/tune.json``.
 
@@ -25,6 +26,7 @@ from . import _lib
 
 STAGE_SYNTH = 1
 STAGE_ANAL = 4
+STAGE_UNPACK = 5
 _lock = threading.Lock()
 
 
@@ -62,6 +64,8 @@ def plan_key(plan):
 
 
 def _time_stage(plan, fn, stage, reps):
+    """Mean time per call (ms) of one library stage, or of the sum of several
+    (a tuple of stage ids)."""
     lib = plan.lib
     fn()
     torch.cuda.synchronize(plan.device)
@@ -73,12 +77,15 @@ def _time_stage(plan, fn, stage, reps):
     ms = (ctypes.c_double * 6)()
     cnt = (ctypes.c_int * 6)()
     _lib.check(lib.shtc_timing_collect(ms, cnt, 6))
-    return ms[stage] / max(1, cnt[stage])
+    stages = stage if isinstance(stage, tuple) else (stage,)
+    return sum(ms[s] / max(1, cnt[s]) for s in stages)
 
 
 def candidates(npair):
     synth = [t for t in (1, 2, 4, 8) if t * 128 <= max(256, 2 * npair)]
-    anal = [(t, w) for t in (1, 2, 4, 8) for w in (2, 4, 8)
+    # one-warp CTAs skip the cross-warp reduction but make more ring-pair
+    # tiles, whose partial sums the unpack adds (timed with the analysis)
+    anal = [(t, w) for t in (1, 2, 4, 8) for w in (1, 2, 4, 8)
             if t * w * 32 <= max(128, 2 * npair)]
     return synth, anal
 
@@ -123,7 +130,7 @@ def tune_plan(plan, reps=3, use_cache=True, verbose=False):
         best_a, best_at = None, float("inf")
         for t, w in a_c:
             set_shape(plan, 0, t, w)
-            ms = _time_stage(plan, lambda: anal(grid), STAGE_ANAL, reps)
+            ms = _time_stage(plan, lambda: anal(grid), (STAGE_ANAL, STAGE_UNPACK), reps)
             times["anal_T%d_W%d" % (t, w)] = ms
             if ms < best_at:
                 best_a, best_at = (t, w), ms

@@ -20,8 +20,10 @@
 //     pot   =  S0 g1
 //     theta = -sin(theta) (q S1 - z S2) / u^2 g2   (zero on the poles)
 //     phi   =  i m S0 g2 / sin(theta)              (zero on the poles)
-// then four c2r FFTs and one pointwise pass that adds the centrifugal terms,
-// forms |g| and removes the normal gravity (MakeGravGridDH.f95:987-1044).
+// The centrifugal terms of a row (MakeGravGridDH.f95:987-1013) are constants
+// added to the m = 0 Fourier bin, which adds them to every sample of the
+// c2r output; four c2r FFTs then write rad, theta, phi and pot, and one
+// pointwise pass forms |g| and removes the normal gravity (:1015-1044).
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -146,11 +148,13 @@ static int launch_synth_rad_t(const shtc_plan* P, const double2* packed, double2
 }
 
 // spec fields 3u..3u+2 -> c2r inputs of rad (field u), theta (nfield + u),
-// phi (2 nfield + u) and pot (3 nfield + u)
+// phi (2 nfield + u) and pot (3 nfield + u); with rotation, the m = 0 bins
+// of rad, theta and pot also take the row's centrifugal terms
 __global__ void k_grav_combine(const double2* __restrict__ spec, double2* __restrict__ out,
                                const double* __restrict__ zp, const double2* __restrict__ radq,
-                               const double2* __restrict__ ringg, int npair, int lc, int n,
-                               int nfield) {
+                               const double2* __restrict__ ringg, const int* __restrict__ rowN,
+                               const int* __restrict__ rowS, const double* __restrict__ rows,
+                               int has_omega, int npair, int lc, int n, int nfield) {
     const long long per = (long long)npair * (lc + 1) * 2;   // one field
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int u = blockIdx.y;
@@ -163,8 +167,8 @@ __global__ void k_grav_combine(const double2* __restrict__ spec, double2* __rest
     const double2 x2 = spec[(3LL * u + 2) * per + i];
     const double2 gg = ringg[p];
     const double q = radq[p].x;
-    const double2 rad = make_double2(-(x2.x + x0.x) * gg.x, -(x2.y + x0.y) * gg.x);
-    const double2 pot = make_double2(x0.x * gg.y, x0.y * gg.y);
+    double2 rad = make_double2(-(x2.x + x0.x) * gg.x, -(x2.y + x0.y) * gg.x);
+    double2 pot = make_double2(x0.x * gg.y, x0.y * gg.y);
     double2 t = make_double2(0.0, 0.0), f = make_double2(0.0, 0.0);
     if (p > 0) {
         const double z = h ? -zp[p] : zp[p];
@@ -175,32 +179,31 @@ __global__ void k_grav_combine(const double2* __restrict__ spec, double2* __rest
         const double cp = (double)m * gg.x / st;
         f = make_double2(-cp * x0.y, cp * x0.x);
     }
+    if (has_omega && m == 0) {
+        const int row = h ? rowS[p] : rowN[p];
+        if (row >= 0) {
+            rad.x += rows[4 * row + 0];
+            t.x += rows[4 * row + 1];
+            pot.x += rows[4 * row + 2];
+        }
+    }
     out[(long long)u * per + i] = rad;
     out[((long long)nfield + u) * per + i] = t;
     out[(2LL * nfield + u) * per + i] = f;
     out[(3LL * nfield + u) * per + i] = pot;
 }
 
-// centrifugal terms, |g| and the normal gravity, per grid point of every
-// output row (the extend column included: it repeats column 0)
-__global__ void k_grav_post(double* __restrict__ rad, double* __restrict__ theta,
+// |g| and the normal gravity, per grid point of every output row (the
+// extend column included: it repeats column 0)
+__global__ void k_grav_post(const double* __restrict__ rad, const double* __restrict__ theta,
                             const double* __restrict__ phi, double* __restrict__ total,
-                            double* __restrict__ pot, long long gf, long long grs,
-                            long long gcs, int ncol, const double* __restrict__ rows,
-                            int has_omega) {
+                            long long gf, long long grs, long long gcs, int ncol,
+                            const double* __restrict__ rows) {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= ncol) return;
     const int row = blockIdx.y;
     const long long o = (long long)blockIdx.z * gf + (long long)row * grs + (long long)col * gcs;
-    double r = rad[o], t = theta[o];
-    const double ph = phi[o];
-    if (has_omega) {
-        r += rows[4 * row + 0];
-        t += rows[4 * row + 1];
-        rad[o] = r;
-        theta[o] = t;
-        if (pot) pot[o] += rows[4 * row + 2];
-    }
+    const double r = rad[o], t = theta[o], ph = phi[o];
     total[o] = sqrt(r * r + ph * ph + t * t) - rows[4 * row + 3];
 }
 
@@ -243,8 +246,9 @@ int launch_gravity_dh(const shtc_plan* P, const double* cilm, long long sf, long
     {
         const long long per = (long long)np * (lc + 1) * 2;
         dim3 grid((unsigned)((per + 255) / 256), nfield);
-        k_grav_combine<<<grid, 256, 0, st>>>(spec, spec2, P->d_z, radq, ringg, np, lc,
-                                             P->nlat, nfield);
+        k_grav_combine<<<grid, 256, 0, st>>>(spec, spec2, P->d_z, radq, ringg, P->d_rowN,
+                                             P->d_rowS, rows, g.has_omega, np, lc, P->nlat,
+                                             nfield);
         rc = map_cuda(cudaGetLastError());
         double* outs[4] = {rad, theta, phi, pot};
         for (int k = 0; k < 4 && !rc; ++k) {
@@ -254,8 +258,8 @@ int launch_gravity_dh(const shtc_plan* P, const double* cilm, long long sf, long
         }
         if (!rc) {
             dim3 pg((unsigned)((P->nlon_out + 255) / 256), P->nlat_out, nfield);
-            k_grav_post<<<pg, 256, 0, st>>>(rad, theta, phi, total, pot, gf, grs, gcs,
-                                            P->nlon_out, rows, g.has_omega);
+            k_grav_post<<<pg, 256, 0, st>>>(rad, theta, phi, total, gf, grs, gcs,
+                                            P->nlon_out, rows);
             rc = map_cuda(cudaGetLastError());
         }
     }

@@ -20,6 +20,11 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <utility>
+
 #include "fft.cuh"
 #include "legendre.cuh"
 #include "shtc_internal.cuh"
@@ -290,6 +295,36 @@ k_fft_r2c(FftArgs F, int tw_smem, int jobs, int nitems, const GT* __restrict__ g
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+// Host-side launch configuration, cached: a kernel's shared-memory
+// attributes are set once per device (again only for a larger size), and
+// its resident CTAs per device once per (device, kernel, CTA shape), so a
+// transform issues no attribute or occupancy calls after its first run.
+namespace {
+std::mutex g_launch_mu;
+std::map<std::pair<int, const void*>, size_t> g_smem_set;
+std::map<std::tuple<int, const void*, int, size_t>, int> g_resident;
+}  // namespace
+
+// the dynamic shared memory limit of kernel fn raised to smem; with
+// max_shared the largest carveout is preferred (kernels that live on shared
+// memory, so that registers, not the L1 split, limit the resident CTAs)
+static int kernel_smem_attr(const void* fn, size_t smem, bool max_shared) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return map_cuda(e);
+    std::lock_guard<std::mutex> g(g_launch_mu);
+    const auto key = std::make_pair(dev, fn);
+    auto it = g_smem_set.find(key);
+    if (it != g_smem_set.end() && it->second >= smem) return SHTC_OK;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess && max_shared)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return map_cuda(e);
+    g_smem_set[key] = smem;
+    return SHTC_OK;
+}
+
 FftArgs fft_args(const FftPlan& f) {
     FftArgs a;
     a.n = f.n; a.mode = f.mode; a.m = f.m; a.nfac = f.nfac;
@@ -408,9 +443,8 @@ static int launch_anal_t(const shtc_plan* P, const double2* spec,
                  const double2*, double2*, int, int, long long, int);
     if constexpr (T == 8) kern = k_legendre_anal_capped<T, NF>;
     else kern = k_legendre_anal<T, NF>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return map_cuda(e);
+    const int rc = kernel_smem_attr((const void*)kern, smem, false);
+    if (rc) return rc;
     dim3 grid(tiles, P->lc + 1, (nfield + NF - 1) / NF);
     kern<<<grid, threads, smem, st>>>(
         P->d_rec, P->d_pmm, P->d_rtab, P->d_z, spec, partial, P->lc, P->npair,
@@ -465,17 +499,6 @@ int launch_unpack_coef(const shtc_plan* P, const double2* partial, int ntiles,
     return map_cuda(cudaGetLastError());
 }
 
-// the FFT kernels live on shared memory: ask for the largest carveout so
-// that the resident CTAs are limited by registers, not by the L1 split
-static int fft_smem_setup(const void* fn, const FftPlan& f) {
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)f.smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 cudaSharedmemCarveoutMaxShared);
-    return map_cuda(e);
-}
-
 // the register-capped build pays off when every radix of the plan
 // (Bluestein: of its convolution length) is <= 8 and shared memory leaves
 // room for more than one CTA per SM (at lmax 2799, 179 KB per CTA, the cap
@@ -487,17 +510,30 @@ static bool fft_lean(const FftPlan& f) {
     return true;
 }
 
-// persistent grid: as many CTAs as fit on the device at once, at most one
-// per item
-template <typename K>
-static int fft_grid(K kernel, const FftPlan& f, int nitems, int* blocks) {
-    int dev = 0, sms = 0, occ = 0;
+// persistent grid of an FFT kernel: as many CTAs as fit on the device at
+// once, at most one per item (and one per global-scratch slice)
+static int fft_launch_setup(const void* fn, const FftPlan& f, int nitems, int* blocks) {
+    int rc = kernel_smem_attr(fn, f.smem, true);
+    if (rc) return rc;
+    int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, f.threads,
-                                                                  f.smem);
-    if (e != cudaSuccess) return map_cuda(e);
-    long long cap = (long long)(sms > 0 ? sms : 1) * (occ > 0 ? occ : 1);
+    long long cap;
+    {
+        std::lock_guard<std::mutex> g(g_launch_mu);
+        const auto key = std::make_tuple(dev, fn, f.threads, f.smem);
+        auto it = g_resident.find(key);
+        if (it != g_resident.end()) {
+            cap = it->second;
+        } else {
+            int sms = 0, occ = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, f.threads,
+                                                                          f.smem);
+            if (e != cudaSuccess) return map_cuda(e);
+            cap = (long long)(sms > 0 ? sms : 1) * (occ > 0 ? occ : 1);
+            g_resident[key] = (int)cap;
+        }
+    }
     if (f.gmem && cap > f.gmem_ctas) cap = f.gmem_ctas;   // one scratch slice per CTA
     *blocks = (int)(nitems < cap ? nitems : cap);
     return SHTC_OK;
@@ -516,12 +552,11 @@ static int launch_c2r_t(const shtc_plan* P, const double2* spec, GT* grid, long 
                         cudaStream_t st, double2* gbuf) {
     const FftPlan& f = P->fft;
     if (f.gmem && !gbuf) return SHTC_EWORK;
-    int rc = fft_smem_setup((const void*)k_fft_c2r<GT, MAXR>, f);
-    if (rc) return rc;
+    int rc;
     const int jobs = f.mode == 0 ? P->npair : 2 * P->npair;
     const int nitems = jobs * nfield;
     int blocks = 0;
-    if ((rc = fft_grid(k_fft_c2r<GT, MAXR>, f, nitems, &blocks))) return rc;
+    if ((rc = fft_launch_setup((const void*)k_fft_c2r<GT, MAXR>, f, nitems, &blocks))) return rc;
     if (blocks == 0) return SHTC_OK;
     // synthesis uses the synthesis ring map (with the extend row and column);
     // the analysis adjoint uses the analysis ring map and ring weights
@@ -559,12 +594,11 @@ static int launch_r2c_t(const shtc_plan* P, const GT* grid, long long gf, long l
                         int fold_extend, cudaStream_t st, const GT* grid2, double2* gbuf) {
     const FftPlan& f = P->fft;
     if (f.gmem && !gbuf) return SHTC_EWORK;
-    int rc = fft_smem_setup((const void*)k_fft_r2c<GT, MAXR>, f);
-    if (rc) return rc;
+    int rc;
     const int jobs = f.mode == 0 ? P->npair : 2 * P->npair;
     const int nitems = jobs * nfield;
     int blocks = 0;
-    if ((rc = fft_grid(k_fft_r2c<GT, MAXR>, f, nitems, &blocks))) return rc;
+    if ((rc = fft_launch_setup((const void*)k_fft_r2c<GT, MAXR>, f, nitems, &blocks))) return rc;
     if (blocks == 0) return SHTC_OK;
     if (weighted) {
         // analysis: fcoef = (w * Re) / nlong, the reference's order of operations
@@ -752,12 +786,11 @@ static int launch_c2c_synth_t(const shtc_plan* P, const double2* spec, double2* 
                               cudaStream_t st, double2* gbuf) {
     const FftPlan& f = P->fft;
     if (f.gmem && !gbuf) return SHTC_EWORK;
-    int rc = fft_smem_setup((const void*)k_fft_c2c_synth<MAXR>, f);
-    if (rc) return rc;
+    int rc;
     const int jobs = 2 * P->npair;
     const int nitems = jobs * nfield;
     int blocks = 0;
-    if ((rc = fft_grid(k_fft_c2c_synth<MAXR>, f, nitems, &blocks))) return rc;
+    if ((rc = fft_launch_setup((const void*)k_fft_c2c_synth<MAXR>, f, nitems, &blocks))) return rc;
     if (blocks == 0) return SHTC_OK;
     k_fft_c2c_synth<MAXR><<<blocks, f.threads, f.smem, st>>>(
         fft_args(f), f.tw_smem, jobs, nitems, spec, grid, gf, grs, gcs, P->d_rowN,
@@ -771,12 +804,11 @@ static int launch_c2c_anal_t(const shtc_plan* P, const double2* grid, long long 
                              cudaStream_t st, double2* gbuf) {
     const FftPlan& f = P->fft;
     if (f.gmem && !gbuf) return SHTC_EWORK;
-    int rc = fft_smem_setup((const void*)k_fft_c2c_anal<MAXR>, f);
-    if (rc) return rc;
+    int rc;
     const int jobs = 2 * P->npair;
     const int nitems = jobs * nfield;
     int blocks = 0;
-    if ((rc = fft_grid(k_fft_c2c_anal<MAXR>, f, nitems, &blocks))) return rc;
+    if ((rc = fft_launch_setup((const void*)k_fft_c2c_anal<MAXR>, f, nitems, &blocks))) return rc;
     if (blocks == 0) return SHTC_OK;
     k_fft_c2c_anal<MAXR><<<blocks, f.threads, f.smem, st>>>(
         fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_arowN,

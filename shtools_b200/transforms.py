@@ -30,6 +30,24 @@ def _stream_ptr(device):
     return ctypes_void(torch.cuda.current_stream(device).cuda_stream)
 
 
+class _NoSwitch:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+_NO_SWITCH = _NoSwitch()
+
+
+def _on_device(device):
+    """torch.cuda.device(device), or nothing when it is already current."""
+    if device.index == torch.cuda.current_device():
+        return _NO_SWITCH
+    return torch.cuda.device(device)
+
+
 def ctypes_void(x):
     import ctypes
     return ctypes.c_void_p(int(x))
@@ -94,15 +112,26 @@ class Plan:
     def lc(self):
         return self.info["lmax_comp"]
 
+    def workspace_bytes(self, nfield):
+        """shtc_workspace_bytes for nfield fields, cached per plan and tile
+        shape (the analysis tiles, and so the size, follow the shape that
+        shtools_b200.autotune.set_shape records in self.shape)."""
+        cache = self.__dict__.setdefault("_wsb", {})
+        key = (nfield, getattr(self, "shape", None))
+        nb = cache.get(key)
+        if nb is None:
+            nb = cache[key] = int(self.lib.shtc_workspace_bytes(self.handle, int(nfield)))
+        return nb
+
     def workspace(self, nfield):
-        nb = int(self.lib.shtc_workspace_bytes(self.handle, int(nfield)))
+        nb = self.workspace_bytes(nfield)
         return torch.empty(nb, dtype=torch.uint8, device=self.device), nb
 
     # -- raw transforms on (F, 2, D, D) / (F, rows, cols) tensors -------------
     # float64 or float32 arrays; the kernels compute in FP64 either way
     def _run(self, fn, src, dst, nfield, src_is_coef):
         ws, nb = self.workspace(nfield)
-        with torch.cuda.device(self.device):
+        with _on_device(self.device):
             st = _stream_ptr(self.device)
             c, g = (src, dst) if src_is_coef else (dst, src)
             cargs = (ctypes_void(c.data_ptr()), _DTYPE[c.dtype], c.stride(0),
@@ -134,7 +163,7 @@ class Plan:
     # -- complex transforms (complex plans; complex128 tensors) ---------------
     def _run_c(self, fn, src, dst, nfield, src_is_coef):
         ws, nb = self.workspace(nfield)
-        with torch.cuda.device(self.device):
+        with _on_device(self.device):
             st = _stream_ptr(self.device)
             c, g = (src, dst) if src_is_coef else (dst, src)
             cargs = (ctypes_void(c.data_ptr()), c.stride(0), c.stride(1), c.stride(2),
@@ -313,6 +342,32 @@ def _out_dtype(dtype):
 # ---------------------------------------------------------------------------
 # autograd functions
 # ---------------------------------------------------------------------------
+def _needs_grad(t):
+    return torch.is_grad_enabled() and t.requires_grad
+
+
+def _synthesis(cilm, plan, dtype):
+    """Forward synthesis; through the autograd Function only when cilm
+    requires a gradient (the Function's bookkeeping costs microseconds per
+    call, which small transforms feel)."""
+    if _needs_grad(cilm):
+        return _Synthesis.apply(cilm, plan, dtype)
+    c, lead = _flat(cilm[..., :2, :, :], 3)
+    g = plan.synthesis(c, dtype=dtype)
+    return g.reshape(tuple(lead) + tuple(g.shape[1:]))
+
+
+def _analysis(grid, plan, cdim, dtype):
+    """Forward analysis; through the autograd Function only when grid
+    requires a gradient."""
+    if _needs_grad(grid):
+        return _Analysis.apply(grid, plan, cdim, dtype)
+    nlat, nlon = plan.info["nlat"], plan.info["nlon"]
+    g, lead = _flat(grid, 2)
+    c = plan.analysis(g[:, :nlat, :nlon], cdim, dtype=dtype)
+    return c.reshape(tuple(lead) + tuple(c.shape[1:]))
+
+
 class _Synthesis(torch.autograd.Function):
     @staticmethod
     def forward(ctx, cilm, plan, dtype):
@@ -384,7 +439,7 @@ def MakeGridDH(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
     cilm = _as_cuda(cilm, "cilm")
     plan = get_plan(GRID_DH, lmax, lc, norm, csphase, sampling, int(bool(extend)),
                     device=cilm.device)
-    return _Synthesis.apply(cilm, plan, dtype)
+    return _synthesis(cilm, plan, dtype)
 
 
 def SHExpandDH(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None,
@@ -400,7 +455,7 @@ def SHExpandDH(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None,
     grid = _as_cuda(griddh, "griddh")
     plan = get_plan(GRID_DH, lmax, lc, norm, csphase, sampling, 0,
                     device=grid.device)
-    return _Analysis.apply(grid, plan, lc + 1, dtype)
+    return _analysis(grid, plan, lc + 1, dtype)
 
 
 def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
@@ -417,7 +472,7 @@ def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
     cilm = _as_cuda(cilm, "cilm")
     plan = get_plan(GRID_GLQ, lmax, lc, norm, csphase, 1, int(bool(extend)),
                     zero=z, device=cilm.device)
-    return _Synthesis.apply(cilm, plan, dtype)
+    return _synthesis(cilm, plan, dtype)
 
 
 def SHExpandGLQ(gridglq, w=None, zero=None, norm=1, csphase=1,
@@ -441,7 +496,7 @@ def SHExpandGLQ(gridglq, w=None, zero=None, norm=1, csphase=1,
         wh = ww if wh is None else wh
     plan = get_plan(GRID_GLQ, lmax, lc, norm, csphase, 1, 0, zero=z, w=wh,
                     device=grid.device)
-    return _Analysis.apply(grid, plan, lc + 1, dtype)
+    return _analysis(grid, plan, lc + 1, dtype)
 
 
 # ---------------------------------------------------------------------------
@@ -557,7 +612,7 @@ def MakeGradientDH(cilm, lmax=None, sampling=1, lmax_calc=None, extend=False,
     lib = plan.lib
     nb = int(lib.shtc_gradient_workspace_bytes(plan.handle, F))
     ws = torch.empty(max(nb, 8), dtype=torch.uint8, device=c.device)
-    with torch.cuda.device(c.device):
+    with _on_device(c.device):
         rc = lib.shtc_gradient_dh(plan.handle, ctypes_void(cf.data_ptr()), cf.stride(0),
                                   cf.stride(1), cf.stride(2), cf.stride(3), cf.shape[2],
                                   ctypes_void(th.data_ptr()), ctypes_void(ph.data_ptr()),
@@ -600,7 +655,7 @@ def MakeGravGridDH(cilm, gm, r0, lmax=None, a=None, f=0.0, sampling=2, lmax_calc
     lib = plan.lib
     nb = int(lib.shtc_gravity_workspace_bytes(plan.handle, F))
     ws = torch.empty(max(nb, 8), dtype=torch.uint8, device=c.device)
-    with torch.cuda.device(c.device):
+    with _on_device(c.device):
         rc = lib.shtc_gravity_dh(plan.handle, ctypes_void(cf.data_ptr()), cf.stride(0),
                                  cf.stride(1), cf.stride(2), cf.stride(3), cf.shape[2],
                                  float(gm), float(r0), a, float(f), int(omega is not None),
@@ -651,7 +706,7 @@ def SHMultiply(cilm1, cilm2, lmax1=None, lmax2=None, precomp=None, norm=1, cspha
     lib = plan.lib
     nb = int(lib.shtc_multiply_workspace_bytes(plan.handle, F))
     ws = torch.empty(max(nb, 8), dtype=torch.uint8, device=c1.device)
-    with torch.cuda.device(c1.device):
+    with _on_device(c1.device):
         rc = lib.shtc_multiply(plan.handle, ctypes_void(f1.data_ptr()), f1.stride(0),
                                f1.stride(1), f1.stride(2), f1.stride(3), L1,
                                ctypes_void(f2.data_ptr()), f2.stride(0), f2.stride(1),
@@ -683,7 +738,7 @@ def PreGLQ(x1, x2, n, device=None):
         else torch.device(device)
     zero = torch.empty(int(n), dtype=torch.float64, device=dev)
     w = torch.empty(int(n), dtype=torch.float64, device=dev)
-    with torch.cuda.device(dev):
+    with _on_device(dev):
         rc = lib.shtc_preglq(float(x1), float(x2), int(n),
                              ctypes_void(zero.data_ptr()),
                              ctypes_void(w.data_ptr()), _stream_ptr(dev))
@@ -704,7 +759,7 @@ def DHaj(n, extend=0, device=None):
     dev = torch.device("cuda", torch.cuda.current_device()) if device is None \
         else torch.device(device)
     aj = torch.empty(int(n) + int(extend), dtype=torch.float64, device=dev)
-    with torch.cuda.device(dev):
+    with _on_device(dev):
         rc = lib.shtc_dhaj(int(n), ctypes_void(aj.data_ptr()), int(extend),
                            _stream_ptr(dev))
     _lib.check(rc, "DHaj")

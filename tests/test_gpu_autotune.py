@@ -16,7 +16,7 @@ def test_autotune_real_and_complex_plans(cuda, oracle, tmp_path, monkeypatch):
         p = T.Plan(T.GRID_DH, L, L, 1, 1, 2, 0, cplx=cplx)
         r = autotune.tune_plan(p, reps=1, use_cache=True)
         assert r["synth_T"] in (1, 2, 4, 8) and r["anal_T"] in (1, 2, 4, 8)
-        assert r["anal_W"] in (2, 4, 8)
+        assert r["anal_W"] in (1, 2, 4, 8)
         assert any(k.startswith("anal_T") for k in r["times_ms"])
         # a second call is answered from the cache
         assert autotune.tune_plan(p, reps=1, use_cache=True)["synth_T"] == r["synth_T"]
