@@ -134,17 +134,35 @@ k_legendre_synth_rad(const double2* __restrict__ rec, const double* __restrict__
                              blockIdx.y, blockIdx.x, blockIdx.z * NF, NF, radq, qtab, nseg);
 }
 
-template <int T>
+template <int T, int NF>
 static int launch_synth_rad_t(const shtc_plan* P, const double2* packed, double2* spec,
                               int nfield, const double2* radq, const double* qtab,
                               cudaStream_t st) {
     const int threads = 128;
     const int tiles = (P->npair + threads * T - 1) / (threads * T);
-    dim3 grid(tiles, P->lc + 1, nfield / 3);
-    k_legendre_synth_rad<T, 3><<<grid, threads, 0, st>>>(
+    dim3 grid(tiles, P->lc + 1, nfield / NF);
+    k_legendre_synth_rad<T, NF><<<grid, threads, 0, st>>>(
         P->d_rec, P->d_pmm, P->d_rtab, P->d_z, radq, qtab, grav_nseg(P), packed, spec, P->lc,
         P->npair, nfield);
     return map_cuda(cudaGetLastError());
+}
+
+// nfield internal fields (three sums per user field) share the recursion and
+// the radial powers in groups of NF, with the plain synthesis' shapes
+static int launch_synth_rad(const shtc_plan* P, const double2* packed, double2* spec,
+                            int nfield, const double2* radq, const double* qtab,
+                            cudaStream_t st) {
+    const bool wide = P->npair > 512;
+    if (nfield % 8 == 0)
+        return wide ? launch_synth_rad_t<2, 8>(P, packed, spec, nfield, radq, qtab, st)
+                    : launch_synth_rad_t<1, 8>(P, packed, spec, nfield, radq, qtab, st);
+    if (nfield % 4 == 0)
+        return launch_synth_rad_t<2, 4>(P, packed, spec, nfield, radq, qtab, st);
+    if (nfield % 2 == 0)
+        return wide ? launch_synth_rad_t<4, 2>(P, packed, spec, nfield, radq, qtab, st)
+                    : launch_synth_rad_t<2, 2>(P, packed, spec, nfield, radq, qtab, st);
+    return wide ? launch_synth_rad_t<2, 3>(P, packed, spec, nfield, radq, qtab, st)
+                : launch_synth_rad_t<1, 3>(P, packed, spec, nfield, radq, qtab, st);
 }
 
 // spec fields 3u..3u+2 -> c2r inputs of rad (field u), theta (nfield + u),
@@ -238,8 +256,7 @@ int launch_gravity_dh(const shtc_plan* P, const double* cilm, long long sf, long
     stage_end(SHTC_STAGE_PACK, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_SYNTH, st);
-    rc = np > 512 ? launch_synth_rad_t<2>(P, packed, spec, 3 * nfield, radq, qtab, st)
-                  : launch_synth_rad_t<1>(P, packed, spec, 3 * nfield, radq, qtab, st);
+    rc = launch_synth_rad(P, packed, spec, 3 * nfield, radq, qtab, st);
     stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_FFT_C2R, st);

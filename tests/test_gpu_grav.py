@@ -74,6 +74,23 @@ def test_grav_lmax719_and_batch(cuda, oracle):
         assert torch.equal(a, b[0])
 
 
+@pytest.mark.parametrize("F", [2, 4, 8])
+def test_grav_grouped_fields(cuda, oracle, F):
+    """2, 4 and 8 fields: their 6, 12 and 24 sums share recursions in groups
+    of 2, 4 and 8 (across fields); each field equals its single-field call
+    and the oracle."""
+    L = 95
+    cs = np.stack([oracle.power_law_cilm(L, 120 + i) * 1e-3 for i in range(F)])
+    cs[:, 0, 0, 0] = 1.0
+    kw = dict(a=MARS["a"], f=MARS["f"], omega=MARS["omega"], normal_gravity=1)
+    g = cuda.MakeGravGridDH(torch.from_numpy(cs).cuda(), MARS["gm"], MARS["r0"], **kw)
+    for i in (0, F - 1):
+        gi = cuda.MakeGravGridDH(cs[i], MARS["gm"], MARS["r0"], **kw)
+        for a, b in zip(gi, g):
+            assert rel(b[i].cpu().numpy(), a.cpu().numpy()) <= 1e-14
+    check([x[F - 1] for x in g], oracle.makegravgrid_dh(cs[F - 1], MARS["gm"], MARS["r0"], **kw))
+
+
 def test_grav_default_arguments(cuda, oracle):
     """pyshtools defaults: a = r0, f = 0, sampling 2, omega 0, normal gravity
     removed with GM."""
