@@ -251,9 +251,14 @@ __device__ __forceinline__ double2* fft_buffers(const FftArgs& F, double2* smem_
 }
 
 // MAXR = 8: plans whose radices are all <= 8, built for <= 64 registers
-// (four 256-thread CTAs per SM); MAXR = 13 carries the radix-11/13 passes
-template <typename GT, int MAXR>
-__global__ void __launch_bounds__(512, MAXR <= 8 ? 2 : 1)
+// (four 256-thread CTAs per SM, or one 1024-thread CTA for rings too long
+// for two CTAs' shared memory: MAXT = 1024); MAXR = 13 carries the
+// radix-11/13 passes
+template <int MAXR, int MAXT>
+constexpr int fft_min_ctas() { return MAXR <= 8 ? 65536 / (64 * MAXT) : 1; }
+
+template <typename GT, int MAXR, int MAXT = 512>
+__global__ void __launch_bounds__(MAXT, fft_min_ctas<MAXR, MAXT>())
 k_fft_c2r(FftArgs F, int tw_smem, int jobs, int nitems, const double2* __restrict__ spec,
           GT* __restrict__ grid, long long gf, long long grs, long long gcs,
           const int* __restrict__ rowN, const int* __restrict__ rowS,
@@ -271,8 +276,8 @@ k_fft_c2r(FftArgs F, int tw_smem, int jobs, int nitems, const double2* __restric
     }
 }
 
-template <typename GT, int MAXR>
-__global__ void __launch_bounds__(512, MAXR <= 8 ? 2 : 1)
+template <typename GT, int MAXR, int MAXT = 512>
+__global__ void __launch_bounds__(MAXT, fft_min_ctas<MAXR, MAXT>())
 k_fft_r2c(FftArgs F, int tw_smem, int jobs, int nitems, const GT* __restrict__ grid,
           long long gf, long long grs, long long gcs, double2* __restrict__ spec,
           const int* __restrict__ rowN, const int* __restrict__ rowS,
@@ -499,15 +504,26 @@ int launch_unpack_coef(const shtc_plan* P, const double2* partial, int ntiles,
     return map_cuda(cudaGetLastError());
 }
 
-// the register-capped build pays off when every radix of the plan
-// (Bluestein: of its convolution length) is <= 8 and shared memory leaves
-// room for more than one CTA per SM (at lmax 2799, 179 KB per CTA, the cap
-// only costs spills: 2-3% slower on B200)
-static bool fft_lean(const FftPlan& f) {
-    if (f.smem > 100 * 1024) return false;
+// Which FFT build runs a plan: 0 the full one (the plan's CTA size); 1 the
+// register-capped one (radices <= 8, every Bluestein length among them)
+// when shared memory leaves room for more than one CTA per SM; 2 the
+// register-capped one in 1024-thread CTAs for rings of more than 4096
+// points held in shared memory (one CTA per SM either way, but twice the
+// warps; with 512 threads the cap alone cost 2-3% at lmax 2799)
+static int fft_variant(const FftPlan& f) {
     for (int i = 0; i < f.nfac; ++i)
-        if (f.fac[i] > 8) return false;
-    return true;
+        if (f.fac[i] > 8) return 0;
+    if (f.smem <= 100 * 1024) return 1;
+    const int len = f.bluestein ? f.mb : f.m;
+    return (!f.gmem && len > 4096) ? 2 : 0;
+}
+
+// the plan's FFT arguments with the CTA size of the build that runs them
+template <int MAXT>
+static FftPlan fft_shape(const FftPlan& f) {
+    FftPlan g = f;
+    if (MAXT > 512) g.threads = MAXT;
+    return g;
 }
 
 // persistent grid of an FFT kernel: as many CTAs as fit on the device at
@@ -546,26 +562,26 @@ size_t fft_scratch_bytes(const shtc_plan* P) {
     return (size_t)f.gmem_ctas * 2 * len * sizeof(double2);
 }
 
-template <typename GT, int MAXR>
+template <typename GT, int MAXR, int MAXT = 512>
 static int launch_c2r_t(const shtc_plan* P, const double2* spec, GT* grid, long long gf,
                         long long grs, long long gcs, int nfield, int weighted,
                         cudaStream_t st, double2* gbuf) {
-    const FftPlan& f = P->fft;
+    const FftPlan f = fft_shape<MAXT>(P->fft);
     if (f.gmem && !gbuf) return SHTC_EWORK;
     int rc;
     const int jobs = f.mode == 0 ? P->npair : 2 * P->npair;
     const int nitems = jobs * nfield;
     int blocks = 0;
-    if ((rc = fft_launch_setup((const void*)k_fft_c2r<GT, MAXR>, f, nitems, &blocks))) return rc;
+    if ((rc = fft_launch_setup((const void*)k_fft_c2r<GT, MAXR, MAXT>, f, nitems, &blocks))) return rc;
     if (blocks == 0) return SHTC_OK;
     // synthesis uses the synthesis ring map (with the extend row and column);
     // the analysis adjoint uses the analysis ring map and ring weights
     if (weighted) {
-        k_fft_c2r<GT, MAXR><<<blocks, f.threads, f.smem, st>>>(
+        k_fft_c2r<GT, MAXR, MAXT><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, spec, grid, gf, grs, gcs, P->d_arowN,
             P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, 0, gbuf);
     } else {
-        k_fft_c2r<GT, MAXR><<<blocks, f.threads, f.smem, st>>>(
+        k_fft_c2r<GT, MAXR, MAXT><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, spec, grid, gf, grs, gcs, P->d_rowN,
             P->d_rowS, nullptr, nullptr, 1.0, P->lc, P->npair, P->extend, gbuf);
     }
@@ -575,12 +591,19 @@ static int launch_c2r_t(const shtc_plan* P, const double2* spec, GT* grid, long 
 int launch_fft_c2r(const shtc_plan* P, const double2* spec, void* grid, int dtype,
                    long long gf, long long grs, long long gcs, int nfield,
                    int weighted, cudaStream_t st, double2* gbuf) {
-    if (fft_lean(P->fft))
+    const int v = fft_variant(P->fft);
+    if (v == 1)
         return dtype == SHTC_F32
                    ? launch_c2r_t<float, 8>(P, spec, (float*)grid, gf, grs, gcs, nfield,
                                             weighted, st, gbuf)
                    : launch_c2r_t<double, 8>(P, spec, (double*)grid, gf, grs, gcs, nfield,
                                              weighted, st, gbuf);
+    if (v == 2)
+        return dtype == SHTC_F32
+                   ? launch_c2r_t<float, 8, 1024>(P, spec, (float*)grid, gf, grs, gcs, nfield,
+                                                  weighted, st, gbuf)
+                   : launch_c2r_t<double, 8, 1024>(P, spec, (double*)grid, gf, grs, gcs,
+                                                   nfield, weighted, st, gbuf);
     return dtype == SHTC_F32
                ? launch_c2r_t<float, 13>(P, spec, (float*)grid, gf, grs, gcs, nfield, weighted,
                                          st, gbuf)
@@ -588,28 +611,28 @@ int launch_fft_c2r(const shtc_plan* P, const double2* spec, void* grid, int dtyp
                                           weighted, st, gbuf);
 }
 
-template <typename GT, int MAXR>
+template <typename GT, int MAXR, int MAXT = 512>
 static int launch_r2c_t(const shtc_plan* P, const GT* grid, long long gf, long long grs,
                         long long gcs, double2* spec, int nfield, int weighted,
                         int fold_extend, cudaStream_t st, const GT* grid2, double2* gbuf) {
-    const FftPlan& f = P->fft;
+    const FftPlan f = fft_shape<MAXT>(P->fft);
     if (f.gmem && !gbuf) return SHTC_EWORK;
     int rc;
     const int jobs = f.mode == 0 ? P->npair : 2 * P->npair;
     const int nitems = jobs * nfield;
     int blocks = 0;
-    if ((rc = fft_launch_setup((const void*)k_fft_r2c<GT, MAXR>, f, nitems, &blocks))) return rc;
+    if ((rc = fft_launch_setup((const void*)k_fft_r2c<GT, MAXR, MAXT>, f, nitems, &blocks))) return rc;
     if (blocks == 0) return SHTC_OK;
     if (weighted) {
         // analysis: fcoef = (w * Re) / nlong, the reference's order of operations
         // is reproduced up to one rounding by folding 1/nlong into the weight
-        k_fft_r2c<GT, MAXR><<<blocks, f.threads, f.smem, st>>>(
+        k_fft_r2c<GT, MAXR, MAXT><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_arowN,
             P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, 0,
             grid2, gbuf);
     } else {
         // synthesis adjoint: plain (Re, -Im) of the rows of the cotangent
-        k_fft_r2c<GT, MAXR><<<blocks, f.threads, f.smem, st>>>(
+        k_fft_r2c<GT, MAXR, MAXT><<<blocks, f.threads, f.smem, st>>>(
             fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_rowN,
             P->d_rowS, nullptr, nullptr, 1.0, P->lc, P->npair, fold_extend, grid2, gbuf);
     }
@@ -620,22 +643,37 @@ static int launch_r2c_t(const shtc_plan* P, const GT* grid, long long gf, long l
 int launch_fft_r2c_product(const shtc_plan* P, const double* grid, const double* grid2,
                            long long gf, long long grs, long long gcs, double2* spec,
                            int nfield, cudaStream_t st, double2* gbuf) {
-    return fft_lean(P->fft)
-               ? launch_r2c_t<double, 8>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st, grid2,
-                                         gbuf)
-               : launch_r2c_t<double, 13>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st, grid2,
-                                          gbuf);
+    switch (fft_variant(P->fft)) {
+        case 1:
+            return launch_r2c_t<double, 8>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st,
+                                           grid2, gbuf);
+        case 2:
+            return launch_r2c_t<double, 8, 1024>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st,
+                                                 grid2, gbuf);
+        default:
+            return launch_r2c_t<double, 13>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st,
+                                            grid2, gbuf);
+    }
 }
 
 int launch_fft_r2c(const shtc_plan* P, const void* grid, int dtype, long long gf,
                    long long grs, long long gcs, double2* spec, int nfield,
                    int weighted, int fold_extend, cudaStream_t st, double2* gbuf) {
-    if (fft_lean(P->fft))
+    const int v = fft_variant(P->fft);
+    if (v == 1)
         return dtype == SHTC_F32
                    ? launch_r2c_t<float, 8>(P, (const float*)grid, gf, grs, gcs, spec, nfield,
                                             weighted, fold_extend, st, nullptr, gbuf)
                    : launch_r2c_t<double, 8>(P, (const double*)grid, gf, grs, gcs, spec,
                                              nfield, weighted, fold_extend, st, nullptr, gbuf);
+    if (v == 2)
+        return dtype == SHTC_F32
+                   ? launch_r2c_t<float, 8, 1024>(P, (const float*)grid, gf, grs, gcs, spec,
+                                                  nfield, weighted, fold_extend, st, nullptr,
+                                                  gbuf)
+                   : launch_r2c_t<double, 8, 1024>(P, (const double*)grid, gf, grs, gcs, spec,
+                                                   nfield, weighted, fold_extend, st, nullptr,
+                                                   gbuf);
     return dtype == SHTC_F32
                ? launch_r2c_t<float, 13>(P, (const float*)grid, gf, grs, gcs, spec, nfield,
                                          weighted, fold_extend, st, nullptr, gbuf)
@@ -727,8 +765,8 @@ k_unpack_coef_c(const double2* __restrict__ partial, int ntiles, double2* __rest
 }
 
 // persistent complex-grid FFT kernels over (job, field) items, as k_fft_c2r
-template <int MAXR>
-__global__ void __launch_bounds__(512, MAXR <= 8 ? 2 : 1)
+template <int MAXR, int MAXT = 512>
+__global__ void __launch_bounds__(MAXT, fft_min_ctas<MAXR, MAXT>())
 k_fft_c2c_synth(FftArgs F, int tw_smem, int jobs, int nitems,
                 const double2* __restrict__ spec, double2* __restrict__ grid, long long gf,
                 long long grs, long long gcs, const int* __restrict__ rowN,
@@ -743,8 +781,8 @@ k_fft_c2c_synth(FftArgs F, int tw_smem, int jobs, int nitems,
     }
 }
 
-template <int MAXR>
-__global__ void __launch_bounds__(512, MAXR <= 8 ? 2 : 1)
+template <int MAXR, int MAXT = 512>
+__global__ void __launch_bounds__(MAXT, fft_min_ctas<MAXR, MAXT>())
 k_fft_c2c_anal(FftArgs F, int tw_smem, int jobs, int nitems,
                const double2* __restrict__ grid, long long gf, long long grs, long long gcs,
                double2* __restrict__ spec, const int* __restrict__ rowN,
@@ -780,37 +818,37 @@ int launch_unpack_coef_c(const shtc_plan* P, const double2* partial, int ntiles,
     return map_cuda(cudaGetLastError());
 }
 
-template <int MAXR>
+template <int MAXR, int MAXT = 512>
 static int launch_c2c_synth_t(const shtc_plan* P, const double2* spec, double2* grid,
                               long long gf, long long grs, long long gcs, int nfield,
                               cudaStream_t st, double2* gbuf) {
-    const FftPlan& f = P->fft;
+    const FftPlan f = fft_shape<MAXT>(P->fft);
     if (f.gmem && !gbuf) return SHTC_EWORK;
     int rc;
     const int jobs = 2 * P->npair;
     const int nitems = jobs * nfield;
     int blocks = 0;
-    if ((rc = fft_launch_setup((const void*)k_fft_c2c_synth<MAXR>, f, nitems, &blocks))) return rc;
+    if ((rc = fft_launch_setup((const void*)k_fft_c2c_synth<MAXR, MAXT>, f, nitems, &blocks))) return rc;
     if (blocks == 0) return SHTC_OK;
-    k_fft_c2c_synth<MAXR><<<blocks, f.threads, f.smem, st>>>(
+    k_fft_c2c_synth<MAXR, MAXT><<<blocks, f.threads, f.smem, st>>>(
         fft_args(f), f.tw_smem, jobs, nitems, spec, grid, gf, grs, gcs, P->d_rowN,
         P->d_rowS, P->lc, P->npair, P->extend, gbuf);
     return map_cuda(cudaGetLastError());
 }
 
-template <int MAXR>
+template <int MAXR, int MAXT = 512>
 static int launch_c2c_anal_t(const shtc_plan* P, const double2* grid, long long gf,
                              long long grs, long long gcs, double2* spec, int nfield,
                              cudaStream_t st, double2* gbuf) {
-    const FftPlan& f = P->fft;
+    const FftPlan f = fft_shape<MAXT>(P->fft);
     if (f.gmem && !gbuf) return SHTC_EWORK;
     int rc;
     const int jobs = 2 * P->npair;
     const int nitems = jobs * nfield;
     int blocks = 0;
-    if ((rc = fft_launch_setup((const void*)k_fft_c2c_anal<MAXR>, f, nitems, &blocks))) return rc;
+    if ((rc = fft_launch_setup((const void*)k_fft_c2c_anal<MAXR, MAXT>, f, nitems, &blocks))) return rc;
     if (blocks == 0) return SHTC_OK;
-    k_fft_c2c_anal<MAXR><<<blocks, f.threads, f.smem, st>>>(
+    k_fft_c2c_anal<MAXR, MAXT><<<blocks, f.threads, f.smem, st>>>(
         fft_args(f), f.tw_smem, jobs, nitems, grid, gf, grs, gcs, spec, P->d_arowN,
         P->d_arowS, P->d_wN, P->d_wS, 1.0 / (double)P->nlon, P->lc, P->npair, gbuf);
     return map_cuda(cudaGetLastError());
@@ -819,17 +857,23 @@ static int launch_c2c_anal_t(const shtc_plan* P, const double2* grid, long long 
 int launch_fft_c2c_synth(const shtc_plan* P, const double2* spec, double2* grid,
                          long long gf, long long grs, long long gcs, int nfield,
                          cudaStream_t st, double2* gbuf) {
-    return fft_lean(P->fft)
-               ? launch_c2c_synth_t<8>(P, spec, grid, gf, grs, gcs, nfield, st, gbuf)
-               : launch_c2c_synth_t<13>(P, spec, grid, gf, grs, gcs, nfield, st, gbuf);
+    switch (fft_variant(P->fft)) {
+        case 1: return launch_c2c_synth_t<8>(P, spec, grid, gf, grs, gcs, nfield, st, gbuf);
+        case 2:
+            return launch_c2c_synth_t<8, 1024>(P, spec, grid, gf, grs, gcs, nfield, st, gbuf);
+        default: return launch_c2c_synth_t<13>(P, spec, grid, gf, grs, gcs, nfield, st, gbuf);
+    }
 }
 
 int launch_fft_c2c_anal(const shtc_plan* P, const double2* grid, long long gf,
                         long long grs, long long gcs, double2* spec, int nfield,
                         cudaStream_t st, double2* gbuf) {
-    return fft_lean(P->fft)
-               ? launch_c2c_anal_t<8>(P, grid, gf, grs, gcs, spec, nfield, st, gbuf)
-               : launch_c2c_anal_t<13>(P, grid, gf, grs, gcs, spec, nfield, st, gbuf);
+    switch (fft_variant(P->fft)) {
+        case 1: return launch_c2c_anal_t<8>(P, grid, gf, grs, gcs, spec, nfield, st, gbuf);
+        case 2:
+            return launch_c2c_anal_t<8, 1024>(P, grid, gf, grs, gcs, spec, nfield, st, gbuf);
+        default: return launch_c2c_anal_t<13>(P, grid, gf, grs, gcs, spec, nfield, st, gbuf);
+    }
 }
 
 // ---------------------------------------------------------------------------
