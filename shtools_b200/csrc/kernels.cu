@@ -408,9 +408,21 @@ int launch_legendre_synth(const shtc_plan* P, const double2* packed,
     return map_cuda(cudaGetLastError());
 }
 
+// The tensor-path analysis (anal_mma.cu) takes 8 or more fields on grids
+// with at least one full tile of ring pairs
+static bool anal_use_mma(const shtc_plan* P, int nfield) {
+    return nfield >= 8 && P->npair >= anal_mma_pairs();
+}
+
 // analysis CTA shape for nfield (internal) fields: T pairs per thread, W warps
 static void anal_shape(const shtc_plan* P, int nfield, int* T, int* W, int* tiles) {
     const int np = P->npair;
+    if (anal_use_mma(P, nfield)) {
+        *T = 1;
+        *W = anal_mma_pairs() / 32;
+        *tiles = (np + anal_mma_pairs() - 1) / anal_mma_pairs();
+        return;
+    }
     int w = P->tune_anal_W ? P->tune_anal_W : 2;
     int t = P->tune_anal_T;
     if (t == 0) {
@@ -478,6 +490,8 @@ int launch_legendre_anal(const shtc_plan* P, const double2* spec,
     int T, W, tiles;
     anal_shape(P, nfield, &T, &W, &tiles);
     if (tiles != ntiles_out) return SHTC_EBOUND;
+    if (anal_use_mma(P, nfield))
+        return launch_legendre_anal_mma(P, spec, partial, tiles, nfield, st);
     switch (T) {
         case 8: return launch_anal_nf<8>(P, spec, partial, nfield, W, tiles, st);
         case 4: return launch_anal_nf<4>(P, spec, partial, nfield, W, tiles, st);

@@ -136,6 +136,11 @@ int launch_unpack_coef(const shtc_plan* P, const double2* partial, int ntiles,
                        long long sm, int cdim, int nfield, int normalise,
                        cudaStream_t st);
 int anal_tiles(const shtc_plan* P, int nfield);
+// anal_mma.cu: the analysis of 8 or more fields on the FP64 tensor path,
+// tiles of anal_mma_pairs() ring pairs, output as launch_legendre_anal
+int anal_mma_pairs();
+int launch_legendre_anal_mma(const shtc_plan* P, const double2* spec, double2* partial,
+                             int ntiles, int nfield, cudaStream_t st);
 // complex plans: cilm (nfield, 2, cdim, cdim) and grids of interleaved complex
 // doubles, strides in complex elements; internal fields 2u (+m), 2u+1 (-m)
 int launch_pack_coef_c(const shtc_plan* P, const double2* cilm, long long sf, long long sk,

@@ -226,7 +226,9 @@ def test_linearity_batched(cuda, oracle):
 def test_field_groups_equal_single_fields(cuda, oracle, nf, kind, L):
     """Fields analysed together (groups of 4 or 2 sharing one recursion) give
     bit-identical coefficients to the same fields analysed one at a time:
-    the per-field sums run in the same order in every kernel variant."""
+    the per-field sums run in the same order in every scalar kernel variant.
+    8 or more fields on 256 or more ring pairs take the tensor path, whose
+    sums run in another order: there the fields agree to 1e-13 per degree."""
     if L > 1000 and nf not in (4, 5):
         pytest.skip("large case: one grouped and one ragged count")
     cs = np.stack([oracle.power_law_cilm(L, 300 + i) for i in range(nf)])
@@ -239,8 +241,14 @@ def test_field_groups_equal_single_fields(cuda, oracle, nf, kind, L):
         g = cuda.MakeGridDH(ct, sampling=1)
         b = cuda.SHExpandDH(g, sampling=1)
         singles = [cuda.SHExpandDH(g[i], sampling=1) for i in range(nf)]
+    npair = L + 2 if kind == "dh" else (L + 2) // 2
+    tensor_path = nf >= 8 and npair >= 256
     for i in range(nf):
-        assert torch.equal(b[i], singles[i]), (i, (b[i] - singles[i]).abs().max().item())
+        if tensor_path:
+            d = perdeg(b[i].cpu().numpy(), singles[i].cpu().numpy())
+            assert d.max() <= 1e-13, (i, d.max())
+        else:
+            assert torch.equal(b[i], singles[i]), (i, (b[i] - singles[i]).abs().max().item())
     e = perdeg(b[-1].cpu().numpy(), cs[-1])
     assert e.max() < 1e-9
 
