@@ -408,7 +408,7 @@ int launch_legendre_synth(const shtc_plan* P, const double2* packed,
     return map_cuda(cudaGetLastError());
 }
 
-// The tensor-path analysis (anal_mma.cu) takes 8 or more fields on grids
+// The tensor-path analysis (legendre_mma.cu) takes 8 or more fields on grids
 // with at least one full tile of ring pairs
 static bool anal_use_mma(const shtc_plan* P, int nfield) {
     return nfield >= 8 && P->npair >= anal_mma_pairs();

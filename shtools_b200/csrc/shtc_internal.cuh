@@ -136,7 +136,7 @@ int launch_unpack_coef(const shtc_plan* P, const double2* partial, int ntiles,
                        long long sm, int cdim, int nfield, int normalise,
                        cudaStream_t st);
 int anal_tiles(const shtc_plan* P, int nfield);
-// anal_mma.cu: the analysis of 8 or more fields on the FP64 tensor path,
+// legendre_mma.cu: the analysis of 8 or more fields on the FP64 tensor path,
 // tiles of anal_mma_pairs() ring pairs, output as launch_legendre_anal
 int anal_mma_pairs();
 int launch_legendre_anal_mma(const shtc_plan* P, const double2* spec, double2* partial,
