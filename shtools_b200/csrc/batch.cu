@@ -151,8 +151,8 @@ k_batch_synth(const BatchGroup* __restrict__ G, const int4* __restrict__ items,
 __global__ void __launch_bounds__(32 * kBatchAnalWarps)
 k_batch_anal(const BatchGroup* __restrict__ G, const int4* __restrict__ items,
              int nitems, int* __restrict__ counter, double2* __restrict__ work) {
-    extern __shared__ double smem_anal[];
-    __shared__ __align__(16) double2 rstage[2][kAnalChunk];
+    extern __shared__ __align__(16) double smem_anal[];
+    __shared__ __align__(16) double2 rstage[2][kAnalStage];
     __shared__ int s_item;
     for (;;) {
         const int i = next_item(counter, &s_item);

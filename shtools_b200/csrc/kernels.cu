@@ -139,8 +139,8 @@ k_legendre_anal(const double2* __restrict__ rec, const double* __restrict__ pmm,
                 const double* __restrict__ rtab, const double* __restrict__ zp,
                 const double2* __restrict__ spec, double2* __restrict__ partial,
                 int lc, int npair, long long nlm, int nfield) {
-    extern __shared__ double smem_anal[];
-    __shared__ __align__(16) double2 rstage[2][kAnalChunk];
+    extern __shared__ __align__(16) double smem_anal[];
+    __shared__ __align__(16) double2 rstage[2][kAnalStage];
     const int f0 = blockIdx.z * NF;
     const long long sstride = (long long)npair * (lc + 1) * 2;
     anal_order<T, NF>(smem_anal, rstage, rec, pmm, rtab, zp, spec + f0 * sstride, sstride,
@@ -154,8 +154,8 @@ k_legendre_anal_capped(const double2* __restrict__ rec, const double* __restrict
                 const double* __restrict__ rtab, const double* __restrict__ zp,
                 const double2* __restrict__ spec, double2* __restrict__ partial,
                 int lc, int npair, long long nlm, int nfield) {
-    extern __shared__ double smem_anal[];
-    __shared__ __align__(16) double2 rstage[2][kAnalChunk];
+    extern __shared__ __align__(16) double smem_anal[];
+    __shared__ __align__(16) double2 rstage[2][kAnalStage];
     const int f0 = blockIdx.z * NF;
     const long long sstride = (long long)npair * (lc + 1) * 2;
     anal_order<T, NF>(smem_anal, rstage, rec, pmm, rtab, zp, spec + f0 * sstride, sstride,

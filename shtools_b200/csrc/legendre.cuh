@@ -97,14 +97,21 @@ __device__ __forceinline__ void synth_step(bool odd, double2 f, const double2* c
 }
 
 // Per degree the item needs {ff1, ff2} and NF x {C, S} (16 bytes each);
-// chunks of kSynthChunk degrees are copied into shared memory with cp.async
-// one chunk ahead of their use.
+// chunks of kSynthChunk degrees are copied into shared memory with cp.async.
+// Up to 4 fields: three buffers, each chunk copied two chunks ahead of its
+// use and the copy issued after the barrier that ends the buffer's last
+// use, so one CTA barrier per chunk suffices (on B200 2.5% faster for one
+// field at lmax 2047, 1% for the 4-field groups of the batched launch, the
+// same for 2 fields).  8 fields: two buffers, one chunk ahead, two barriers
+// per chunk (three buffers measured 2.5-4.5% slower at lmax 719 and 2799).
 constexpr int kSynthChunk = 32;
 static_assert(kSynthChunk % kRecSegment == 0, "chunks hold whole segments");
 
+__host__ __device__ constexpr int synth_buffers(int NF) { return NF <= 4 ? 3 : 2; }
+
 template <int NF>
 struct SynthStage {
-    double2 buf[2][kSynthChunk * (1 + NF)];
+    double2 buf[synth_buffers(NF)][kSynthChunk * (1 + NF)];
 };
 
 // Synthesis of order m for the ring pairs of tile `tile` and the fields
@@ -129,6 +136,7 @@ __device__ __forceinline__ void synth_order(
     int f0, int nvalid, const double2* __restrict__ radq = nullptr,
     const double* __restrict__ qtab = nullptr, int nseg = 0) {
     constexpr int R = 1 + NF;                       // 16-byte items per degree
+    constexpr int NB = synth_buffers(NF);
     const int p0 = tile * (blockDim.x * T) + threadIdx.x;
     double z[T], qs[T], qstep[T], lq[T];
     int pv[T];
@@ -159,7 +167,7 @@ __device__ __forceinline__ void synth_order(
     const int nchunks = (nsteps + kSynthChunk - 1) / kSynthChunk;
 
     auto load_chunk = [&](int c) {
-        double2* dst = sm.buf[c & 1];
+        double2* dst = sm.buf[c % NB];
         const int s0 = 1 + c * kSynthChunk;
         for (int it = threadIdx.x; it < kSynthChunk * R; it += blockDim.x) {
             const int k = it / R, j = it - k * R;
@@ -171,6 +179,7 @@ __device__ __forceinline__ void synth_order(
         cp_async_commit();
     };
     if (nchunks > 0) load_chunk(0);
+    if (NB == 3 && nchunks > 1) load_chunk(1);
 
     const double start = pmm[m];
     double q1[T], q2[T];
@@ -190,14 +199,20 @@ __device__ __forceinline__ void synth_order(
     for (int t = 0; t < T; ++t) { q1[t] = start; q2[t] = 0.0; }
 
     for (int c = 0; c < nchunks; ++c) {
-        if (c + 1 < nchunks) {
-            load_chunk(c + 1);
-            cp_async_wait<1>();
+        if constexpr (NB == 3) {
+            if (c + 1 < nchunks) cp_async_wait<1>(); else cp_async_wait<0>();
+            __syncthreads();
+            if (c + 2 < nchunks) load_chunk(c + 2);
         } else {
-            cp_async_wait<0>();
+            if (c + 1 < nchunks) {
+                load_chunk(c + 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
         }
-        __syncthreads();
-        const double2* st = sm.buf[c & 1];
+        const double2* st = sm.buf[c % NB];
         const int cn = min(kSynthChunk, nsteps - c * kSynthChunk);
         // s = 1 + c*kSynthChunk + k: odd for even k (the chunk length is even)
         // segments end at s = 32c + 16 and 32c + 32, i.e. k = 15 and 31
@@ -225,8 +240,9 @@ __device__ __forceinline__ void synth_order(
                     rec_rescale<T>(st[k * R].y, q1, q2);
             }
         }
-        __syncthreads();
+        if constexpr (NB == 2) __syncthreads();
     }
+    if constexpr (NB == 3) __syncthreads();
 
     const double h = m ? 0.5 : 1.0;
 #pragma unroll
@@ -264,9 +280,16 @@ __device__ __forceinline__ void synth_order(
 // to partial[tile][field][...] and the unpack kernel adds them, again in a
 // fixed order.  NF fields share one recursion: per degree a lane does 2T
 // recursion operations and 2*T*NF multiply-adds.
-constexpr int kAnalChunk = 16;   // degrees per stage of staged {beta, D}
-constexpr int kAnalPad = 33;
-static_assert(kAnalChunk == kRecSegment, "segment ends fall on stage starts");
+constexpr int kAnalChunk = 16;   // degrees per transpose of one field (NF = 1)
+// row pitch of the per-warp transpose, in doubles: even, so every row starts
+// on 16 bytes and is summed with 16-byte loads; with 34 the 8 lanes of each
+// load phase hit disjoint banks
+constexpr int kAnalPad = 34;
+static_assert(kAnalChunk == kRecSegment, "segment ends fall on chunk starts");
+// degrees per stage of staged {beta, D} and per CTA barrier: 32 measured 2%
+// faster than 16 at lmax 2047 (no gain at 64)
+constexpr int kAnalStage = 32;
+static_assert(kAnalStage % kRecSegment == 0, "stages hold whole segments");
 
 // degrees per transpose chunk for NF fields: 2*NF*CH = 32 rows, one per lane
 __host__ __device__ constexpr int anal_chunk(int NF) { return kAnalChunk / NF; }
@@ -274,7 +297,7 @@ __host__ __device__ constexpr int anal_chunk(int NF) { return kAnalChunk / NF; }
 // dynamic shared memory of an analysis CTA of W warps for NF fields
 __host__ __device__ inline size_t anal_smem_bytes(int W, int NF) {
     return (size_t)W * 32 * kAnalPad * sizeof(double) +             // per-warp transpose
-           (size_t)2 * W * (2 * NF * kAnalChunk) * sizeof(double);  // per-warp stage sums x2
+           (size_t)2 * W * (2 * NF * kAnalStage) * sizeof(double);  // per-warp stage sums x2
 }
 
 // one degree step for T ring pairs and NF fields: the lane's sums over its
@@ -311,20 +334,22 @@ __device__ __forceinline__ void anal_step(bool odd, double2 fr, const double* z,
 //   sp:   spec of field f0, [pair][m][ring]; field j at sp + j*sstride
 //   outp: the tile's packed {C, S} sums of field f0, [packed (l, m)];
 //         field j at outp + j*ostride
-// smem: anal_smem_bytes(W, NF) bytes; rstage: 2 x kAnalChunk staged
-// {beta, D}.  Degrees go in stages of kAnalChunk (one CTA barrier each),
-// each stage in NF transpose chunks of kAnalChunk/NF degrees (warp-local).
+// smem: anal_smem_bytes(W, NF) bytes, 16-byte aligned; rstage: 2 x kAnalStage staged
+// {beta, D}.  Degrees go in stages of kAnalStage (one CTA barrier each),
+// each stage in transpose chunks of kAnalChunk/NF degrees (warp-local); the
+// recursion is rescaled at the first step of every chunk that starts a
+// segment.
 // Ends with the tile's sums written by warp 0 after a barrier; the caller
 // must pass another barrier before reusing the shared memory.
 template <int T, int NF>
 __device__ __forceinline__ void anal_order(
-    double* smem, double2 (*rstage)[kAnalChunk], const double2* __restrict__ rec,
+    double* smem, double2 (*rstage)[kAnalStage], const double2* __restrict__ rec,
     const double* __restrict__ pmm, const double* __restrict__ rtab,
     const double* __restrict__ zp, const double2* __restrict__ sp, long long sstride,
     double2* __restrict__ outp, long long ostride, int lc, int npair, int m, int tile,
     int nvalid) {
     constexpr int CH = anal_chunk(NF);
-    constexpr int SROWS = 2 * NF * kAnalChunk;   // (field, Re/Im, degree) rows per stage
+    constexpr int SROWS = 2 * NF * kAnalStage;   // (field, Re/Im, degree) rows per stage
     static_assert(2 * NF * CH == 32, "one transpose row per lane");
     const int nwarps = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5;
@@ -344,10 +369,12 @@ __device__ __forceinline__ void anal_order(
     const long long o = packed_off(m, lc);
     const double2* __restrict__ rm = rec + o;
     const int nsteps = lc - m + 1;   // degrees l = m .. lc, s = l - m
-    const int nstages = (nsteps + kAnalChunk - 1) / kAnalChunk;
+    const int nstages = (nsteps + kAnalStage - 1) / kAnalStage;
+    // the first warp copies a stage: kAnalStage = 32 entries, one per lane
+    static_assert(kAnalStage == 32, "one stage entry per lane of a warp");
     auto load_stage = [&](int c) {
-        const int sidx = c * kAnalChunk + threadIdx.x;
-        if (threadIdx.x < kAnalChunk && sidx < nsteps)
+        const int sidx = c * kAnalStage + threadIdx.x;
+        if (threadIdx.x < kAnalStage && sidx < nsteps)
             cp_async16(&rstage[c & 1][threadIdx.x], &rm[sidx]);
         cp_async_commit();
     };
@@ -381,13 +408,13 @@ __device__ __forceinline__ void anal_order(
     __syncthreads();
     int buf = 0;
     for (int sg = 0; sg < nstages; ++sg) {
-        const int s0 = sg * kAnalChunk;
+        const int s0 = sg * kAnalStage;
         const double2* stg = rstage[sg & 1];
         double* ws = wsum + (buf * nwarps + warp) * SROWS;
-        // the stage starts at s0, a multiple of kRecSegment: the first step
-        // ends a recursion segment (D(0) = 1 for the first stage)
+        // a chunk whose first degree is a multiple of kRecSegment starts by
+        // ending a recursion segment (D(0) = 1 for the first one)
 #pragma unroll 1
-        for (int ci = 0; ci < NF; ++ci) {
+        for (int ci = 0; ci < kAnalStage / CH; ++ci) {
             const int c0 = s0 + ci * CH;
             const int cn = min(CH, nsteps - c0);
             if (cn <= 0) break;
@@ -399,7 +426,7 @@ __device__ __forceinline__ void anal_order(
                 for (int k = 0; k < CH; ++k) {
                     anal_step<T, NF>((k & 1) != 0, wcoef[k], z, q1, q2, gsR, gsI, gaR, gaI,
                                      accR, accI);
-                    if (k == 0 && ci == 0) rec_rescale<T>(wcoef[0].y, q1, q2);
+                    if (k == 0 && ci % NF == 0) rec_rescale<T>(wcoef[0].y, q1, q2);
 #pragma unroll
                     for (int j = 0; j < NF; ++j) {
                         tb[((2 * j + 0) * CH + k) * kAnalPad + lane] = accR[j];
@@ -410,7 +437,7 @@ __device__ __forceinline__ void anal_order(
                 for (int k = 0; k < cn; ++k) {
                     anal_step<T, NF>((k & 1) != 0, wcoef[k], z, q1, q2, gsR, gsI, gaR, gaI,
                                      accR, accI);
-                    if (k == 0 && ci == 0) rec_rescale<T>(wcoef[0].y, q1, q2);
+                    if (k == 0 && ci % NF == 0) rec_rescale<T>(wcoef[0].y, q1, q2);
 #pragma unroll
                     for (int j = 0; j < NF; ++j) {
                         tb[((2 * j + 0) * CH + k) * kAnalPad + lane] = accR[j];
@@ -426,13 +453,19 @@ __device__ __forceinline__ void anal_order(
                 const double* b = tb + lane * kAnalPad;
                 double sum = 0.0;
                 if (k < cn) {
+                    // element q of the row goes to partial sum q % 4
                     double s4[4] = {0.0, 0.0, 0.0, 0.0};
+                    const double2* b2 = reinterpret_cast<const double2*>(b);
 #pragma unroll
-                    for (int q = 0; q < 32; ++q) s4[q & 3] += b[q];
+                    for (int q = 0; q < 16; ++q) {
+                        const double2 v = b2[q];
+                        s4[(2 * q) & 3] += v.x;
+                        s4[(2 * q + 1) & 3] += v.y;
+                    }
                     sum = ((s4[0] + s4[1]) + (s4[2] + s4[3])) * wcoef[k].y;   // Q -> P sums
                 }
-                // stage row layout: (2*field + Re/Im)*kAnalChunk + degree in stage
-                ws[(lane / CH) * kAnalChunk + ci * CH + k] = sum;
+                // stage row layout: (2*field + Re/Im)*kAnalStage + degree in stage
+                ws[(lane / CH) * kAnalStage + ci * CH + k] = sum;
             }
             __syncwarp();
         }
@@ -442,12 +475,12 @@ __device__ __forceinline__ void anal_order(
         __syncthreads();
         if (sg + 2 < nstages) load_stage(sg + 2);
         if (warp == 0) {
-            const int sn = min(kAnalChunk, nsteps - s0);
+            const int sn = min(kAnalStage, nsteps - s0);
 #pragma unroll
             for (int i = 0; i < SROWS / 32; ++i) {
                 const int r = lane + 32 * i;
-                const int k = r % kAnalChunk;
-                const int fc = r / kAnalChunk;   // 2*field + Re/Im
+                const int k = r % kAnalStage;
+                const int fc = r / kAnalStage;   // 2*field + Re/Im
                 double sum = 0.0;
                 for (int w = 0; w < nwarps; ++w) sum += wsum[(buf * nwarps + w) * SROWS + r];
                 if (k < sn && (fc >> 1) < nvalid) {
