@@ -7,7 +7,9 @@ runs a sequence of such steps on three streams instead: uploads on one, the
 transform on the caller's current stream, downloads on a third, with
 ``depth`` sets of device input buffers in rotation, so that the upload of
 step i+1 and the download of step i-1 overlap the transform of step i (PCIe
-is full duplex).
+is full duplex).  Steps may differ in the shapes of their inputs: splitting
+a synthesis + analysis pair into two steps lets the synthesis start once the
+coefficients are on the device, while the grid is still being uploaded.
 
     from shtools_b200 import MakeGridGLQ, SHExpandGLQ
     from shtools_b200.pipeline import pipelined
@@ -25,7 +27,10 @@ def pipelined(fn, host_inputs, host_outputs, device=None, depth=2):
     (a tuple of device tensors), and copy ``outs`` into the pinned host
     tensors of ``host_outputs[i]``.  Returns once every copy is queued; the
     host outputs are valid after ``torch.cuda.synchronize()``.  A host
-    output tensor reused by a later step is overwritten in step order."""
+    output tensor reused by a later step is overwritten in step order.
+    Device input buffers are kept per input signature (the shapes and
+    dtypes of a step's inputs), ``depth`` sets of each, so steps of
+    different kinds may alternate."""
     if len(host_inputs) != len(host_outputs):
         raise ValueError("host_inputs and host_outputs differ in length")
     if depth < 1:
@@ -37,26 +42,35 @@ def pipelined(fn, host_inputs, host_outputs, device=None, depth=2):
     comp = torch.cuda.current_stream(dev)
     s_in = torch.cuda.Stream(dev)
     s_out = torch.cuda.Stream(dev)
-    first = host_inputs[0]
-    bufs = [tuple(torch.empty(t.shape, dtype=t.dtype, device=dev) for t in first)
-            for _ in range(depth)]
-    free = [torch.cuda.Event() for _ in range(depth)]   # buffer k consumed
-    for e in free:
-        e.record(comp)
+    sig = lambda hin: tuple((tuple(t.shape), t.dtype) for t in hin)
+    # signature -> [buffer sets, "set consumed" events (None before the first
+    # use), steps so far]; every buffer is allocated on the caller's stream
+    # before any step is queued, and a first use waits for the work queued
+    # there before this call only
+    pools = {}
+    for hin in host_inputs:
+        if sig(hin) not in pools:
+            pools[sig(hin)] = [
+                [tuple(torch.empty(t.shape, dtype=t.dtype, device=dev) for t in hin)
+                 for _ in range(depth)], [None] * depth, 0]
+    start = torch.cuda.Event()
+    start.record(comp)
     for i, (hin, hout) in enumerate(zip(host_inputs, host_outputs)):
-        k = i % depth
+        pool = pools[sig(hin)]
+        bufs, free, n = pool
+        k = n % depth
+        pool[2] = n + 1
         loaded = torch.cuda.Event()
         with torch.cuda.stream(s_in):
-            s_in.wait_event(free[k])
+            s_in.wait_event(start if free[k] is None else free[k])
             for d, h in zip(bufs[k], hin):
-                if d.shape != h.shape or d.dtype != h.dtype:
-                    raise ValueError("every step's inputs must match the first step's")
                 d.copy_(h, non_blocking=True)
             loaded.record(s_in)
         comp.wait_event(loaded)
         outs = fn(*bufs[k])
         if isinstance(outs, torch.Tensor):
             outs = (outs,)
+        free[k] = torch.cuda.Event()
         free[k].record(comp)
         done = torch.cuda.Event()
         done.record(comp)
@@ -70,6 +84,7 @@ def pipelined(fn, host_inputs, host_outputs, device=None, depth=2):
     end = torch.cuda.Event()
     end.record(s_out)
     comp.wait_event(end)
-    for b in bufs:
-        for d in b:
-            d.record_stream(s_in)
+    for bufs, _, _ in pools.values():
+        for b in bufs:
+            for d in b:
+                d.record_stream(s_in)

@@ -32,3 +32,24 @@ def test_pipelined_reused_outputs_and_errors(cuda, oracle):
     assert torch.equal(out[0], cuda.MakeGridGLQ(c.cuda()).cpu())
     with pytest.raises(ValueError):
         pipelined(lambda x: x, [(c,)], [], depth=2)
+
+
+def test_pipelined_alternating_step_kinds(cuda, oracle):
+    """Synthesis and analysis as separate steps of one pipeline (inputs of
+    two shapes, each with its own rotation of device buffers): the same
+    results as the transforms run one at a time."""
+    from shtools_b200.pipeline import pipelined
+    L = 95
+    cs = [torch.from_numpy(oracle.power_law_cilm(L, 60 + i)).pin_memory() for i in range(3)]
+    grids = [cuda.MakeGridGLQ(c.cuda()).cpu().pin_memory() for c in cs]
+    ins, outs = [], []
+    for i in range(3):
+        ins += [(cs[i],), (grids[2 - i],)]
+        outs += [(torch.empty_like(grids[0]).pin_memory(),),
+                 (torch.empty_like(cs[0]).pin_memory(),)]
+    fn = lambda t: cuda.MakeGridGLQ(t) if t.dim() == 3 else cuda.SHExpandGLQ(t)
+    pipelined(fn, ins, outs, depth=2)
+    torch.cuda.synchronize()
+    for i in range(3):
+        assert torch.equal(outs[2 * i][0], grids[i])
+        assert torch.equal(outs[2 * i + 1][0], cuda.SHExpandGLQ(grids[2 - i].cuda()).cpu())
