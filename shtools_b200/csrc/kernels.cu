@@ -313,7 +313,7 @@ std::map<std::tuple<int, const void*, int, size_t>, int> g_resident;
 // the dynamic shared memory limit of kernel fn raised to smem; with
 // max_shared the largest carveout is preferred (kernels that live on shared
 // memory, so that registers, not the L1 split, limit the resident CTAs)
-static int kernel_smem_attr(const void* fn, size_t smem, bool max_shared) {
+int kernel_smem_attr(const void* fn, size_t smem, bool max_shared) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return map_cuda(e);

@@ -136,6 +136,10 @@ int launch_unpack_coef(const shtc_plan* P, const double2* partial, int ntiles,
                        long long sm, int cdim, int nfield, int normalise,
                        cudaStream_t st);
 int anal_tiles(const shtc_plan* P, int nfield);
+// kernels.cu: raise the dynamic shared memory limit of kernel fn to smem
+// (with max_shared, prefer the largest carveout); set once per device and
+// kernel, later calls return at once
+int kernel_smem_attr(const void* fn, size_t smem, bool max_shared);
 // legendre_mma.cu: the analysis of 8 or more fields on the FP64 tensor path,
 // tiles of anal_mma_pairs() ring pairs, output as launch_legendre_anal
 int anal_mma_pairs();
