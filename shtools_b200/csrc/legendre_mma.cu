@@ -6,7 +6,7 @@
 // Re/Im), G the symmetric (l - m even) or antisymmetric (odd) combination of
 // the pair's two rings times the ring weight (SHExpandDH.f95:463-580,
 // SHExpandGLQ.f95:445-649).  The scalar kernel (legendre.cuh, anal_order)
-// runs the recursion once per group of at most two fields and reduces every
+// runs the recursion once per group of at most four fields and reduces every
 // degree across the lanes; here each lane runs the recursion for one pair,
 // once for all the fields of the CTA, writes its 16 values of a recursion
 // segment to shared memory, and the warp multiplies them by the pair
@@ -43,8 +43,8 @@ constexpr int kMmaPitch = 34;                   // doubles per degree row of a w
 // volatile, so the compiler may interleave it with the recursion
 __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
     asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-                 : "+d"(d[0]), "+d"(d[1])
-                 : "d"(a), "d"(b));
+        : "+d"(d[0]), "+d"(d[1])
+        : "d"(a), "d"(b));
 }
 
 // row pitch (doubles) of a warp's partial sums for NT column tiles: 8 NT + 4,
