@@ -35,23 +35,23 @@ sys.path.insert(0, ROOT)
 METRIC = "transforms/s at lmax 2047 & 2799: mixed-prec vs FP64 GPU, rel err vs FP64"
 
 WORKLOADS = {
-    # config 2: plain FP64 GLQ, single field, lmax 2047, 2048 x 4095 grid
+    # the headline workload: plain FP64 GLQ, single field, lmax 2047, 2048 x
+    # 4095 grid
     "glq2047": dict(kind="glq", lmax=2047, nfield=1, sampling=1, beta=2.0,
                     seed=2000),
-    # config 5 shape in FP64: 16 DH fields, lmax 2799, sampling 2
+    # 16 DH fields, lmax 2799, sampling 2, FP64 grids
     "dh2799x16": dict(kind="dh", lmax=2799, nfield=16, sampling=2, beta=3.0,
                       seed=5000),
-    # config 3 shape: 8 DH fields, lmax 719, sampling 2
+    # 8 DH fields, lmax 719, sampling 2
     "dh719x8": dict(kind="dh", lmax=719, nfield=8, sampling=2, beta=2.0,
                     seed=3000),
-    # complex DH (MakeGridDHC / SHExpandDHC), config 3 shape: 8 fields,
-    # lmax 719, sampling 2
+    # complex DH (MakeGridDHC / SHExpandDHC): 8 fields, lmax 719, sampling 2
     "dhc719x8": dict(kind="dhc", lmax=719, nfield=8, sampling=2, beta=2.0,
                      seed=3500),
-    # MakeGradientDH, config 3 shape: 8 fields, lmax 719, sampling 2
+    # MakeGradientDH: 8 fields, lmax 719, sampling 2
     "gradient719x8": dict(kind="gradient", lmax=719, nfield=8, sampling=2, beta=2.0,
                           seed=3700),
-    # MakeGravGridDH, config 3 shape: 8 fields, lmax 719, sampling 2, on a
+    # MakeGravGridDH: 8 fields, lmax 719, sampling 2, on a
     # rotating ellipsoid with the normal gravity removed
     "gravity719x8": dict(kind="gravity", lmax=719, nfield=8, sampling=2, beta=2.0,
                          seed=3800),
@@ -59,15 +59,15 @@ WORKLOADS = {
     # GLQ grid of the headline configuration, 2048 x 4095)
     "multiply1024": dict(kind="multiply", lmax=1024, lmax2=1023, nfield=1, sampling=1,
                          beta=2.0, seed=2100),
-    # config 1 shape: one DH field, lmax 255, sampling 2
+    # one DH field, lmax 255, sampling 2
     "dh255": dict(kind="dh", lmax=255, nfield=1, sampling=2, beta=2.0,
                   seed=1000),
-    # config 5: 16 DH fields, lmax 2799, sampling 2, float32 grids and float64
+    # 16 DH fields, lmax 2799, sampling 2, float32 grids and float64
     # coefficients; synthesis, analysis and the adjoint backward of a
     # weighted L2 misfit per step (3 transforms per field)
     "dh2799x16_grad": dict(kind="dh_grad", lmax=2799, nfield=16, sampling=2,
                            beta=3.0, seed=5000),
-    # config 4: 4096 GLQ fields of lmax ~ U{31..511}, each on its own grid,
+    # 4096 GLQ fields of lmax ~ U{31..511}, each on its own grid,
     # one persistent Legendre launch per direction, replayed as CUDA graphs
     "glq_uneven4096": dict(kind="glq_batch", lmax=511, lmin=31, nfield=4096,
                            sampling=1, beta=2.0, seed=4000),

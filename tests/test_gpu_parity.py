@@ -272,7 +272,8 @@ def test_preglq_dhaj_gpu(cuda, oracle):
 
 def test_odd_lengths_bluestein(cuda, oracle):
     """GLQ grids whose longitude FFT length 2*lmax+1 has a prime factor above
-    13 go through Bluestein's algorithm (config 4 sizes)."""
+    13 go through Bluestein's algorithm (sizes of the uneven-lmax batch,
+    lmax 31..511)."""
     for L in (31, 36, 58, 100, 256, 509):
         c = oracle.power_law_cilm(L, 4000 + L)
         z, w = oracle.shglq(L)
