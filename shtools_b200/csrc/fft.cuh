@@ -195,6 +195,59 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
     }
 }
 
+// The same pass with its inputs read through ld(i) and its outputs written
+// through st(i, v): the first pass of a transform reading a grid row or the
+// last one writing it, without a staging copy through shared memory.  Reads
+// x[j + q nr] and writes y[j' + q ns] are coalesced across the threads for
+// each q: the first pass (ns = 1) reads and the last pass (ns = M/R, where
+// d = j) writes contiguous runs.
+template <int R, int SIGN, typename Ld, typename St>
+__device__ __forceinline__ void fft_pass_io(Ld ld, St st, int M, int ns,
+                                            const double2* __restrict__ tw) {
+    const int nr = M / R;
+    const int kstep = (int)(blockDim.x % (unsigned)ns);
+    int k = (int)(threadIdx.x % (unsigned)ns);
+    for (int j = threadIdx.x; j < nr; j += blockDim.x) {
+        double2 v[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = ld(j + q * nr);
+        if (k != 0) {
+            double2 wp[R];
+            wp[1] = twv<SIGN>(tw, k);
+#pragma unroll
+            for (int q = 2; q < R; ++q) wp[q] = cmul(wp[q / 2], wp[q - q / 2]);
+#pragma unroll
+            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], wp[q]);
+        }
+        dft_small<R, SIGN>(v);
+        const int d = (j - k) * R + k;
+#pragma unroll
+        for (int q = 0; q < R; ++q) st(d + q * ns, v[q]);
+        k += kstep;
+        if (k >= ns) k -= ns;
+    }
+}
+
+template <int SIGN, int MAXR, typename Ld, typename St>
+__device__ __forceinline__ void fft_pass_io_r(int r, Ld ld, St st, int M, int ns,
+                                              const double2* __restrict__ t) {
+    switch (r) {
+        case 2: fft_pass_io<2, SIGN>(ld, st, M, ns, t); break;
+        case 3: fft_pass_io<3, SIGN>(ld, st, M, ns, t); break;
+        case 4: fft_pass_io<4, SIGN>(ld, st, M, ns, t); break;
+        case 8: fft_pass_io<8, SIGN>(ld, st, M, ns, t); break;
+        case 5: fft_pass_io<5, SIGN>(ld, st, M, ns, t); break;
+        case 7: fft_pass_io<7, SIGN>(ld, st, M, ns, t); break;
+        case 11:
+            if constexpr (MAXR >= 11) fft_pass_io<11, SIGN>(ld, st, M, ns, t);
+            break;
+        case 13:
+            if constexpr (MAXR >= 13) fft_pass_io<13, SIGN>(ld, st, M, ns, t);
+            break;
+        default: break;
+    }
+}
+
 // L2 prefetch of the 128-byte lines of [p, p + bytes), spread over the CTA;
 // every address issued lies inside the range's lines
 __device__ __forceinline__ void prefetch_l2_range(const void* p, size_t bytes) {
@@ -234,6 +287,54 @@ __device__ __forceinline__ double2* fft_run(double2* a, double2* b, int M, const
                 if constexpr (MAXR >= 13) fft_pass<13, SIGN>(a, b, M, ns, t);
                 break;
             default: break;
+        }
+        ns *= r;
+        double2* sw = a;
+        a = b;
+        b = sw;
+    }
+    __syncthreads();
+    return a;
+}
+
+// fft_run with the first pass reading through ld(i) (LD) and/or the last
+// pass writing through st(i, v) (ST); the middle passes ping-pong between a
+// and b as in fft_run.  Needs nfac >= 1.  Returns the buffer that holds the
+// result when the last pass does not write through st.
+template <int SIGN, int MAXR, bool LD, bool ST, typename Ld, typename St>
+__device__ __forceinline__ double2* fft_run_io(double2* a, double2* b, int M, const int* fac,
+                                               int nfac, const double2* __restrict__ tw,
+                                               const int* tw_off, Ld ld, St st) {
+    int ns = 1;
+    for (int i = 0; i < nfac; ++i) {
+        __syncthreads();
+        const int r = fac[i];
+        const double2* t = tw + tw_off[i];
+        const bool first = LD && i == 0, last = ST && i == nfac - 1;
+        if (first || last) {
+            const double2* x = a;
+            double2* y = b;
+            auto lds = [x](int q) { return x[q]; };
+            auto sts = [y](int q, double2 v) { y[q] = v; };
+            if (first && last) fft_pass_io_r<SIGN, MAXR>(r, ld, st, M, ns, t);
+            else if (first) fft_pass_io_r<SIGN, MAXR>(r, ld, sts, M, ns, t);
+            else fft_pass_io_r<SIGN, MAXR>(r, lds, st, M, ns, t);
+        } else {
+            switch (r) {
+                case 2: fft_pass<2, SIGN>(a, b, M, ns, t); break;
+                case 3: fft_pass<3, SIGN>(a, b, M, ns, t); break;
+                case 4: fft_pass<4, SIGN>(a, b, M, ns, t); break;
+                case 8: fft_pass<8, SIGN>(a, b, M, ns, t); break;
+                case 5: fft_pass<5, SIGN>(a, b, M, ns, t); break;
+                case 7: fft_pass<7, SIGN>(a, b, M, ns, t); break;
+                case 11:
+                    if constexpr (MAXR >= 11) fft_pass<11, SIGN>(a, b, M, ns, t);
+                    break;
+                case 13:
+                    if constexpr (MAXR >= 13) fft_pass<13, SIGN>(a, b, M, ns, t);
+                    break;
+                default: break;
+            }
         }
         ns *= r;
         double2* sw = a;
@@ -332,11 +433,25 @@ __device__ __forceinline__ void fft_c2r_body(
             a[k] = make_double2(xn.x - xs.y, xn.y + xs.x);
             if (k > 0) a[n - k] = make_double2(xn.x + xs.y, -xn.y + xs.x);
         }
-        const double2* r = fft_exec<+1, MAXR>(F, tw, a, b);
         const double sN = wN ? wN[p] * wscale : 1.0;
         const double sS = wS ? wS[p] * wscale : 1.0;
         GT* gN = rN >= 0 ? grid + f * gf + rN * grs : nullptr;
         GT* gS = rS >= 0 ? grid + f * gf + rS * grs : nullptr;
+        if (!F.bluestein && F.nfac > 0) {
+            // the last pass writes the two rings
+            auto st = [&](int j, double2 v) {
+                if (gN) gN[j * gcs] = (GT)(v.x * sN);
+                if (gS) gS[j * gcs] = (GT)(v.y * sS);
+                if (extend_col && j == 0) {
+                    if (gN) gN[(long long)n * gcs] = (GT)(v.x * sN);
+                    if (gS) gS[(long long)n * gcs] = (GT)(v.y * sS);
+                }
+            };
+            fft_run_io<+1, MAXR, false, true>(a, b, F.m, F.fac, F.nfac, tw, F.tw_off,
+                                               [](int) { return make_double2(0.0, 0.0); }, st);
+            return;
+        }
+        const double2* r = fft_exec<+1, MAXR>(F, tw, a, b);
 #pragma unroll 4
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
             const double2 v = r[j];
@@ -369,12 +484,31 @@ __device__ __forceinline__ void fft_c2r_body(
             const double2 wb = cmul(w, B);
             a[k] = make_double2(A.x - wb.y, A.y + wb.x);
         }
-        const double2* r = fft_exec<+1, MAXR>(F, tw, a, b);
         const double sc = (h ? (wS ? wS[p] * wscale : 1.0) : (wN ? wN[p] * wscale : 1.0));
         GT* g = grid + f * gf + row * grs;
-        if (gcs == 1 && ((uintptr_t)g & (2 * sizeof(GT) - 1)) == 0) {
+        using GT2 = typename std::conditional<sizeof(GT) == 8, double2, float2>::type;
+        const bool vec = gcs == 1 && ((uintptr_t)g & (2 * sizeof(GT) - 1)) == 0;
+        if (!F.bluestein && F.nfac > 0) {
+            // the last pass writes the ring: sample pair j from element j
+            auto st = [&](int j, double2 v) {
+                if (vec) {
+                    GT2 o;
+                    o.x = (GT)(v.x * sc);
+                    o.y = (GT)(v.y * sc);
+                    reinterpret_cast<GT2*>(g)[j] = o;
+                } else {
+                    g[(2LL * j) * gcs] = (GT)(v.x * sc);
+                    g[(2LL * j + 1) * gcs] = (GT)(v.y * sc);
+                }
+                if (extend_col && j == 0) g[(long long)n * gcs] = (GT)(v.x * sc);
+            };
+            fft_run_io<+1, MAXR, false, true>(a, b, M, F.fac, F.nfac, tw, F.tw_off,
+                                               [](int) { return make_double2(0.0, 0.0); }, st);
+            return;
+        }
+        const double2* r = fft_exec<+1, MAXR>(F, tw, a, b);
+        if (vec) {
             // contiguous, aligned row: one vector store per sample pair
-            using GT2 = typename std::conditional<sizeof(GT) == 8, double2, float2>::type;
             GT2* g2 = reinterpret_cast<GT2*>(g);
 #pragma unroll 4
             for (int j = threadIdx.x; j < M; j += blockDim.x) {
@@ -418,8 +552,8 @@ __device__ __forceinline__ void fft_r2c_body(
         const int rN = rowN[p], rS = rowS[p];
         const GT* gN = rN >= 0 ? grid + f * gf + rN * grs : nullptr;
         const GT* gS = rS >= 0 ? grid + f * gf + rS * grs : nullptr;
-#pragma unroll 4
-        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        // sample j of the two rings as one complex value
+        auto ld = [&](int j) {
             double xn = gN ? (double)gN[j * gcs] : 0.0;
             double xs = gS ? (double)gS[j * gcs] : 0.0;
             if (fold_extend && j == 0) {
@@ -430,9 +564,18 @@ __device__ __forceinline__ void fft_r2c_body(
                 if (gN) xn = xn * (double)(grid2 + f * gf + rN * grs)[j * gcs];
                 if (gS) xs = xs * (double)(grid2 + f * gf + rS * grs)[j * gcs];
             }
-            a[j] = make_double2(xn, xs);
+            return make_double2(xn, xs);
+        };
+        const double2* r;
+        if (!F.bluestein && F.nfac > 0) {
+            // the first pass reads the rings
+            r = fft_run_io<-1, MAXR, true, false>(a, b, F.m, F.fac, F.nfac, tw, F.tw_off, ld,
+                                                  [](int, double2) {});
+        } else {
+#pragma unroll 4
+            for (int j = threadIdx.x; j < n; j += blockDim.x) a[j] = ld(j);
+            r = fft_exec<-1, MAXR>(F, tw, a, b);
         }
-        const double2* r = fft_exec<-1, MAXR>(F, tw, a, b);
         const double sN = wN ? wN[p] * wscale : wscale;
         const double sS = wS ? wS[p] * wscale : wscale;
         double2* X = spec + ((long long)f * npair + p) * (lc + 1) * 2;
@@ -459,8 +602,8 @@ __device__ __forceinline__ void fft_r2c_body(
         const GT* g = grid + f * gf + row * grs;
         using GT2 = typename std::conditional<sizeof(GT) == 8, double2, float2>::type;
         const bool vec = gcs == 1 && ((uintptr_t)g & (2 * sizeof(GT) - 1)) == 0;
-#pragma unroll 4
-        for (int j = threadIdx.x; j < M; j += blockDim.x) {
+        // samples 2j and 2j + 1 of the ring as one complex value
+        auto ld = [&](int j) {
             double x0, x1;
             if (vec) {
                 const GT2 v = reinterpret_cast<const GT2*>(g)[j];
@@ -476,9 +619,18 @@ __device__ __forceinline__ void fft_r2c_body(
                 x0 = x0 * (double)g2[(2LL * j) * gcs];
                 x1 = x1 * (double)g2[(2LL * j + 1) * gcs];
             }
-            a[j] = make_double2(x0, x1);
+            return make_double2(x0, x1);
+        };
+        const double2* r;
+        if (!F.bluestein && F.nfac > 0) {
+            // the first pass reads the ring
+            r = fft_run_io<-1, MAXR, true, false>(a, b, M, F.fac, F.nfac, tw, F.tw_off, ld,
+                                                  [](int, double2) {});
+        } else {
+#pragma unroll 4
+            for (int j = threadIdx.x; j < M; j += blockDim.x) a[j] = ld(j);
+            r = fft_exec<-1, MAXR>(F, tw, a, b);
         }
-        const double2* r = fft_exec<-1, MAXR>(F, tw, a, b);
         const double sc = h ? (wS ? wS[p] * wscale : wscale) : (wN ? wN[p] * wscale : wscale);
 #pragma unroll 4
         for (int k = threadIdx.x; k <= lc; k += blockDim.x) {
