@@ -297,6 +297,12 @@ __device__ __forceinline__ double2* fft_run(double2* a, double2* b, int M, const
     return a;
 }
 
+// Transforms of at least this length read or write their grid rows in the
+// first / last pass (fft_run_io); shorter ones stage them through shared
+// memory.  On B200 the direct passes made lengths 1440..5600 3-11% faster
+// and lengths up to 512 up to 9% (r2c) and 48% (c2r) slower.
+constexpr int kFftIoMin = 1024;
+
 // fft_run with the first pass reading through ld(i) (LD) and/or the last
 // pass writing through st(i, v) (ST); the middle passes ping-pong between a
 // and b as in fft_run.  Needs nfac >= 1.  Returns the buffer that holds the
@@ -419,6 +425,13 @@ __device__ __forceinline__ void fft_c2r_body(
         const int p = job;
         const int rN = rowN[p], rS = rowS[p];
         const double2* X = spec + ((long long)f * npair + p) * (lc + 1) * 2;
+        const double sN = wN ? wN[p] * wscale : 1.0;
+        const double sS = wS ? wS[p] * wscale : 1.0;
+        GT* gN = rN >= 0 ? grid + f * gf + rN * grs : nullptr;
+        GT* gS = rS >= 0 ? grid + f * gf + rS * grs : nullptr;
+        // the spectra are staged in shared memory: each X_k feeds two entries
+        // (reading them in the first pass instead, twice, measured 12-14%
+        // slower at lmax 1023 and 2047)
         for (int k = threadIdx.x; k < n; k += blockDim.x) a[k] = make_double2(0.0, 0.0);
         __syncthreads();
 #pragma unroll 4
@@ -433,11 +446,7 @@ __device__ __forceinline__ void fft_c2r_body(
             a[k] = make_double2(xn.x - xs.y, xn.y + xs.x);
             if (k > 0) a[n - k] = make_double2(xn.x + xs.y, -xn.y + xs.x);
         }
-        const double sN = wN ? wN[p] * wscale : 1.0;
-        const double sS = wS ? wS[p] * wscale : 1.0;
-        GT* gN = rN >= 0 ? grid + f * gf + rN * grs : nullptr;
-        GT* gS = rS >= 0 ? grid + f * gf + rS * grs : nullptr;
-        if (!F.bluestein && F.nfac > 0) {
+        if (!F.bluestein && F.nfac > 0 && F.m >= kFftIoMin) {
             // the last pass writes the two rings
             auto st = [&](int j, double2 v) {
                 if (gN) gN[j * gcs] = (GT)(v.x * sN);
@@ -447,6 +456,7 @@ __device__ __forceinline__ void fft_c2r_body(
                     if (gS) gS[(long long)n * gcs] = (GT)(v.y * sS);
                 }
             };
+            // the last pass writes the two rings
             fft_run_io<+1, MAXR, false, true>(a, b, F.m, F.fac, F.nfac, tw, F.tw_off,
                                                [](int) { return make_double2(0.0, 0.0); }, st);
             return;
@@ -470,8 +480,7 @@ __device__ __forceinline__ void fft_c2r_body(
         const int M = F.m;   // n/2
         const double2* X = spec + ((long long)f * npair + p) * (lc + 1) * 2 + h;
         // Z'_k = (X_k + conj X_{M-k}) + i w^{-k} (X_k - conj X_{M-k}), w = exp(-2 pi i/n)
-#pragma unroll 4
-        for (int k = threadIdx.x; k < M; k += blockDim.x) {
+        auto ld = [&](int k) {
             double2 xk = k <= lc ? X[2 * k] : make_double2(0.0, 0.0);
             if (k == 0) xk.y = 0.0;
             const int km = M - k;
@@ -482,13 +491,13 @@ __device__ __forceinline__ void fft_c2r_body(
             double2 w = F.twn[k];
             w.y = -w.y;                         // exp(+2 pi i k/n)
             const double2 wb = cmul(w, B);
-            a[k] = make_double2(A.x - wb.y, A.y + wb.x);
-        }
+            return make_double2(A.x - wb.y, A.y + wb.x);
+        };
         const double sc = (h ? (wS ? wS[p] * wscale : 1.0) : (wN ? wN[p] * wscale : 1.0));
         GT* g = grid + f * gf + row * grs;
         using GT2 = typename std::conditional<sizeof(GT) == 8, double2, float2>::type;
         const bool vec = gcs == 1 && ((uintptr_t)g & (2 * sizeof(GT) - 1)) == 0;
-        if (!F.bluestein && F.nfac > 0) {
+        if (!F.bluestein && F.nfac > 0 && F.m >= kFftIoMin) {
             // the last pass writes the ring: sample pair j from element j
             auto st = [&](int j, double2 v) {
                 if (vec) {
@@ -502,10 +511,12 @@ __device__ __forceinline__ void fft_c2r_body(
                 }
                 if (extend_col && j == 0) g[(long long)n * gcs] = (GT)(v.x * sc);
             };
-            fft_run_io<+1, MAXR, false, true>(a, b, M, F.fac, F.nfac, tw, F.tw_off,
-                                               [](int) { return make_double2(0.0, 0.0); }, st);
+            // the first pass reads the spectra, the last writes the ring
+            fft_run_io<+1, MAXR, true, true>(a, b, M, F.fac, F.nfac, tw, F.tw_off, ld, st);
             return;
         }
+#pragma unroll 4
+        for (int k = threadIdx.x; k < M; k += blockDim.x) a[k] = ld(k);
         const double2* r = fft_exec<+1, MAXR>(F, tw, a, b);
         if (vec) {
             // contiguous, aligned row: one vector store per sample pair
@@ -567,7 +578,7 @@ __device__ __forceinline__ void fft_r2c_body(
             return make_double2(xn, xs);
         };
         const double2* r;
-        if (!F.bluestein && F.nfac > 0) {
+        if (!F.bluestein && F.nfac > 0 && F.m >= kFftIoMin) {
             // the first pass reads the rings
             r = fft_run_io<-1, MAXR, true, false>(a, b, F.m, F.fac, F.nfac, tw, F.tw_off, ld,
                                                   [](int, double2) {});
@@ -622,7 +633,7 @@ __device__ __forceinline__ void fft_r2c_body(
             return make_double2(x0, x1);
         };
         const double2* r;
-        if (!F.bluestein && F.nfac > 0) {
+        if (!F.bluestein && F.nfac > 0 && F.m >= kFftIoMin) {
             // the first pass reads the ring
             r = fft_run_io<-1, MAXR, true, false>(a, b, M, F.fac, F.nfac, tw, F.tw_off, ld,
                                                   [](int, double2) {});
