@@ -684,21 +684,31 @@ __device__ __forceinline__ void fft_c2c_synth_body(
     const long long fstride = (long long)npair * (lc + 1) * 2;
     const double2* Xp = spec + (2LL * u) * fstride + (long long)p * (lc + 1) * 2 + h;
     const double2* Xn = Xp + fstride;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) a[k] = make_double2(0.0, 0.0);
-    __syncthreads();
-    for (int m = threadIdx.x; m <= lc; m += blockDim.x) {
-        const double2 v = Xp[2 * m];
-        if (m == 0) {
-            a[0] = make_double2(v.x, -v.y);
-        } else {
-            a[m] = make_double2(2.0 * v.x, -2.0 * v.y);
-            const double2 w = Xn[2 * m];
-            const double sg = (m & 1) ? -2.0 : 2.0;
-            a[n - m] = make_double2(sg * w.x, -sg * w.y);
+    // bin j: +m sums for j = m <= lc, -m sums for j = n - m (m <= lc; n > 2 lc,
+    // so the two ranges do not meet), zero elsewhere
+    auto ld = [&](int j) {
+        if (j <= lc) {
+            const double2 v = Xp[2 * j];
+            return j == 0 ? make_double2(v.x, -v.y) : make_double2(2.0 * v.x, -2.0 * v.y);
         }
-    }
-    const double2* r = fft_exec<+1, MAXR>(F, tw, a, b);
+        const int m = n - j;
+        if (m > lc) return make_double2(0.0, 0.0);
+        const double2 w = Xn[2 * m];
+        const double sg = (m & 1) ? -2.0 : 2.0;
+        return make_double2(sg * w.x, -sg * w.y);
+    };
     double2* g = grid + u * gf + row * grs;
+    if (!F.bluestein && F.nfac > 0 && F.m >= kFftIoMin) {
+        // the first pass reads the bins, the last writes the ring
+        auto st = [&](int j, double2 v) {
+            g[j * gcs] = v;
+            if (extend_col && j == 0) g[(long long)n * gcs] = v;
+        };
+        fft_run_io<+1, MAXR, true, true>(a, b, n, F.fac, F.nfac, tw, F.tw_off, ld, st);
+        return;
+    }
+    for (int j = threadIdx.x; j < n; j += blockDim.x) a[j] = ld(j);
+    const double2* r = fft_exec<+1, MAXR>(F, tw, a, b);
 #pragma unroll 4
     for (int j = threadIdx.x; j < n; j += blockDim.x) g[j * gcs] = r[j];
     if (extend_col && threadIdx.x == 0) g[(long long)n * gcs] = r[0];
@@ -732,10 +742,27 @@ __device__ __forceinline__ void fft_c2c_anal_body(
     double2* b = smem_fft + len;
     const int n = F.m;
     const double2* g = grid + u * gf + row * grs;
+    const double sc = (h ? wS[p] : wN[p]) * wscale;
+    if (!F.bluestein && F.nfac > 0 && F.m >= kFftIoMin) {
+        // the first pass reads the ring; the last writes bin i to the +m
+        // sums (i = m <= lc) or the -m sums (i = n - m, m <= lc)
+        auto ld = [&](int j) { return g[j * gcs]; };
+        auto st = [&](int i, double2 z) {
+            if (i <= lc) Xp[2 * i] = make_double2(sc * z.x, sc * z.y);
+            if (i == 0) {
+                Xn[0] = make_double2(0.0, 0.0);
+            } else if (n - i <= lc) {
+                const int m = n - i;
+                const double sg = (m & 1) ? -sc : sc;
+                Xn[2 * m] = make_double2(sg * z.x, sg * z.y);
+            }
+        };
+        fft_run_io<-1, MAXR, true, true>(a, b, n, F.fac, F.nfac, tw, F.tw_off, ld, st);
+        return;
+    }
 #pragma unroll 4
     for (int j = threadIdx.x; j < n; j += blockDim.x) a[j] = g[j * gcs];
     const double2* r = fft_exec<-1, MAXR>(F, tw, a, b);
-    const double sc = (h ? wS[p] : wN[p]) * wscale;
     for (int m = threadIdx.x; m <= lc; m += blockDim.x) {
         const double2 zp = r[m];
         Xp[2 * m] = make_double2(sc * zp.x, sc * zp.y);

@@ -159,3 +159,31 @@ def test_complex_errors(cuda):
         pc.synthesis(c)
     with pytest.raises(Exception):
         pr.synthesis_c(c.to(torch.complex128))
+
+
+@pytest.mark.parametrize("kind", ["dh", "glq"])
+def test_complex_long_rings_match_oracle(cuda, oracle, kind):
+    """Rings of 1024 points or more take the FFT passes that read the bins or
+    the ring in the first pass and write the ring or the bins from the last:
+    DH lmax 260, sampling 2 (1044 points) and GLQ lmax 520 (1041 points),
+    with the extend column, against the oracle."""
+    if kind == "dh":
+        L = 260
+        c = oracle.power_law_cilm_complex(L, 33)
+        g = cuda.MakeGridDHC(c, sampling=2, extend=1).cpu().numpy()
+        gref = oracle.makegrid_dhc(c, sampling=2, extend=1)
+        gin = gref[:2 * L + 2, :2 * (2 * L + 2)]
+        b = cuda.SHExpandDHC(gin, sampling=2).cpu().numpy()
+        bref = oracle.shexpand_dhc(gin, sampling=2)
+    else:
+        L = 520
+        c = oracle.power_law_cilm_complex(L, 34)
+        z, w = oracle.shglq(L)
+        g = cuda.MakeGridGLQC(c, zero=z, extend=1).cpu().numpy()
+        gref = oracle.makegrid_glqc(c, zero=z, extend=1)
+        gin = gref[:, :2 * L + 1]
+        b = cuda.SHExpandGLQC(gin, w=w, zero=z).cpu().numpy()
+        bref = oracle.shexpand_glqc(gin, w=w, zero=z)
+    assert g.shape == gref.shape
+    assert grid_rel(g, gref) <= GRID_TOL
+    coef_check(b, bref, 1, gin)

@@ -190,3 +190,26 @@ def test_batch_rejects_long_fft(cuda):
     from shtools_b200.batch import Batch
     with pytest.raises(_lib.SHTCudaError):
         Batch.glq([2046])
+
+
+def test_long_rings_column_major_grids(cuda, oracle):
+    """Rings of 1024 points or more (DH lmax 511, sampling 2: 2048 points,
+    one ring per item; GLQ lmax 520: 1041 points, two rings per item) go
+    through the direct first / last FFT passes; with column-major grids
+    (column stride other than 1) they give the same values as row-major
+    grids."""
+    from shtools_b200 import transforms as T
+    for kind, L in (("dh", 511), ("glq", 520)):
+        c = torch.from_numpy(oracle.power_law_cilm(L, 70)[None]).cuda()
+        if kind == "dh":
+            plan = T.get_plan(T.GRID_DH, L, L, 1, 1, 2, 0)
+        else:
+            z, w = oracle.shglq(L)
+            plan = T.get_plan(T.GRID_GLQ, L, L, 1, 1, 1, 0, zero=z, w=w)
+        g = plan.synthesis(c)
+        gcm = torch.empty((g.shape[0], g.shape[2], g.shape[1]), dtype=g.dtype,
+                          device=g.device).transpose(1, 2)
+        assert gcm.stride(2) != 1
+        plan.synthesis(c, out=gcm)
+        assert torch.equal(gcm, g)
+        assert torch.equal(plan.analysis(gcm), plan.analysis(g))
