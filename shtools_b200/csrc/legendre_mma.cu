@@ -240,9 +240,10 @@ static int launch_mma_t(const shtc_plan* P, const double2* spec, double2* partia
 int anal_mma_pairs() { return 32 * kMmaWarps; }
 
 // 8 fields per CTA (NT = 2: 126 registers, two CTAs per SM); 16 per CTA
-// (NT = 4: 208 registers, one CTA) measured slower on B200 for 16 fields
-// (lmax 2799: 43.2 against 40.4 ms; 8 complex fields at lmax 719: 1.08
-// against 0.90 ms), the recursion run twice notwithstanding
+// (NT = 4: 208 registers, one CTA) measured slower on B200 for 16 fields,
+// before the recursion overlapped the products (lmax 2799: 43.2 against
+// 40.4 ms; 8 complex fields at lmax 719: 1.08 against 0.90 ms), the
+// recursion run twice notwithstanding
 int launch_legendre_anal_mma(const shtc_plan* P, const double2* spec, double2* partial,
                              int ntiles, int nfield, cudaStream_t st) {
     return launch_mma_t<2>(P, spec, partial, ntiles, nfield, st);
