@@ -420,6 +420,12 @@ SHTC_API void SHGLQ(const int lmax, double* zero, double* w, double* plx,
 SHTC_API void PreGLQ(const double x1, const double x2, const int n, double* zero,
             double* w, int* exitstatus);
 
+/* include/shtools.h:198-206 (src/GLQGridCoord.f95:1, src/cWrapper.f95:419-434):
+ * latitudes (degrees, north first) of the lmax+1 Gauss-Legendre nodes and
+ * the 2 lmax + 1 (+extend) longitudes of a GLQ grid */
+SHTC_API void GLQGridCoord(double* latglq, const int latglq_d0, double* longlq,
+                           const int longlq_d0, const int lmax, int* nlat, int* nlong,
+                           const int* extend, int* exitstatus);
 /* include/shtools.h:1034-1038 (src/DHaj.f95:1) */
 SHTC_API void DHaj(const int n, double* aj, const int aj_d0, const int* extend,
           int* exitstatus);

@@ -20,6 +20,7 @@ import numpy as np
 from . import transforms as _t
 
 __all__ = ["MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ", "SHGLQ",
+           "GLQGridCoord",
            "MakeGridDHC", "SHExpandDHC", "MakeGridGLQC", "SHExpandGLQC",
            "MakeGradientDH", "MakeGravGridDH", "NormalGravity", "SHRotateRealCoef",
            "available", "register", "set_nthreads"]
@@ -85,6 +86,22 @@ def SHGLQ(lmax):
     """zero, w = SHGLQ(lmax) -- Gauss-Legendre nodes and weights from the GPU
     PreGLQ (src/SHGLQ.f95:188)."""
     return _t.SHGLQ(lmax)
+
+
+def GLQGridCoord(lmax, extend=0):
+    """latglq, longlq = GLQGridCoord(lmax, [extend]) -- latitudes (degrees)
+    of the GPU PreGLQ nodes and longitudes of a GLQ grid
+    (src/GLQGridCoord.f95:112-118, pyshtools.pyf:424-438)."""
+    lmax = int(lmax)
+    if lmax < 0:
+        raise ValueError("lmax must be >= 0, got %d" % lmax)
+    if extend not in (0, 1, False, True):
+        raise ValueError("extend must be 0 or 1, got %r" % (extend,))
+    zero = np.asarray(SHGLQ(lmax)[0], dtype=np.float64)
+    nlong = 2 * lmax + 1
+    latglq = np.arcsin(zero) * 180.0 / np.pi
+    longlq = 360.0 * np.arange(nlong + int(extend), dtype=np.float64) / nlong
+    return latglq, longlq
 
 
 def _fallback(name):

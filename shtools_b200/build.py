@@ -53,13 +53,44 @@ def _stale(target, inputs):
     return any(os.path.getmtime(d) > t for d in inputs)
 
 
+def _compile_objects(extra, verbose):
+    """One nvcc per translation unit, run in parallel; returns the objects."""
+    objdir = os.path.join(LIBDIR, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    hdrs = sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + [
+        os.path.join(ROOT, "include", "shtcuda.h"), os.path.abspath(__file__)]
+    objs, procs = [], []
+    for src in sources():
+        obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        if _stale(obj, [src] + hdrs):
+            cmd = [nvcc(), *flags(extra), "-c", "-o", obj + ".tmp", src]
+            cmd.remove("--shared")
+            if verbose:
+                print(" ".join(cmd))
+            procs.append((subprocess.Popen(cmd), obj))
+    failed = []
+    for pr, obj in procs:
+        if pr.wait() != 0:
+            failed.append(obj)
+        else:
+            os.replace(obj + ".tmp", obj)
+    if failed:
+        raise subprocess.CalledProcessError(1, "nvcc -c " + " ".join(failed))
+    return objs
+
+
 def build(force=False, verbose=False, extra=()):
-    """Compile libshtcuda.so and the FP64 probe library; returns the path of
-    libshtcuda.so."""
+    """Compile libshtcuda.so (translation units in parallel, then one link)
+    and the FP64 probe library; returns the path of libshtcuda.so."""
     os.makedirs(LIBDIR, exist_ok=True)
     if force or _stale(LIBPATH, deps()):
+        if force:
+            for o in glob.glob(os.path.join(LIBDIR, "obj", "*.o")):
+                os.remove(o)
+        objs = _compile_objects(extra, verbose)
         tmp = LIBPATH + ".tmp"
-        cmd = [nvcc(), *flags(extra), "-o", tmp, *sources()]
+        cmd = [nvcc(), *ARCH, "--shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs]
         if verbose:
             print(" ".join(cmd))
         subprocess.check_call(cmd)

@@ -994,6 +994,28 @@ extern "C" void SHGLQ(const int lmax, double* zero, double* w, double* plx,
     PreGLQ(-1.0, 1.0, lmax + 1, zero, w, exitstatus);
 }
 
+// GLQGridCoord (GLQGridCoord.f95:1-121): latitudes asin(z_i) in degrees of
+// the GPU PreGLQ nodes (:116-118), longitudes 360 (i-1) / nlong (:112-114).
+extern "C" void GLQGridCoord(double* latglq, const int latglq_d0, double* longlq,
+                             const int longlq_d0, const int lmax, int* nlat, int* nlong,
+                             const int* extend, int* exitstatus) {
+    set_status(exitstatus, SHTC_OK);
+    if (lmax < 0) return set_status(exitstatus, SHTC_EBOUND);
+    const int nl = lmax + 1, nlo = 2 * lmax + 1, ext = opt(extend, 0);
+    if (nlat) *nlat = nl;
+    if (nlong) *nlong = nlo;
+    if (ext != 0 && ext != 1) return set_status(exitstatus, SHTC_EBOUND);
+    if (!latglq || !longlq || latglq_d0 < nl || longlq_d0 < nlo + ext)
+        return set_status(exitstatus, SHTC_EDIM);
+    std::vector<double> zero(nl), w(nl);
+    int rc = SHTC_OK;
+    PreGLQ(-1.0, 1.0, nl, zero.data(), w.data(), &rc);
+    if (rc) return set_status(exitstatus, rc);
+    const double pi = acos(-1.0);
+    for (int i = 0; i < nlo + ext; ++i) longlq[i] = 360.0 * (double)i / (double)nlo;
+    for (int i = 0; i < nl; ++i) latglq[i] = asin(zero[i]) * 180.0 / pi;
+}
+
 extern "C" void DHaj(const int n, double* aj, const int aj_d0, const int* extend,
                      int* exitstatus) {
     set_status(exitstatus, SHTC_OK);

@@ -125,20 +125,21 @@ __global__ void k_rtab(double* __restrict__ rtab, const double* __restrict__ u,
 }
 
 // PreGLQ (PreGLQ.f95:93-149): one thread per root, Newton iteration on P_n
-// with the same non-fused arithmetic.  status[0] is set to 5 when a root
-// does not converge within itermax iterations.
-__global__ void k_preglq(double x1, double x2, int n, double* __restrict__ zero,
-                         double* __restrict__ w, int itermax,
+// with the same non-fused arithmetic.  The starting guesses
+// cos(pi (i - 1/4) / (n + 1/2)) (PreGLQ.f95:101) come from the host's libm,
+// as in the reference: the weight is taken at the last-but-one iterate, so a
+// start one ulp away can move it by far more than an ulp.  status[0] is set
+// to 5 when a root does not converge within itermax iterations.
+__global__ void k_preglq(double x1, double x2, int n, const double* __restrict__ guess,
+                         double* __restrict__ zero, double* __restrict__ w, int itermax,
                          int* __restrict__ status) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int mroots = (n + 1) / 2;
     if (i > mroots) return;
-    const double pi = 3.141592653589793238462643383279502884;
     const double eps = 1.0e-15;
     const double xm = __ddiv_rn(__dadd_rn(x2, x1), 2.0);
     const double xu = __ddiv_rn(__dsub_rn(x2, x1), 2.0);
-    double z = cos(__ddiv_rn(__dmul_rn(pi, __dsub_rn((double)i, 0.25)),
-                             __dadd_rn((double)n, 0.5)));
+    double z = guess[i - 1];
     double p1, p2, p3, pp, z1;
     int iter = 0;
     for (;;) {
@@ -730,20 +731,31 @@ extern "C" int shtc_preglq(double x1, double x2, int n, double* zero, double* w,
                            void* stream) {
     if (n < 1 || !zero || !w) return SHTC_EBOUND;
     cudaStream_t st = (cudaStream_t)stream;
-    int* d_status = nullptr;
-    if (cudaMalloc((void**)&d_status, sizeof(int)) != cudaSuccess) return SHTC_EALLOC;
+    const int mroots = (n + 1) / 2;
+    // starting guesses with the host libm, in the reference's operation order
+    std::vector<double> guess(mroots);
+    const double pi = acos(-1.0);
+    for (int i = 1; i <= mroots; ++i) guess[i - 1] = cos(pi * (i - 0.25) / (n + 0.5));
+    // one allocation: the status word, then the guesses (8-byte aligned)
+    void* d_buf = nullptr;
+    if (cudaMalloc(&d_buf, sizeof(double) * (1 + mroots)) != cudaSuccess) return SHTC_EALLOC;
+    int* d_status = (int*)d_buf;
+    double* d_guess = (double*)d_buf + 1;
     int rc = map_cuda(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+    if (!rc) rc = map_cuda(cudaMemcpyAsync(d_guess, guess.data(), sizeof(double) * mroots,
+                                           cudaMemcpyHostToDevice, st));
     if (!rc) rc = map_cuda(cudaMemsetAsync(zero, 0, sizeof(double) * n, st));
     if (!rc) rc = map_cuda(cudaMemsetAsync(w, 0, sizeof(double) * n, st));
-    const int mroots = (n + 1) / 2;
     if (!rc) {
-        k_preglq<<<(mroots + 63) / 64, 64, 0, st>>>(x1, x2, n, zero, w, 1000, d_status);
+        k_preglq<<<(mroots + 63) / 64, 64, 0, st>>>(x1, x2, n, d_guess, zero, w, 1000,
+                                                    d_status);
         rc = map_cuda(cudaGetLastError());
     }
     int hs = 0;
     if (!rc) rc = map_cuda(cudaMemcpyAsync(&hs, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
     if (!rc) rc = map_cuda(cudaStreamSynchronize(st));
-    cudaFree(d_status);
+    else cudaStreamSynchronize(st);
+    cudaFree(d_buf);
     if (rc) return rc;
     return hs;
 }
