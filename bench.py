@@ -90,6 +90,16 @@ def parse():
     return ap.parse_args()
 
 
+def bench_config(args, w, world):
+    """The workload description printed by both arms (identical dictionaries,
+    so a reader can match the GPU line with the reference line)."""
+    return {"workload": args.workload, "kind": w["kind"], "lmax": w["lmax"],
+            "fields_per_gpu": w["nfield"], "sampling": w["sampling"],
+            "precision": getattr(args, "precision", "fp64"),
+            "step": "synthesis + analysis",
+            "parallelism": "replicas" if world > 1 else "single GPU"}
+
+
 def batch_lmaxes(w):
     """Seeded lmax of every field of a batched workload."""
     import numpy as np
@@ -928,6 +938,48 @@ def run_cuda(args, w, rank, world, local_rank):
     transforms = 2.0 * F * args.steps * world
     value = transforms / (total_ms * 1e-3)
 
+    # ---- end to end through the pyshtools backend call ----------------------
+    # the call a pyshtools user makes after select_preferred_backend('cuda'):
+    # numpy coefficients in, numpy grid out, numpy grid in, numpy
+    # coefficients out, one field per call (shtools_b200.backend); the host
+    # copies (pageable numpy buffers) are inside the timed region
+    from shtools_b200 import backend as B
+    if cplx:
+        s = w["sampling"]
+        b_synth = lambda x: B.MakeGridDHC(x, sampling=s)
+        b_anal = lambda x: B.SHExpandDHC(x, sampling=s)
+    elif w["kind"] == "glq":
+        b_synth = lambda x: B.MakeGridGLQ(x, zero=zero)
+        b_anal = lambda x: B.SHExpandGLQ(x, w=wts, zero=zero)
+    else:
+        s = w["sampling"]
+        b_synth = lambda x: B.MakeGridDH(x, sampling=s)
+        b_anal = lambda x: B.SHExpandDH(x, sampling=s)
+    plug_steps = max(2, min(args.steps, 4 if F > 1 else args.steps))
+
+    def plug_step():
+        out = []
+        for f in range(F):
+            gf = b_synth(cil[f])
+            out.append(b_anal(gf))
+        return gf, out
+
+    plug_step()     # warm-up
+    barrier()
+    torch.cuda.synchronize(dev)
+    pa = torch.cuda.Event(enable_timing=True)
+    pb = torch.cuda.Event(enable_timing=True)
+    pa.record(st)
+    for _ in range(plug_steps):
+        g_last, b_plug = plug_step()
+    pb.record(st)
+    torch.cuda.synchronize(dev)
+    plug_ms = max_over_ranks(pa.elapsed_time(pb), dev)
+    plug_value = 2.0 * F * plug_steps * world / (plug_ms * 1e-3)
+    plug_ok = bool(np.array_equal(b_plug[-1], bb[-1]))
+    plug_h2d = F * (cil[0].nbytes + g_last.nbytes)
+    plug_d2h = F * (cil[0].nbytes + g_last.nbytes)
+
     # ---- end-to-end through the public API with host buffers ---------------
     # every step uploads its inputs (cilm and a grid) from pinned host memory,
     # runs synthesis and analysis, and downloads both results; the steps are
@@ -942,14 +994,15 @@ def run_cuda(args, w, rank, world, local_rank):
              torch.empty(tuple(back.shape), dtype=back.dtype).pin_memory())
             for _ in range(2)]
     e2e_steps = max(2, args.steps)
-    fn = lambda t: synth(t) if t.dim() == c.dim() else anal(t)
-
     def e2e_run(n):
-        ins, outs_n = [], []
+        # per step its own function: the synthesis of a cilm, then the
+        # analysis of a grid
+        ins, outs_n, fns = [], [], []
         for i in range(n):
             ins += [(c_host,), (g_in,)]
             outs_n += [(outs[i % 2][0],), (outs[i % 2][1],)]
-        pipelined(fn, ins, outs_n, device=dev)
+            fns += [synth, anal]
+        pipelined(fns, ins, outs_n, device=dev)
 
     e2e_run(2)     # warm-up
     barrier()
@@ -962,7 +1015,8 @@ def run_cuda(args, w, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     e2e_ms = max_over_ranks(a.elapsed_time(b), dev)
     e2e_value = 2.0 * F * e2e_steps * world / (e2e_ms * 1e-3)
-    e2e_ok = bool(torch.equal(outs[(e2e_steps - 1) % 2][1], back.cpu()))
+    e2e_ok = bool(torch.equal(outs[(e2e_steps - 1) % 2][1], back.cpu()) and
+                  torch.equal(outs[(e2e_steps - 1) % 2][0], g.cpu()))
     h2d = c_host.numel() * esize + g_in.numel() * esize
     d2h = outs[0][0].numel() * esize + outs[0][1].numel() * esize
 
@@ -991,11 +1045,8 @@ def run_cuda(args, w, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "c128" if cplx else "f64",
         "data": "synthetic seeded power-law coefficients, S(l)=(l+1)^-%g" % w["beta"],
-        "config": {"workload": args.workload, "kind": w["kind"], "lmax": L,
-                   "fields_per_gpu": F, "sampling": w["sampling"],
-                   "precision": "fp64", "step": "synthesis + analysis",
-                   "l2": "flushed between steps (256 MiB write, outside step events)",
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "config": bench_config(args, w, world),
+        "l2": "flushed between steps (256 MiB write, outside step events)",
         "roofline": {"kernel": names[dom], "bound": "fp64", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None,
@@ -1004,7 +1055,13 @@ def run_cuda(args, w, rank, world, local_rank):
                      "flops_per_launch": fl, "traffic": traffic},
         "stages": stage,
         "roundtrip_max_perdeg_err": rt_err,
-        "e2e": {"value": e2e_value, "unit": "transforms/s",
+        "e2e": {"value": plug_value, "unit": "transforms/s",
+                "h2d_bytes_per_step": plug_h2d, "d2h_bytes_per_step": plug_d2h,
+                "steps": plug_steps, "result_matches_device_run": plug_ok,
+                "path": "pyshtools backend call (shtools_b200.backend, numpy in and "
+                        "out, one field per call): per field H2D cilm, synthesis, D2H "
+                        "grid, H2D grid, analysis, D2H cilm; pageable host buffers"},
+        "e2e_pipelined": {"value": e2e_value, "unit": "transforms/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps, "result_matches_device_run": e2e_ok,
                 "path": "public torch API on pinned host buffers: per step H2D cilm "
@@ -1041,9 +1098,7 @@ def main():
                "warmup": args.warmup, "ms_per_step": 1e3 * sum(dts) / len(dts),
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                "dtype": "f64", "data": "synthetic seeded power-law coefficients",
-               "config": {"workload": args.workload, "kind": w["kind"],
-                          "lmax": w["lmax"], "fields": w["nfield"],
-                          "sampling": w["sampling"]},
+               "config": bench_config(args, w, world),
                "cpu_baseline": {"value": value, "unit": "transforms/s",
                                 "cores": threads, "kind": "port",
                                 "sample": sample},
@@ -1083,9 +1138,9 @@ def main():
         torch.distributed.destroy_process_group()
     if rank == 0:
         if w["kind"] == "glq_batch":
-            res.setdefault("config", {})["tile_shapes"] = "fixed batched-kernel shapes"
+            res["tile_shapes"] = "fixed batched-kernel shapes"
         else:
-            res.setdefault("config", {})["tile_shapes"] = (
+            res["tile_shapes"] = (
                 "default" if args.no_autotune else "autotuned per plan (shtools_b200.autotune)")
         print(json.dumps(res))
     return 0

@@ -45,11 +45,33 @@ extern "C" {
 #define SHTC_EHANDLE 7   /* null plan handle or null required pointer        */
 #define SHTC_EUNSUP 8    /* FFT length or size beyond the supported range    */
 #define SHTC_EWORK 9     /* workspace smaller than shtc_workspace_bytes()    */
+#define SHTC_ETIMEOUT 10 /* a bounded wait inside a tensor-core kernel ran out */
+
+/* Legendre arithmetic of a plan (shtc_plan_set_precision) */
+#define SHTC_PREC_F64 0     /* FP64 recursion and sums (default; the parity path) */
+#define SHTC_PREC_INT8X6 1  /* FP64 recursion, synthesis sums on INT8 tensor cores:
+                               6-byte fixed-point operands, 7 byte-product weights */
+#define SHTC_PREC_INT8X7 2  /* as INT8X6 with 7-byte operands and 8 weights */
 
 #define SHTC_GRID_DH 1
 #define SHTC_GRID_GLQ 2
 
 typedef struct shtc_plan shtc_plan;
+
+/* Precision of the Legendre sums of a plan (no counterpart in the reference,
+ * whose transforms are FP64 only).  SHTC_PREC_INT8X6 / INT8X7 run the
+ * synthesis of real plans with norm 1, 2 or 4 on the tcgen05 tensor cores:
+ * P_lm and the coefficients as 46-bit (54-bit) fixed-point integers split
+ * into 6 (7) balanced byte digits, the significant byte products summed
+ * exactly in INT32; the recursion stays FP64.  Other transforms of the plan
+ * keep FP64.  Returns SHTC_EUNSUP for norm 3 or complex plans.  Allocates a
+ * small table and synchronises. */
+SHTC_API int shtc_plan_set_precision(shtc_plan* plan, int precision);
+
+/* Error word of the tensor-core kernels on the current device: 0 or
+ * SHTC_ETIMEOUT (a bounded in-kernel wait ran out; the outputs of that call
+ * are invalid).  Reads and clears it; synchronises the stream. */
+SHTC_API int shtc_mixed_status(int* status, void* stream);
 
 /* Library version as 10000*major + 100*minor + patch. */
 SHTC_API int shtc_version(void);

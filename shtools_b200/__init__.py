@@ -19,11 +19,11 @@ from .transforms import (MakeGridDH, SHExpandDH, MakeGridGLQ, SHExpandGLQ,
                          MakeGridDHC, SHExpandDHC, MakeGridGLQC, SHExpandGLQC,
                          MakeGradientDH, MakeGravGridDH, NormalGravity, SHMultiply,
                          PreGLQ, SHGLQ, DHaj, Plan, get_plan,
-                         clear_plan_cache, GRID_DH, GRID_GLQ)
+                         clear_plan_cache, mixed_status, GRID_DH, GRID_GLQ)
 from ._lib import SHTCudaError
 
 __all__ = ["MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ",
            "MakeGridDHC", "SHExpandDHC", "MakeGridGLQC", "SHExpandGLQC",
            "MakeGradientDH", "MakeGravGridDH", "NormalGravity", "SHMultiply", "PreGLQ",
-           "SHGLQ", "DHaj", "Plan", "get_plan", "clear_plan_cache", "GRID_DH",
+           "SHGLQ", "DHaj", "Plan", "get_plan", "clear_plan_cache", "mixed_status", "GRID_DH",
            "GRID_GLQ", "SHTCudaError"]

@@ -28,6 +28,7 @@ EXPORTS = (
     "shtc_version", "shtc_status_string", "shtc_plan_create_dh",
     "shtc_plan_create_glq", "shtc_plan_destroy", "shtc_plan_info",
     "shtc_plan_set_tuning", "shtc_timing_enable", "shtc_timing_collect",
+    "shtc_plan_set_precision", "shtc_mixed_status",
     "shtc_synthesis_noalloc",
     "shtc_workspace_bytes", "shtc_synthesis", "shtc_analysis",
     "shtc_synthesis_adjoint", "shtc_analysis_adjoint", "shtc_synthesis_ex",
@@ -36,7 +37,7 @@ EXPORTS = (
     "shtc_batch_workspace_bytes", "shtc_batch_synthesis", "shtc_batch_analysis",
     "shtc_preglq",
     "shtc_dhaj", "MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ",
-    "SHGLQ", "PreGLQ", "DHaj", "shtc_plan_create_dhc", "shtc_plan_create_glqc",
+    "SHGLQ", "PreGLQ", "DHaj", "GLQGridCoord", "shtc_plan_create_dhc", "shtc_plan_create_glqc",
     "shtc_synthesis_c", "shtc_analysis_c", "MakeGridDHC", "SHExpandDHC",
     "MakeGridGLQC", "SHExpandGLQC", "shtc_gradient_workspace_bytes",
     "shtc_gradient_dh", "MakeGradientDH", "shtc_gravity_workspace_bytes",
@@ -66,6 +67,8 @@ def _bind(L):
     L.shtc_plan_destroy.argtypes = [_P]
     L.shtc_plan_info.argtypes = [_P, ctypes.POINTER(_LL), _I]
     L.shtc_plan_set_tuning.argtypes = [_P, _I, _I, _I]
+    L.shtc_plan_set_precision.argtypes = [_P, _I]
+    L.shtc_mixed_status.argtypes = [ctypes.POINTER(_I), _P]
     L.shtc_workspace_bytes.restype = _SZ
     L.shtc_workspace_bytes.argtypes = [_P, _I]
     coef = [_P, _LL, _LL, _LL, _LL, _I]

@@ -28,6 +28,7 @@ extern "C" const char* shtc_status_string(int s) {
         case SHTC_EHANDLE: return "Null plan handle or required pointer.";
         case SHTC_EUNSUP: return "Transform size not supported.";
         case SHTC_EWORK: return "Workspace too small.";
+        case SHTC_ETIMEOUT: return "A bounded wait inside a tensor-core kernel ran out.";
         default: return "Unknown status.";
     }
 }
@@ -53,10 +54,15 @@ static double2* fft_scratch(const shtc_plan* P, void* work, size_t offset) {
 }
 
 // complex plans carry two internal fields (orders +m and -m) per field
+// INT8X6 plans: the tensor-core synthesis scratch behind the FFT region
+static size_t i8_region(const shtc_plan* P, int nfield) {
+    return P->precision != SHTC_PREC_F64 && !P->cplx ? align256(synth_i8_bytes(P, nfield)) : 0;
+}
+
 extern "C" size_t shtc_workspace_bytes(const shtc_plan* P, int nfield) {
     if (!P || nfield < 1) return 0;
     const int nf = P->cplx ? 2 * nfield : nfield;
-    return coef_region(P, nf) + spec_region(P, nf) + fft_region(P);
+    return coef_region(P, nf) + spec_region(P, nf) + fft_region(P) + i8_region(P, nf);
 }
 
 static int check_call(const shtc_plan* P, const void* a, const void* b,
@@ -94,12 +100,19 @@ extern "C" int shtc_synthesis_ex(const shtc_plan* P, const void* cilm, int cdt,
     double2* packed = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
     double2* fbuf = fft_scratch(P, work, coef_region(P, nfield) + spec_region(P, nfield));
+    const bool i8 = P->precision != SHTC_PREC_F64;
     stage_begin(SHTC_STAGE_PACK, st);
-    rc = launch_pack_coef(P, cilm, cdt, csf, csk, csl, csm, cdim, packed, nfield, 0, st);
+    rc = launch_pack_coef(P, cilm, cdt, csf, csk, csl, csm, cdim, packed, nfield, i8 ? 2 : 0,
+                          st);
     stage_end(SHTC_STAGE_PACK, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_SYNTH, st);
-    rc = launch_legendre_synth(P, packed, spec, nfield, st);
+    if (i8)
+        rc = launch_legendre_synth_i8(
+            P, packed, spec, nfield,
+            (char*)work + coef_region(P, nfield) + spec_region(P, nfield) + fft_region(P), st);
+    else
+        rc = launch_legendre_synth(P, packed, spec, nfield, st);
     stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_FFT_C2R, st);

@@ -37,7 +37,8 @@ int map_cuda(cudaError_t e) { return e == cudaSuccess ? SHTC_OK : SHTC_ECUDA; }
 // coefficient packing
 // ---------------------------------------------------------------------------
 // scale_mode 0: copy; 1: multiply by the analysis normalisation factor
-// (the adjoint of the final divide of SHExpandDH.f95:674-702).
+// (the adjoint of the final divide of SHExpandDH.f95:674-702); 0 and 1 also
+// multiply by the recursion's D(l - m), 2 copies without it.
 __device__ __forceinline__ double anal_norm_factor(int norm, int l,
                                                    const double* nrm3,
                                                    long long idx) {
@@ -89,8 +90,9 @@ k_pack_coef(const CT* __restrict__ cilm, long long sf, long long sk, long long s
             v.x *= a;
             v.y *= a;
         }
-        // D(l - m) of the rescaled recursion (legendre.cuh)
-        const double d = rec[idx].y;
+        // D(l - m) of the rescaled recursion (legendre.cuh); scale_mode 2
+        // keeps the plain coefficients (the INT8 tensor-core synthesis)
+        const double d = scale_mode == 2 ? 1.0 : rec[idx].y;
         packed[idx * nfield + f_off + f] = make_double2(v.x * d, v.y * d);
     }
 }

@@ -381,6 +381,7 @@ using namespace shtc;
 // plan creation (C ABI)
 // ---------------------------------------------------------------------------
 static void plan_free_tables(shtc_plan* P) {
+    cudaFree(P->d_i8_toff);
     cudaFree(P->d_rec);
     cudaFree(P->d_pmm);
     cudaFree(P->d_rtab);

@@ -95,6 +95,12 @@ struct shtc_plan {
     int tune_anal_W;   // warps per CTA of the analysis (0: heuristic)
     size_t device_bytes;
     int device;        // CUDA device the tables live on
+    // Legendre arithmetic (shtc_plan_set_precision): SHTC_PREC_F64, or
+    // SHTC_PREC_INT8X6 for the tensor-core synthesis (legendre_i8.cu)
+    int precision;
+    long long* d_i8_toff;   // INT8X6: K-tiles of 64 degrees before each order (lc + 2)
+    long long i8_ntot;      // INT8X6: K-tiles of all orders
+    double i8_ascale;       // INT8X6: 2^a, fixed-point scale of the P_lm operand
 };
 
 namespace shtc {
@@ -186,6 +192,11 @@ int launch_fft_c2c_anal(const shtc_plan* P, const double2* grid, long long gf,
                         long long grs, long long gcs, double2* spec, int nfield,
                         cudaStream_t st, double2* gbuf = nullptr);
 int map_cuda(cudaError_t e);
+// legendre_i8.cu: INT8 error-free split synthesis (SHTC_PREC_INT8X6 plans)
+size_t synth_i8_bytes(const shtc_plan* P, int nfield);
+int launch_legendre_synth_i8(const shtc_plan* P, const double2* coef, double2* spec,
+                             int nfield, void* scratch, cudaStream_t st);
+int set_precision_tables(shtc_plan* P, int precision);
 
 // timing.cu: event brackets around kernel stages (SHTC_STAGE_* ids)
 void stage_begin(int stage, cudaStream_t st);

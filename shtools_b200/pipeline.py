@@ -24,8 +24,9 @@ import torch
 def pipelined(fn, host_inputs, host_outputs, device=None, depth=2):
     """For each step i: copy the tensors of ``host_inputs[i]`` (a tuple of
     pinned host tensors) to the device, run ``outs = fn(*device_inputs)``
-    (a tuple of device tensors), and copy ``outs`` into the pinned host
-    tensors of ``host_outputs[i]``.  Returns once every copy is queued; the
+    (a tuple of device tensors; ``fn`` may also be a sequence with one
+    callable per step), and copy ``outs`` into the pinned host tensors of
+    ``host_outputs[i]``.  Returns once every copy is queued; the
     host outputs are valid after ``torch.cuda.synchronize()``.  A host
     output tensor reused by a later step is overwritten in step order.
     Device input buffers are kept per input signature (the shapes and
@@ -33,6 +34,9 @@ def pipelined(fn, host_inputs, host_outputs, device=None, depth=2):
     different kinds may alternate."""
     if len(host_inputs) != len(host_outputs):
         raise ValueError("host_inputs and host_outputs differ in length")
+    fns = [fn] * len(host_inputs) if callable(fn) else list(fn)
+    if len(fns) != len(host_inputs):
+        raise ValueError("one function per step is needed")
     if depth < 1:
         raise ValueError("depth must be >= 1")
     dev = torch.device("cuda", torch.cuda.current_device()) if device is None \
@@ -67,7 +71,7 @@ def pipelined(fn, host_inputs, host_outputs, device=None, depth=2):
                 d.copy_(h, non_blocking=True)
             loaded.record(s_in)
         comp.wait_event(loaded)
-        outs = fn(*bufs[k])
+        outs = fns[i](*bufs[k])
         if isinstance(outs, torch.Tensor):
             outs = (outs,)
         free[k] = torch.cuda.Event()

@@ -112,6 +112,14 @@ class Plan:
     def lc(self):
         return self.info["lmax_comp"]
 
+    def set_precision(self, code):
+        """shtc_plan_set_precision: 0 FP64, 1 INT8 tensor-core synthesis."""
+        with _on_device(self.device):
+            _lib.check(self.lib.shtc_plan_set_precision(self.handle, int(code)),
+                       "shtc_plan_set_precision")
+        self.precision = int(code)
+        self.__dict__.pop("_wsb", None)
+
     def workspace_bytes(self, nfield):
         """shtc_workspace_bytes for nfield fields, cached per plan and tile
         shape (the analysis tiles, and so the size, follow the shape that
@@ -211,11 +219,23 @@ _cache_lock = threading.Lock()
 _plans = {}
 
 
+PRECISIONS = {"fp64": 0, "int8x6": 1, "int8x7": 2}
+
+
+def _precision_code(precision):
+    try:
+        return PRECISIONS[precision]
+    except KeyError:
+        raise ValueError("precision must be one of %s; got %r"
+                         % (sorted(PRECISIONS), precision)) from None
+
+
 def get_plan(kind, lmax, lmax_calc, norm, csphase, sampling=1, extend=0,
-             zero=None, w=None, device=None, tune=None, cplx=False):
+             zero=None, w=None, device=None, tune=None, cplx=False, precision="fp64"):
     """Cached Plan for the option set (thread-safe).  New plans are
     autotuned when ``tune`` is true or the environment sets SHTC_AUTOTUNE=1
-    (shtools_b200.autotune)."""
+    (shtools_b200.autotune).  precision "int8x6" runs the plan's syntheses on
+    the INT8 tensor cores with an error-free 6-byte split (norms 1, 2, 4)."""
     import os
     dev = torch.device("cuda", torch.cuda.current_device()) if device is None \
         else torch.device(device)
@@ -223,18 +243,36 @@ def get_plan(kind, lmax, lmax_calc, norm, csphase, sampling=1, extend=0,
         dev = torch.device("cuda", torch.cuda.current_device())
     zkey = None if zero is None else np.asarray(zero, dtype=np.float64).tobytes()
     wkey = None if w is None else np.asarray(w, dtype=np.float64).tobytes()
+    prec = _precision_code(precision)
     key = (kind, int(lmax), int(lmax_calc), int(norm), int(csphase),
-           int(sampling), int(extend), dev.index, zkey, wkey, bool(cplx))
+           int(sampling), int(extend), dev.index, zkey, wkey, bool(cplx), prec)
     with _cache_lock:
         p = _plans.get(key)
         if p is None:
             p = Plan(kind, lmax, lmax_calc, norm, csphase, sampling, extend,
                      zero, w, dev, cplx=cplx)
+            if prec:
+                p.set_precision(prec)
             _plans[key] = p
             if tune or (tune is None and os.environ.get("SHTC_AUTOTUNE") == "1"):
                 from . import autotune
                 autotune.tune_plan(p)
         return p
+
+
+def mixed_status(device=None):
+    """Error word of the tensor-core kernels on the device: 0, or
+    SHTC_ETIMEOUT (10) when a bounded in-kernel wait ran out since the last
+    call (the outputs of that transform are then invalid); clears it."""
+    import ctypes
+    lib = _lib.load()
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None \
+        else torch.device(device)
+    st = ctypes.c_int(0)
+    with _on_device(dev):
+        _lib.check(lib.shtc_mixed_status(ctypes.byref(st), _stream_ptr(dev)),
+                   "shtc_mixed_status")
+    return st.value
 
 
 def clear_plan_cache():
@@ -422,13 +460,14 @@ class _Analysis(torch.autograd.Function):
 # public API
 # ---------------------------------------------------------------------------
 def MakeGridDH(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
-               extend=False, dtype=None):
+               extend=False, dtype=None, precision="fp64"):
     """Driscoll-Healy synthesis on the GPU (src/MakeGridDH.f95:1).
 
     cilm: (..., 2, D, D) float64 or float32.  Returns (..., n+extend,
     sampling*n+extend) with n = 2*lmax+2; row 0 is 90 N, column 0 is 0 E.
     dtype: element type of the grid (default: that of cilm); the arithmetic
-    is FP64 either way.
+    is FP64 either way.  precision "int8x6": the Legendre sums on the INT8
+    tensor cores with an error-free 6-byte split (norms 1, 2, 4).
     """
     _check_common(norm, csphase)
     if sampling not in (1, 2):
@@ -438,7 +477,7 @@ def MakeGridDH(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
     dtype = _out_dtype(dtype)
     cilm = _as_cuda(cilm, "cilm")
     plan = get_plan(GRID_DH, lmax, lc, norm, csphase, sampling, int(bool(extend)),
-                    device=cilm.device)
+                    device=cilm.device, precision=precision)
     return _synthesis(cilm, plan, dtype)
 
 
@@ -459,11 +498,12 @@ def SHExpandDH(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None,
 
 
 def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
-                extend=False, dtype=None):
+                extend=False, dtype=None, precision="fp64"):
     """Gauss-Legendre synthesis on the GPU (src/MakeGridGLQ.f95:1).
 
     zero: the lmax+1 Gauss-Legendre nodes (e.g. from SHGLQ); None computes
     them with the GPU PreGLQ.  Returns (..., lmax+1, 2*lmax+1+extend).
+    precision: as for MakeGridDH.
     """
     _check_common(norm, csphase)
     lmax, lc = _resolve_synth(np.shape(cilm), lmax, lmax_calc)
@@ -471,7 +511,7 @@ def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
     z = None if zero is None else _host64(zero, lmax + 1, "zero")
     cilm = _as_cuda(cilm, "cilm")
     plan = get_plan(GRID_GLQ, lmax, lc, norm, csphase, 1, int(bool(extend)),
-                    zero=z, device=cilm.device)
+                    zero=z, device=cilm.device, precision=precision)
     return _synthesis(cilm, plan, dtype)
 
 

@@ -32,6 +32,8 @@ def test_pipelined_reused_outputs_and_errors(cuda, oracle):
     assert torch.equal(out[0], cuda.MakeGridGLQ(c.cuda()).cpu())
     with pytest.raises(ValueError):
         pipelined(lambda x: x, [(c,)], [], depth=2)
+    with pytest.raises(ValueError):
+        pipelined([lambda x: x] * 2, [(c,)], [(c,)], depth=2)
 
 
 def test_pipelined_alternating_step_kinds(cuda, oracle):
@@ -47,8 +49,8 @@ def test_pipelined_alternating_step_kinds(cuda, oracle):
         ins += [(cs[i],), (grids[2 - i],)]
         outs += [(torch.empty_like(grids[0]).pin_memory(),),
                  (torch.empty_like(cs[0]).pin_memory(),)]
-    fn = lambda t: cuda.MakeGridGLQ(t) if t.dim() == 3 else cuda.SHExpandGLQ(t)
-    pipelined(fn, ins, outs, depth=2)
+    fns = [lambda t: cuda.MakeGridGLQ(t), lambda t: cuda.SHExpandGLQ(t)] * 3
+    pipelined(fns, ins, outs, depth=2)
     torch.cuda.synchronize()
     for i in range(3):
         assert torch.equal(outs[2 * i][0], grids[i])
