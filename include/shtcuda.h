@@ -239,8 +239,10 @@ SHTC_API int shtc_dhaj(int n, double* aj, int extend, void* stream);
  * afford cudaMalloc's implicit synchronisation).  The array holds
  * SHTC_NOALLOC_SCRATCH_BYTES on every GPU that loads the library, until
  * exit.  Transforms needing more (shtc_workspace_bytes(plan, nfield) above
- * that size, e.g. one DH field beyond lmax ~600) return SHTC_EWORK without
- * launching.  The first call on a device looks up the array's device
+ * that size, e.g. one DH field beyond lmax ~600; that size includes the
+ * plan's analysis tiles, set by its tile shape, and its precision's
+ * scratch) return SHTC_EWORK without launching; a plan of another device
+ * than the current one returns SHTC_EHANDLE.  The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress) and caches it: make it before any stream
  * capture.  All calls share the array; calls that overlap on the GPU race. */
 #define SHTC_NOALLOC_SCRATCH_BYTES (16u << 20)

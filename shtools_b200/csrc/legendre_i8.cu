@@ -64,7 +64,7 @@ constexpr int kPairs = 128;          // ring pairs per CTA (TMEM lanes, MMA M)
 constexpr int kTileDeg = 64;         // degrees per K-tile (32 of each parity)
 constexpr int kStages = 8;           // B / recursion-table stages in shared memory
 constexpr int kProducers = 256;      // eight producer warps
-constexpr int kThreads = kProducers + 32;
+constexpr int kThreads = kProducers + 64;   // + MMA warp + stage-loader warp
 constexpr unsigned kSpinLimit = 1u << 22;   // bounded mbarrier waits (seconds)
 constexpr int kTmemAlloc = 512;
 
@@ -90,7 +90,7 @@ __host__ __device__ constexpr int bimage_bytes(int N, int DB) { return 2 * DB * 
 // shared-memory stack of one parity: KW - DB zero tiles, the DB digit
 // tiles, DA - 1 zero tiles
 __host__ __device__ constexpr int bstack_tiles(int DA, int DB, int KW) { return DA + KW - 1; }
-constexpr int kRecBytes = kTileDeg * 16;   // 64 x {beta, D}
+constexpr int kRecBytes = kTileDeg * 32;   // 64 x {gamma, delta, D, 0}
 __host__ __device__ constexpr int stage_bytes(int N, int DA, int DB, int KW) {
     return 2 * bstack_tiles(DA, DB, KW) * btile_bytes(N) + kRecBytes;
 }
@@ -191,6 +191,15 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
             "r"(smem_u32(dst)),
         "l"(src), "r"(bytes), "r"(smem_u32(b))
         : "memory");
+}
+
+// true in one lane of the (converged) warp
+__device__ __forceinline__ bool elect_one() {
+    uint32_t pred;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\telect.sync _|p, 0xffffffff;\n\tselp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(pred));
+    return pred != 0;
 }
 
 __device__ __forceinline__ void tc_fence_before() {
@@ -335,7 +344,7 @@ __device__ __forceinline__ void pack4(const uint32_t* lo, const uint32_t* hi, ui
 }
 
 struct SynthArgs {
-    const double2* rec;      // plan {beta, D} per packed (l, m)
+    const double4* rec2;     // plan {gamma, delta, D, 0} per packed (l, m)
     const double* pmm;       // sectoral start values
     const double* rtab;      // u^m / 1e-280 per (m, pair)
     const double* zp;        // z of the northern ring of each pair
@@ -358,15 +367,23 @@ __device__ __forceinline__ void item_decode(long long i, int ptiles, int ngroups
     *tile = r - (*g) * ptiles;
 }
 
-// One 64-degree K-tile of a producer thread: advances the pair's recursion
-// (q1, q2) by 64 degrees (table entries recs[0..63] = {beta(s), D(s)}) and
-// writes the digit words of the degrees of parity QR: W[i * 8 + g] holds
-// digit i of the K indices 4 g .. 4 g + 3 of that parity.  Degrees past lc
-// in the last tile read stale table entries: their digits are garbage but
-// finite integers, and the coefficient image is zero there.
+// One 64-degree K-tile of a producer thread: advances the chain of the
+// pair's recursion values of parity QR (degrees s = 64 t + j, j % 2 = QR)
+// by 32 steps of the same-parity two-step form of the rescaled recursion
+//     Q(r) = (z^2 - gamma(r)) Q(r-2) - delta(r) Q(r-4),
+//     gamma(r) = beta(r-1) + beta(r),  delta(r) = beta(r-1) beta(r-2)
+// (recs[j] = {gamma, delta, D, 0}), and writes the digit words of those
+// degrees: W[i * 8 + g] holds digit i of the K indices 4 g .. 4 g + 3 of the
+// parity.  c1, c2 = Q(r-2), Q(r-4).  Segment ends (s % 16 == 0) rescale the
+// chains as the one-step form rescales at s: the even chain after Q(s), the
+// odd chain before Q(s+1), both by D(s).  The first tile starts the chains
+// from Q(0) = start, Q(-2) = start (beta(0) = -1) and Q(1) = z start,
+// Q(-1) = 0, set by the caller.  Degrees past lc in the last tile read stale
+// table entries: their digits are garbage but finite integers, and the
+// coefficient image is zero there.
 template <int DA, int QR>
-__device__ __forceinline__ void tile_digits(const double2* recs, double z, double rp, double& q1,
-                                            double& q2, uint32_t* W) {
+__device__ __forceinline__ void tile_digits(const double4* recs, double z2, double rp,
+                                            bool first, double& c1, double& c2, uint32_t* W) {
     // 1.5 * 2^52 + 0x808080808080: for |X| < 2^46 the low 48 bits of the
     // rounded sum are X + 0x808080808080 (DA = 6)
     constexpr double kMagic6 = 6896688841130112.0;
@@ -375,32 +392,36 @@ __device__ __forceinline__ void tile_digits(const double2* recs, double z, doubl
 #pragma unroll
     for (int g8 = 0; g8 < 8; ++g8) {
         uint32_t lo[4], hi[4];
-        double2 f8[8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) f8[u] = recs[g8 * 8 + u];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int j = g8 * 8 + u;     // s = 64 t + j: segment ends at j % 16 == 0
-            const double2 f = f8[u];
-            const double pv = fma(z, q1, -(f.x * q2));
-            q2 = q1;
-            q1 = pv;
-            if ((u & 1) == QR) {
-                unsigned long long y;
-                if constexpr (DA == 6) {
-                    y = (unsigned long long)__double_as_longlong(fma(pv * f.y, rp, kMagic6));
-                } else {
-                    // bits(1.5 * 2^52 + X) = 0x4338000000000000 + X for
-                    // |X| < 2^51; adding kOffset7 leaves X + 0x80..80 (7 bytes)
-                    y = (unsigned long long)__double_as_longlong(fma(pv * f.y, rp, kMagic)) +
-                        kOffset7;
-                }
-                lo[u >> 1] = (uint32_t)y;
-                hi[u >> 1] = (uint32_t)(y >> 32);
+        for (int k = 0; k < 4; ++k) {
+            const int j = g8 * 8 + 2 * k + QR;
+            const double4 f = recs[j];
+            if (QR == 1 && (j & (kRecSegment - 1)) == 1) {
+                const double d = recs[j - 1].z;
+                c1 *= d;
+                c2 *= d;
             }
-            if ((j & (kRecSegment - 1)) == 0) {
-                q1 *= f.y;
-                q2 *= f.y;
+            double q;
+            if (j < 2 && first) {
+                q = c1;                          // Q(0) or Q(1), set by the caller
+            } else {
+                q = fma(z2 - f.x, c1, -(f.y * c2));
+                c2 = c1;
+                c1 = q;
+            }
+            unsigned long long y;
+            if constexpr (DA == 6) {
+                y = (unsigned long long)__double_as_longlong(fma(q * f.z, rp, kMagic6));
+            } else {
+                // bits(1.5 * 2^52 + X) = 0x4338000000000000 + X for |X| < 2^51;
+                // adding kOffset7 leaves X + 0x80..80 (7 bytes)
+                y = (unsigned long long)__double_as_longlong(fma(q * f.z, rp, kMagic)) + kOffset7;
+            }
+            lo[k] = (uint32_t)y;
+            hi[k] = (uint32_t)(y >> 32);
+            if (QR == 0 && (j & (kRecSegment - 1)) == 0) {
+                c1 *= f.z;
+                c2 *= f.z;
             }
         }
         uint32_t w[DA];
@@ -470,90 +491,104 @@ __global__ void __launch_bounds__(kThreads, 1) k_legendre_synth_i8(SynthArgs a) 
     tc_fence_after();
     const uint32_t tmem = tmem_base;
 
-    if (warp == 8) {
-        // ------------------------------------------------ MMA / copy issue
-        long long issued = 0, consumed = 0;   // stages loaded / tiles multiplied
+    if (warp == 9) {
+        // ------------------------------------------------ stage loader
+        // fills stage T % kStages with the coefficient digits and the
+        // recursion table of K-tile T, item by item; the image and table
+        // addresses are set up once per item
         if (lane == 0) {
-            long long li = blockIdx.x;        // loader cursor: item and tile
-            int lt = 0;
-            int kitem = 0;
-            for (long long it = blockIdx.x; it < nitems && !abort_flag;
-                 it += gridDim.x, ++kitem) {
+            long long L = 0;                  // stages issued
+            for (long long it = blockIdx.x; it < nitems && !abort_flag; it += gridDim.x) {
                 int m, g, tile;
                 item_decode(it, a.ptiles, a.ngroups, &m, &g, &tile);
                 const int nt = ntiles_of(a.lc, m);
-                for (int t = 0; t < nt && !abort_flag; ++t) {
-                    const long long T = consumed;
-                    // copies run up to two tiles ahead of the stage being
-                    // refilled, so every wait on empty[] is for its latest phase
-                    while (issued <= T + kStages - 2 && li < nitems && !abort_flag) {
-                        const int st = (int)(issued % kStages);
-                        if (issued >= kStages &&
-                            !mbar_wait(&empty[st], (uint32_t)((issued / kStages - 1) & 1),
-                                       &abort_flag))
-                            break;
-                        int lm, lg, ltile;
-                        item_decode(li, a.ptiles, a.ngroups, &lm, &lg, &ltile);
-                        const int lnt = ntiles_of(a.lc, lm);
-                        const int rdeg = min(kTileDeg, a.lc - lm + 1 - kTileDeg * lt);
-                        uint8_t* sb = smem_i8 + st * SB;
-                        const uint8_t* src =
-                            a.image + ((a.toff[lm] * a.ngroups + (long long)lg * lnt + lt) *
-                                       (long long)bimage_bytes(N, DB));
-                        const double2* rsrc = a.rec + packed_off(lm, a.lc) + kTileDeg * lt;
-                        constexpr uint32_t half = DB * BT;
-                        mbar_expect_tx(&full[st], (uint32_t)(2 * half + rdeg * 16));
-                        bulk_g2s(sb + (KW - DB) * BT, src, half, &full[st]);
-                        bulk_g2s(sb + NBLK * BT + (KW - DB) * BT, src + half, half, &full[st]);
-                        bulk_g2s(sb + 2 * NBLK * BT, rsrc, (uint32_t)(rdeg * 16), &full[st]);
-                        ++issued;
-                        if (++lt == lnt) {
-                            lt = 0;
-                            li += gridDim.x;
-                        }
-                    }
-                    if (abort_flag) break;
-                    const int st = (int)(T % kStages);
-                    const int buf = (int)(T & 1);
-                    if (!mbar_wait(&full[st], (uint32_t)((T / kStages) & 1), &abort_flag)) break;
-                    if (!mbar_wait(&afull[buf], (uint32_t)((T >> 1) & 1), &abort_flag)) break;
-                    if (t == 0 && kitem > 0 &&
-                        !mbar_wait(&dfree, (uint32_t)((kitem - 1) & 1), &abort_flag))
+                const int nsteps = a.lc - m + 1;
+                const uint8_t* src0 =
+                    a.image + ((a.toff[m] * a.ngroups + (long long)g * nt) *
+                               (long long)bimage_bytes(N, DB));
+                const double4* rsrc0 = a.rec2 + packed_off(m, a.lc);
+                for (int t = 0; t < nt && !abort_flag; ++t, ++L) {
+                    const int st = (int)(L % kStages);
+                    // the MMAs of the stage's previous tile have completed
+                    if (L >= kStages &&
+                        !mbar_wait(&empty[st], (uint32_t)((L / kStages - 1) & 1), &abort_flag))
                         break;
-                    tc_fence_after();
-                    const uint32_t sbase = smem_u32(smem_i8 + st * SB);
-                    // A digit i times the window of coefficient digits
-                    // TOP - KW + 1 - i .. TOP - i into the KW weight blocks
-                    // of the parity's accumulator; the parities alternate.
-                    // The first MMA of an item overwrites every block.
-#pragma unroll
-                    for (int i = 0; i < DA; ++i) {
-#pragma unroll
-                        for (int q = 0; q < 2; ++q) {
-                            const uint32_t acc = (t > 0 || i > 0) ? 1u : 0u;
-                            const uint32_t d = tmem + (uint32_t)(q * KW * N);
-                            const uint32_t at = tmem + kColA +
-                                                (uint32_t)(buf * tmem_cols_a(DA) + (q * DA + i) * 8);
-                            const uint64_t bd = smem_desc(
-                                sbase + (uint32_t)(q * NBLK * BT + (DA - 1 - i) * BT), 128, 256);
-                            mma_ts(d, at, bd, idesc_i8(128, KW * N, 1, 1), acc);
-                        }
-                    }
-                    tc_commit(&mdone[buf]);
-                    tc_commit(&empty[st]);
-                    ++consumed;
+                    const int rdeg = min(kTileDeg, nsteps - kTileDeg * t);
+                    uint8_t* sb = smem_i8 + st * SB;
+                    const uint8_t* src = src0 + (long long)t * bimage_bytes(N, DB);
+                    constexpr uint32_t half = DB * BT;
+                    mbar_expect_tx(&full[st], (uint32_t)(2 * half + rdeg * 32));
+                    bulk_g2s(sb + (KW - DB) * BT, src, half, &full[st]);
+                    bulk_g2s(sb + NBLK * BT + (KW - DB) * BT, src + half, half, &full[st]);
+                    bulk_g2s(sb + 2 * NBLK * BT, rsrc0 + kTileDeg * t, (uint32_t)(rdeg * 32),
+                             &full[st]);
                 }
             }
-            // drain (bounded, also after an abort): copies issued but not
-            // consumed, then the MMAs of the last tile
-            for (long long T = consumed; T < issued; ++T)
+            // drain (bounded): every copy issued has landed before exit
+            for (long long T = L - kStages < 0 ? 0 : L - kStages; T < L; ++T)
                 for (unsigned k = 0; k < kSpinLimit; ++k)
                     if (mbar_try(&full[T % kStages], (uint32_t)((T / kStages) & 1))) break;
-            if (consumed > 0) {
-                const long long T = consumed - 1;
-                for (unsigned k = 0; k < kSpinLimit; ++k)
-                    if (mbar_try(&mdone[T & 1], (uint32_t)((T >> 1) & 1))) break;
+        }
+        __syncwarp();
+    } else if (warp == 8) {
+        // ------------------------------------------------ MMA issue
+        // The whole warp runs the loop on warp-uniform values (the TMEM base
+        // broadcast from lane 0, descriptors from the shared-memory base and
+        // loop counters), so they stay in uniform registers; one elected lane
+        // issues each MMA and commit.  A single thread computing per-lane
+        // values spends about 100 cycles per MMA on moving them into uniform
+        // registers (measured on B200), more than the MMA itself.
+        const uint32_t tm = __shfl_sync(0xffffffffu, tmem, 0);
+        const bool leader = elect_one();
+        const uint64_t desc0 = smem_desc(smem_u32(smem_i8), 128, 256);
+        constexpr uint32_t idesc = idesc_i8(128, KW * N, 1, 1);
+        long long T = 0;                      // tiles multiplied
+        int kitem = 0;
+        for (long long it = blockIdx.x; it < nitems && !abort_flag; it += gridDim.x, ++kitem) {
+            int m, g, tile;
+            item_decode(it, a.ptiles, a.ngroups, &m, &g, &tile);
+            const int nt = ntiles_of(a.lc, m);
+            for (int t = 0; t < nt && !abort_flag; ++t) {
+                const int st = (int)(T % kStages);
+                const int buf = (int)(T & 1);
+                bool ok = mbar_wait(&full[st], (uint32_t)((T / kStages) & 1), &abort_flag) &&
+                          mbar_wait(&afull[buf], (uint32_t)((T >> 1) & 1), &abort_flag) &&
+                          (t > 0 || kitem == 0 ||
+                           mbar_wait(&dfree, (uint32_t)((kitem - 1) & 1), &abort_flag));
+                if (!__all_sync(0xffffffffu, ok)) break;
+                tc_fence_after();
+                // descriptor start addresses advance in 16-byte units
+                const uint64_t dst = desc0 + (uint64_t)((st * SB) >> 4);
+                // A digit i times the window of coefficient digits
+                // TOP - KW + 1 - i .. TOP - i into the KW weight blocks of
+                // the parity's accumulator; the parities alternate.  The
+                // first MMA of an item overwrites every block.
+#pragma unroll
+                for (int i = 0; i < DA; ++i) {
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const uint32_t acc = (t > 0 || i > 0) ? 1u : 0u;
+                        const uint32_t d = tm + (uint32_t)(q * KW * N);
+                        const uint32_t at =
+                            tm + kColA + (uint32_t)(buf * tmem_cols_a(DA) + (q * DA + i) * 8);
+                        const uint64_t bd =
+                            dst + (uint64_t)((q * NBLK * BT + (DA - 1 - i) * BT) >> 4);
+                        if (leader) mma_ts(d, at, bd, idesc, acc);
+                    }
+                }
+                if (leader) {
+                    tc_commit(&mdone[buf]);
+                    tc_commit(&empty[st]);
+                }
+                __syncwarp();
+                ++T;
             }
+        }
+        // drain (bounded): the MMAs of the last tile
+        if (T > 0) {
+            const long long Tl = T - 1;
+            for (unsigned k = 0; k < kSpinLimit; ++k)
+                if (mbar_try(&mdone[Tl & 1], (uint32_t)((Tl >> 1) & 1))) break;
         }
         __syncwarp();
     } else {
@@ -571,7 +606,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_legendre_synth_i8(SynthArgs a) 
             const bool valid = p < a.npair;
             const double z = valid ? a.zp[p] : 0.0;
             const double rp = valid ? a.rtab[(long long)m * a.npair + p] * a.ascale : 0.0;
-            double q1 = 0.0, q2 = a.pmm[m];     // step s = 0 (beta = -1) gives Q(0) = start
+            // the chain of this warp's parity: Q(0) = start, Q(-2) = start
+            // (with beta(0) = -1 the two-step form gives Q(2)), or Q(1) =
+            // z start, Q(-1) = 0
+            const double start = a.pmm[m];
+            double c1 = qrole == 0 ? start : z * start;
+            double c2 = qrole == 0 ? start : 0.0;
+            const double z2 = z * z;
             // output scales of this warp's epilogue columns, loaded early:
             // 2^(8 WB) 2^-a 2^-b(m, n)
             double sc[8];
@@ -600,11 +641,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_legendre_synth_i8(SynthArgs a) 
                     mbar_arrive(&afull[pbuf]);
                     pending = false;
                 }
-                const double2* recs =
-                    reinterpret_cast<const double2*>(smem_i8 + st * SB + 2 * NBLK * BT);
+                const double4* recs =
+                    reinterpret_cast<const double4*>(smem_i8 + st * SB + 2 * NBLK * BT);
                 uint32_t W[DA * 8];     // [digit][word]: word g8 = K indices 4 g8 .. 4 g8 + 3
-                if (qrole == 0) tile_digits<DA, 0>(recs, z, rp, q1, q2, W);
-                else tile_digits<DA, 1>(recs, z, rp, q1, q2, W);
+                if (qrole == 0) tile_digits<DA, 0>(recs, z2, rp, t == 0, c1, c2, W);
+                else tile_digits<DA, 1>(recs, z2, rp, t == 0, c1, c2, W);
                 // the MMAs of tile T - 2 have read this A buffer
                 if (!__all_sync(0xffffffffu,
                                 T < 2 || mbar_wait(&mdone[buf], (uint32_t)(((T >> 1) - 1) & 1),
@@ -678,6 +719,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_legendre_synth_i8(SynthArgs a) 
 }
 
 // --------------------------------------------------------------------------
+// {gamma(r), delta(r), D(r), 0} of the same-parity two-step recursion from
+// the plan's {beta(r), D(r)}: gamma = beta(r-1) + beta(r), delta =
+// beta(r-1) beta(r-2) (r >= 2; entries r < 2 are not used by the chains)
+// --------------------------------------------------------------------------
+__global__ void k_i8_rec2(const double2* __restrict__ rec, double4* __restrict__ rec2, int lc) {
+    const int m = blockIdx.y;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m + r > lc) return;
+    const long long o = packed_off(m, lc);
+    const double2 f = rec[o + r];
+    double g = 0.0, d = 0.0;
+    if (r >= 2) {
+        const double b1 = rec[o + r - 1].x, b2 = rec[o + r - 2].x;
+        g = b1 + f.x;
+        d = b1 * b2;
+    }
+    rec2[o + r] = make_double4(g, d, f.y, 0.0);
+}
+
+// --------------------------------------------------------------------------
 // host side
 // --------------------------------------------------------------------------
 // columns of a field group: 2 x 8 fields (MMA N of the weight window =
@@ -726,6 +787,17 @@ int set_precision_tables(shtc_plan* P, int precision) {
         P->d_i8_toff = d;
         P->i8_ntot = acc;
     }
+    if (!P->d_i8_rec2) {
+        double4* d = nullptr;
+        if (cudaMalloc((void**)&d, sizeof(double4) * (size_t)P->nlm) != cudaSuccess)
+            return SHTC_EALLOC;
+        k_i8_rec2<<<dim3((P->lc + 1 + 127) / 128, P->lc + 1), 128>>>(P->d_rec, d, P->lc);
+        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+            cudaFree(d);
+            return SHTC_ECUDA;
+        }
+        P->d_i8_rec2 = d;
+    }
     // |P_lm| bound over l <= lc: sqrt(2l+1) (4pi), 1 (Schmidt), sqrt((2l+1)/4pi)
     const double pi = 3.141592653589793238462643383279502884;
     double bound = 1.0;
@@ -751,10 +823,11 @@ static int launch_synth_i8_n(const shtc_plan* P, const double2* coef, double2* s
         coef, (uint32_t*)image, P->d_i8_toff, colinv, P->lc, nfield, ngroups);
     int rc = map_cuda(cudaGetLastError());
     if (rc) return rc;
-    // 120 KB of shared memory keeps one CTA (and one 512-column TMEM
-    // allocation) per SM
-    const size_t smem = 120 * 1024;
-    static_assert(kStages * stage_bytes(N, DA, DA, KW) <= 120 * 1024, "stages fit the reservation");
+    // at least 120 KB of shared memory keeps one CTA (and one 512-column
+    // TMEM allocation) per SM
+    constexpr size_t stages = (size_t)kStages * stage_bytes(N, DA, DA, KW);
+    const size_t smem = stages > 120 * 1024 ? stages : 120 * 1024;
+    static_assert(stages <= 200 * 1024, "stages fit in shared memory");
     if ((rc = kernel_smem_attr((const void*)k_legendre_synth_i8<N, DA>, smem, true))) return rc;
     static int nsm[64] = {0};
     const int dev = P->device;
@@ -762,7 +835,7 @@ static int launch_synth_i8_n(const shtc_plan* P, const double2* coef, double2* s
         cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
     const int sms = dev < 64 && nsm[dev] > 0 ? nsm[dev] : 148;
     SynthArgs a;
-    a.rec = P->d_rec;
+    a.rec2 = P->d_i8_rec2;
     a.pmm = P->d_pmm;
     a.rtab = P->d_rtab;
     a.zp = P->d_z;

@@ -9,7 +9,11 @@
 // a transform without managing a workspace buffer themselves.
 //
 // The array, g_scratch, is a file-scope __device__ array of
-// SHTC_NOALLOC_SCRATCH_BYTES (16 MiB).  Every GPU that loads this library
+// SHTC_NOALLOC_SCRATCH_BYTES (16 MiB).  A call fits when
+// shtc_workspace_bytes(plan, nfield) does: that size includes the plan's
+// analysis partial-sum tiles (which follow its tile shape, set by the
+// autotuner or shtc_plan_set_tuning) and, for a plan of tensor-core
+// precision, the coefficient image of that path.  Every GPU that loads this library
 // holds it until the process exits.  Host code cannot use the name
 // g_scratch as a device address (it is a host-side stand-in), so the first
 // call on each device looks up the real address with cudaGetSymbolAddress,
@@ -63,6 +67,12 @@ extern "C" SHTC_API int shtc_synthesis_noalloc(
     long long gsr, long long gsc, int nfield, void* stream) {
     if (!plan || !cilm || !grid) return SHTC_EHANDLE;
     if (nfield < 1) return SHTC_EBOUND;
+    // the plan's device must be current before the first call sets up the
+    // array's address there (otherwise a device the caller never uses would
+    // be initialised, and the synthesis would refuse the call anyway)
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return SHTC_ECUDA;
+    if (dev != plan->device) return SHTC_EHANDLE;
     const size_t need = shtc_workspace_bytes(plan, nfield);
     if (need == 0) return SHTC_EHANDLE;
     if (need > kScratchBytes) return SHTC_EWORK;   // beyond the fixed array

@@ -99,6 +99,8 @@ struct shtc_plan {
     // SHTC_PREC_INT8X6 for the tensor-core synthesis (legendre_i8.cu)
     int precision;
     long long* d_i8_toff;   // INT8X6: K-tiles of 64 degrees before each order (lc + 2)
+    double4* d_i8_rec2;     // INT8X6: {gamma, delta, D, 0} per packed (l, m): the
+                            // same-parity two-step form of the rescaled recursion
     long long i8_ntot;      // INT8X6: K-tiles of all orders
     double i8_ascale;       // INT8X6: 2^a, fixed-point scale of the P_lm operand
 };

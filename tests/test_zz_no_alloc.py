@@ -51,9 +51,13 @@ def _call(fn, plan, c, out):
 def test_noalloc_synthesis_matches_synthesis_twice(cuda):
     from shtools_b200 import _lib
     fn = _bind(_lib.load())
+    small = (cuda.get_plan(cuda.GRID_GLQ, 63, 63, 1, 1, 1, 0), _power_law(63, 1, 1))
+    # the small plan again after the larger one has filled more of the array:
+    # no stale bytes of an earlier call may be read
     cases = [
-        (cuda.get_plan(cuda.GRID_GLQ, 63, 63, 1, 1, 1, 0), _power_law(63, 1, 1)),
+        small,
         (cuda.get_plan(cuda.GRID_DH, 200, 200, 4, -1, 2, 1), _power_law(200, 2, 2)),
+        small,
     ]
     for plan, c in cases:
         ref = plan.synthesis(c)                      # existing entry point
