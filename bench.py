@@ -81,6 +81,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--workload", default="glq2047", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "int8x6", "int8x7"],
+                    help="Legendre sums of the synthesis: FP64, or the INT8 tensor-core "
+                         "error-free split with 6 or 7 byte digits (real DH/GLQ workloads)")
+    ap.add_argument("--no-2799", action="store_true",
+                    help="skip the lmax-2799 (16 DH fields) FP64 / int8x7 comparison "
+                         "that the default workload adds to its line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the default Legendre tile shapes instead of tuning "
@@ -369,6 +375,14 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
 def fp64_peak(torch, dev):
     """Measured FP64 FMA throughput of this GPU (TFLOP/s), from the probe."""
     import ctypes
@@ -864,6 +878,83 @@ def run_cuda_multiply(args, w, rank, world, local_rank):
     }
 
 
+def i8_tensor_ops(w, nfield, precision):
+    """INT8 multiply-add operations (2 per MAC) that one tensor-core synthesis
+    launch executes: per 64-degree K-tile of a 128-pair tile and a group of 8
+    fields, 2 x DA MMAs of M = 128, N = KW x 16, K = 32 (the weight windows
+    of shtools_b200/csrc/legendre_i8.cu)."""
+    DA, KW = (7, 8) if precision == "int8x7" else (6, 7)
+    L = w["lmax"]
+    # ring pairs: GLQ (L+1 rings) (L+2)//2, DH (2L+2 rings, with the pole
+    # and the equator) L+2
+    npair = (L + 2) // 2 if w["kind"] == "glq" else L + 2
+    ptiles = (npair + 127) // 128
+    groups = (nfield + 7) // 8
+    ktiles = sum((L - m + 1 + 63) // 64 for m in range(L + 1))
+    return 2.0 * ktiles * ptiles * groups * 2 * DA * (128 * KW * 16 * 32)
+
+
+def compare_2799(dev, steps=3):
+    """The lmax-2799 half of the metric, added to the default line: 16 DH
+    fields, lmax 2799, sampling 2 (5600 x 11200), S(l) = (l+1)^-3; synthesis
+    + FP64 analysis with the FP64 synthesis and with the int8x7 tensor-core
+    synthesis; transforms/s of each and the per-degree error of the int8x7
+    result against the FP64 one (both analysed in FP64)."""
+    import ctypes
+    import numpy as np
+    import torch
+    import shtools_b200 as sht
+    from shtools_b200 import _lib
+    lib = _lib.load()
+    w = WORKLOADS["dh2799x16"]
+    L, F, smp = w["lmax"], w["nfield"], w["sampling"]
+    c = torch.from_numpy(np.stack([power_law(L, w["seed"] + i, w["beta"])
+                                   for i in range(F)])).to(dev)
+    st = torch.cuda.current_stream(dev)
+    res, ref = {}, None
+    for prec in ("fp64", "int8x7"):
+        ps = sht.get_plan(sht.GRID_DH, L, L, 1, 1, smp, 0, device=dev, precision=prec)
+        pa = sht.get_plan(sht.GRID_DH, L, L, 1, 1, smp, 0, device=dev)
+        g = ps.synthesis(c)
+        b = pa.analysis(g)
+        torch.cuda.synchronize(dev)
+        ms = (ctypes.c_double * 6)()
+        cnt = (ctypes.c_int * 6)()
+        lib.shtc_timing_enable(1)
+        lib.shtc_timing_collect(ms, cnt, 6)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(steps)]
+        for i in range(steps):
+            evs[i][0].record(st)
+            ps.synthesis(c, out=g)
+            pa.analysis(g, out=b)
+            evs[i][1].record(st)
+        torch.cuda.synchronize(dev)
+        lib.shtc_timing_enable(0)
+        lib.shtc_timing_collect(ms, cnt, 6)
+        t = sum(a.elapsed_time(e) for a, e in evs)
+        entry = {"transforms_per_s": 2.0 * F * steps / (t * 1e-3),
+                 "ms_per_step": t / steps,
+                 "legendre_synth_ms": ms[1] / max(1, cnt[1]),
+                 "legendre_anal_ms": ms[4] / max(1, cnt[4]),
+                 "fft_c2r_ms": ms[2] / max(1, cnt[2]), "fft_r2c_ms": ms[3] / max(1, cnt[3])}
+        if prec == "fp64":
+            ref = b.clone()
+        else:
+            d = (b - ref).pow(2).sum(dim=(1, 3)).sqrt()
+            n = ref.pow(2).sum(dim=(1, 3)).sqrt()
+            e = torch.where(n > 0, d / n, d)
+            entry["max_perdeg_rel_err_vs_fp64"] = float(e.max())
+            entry["status"] = sht.mixed_status(dev)
+        res[prec] = entry
+        del g, b
+    res["workload"] = "16 DH fields, lmax 2799, sampling 2 (5600 x 11200), S(l)=(l+1)^-3"
+    res["step"] = "synthesis (FP64 or int8x7) + FP64 analysis, L2 not flushed"
+    res["synthesis_speedup_int8x7"] = (res["fp64"]["legendre_synth_ms"] /
+                                       res["int8x7"]["legendre_synth_ms"])
+    return res
+
+
 def run_cuda(args, w, rank, world, local_rank):
     import numpy as np
     import torch
@@ -886,11 +977,11 @@ def run_cuda(args, w, rank, world, local_rank):
     elif w["kind"] == "glq":
         zero_t, w_t = sht.PreGLQ(-1.0, 1.0, L + 1, device=dev)
         zero, wts = zero_t.cpu().numpy(), w_t.cpu().numpy()
-        synth = lambda x: sht.MakeGridGLQ(x, zero=zero)
+        synth = lambda x: sht.MakeGridGLQ(x, zero=zero, precision=args.precision)
         anal = lambda g: sht.SHExpandGLQ(g, w=wts, zero=zero)
     else:
         s = w["sampling"]
-        synth = lambda x: sht.MakeGridDH(x, sampling=s)
+        synth = lambda x: sht.MakeGridDH(x, sampling=s, precision=args.precision)
         anal = lambda g: sht.SHExpandDH(g, sampling=s)
 
     def step(x):
@@ -1071,6 +1162,19 @@ def run_cuda(args, w, rank, world, local_rank):
         "gpu_launches": int(sum(cnt)),
         "clocks": clk.summary(),
     }
+    if args.precision != "fp64" and not cplx:
+        ops = i8_tensor_ops(w, F, args.precision)
+        syn_ms = ms[1] / max(1, cnt[1])
+        tops = ops / (syn_ms * 1e-3) / 1e12
+        peak_i8 = 2.0 * measured_peaks().get("bf16_tflops", 1590.0)
+        res["tensor_synthesis"] = {
+            "kernel": "k_legendre_synth_i8", "precision": args.precision,
+            "ms_per_launch": syn_ms, "int8_ops_per_launch": ops, "achieved_tops": tops,
+            "peak_tops": peak_i8, "frac": tops / peak_i8,
+            "peak_source": "2 x the measured bf16 dense rate (MEASURED_PEAKS.json "
+                           "has no INT8 entry; B200 INT8 dense = 2 x BF16 nominal)"}
+    if args.workload == "glq2047" and world == 1 and not args.no_2799:
+        res["lmax2799"] = compare_2799(dev)
     return res
 
 

@@ -309,6 +309,11 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* w) {
         "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7])
         : "memory");
 }
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, const uint32_t* w) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr),
+                 "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3])
+                 : "memory");
+}
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t* v) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
@@ -374,14 +379,14 @@ __device__ __forceinline__ void item_decode(long long i, int ptiles, int ngroups
 //     gamma(r) = beta(r-1) + beta(r),  delta(r) = beta(r-1) beta(r-2)
 // (recs[j] = {gamma, delta, D, 0}), and writes the digit words of those
 // degrees: W[i * 8 + g] holds digit i of the K indices 4 g .. 4 g + 3 of the
-// parity.  c1, c2 = Q(r-2), Q(r-4).  Segment ends (s % 16 == 0) rescale the
+// parity; groups G0 .. G1 - 1 of 8 degrees.  c1, c2 = Q(r-2), Q(r-4).  Segment ends (s % 16 == 0) rescale the
 // chains as the one-step form rescales at s: the even chain after Q(s), the
 // odd chain before Q(s+1), both by D(s).  The first tile starts the chains
 // from Q(0) = start, Q(-2) = start (beta(0) = -1) and Q(1) = z start,
 // Q(-1) = 0, set by the caller.  Degrees past lc in the last tile read stale
 // table entries: their digits are garbage but finite integers, and the
 // coefficient image is zero there.
-template <int DA, int QR>
+template <int DA, int QR, int G0, int G1>
 __device__ __forceinline__ void tile_digits(const double4* recs, double z2, double rp,
                                             bool first, double& c1, double& c2, uint32_t* W) {
     // 1.5 * 2^52 + 0x808080808080: for |X| < 2^46 the low 48 bits of the
@@ -390,7 +395,7 @@ __device__ __forceinline__ void tile_digits(const double4* recs, double z2, doub
     constexpr double kMagic = 6755399441055744.0;                 // 1.5 * 2^52
     constexpr unsigned long long kOffset7 = 0xBD48808080808080ull;   // 0x80..80 - bits(kMagic)
 #pragma unroll
-    for (int g8 = 0; g8 < 8; ++g8) {
+    for (int g8 = G0; g8 < G1; ++g8) {
         uint32_t lo[4], hi[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -644,17 +649,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_legendre_synth_i8(SynthArgs a) 
                 const double4* recs =
                     reinterpret_cast<const double4*>(smem_i8 + st * SB + 2 * NBLK * BT);
                 uint32_t W[DA * 8];     // [digit][word]: word g8 = K indices 4 g8 .. 4 g8 + 3
-                if (qrole == 0) tile_digits<DA, 0>(recs, z2, rp, t == 0, c1, c2, W);
-                else tile_digits<DA, 1>(recs, z2, rp, t == 0, c1, c2, W);
-                // the MMAs of tile T - 2 have read this A buffer
+                const uint32_t acol = kColA + (uint32_t)(buf * tmem_cols_a(DA) + qrole * DA * 8);
+                // first half of the tile (32 degrees), then its stores, which
+                // overlap the second half; the MMAs of tile T - 2 have read
+                // this A buffer before the first store
+                if (qrole == 0) tile_digits<DA, 0, 0, 4>(recs, z2, rp, t == 0, c1, c2, W);
+                else tile_digits<DA, 1, 0, 4>(recs, z2, rp, t == 0, c1, c2, W);
                 if (!__all_sync(0xffffffffu,
                                 T < 2 || mbar_wait(&mdone[buf], (uint32_t)(((T >> 1) - 1) & 1),
                                                    &abort_flag)))
                     break;
                 tc_fence_after();
-                const uint32_t acol = kColA + (uint32_t)(buf * tmem_cols_a(DA) + qrole * DA * 8);
 #pragma unroll
-                for (int i = 0; i < DA; ++i) tmem_st8(lane_base + acol + i * 8, W + i * 8);
+                for (int i = 0; i < DA; ++i) tmem_st4(lane_base + acol + i * 8, W + i * 8);
+                if (qrole == 0) tile_digits<DA, 0, 4, 8>(recs, z2, rp, t == 0, c1, c2, W);
+                else tile_digits<DA, 1, 4, 8>(recs, z2, rp, t == 0, c1, c2, W);
+#pragma unroll
+                for (int i = 0; i < DA; ++i) tmem_st4(lane_base + acol + i * 8 + 4, W + i * 8 + 4);
                 pending = true;
                 pbuf = buf;
             }
@@ -670,9 +681,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_legendre_synth_i8(SynthArgs a) 
                                                    &abort_flag)))
                 break;
             tc_fence_after();
-            if (qrole * 8 < N) {
-                const int c0 = qrole * 8;
-                double v[2][8];
+            const int c0 = qrole * 8;
+            double v[2][8];
+            if (c0 < N) {
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     uint32_t acc[KW][8];
@@ -691,22 +702,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_legendre_synth_i8(SynthArgs a) 
                                       fma((double)gsum[1], 16777216.0, (double)gsum[0])) * sc[c];
                     }
                 }
-                if (valid) {
-                    const double h = m ? 0.5 : 1.0;
-#pragma unroll
-                    for (int c = 0; c < 8; c += 2) {
-                        const int f = (c0 + c) >> 1, fg = g * NFG + f;
-                        if (fg >= a.nfield) continue;
-                        const double eR = v[0][c], oR = v[1][c];
-                        const double eI = v[0][c + 1], oI = v[1][c + 1];
-                        double2* o2 = a.spec + (((long long)fg * a.npair + p) * (a.lc + 1) + m) * 2;
-                        o2[0] = make_double2((eR + oR) * h, -(eI + oI) * h);
-                        o2[1] = make_double2((eR - oR) * h, -(eI - oI) * h);
-                    }
-                }
             }
+            // the accumulators are in registers: the next item's MMAs may
+            // overwrite them while the results are stored
             tc_fence_before();
             mbar_arrive(&dfree);
+            if (c0 < N && valid) {
+                const double h = m ? 0.5 : 1.0;
+#pragma unroll
+                for (int c = 0; c < 8; c += 2) {
+                    const int f = (c0 + c) >> 1, fg = g * NFG + f;
+                    if (fg >= a.nfield) continue;
+                    const double eR = v[0][c], oR = v[1][c];
+                    const double eI = v[0][c + 1], oI = v[1][c + 1];
+                    double2* o2 = a.spec + (((long long)fg * a.npair + p) * (a.lc + 1) + m) * 2;
+                    o2[0] = make_double2((eR + oR) * h, -(eI + oI) * h);
+                    o2[1] = make_double2((eR - oR) * h, -(eI - oI) * h);
+                }
+            }
         }
     }
     tc_fence_before();
