@@ -1033,7 +1033,8 @@ def run_cuda(args, w, rank, world, local_rank):
     # the call a pyshtools user makes after select_preferred_backend('cuda'):
     # numpy coefficients in, numpy grid out, numpy grid in, numpy
     # coefficients out, one field per call (shtools_b200.backend); the host
-    # copies (pageable numpy buffers) are inside the timed region
+    # copies (numpy buffers staged through pinned memory by
+    # shtools_b200.hostio) are inside the timed region
     from shtools_b200 import backend as B
     if cplx:
         s = w["sampling"]
@@ -1151,7 +1152,8 @@ def run_cuda(args, w, rank, world, local_rank):
                 "steps": plug_steps, "result_matches_device_run": plug_ok,
                 "path": "pyshtools backend call (shtools_b200.backend, numpy in and "
                         "out, one field per call): per field H2D cilm, synthesis, D2H "
-                        "grid, H2D grid, analysis, D2H cilm; pageable host buffers"},
+                        "grid, H2D grid, analysis, D2H cilm; numpy buffers staged "
+                        "through pinned chunks (shtools_b200.hostio)"},
         "e2e_pipelined": {"value": e2e_value, "unit": "transforms/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps, "result_matches_device_run": e2e_ok,

@@ -72,6 +72,10 @@ def lib():
         L.orc_fft_c2c.argtypes = [_I, _D, _D, _I]
         L.orc_fft_r2c.argtypes = [_I, _D, _D, _D]
         L.orc_fft_c2r.argtypes = [_I, _D, _D, _D]
+        L.orc_makegrid_dh_adjoint.argtypes = [_D, _I, _D, _I, _I, _I, _I, _I, _I]
+        L.orc_makegrid_glq_adjoint.argtypes = [_D, _I, _D, _I, _D, _I, _I, _I, _I]
+        L.orc_shexpand_dh_adjoint.argtypes = [_D, _D, _I, _I, _I, _I, _I, _I]
+        L.orc_shexpand_glq_adjoint.argtypes = [_D, _D, _I, _I, _D, _D, _I, _I, _I]
         _lib = L
     return _lib
 
@@ -248,6 +252,69 @@ def shexpand_glq(grid, w=None, zero=None, norm=1, csphase=1, lmax_calc=None,
                                            int(pair_window[1]))
     _check(st)
     return cilm
+
+
+def makegrid_dh_adjoint(grid, lmax, norm=1, sampling=1, csphase=1,
+                        lmax_calc=None, extend=0):
+    """Transpose of makegrid_dh (MakeGridDH.f95:504-639) applied to a grid
+    cotangent of the synthesis output shape.  Returns (2, lmax+1, lmax+1)."""
+    grid = _f64(grid)
+    lmax = int(lmax)
+    lmax_calc = lmax if lmax_calc is None else int(lmax_calc)
+    n = 2 * lmax + 2
+    assert grid.shape == (n + int(extend), sampling * n + int(extend))
+    cilm = np.zeros((2, lmax + 1, lmax + 1))
+    _check(lib().orc_makegrid_dh_adjoint(_p(cilm), lmax + 1, _p(grid), lmax,
+                                         int(norm), int(sampling), int(csphase),
+                                         lmax_calc, int(extend)))
+    return cilm
+
+
+def makegrid_glq_adjoint(grid, lmax, zero=None, norm=1, csphase=1,
+                         lmax_calc=None, extend=0):
+    """Transpose of makegrid_glq (MakeGridGLQ.f95:547-665).  Returns
+    (2, lmax+1, lmax+1)."""
+    grid = _f64(grid)
+    lmax = int(lmax)
+    lmax_calc = lmax if lmax_calc is None else int(lmax_calc)
+    if zero is None:
+        zero, _ = shglq(lmax)
+    zero = _f64(zero)
+    assert grid.shape == (lmax + 1, 2 * lmax + 1 + int(extend))
+    cilm = np.zeros((2, lmax + 1, lmax + 1))
+    _check(lib().orc_makegrid_glq_adjoint(_p(cilm), lmax + 1, _p(grid), lmax,
+                                          _p(zero), int(norm), int(csphase),
+                                          lmax_calc, int(extend)))
+    return cilm
+
+
+def shexpand_dh_adjoint(cilm, n, norm=1, sampling=1, csphase=1, lmax_calc=None):
+    """Transpose of shexpand_dh (SHExpandDH.f95:463-702) applied to a
+    coefficient cotangent.  Returns the (n, sampling*n) grid cotangent."""
+    cilm = _f64(cilm)
+    n = int(n)
+    lmax_calc = n // 2 - 1 if lmax_calc is None else int(lmax_calc)
+    grid = np.zeros((n, sampling * n))
+    _check(lib().orc_shexpand_dh_adjoint(_p(grid), _p(cilm), cilm.shape[1], n,
+                                         int(norm), int(sampling), int(csphase),
+                                         lmax_calc))
+    return grid
+
+
+def shexpand_glq_adjoint(cilm, lmax, w=None, zero=None, norm=1, csphase=1,
+                         lmax_calc=None):
+    """Transpose of shexpand_glq (SHExpandGLQ.f95:445-649).  Returns the
+    (lmax+1, 2*lmax+1) grid cotangent."""
+    cilm = _f64(cilm)
+    lmax = int(lmax)
+    lmax_calc = lmax if lmax_calc is None else int(lmax_calc)
+    if zero is None or w is None:
+        zero, w = shglq(lmax)
+    grid = np.zeros((lmax + 1, 2 * lmax + 1))
+    _check(lib().orc_shexpand_glq_adjoint(_p(grid), _p(cilm), cilm.shape[1], lmax,
+                                          _p(_f64(w)), _p(_f64(zero)), int(norm),
+                                          int(csphase), lmax_calc))
+    return grid
 
 
 def power_law_cilm(lmax, seed, beta=2.0):

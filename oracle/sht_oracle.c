@@ -2185,3 +2185,177 @@ int orc_max_threads(void) {
     return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------------ */
+/*  Transposes (adjoints) of the four real transforms, built from the same   */
+/*  ring loops: they pin the GPU's autograd backward passes.                 */
+/*  The synthesis writes per ring x_j = sum_m (a_m cos m phi_j + b_m sin m   */
+/*  phi_j) with a_m = sum_l C_lm P_lm, b_m = sum_l S_lm P_lm                 */
+/*  (MakeGridDH.f95:504-639, c2r of (a_m - i b_m)/2 for m >= 1), so its      */
+/*  transpose takes Y = r2c(row) of the grid cotangent, unweighted, and      */
+/*  accumulates C_lm += P_lm Re Y_m, S_lm += P_lm (-Im Y_m) over every ring   */
+/*  the synthesis writes (poles included, the extend column folded into      */
+/*  column 0), without the analysis normalisation.  The analysis             */
+/*  (SHExpandDH.f95:463-702) is C = N^-1 sum_i w_i P_lm (Re, -Im) Y_m(row i)   */
+/*  with w_i = sqrt(2 pi) a_i sqrt(4 pi) / nlong (DH) or 2 pi w_i / nlong     */
+/*  (GLQ); its transpose is the synthesis of N^-1 cbar with row i scaled by   */
+/*  w_i.                                                                     */
+/* ------------------------------------------------------------------------ */
+
+/* grid: (n + extend) x (nlong + extend) row-major (the synthesis output shape) */
+int orc_makegrid_dh_adjoint(double *cilm, int cdim, const double *grid, int lmax,
+                            int norm, int sampling, int csphase, int lmax_calc,
+                            int extend) {
+    if (sampling != 1 && sampling != 2) return ORC_EBOUND;
+    if (extend != 0 && extend != 1) return ORC_EBOUND;
+    if (norm < 1 || norm > 4) return ORC_EBOUND;
+    if (csphase != 1 && csphase != -1) return ORC_EBOUND;
+    const int n = 2 * lmax + 2;
+    const int nlong = sampling == 1 ? n : 2 * n;
+    const int ncols = nlong + extend;
+    int lc = lmax_calc < 0 ? lmax : lmax_calc;
+    if (lc > lmax) lc = lmax;
+    if (lc > cdim - 1) lc = cdim - 1;
+    const double pi = acos(-1.0);
+    memset(cilm, 0, sizeof(double) * 2 * (size_t)cdim * cdim);
+    rec_tab t;
+    if (rec_build(&t, lc, norm)) return ORC_EALLOC;
+    orc_fft *plan = fft_plan(nlong);
+    const int nh = nlong / 2 + 1;
+    double *row = malloc(sizeof(double) * (size_t)nlong);
+    double *ccr = malloc(sizeof(double) * (size_t)nh), *cci = malloc(sizeof(double) * (size_t)nh);
+    double *f1r = calloc((size_t)lmax + 2, sizeof(double)), *f1i = calloc((size_t)lmax + 2, sizeof(double));
+    double *f2r = calloc((size_t)lmax + 2, sizeof(double)), *f2i = calloc((size_t)lmax + 2, sizeof(double));
+    double *wr = malloc(sizeof(double) * (size_t)nlong), *wi = malloc(sizeof(double) * (size_t)nlong);
+    const int i_eq = n / 2 + 1;
+    /* spectrum (Re Y, -Im Y) of a row with the extend column folded in */
+    #define ROWSPEC(r, fr, fi) do {                                              \
+        for (int j = 0; j < nlong; ++j) row[j] = grid[(size_t)(r) * ncols + j];  \
+        if (extend) row[0] += grid[(size_t)(r) * ncols + nlong];                \
+        fft_r2c(plan, row, ccr, cci, wr, wi);                                    \
+        for (int k = 0; k <= lc; ++k) { fr[k] = ccr[k]; fi[k] = -cci[k]; }        \
+    } while (0)
+    for (int i = 1; i <= i_eq - 1; ++i) {
+        const double theta = pi * (double)(i - 1) / (double)n;
+        const double z = cos(theta);
+        const double u = sqrt((1.0 - z) * (1.0 + z));
+        const int i_s = 2 * i_eq - i;
+        ROWSPEC(i - 1, f1r, f1i);
+        if (i == 1 && extend == 0) {
+            for (int k = 0; k <= lc; ++k) { f2r[k] = 0.0; f2i[k] = 0.0; }
+        } else {
+            ROWSPEC(i_s - 1, f2r, f2i);
+        }
+        if (lc == 0) {
+            CIL(0, 0, 0) += p00(norm) * (f1r[0] + f2r[0]);
+        } else {
+            anal_ring(&t, cilm, cdim, csphase, z, u, f1r, f1i, f2r, f2i);
+        }
+    }
+    ROWSPEC(i_eq - 1, f1r, f1i);
+    if (lc == 0) CIL(0, 0, 0) += p00(norm) * f1r[0];
+    else anal_equator(&t, cilm, cdim, csphase, f1r, f1i);
+    #undef ROWSPEC
+    free(row); free(ccr); free(cci); free(f1r); free(f1i); free(f2r); free(f2i);
+    free(wr); free(wi);
+    fft_free(plan);
+    rec_free(&t);
+    return ORC_OK;
+}
+
+/* grid: (lmax + 1) x (2 lmax + 1 + extend) row-major */
+int orc_makegrid_glq_adjoint(double *cilm, int cdim, const double *grid, int lmax,
+                             const double *zero, int norm, int csphase, int lmax_calc,
+                             int extend) {
+    if (extend != 0 && extend != 1) return ORC_EBOUND;
+    if (!zero) return ORC_ECONV;
+    if (norm < 1 || norm > 4) return ORC_EBOUND;
+    if (csphase != 1 && csphase != -1) return ORC_EBOUND;
+    const int nlong = 2 * lmax + 1, nlat = lmax + 1, ncols = nlong + extend;
+    int lc = lmax_calc < 0 ? lmax : lmax_calc;
+    if (lc > lmax) lc = lmax;
+    if (lc > cdim - 1) lc = cdim - 1;
+    memset(cilm, 0, sizeof(double) * 2 * (size_t)cdim * cdim);
+    rec_tab t;
+    if (rec_build(&t, lc, norm)) return ORC_EALLOC;
+    orc_fft *plan = fft_plan(nlong);
+    const int nh = nlong / 2 + 1;
+    double *row = malloc(sizeof(double) * (size_t)nlong);
+    double *ccr = malloc(sizeof(double) * (size_t)nh), *cci = malloc(sizeof(double) * (size_t)nh);
+    double *f1r = calloc((size_t)lmax + 2, sizeof(double)), *f1i = calloc((size_t)lmax + 2, sizeof(double));
+    double *f2r = calloc((size_t)lmax + 2, sizeof(double)), *f2i = calloc((size_t)lmax + 2, sizeof(double));
+    double *wr = malloc(sizeof(double) * (size_t)nlong), *wi = malloc(sizeof(double) * (size_t)nlong);
+    #define ROWSPEC(r, fr, fi) do {                                              \
+        for (int j = 0; j < nlong; ++j) row[j] = grid[(size_t)(r) * ncols + j];  \
+        if (extend) row[0] += grid[(size_t)(r) * ncols + nlong];                \
+        fft_r2c(plan, row, ccr, cci, wr, wi);                                    \
+        for (int k = 0; k <= lc; ++k) { fr[k] = ccr[k]; fi[k] = -cci[k]; }        \
+    } while (0)
+    for (int i = 1; i <= (nlat + 1) / 2; ++i) {
+        ROWSPEC(i - 1, f1r, f1i);
+        if (i == (nlat + 1) / 2 && nlat % 2 != 0) {
+            if (lc == 0) CIL(0, 0, 0) += p00(norm) * f1r[0];
+            else anal_equator(&t, cilm, cdim, csphase, f1r, f1i);
+        } else {
+            const double z = zero[i - 1];
+            const double u = sqrt((1.0 - z) * (1.0 + z));
+            ROWSPEC(nlat - i, f2r, f2i);
+            if (lc == 0) CIL(0, 0, 0) += p00(norm) * (f1r[0] + f2r[0]);
+            else anal_ring(&t, cilm, cdim, csphase, z, u, f1r, f1i, f2r, f2i);
+        }
+    }
+    #undef ROWSPEC
+    free(row); free(ccr); free(cci); free(f1r); free(f1i); free(f2r); free(f2i);
+    free(wr); free(wi);
+    fft_free(plan);
+    rec_free(&t);
+    return ORC_OK;
+}
+
+/* grid (output): n x nlong row-major; cilm: (2, cdim, cdim), l, m <= lmax_calc used */
+int orc_shexpand_dh_adjoint(double *grid, const double *cilm, int cdim, int n, int norm,
+                            int sampling, int csphase, int lmax_calc) {
+    if (n % 2 != 0) return ORC_EBOUND;
+    if (sampling != 1 && sampling != 2) return ORC_EBOUND;
+    const int lmax = n / 2 - 1;
+    const int lc = lmax_calc < 0 ? lmax : lmax_calc;
+    if (lc > lmax || cdim < lc + 1) return ORC_EBOUND;
+    const int nlong = sampling == 1 ? n : 2 * n;
+    const double pi = acos(-1.0);
+    double *cn = calloc(2 * (size_t)cdim * cdim, sizeof(double));
+    memcpy(cn, cilm, sizeof(double) * 2 * (size_t)cdim * cdim);
+    anal_normalise(cn, cdim, lc, norm);
+    int rc = orc_makegrid_dh(grid, cn, cdim, lmax, norm, sampling, csphase, lc, 0);
+    free(cn);
+    if (rc) return rc;
+    double *aj = malloc(sizeof(double) * (size_t)n);
+    orc_dhaj(n, aj, 0);
+    for (int i = 0; i < n; ++i) {
+        const double wi = sqrt(2 * pi) * (aj[i] * sqrt(4.0 * pi)) / (double)nlong;
+        for (int j = 0; j < nlong; ++j) grid[(size_t)i * nlong + j] *= wi;
+    }
+    free(aj);
+    return ORC_OK;
+}
+
+/* grid (output): (lmax + 1) x (2 lmax + 1) row-major */
+int orc_shexpand_glq_adjoint(double *grid, const double *cilm, int cdim, int lmax,
+                             const double *w, const double *zero, int norm, int csphase,
+                             int lmax_calc) {
+    const int lc = lmax_calc < 0 ? lmax : lmax_calc;
+    if (lc > lmax || cdim < lc + 1) return ORC_EBOUND;
+    if (!w || !zero) return ORC_ECONV;
+    const int nlong = 2 * lmax + 1, nlat = lmax + 1;
+    const double pi = acos(-1.0);
+    double *cn = calloc(2 * (size_t)cdim * cdim, sizeof(double));
+    memcpy(cn, cilm, sizeof(double) * 2 * (size_t)cdim * cdim);
+    anal_normalise(cn, cdim, lc, norm);
+    int rc = orc_makegrid_glq(grid, cn, cdim, lmax, zero, norm, csphase, lc, 0);
+    free(cn);
+    if (rc) return rc;
+    for (int i = 0; i < nlat; ++i) {
+        const double wi = 2 * w[i] * pi / (double)nlong;
+        for (int j = 0; j < nlong; ++j) grid[(size_t)i * nlong + j] *= wi;
+    }
+    return ORC_OK;
+}

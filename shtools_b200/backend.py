@@ -17,6 +17,7 @@ import sys
 
 import numpy as np
 
+from . import hostio
 from . import transforms as _t
 
 __all__ = ["MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ", "SHGLQ",
@@ -44,14 +45,20 @@ def set_nthreads(ntnew):
 
 
 def _np(t):
-    return t.detach().cpu().numpy()
+    """The result as a new numpy array (through pinned staging buffers)."""
+    return hostio.to_host(t)
+
+
+def _dev(a, dtype=np.float64):
+    """The numpy input on the current CUDA device (through pinned staging)."""
+    return hostio.to_device(np.asarray(a, dtype=dtype))
 
 
 def MakeGridDH(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
                extend=False):
     """griddh = MakeGridDH(cilm, [lmax, norm, sampling, csphase, lmax_calc,
     extend]) -- see src/MakeGridDH.f95:1 and ducc0_wrapper.py:454."""
-    return _np(_t.MakeGridDH(np.asarray(cilm, dtype=np.float64), lmax=lmax,
+    return _np(_t.MakeGridDH(_dev(cilm), lmax=lmax,
                              norm=norm, sampling=sampling, csphase=csphase,
                              lmax_calc=lmax_calc, extend=extend))
 
@@ -59,7 +66,7 @@ def MakeGridDH(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
 def SHExpandDH(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None):
     """cilm = SHExpandDH(griddh, [norm, sampling, csphase, lmax_calc]) -- see
     src/SHExpandDH.f95:1 and ducc0_wrapper.py:659."""
-    return _np(_t.SHExpandDH(np.asarray(griddh, dtype=np.float64), norm=norm,
+    return _np(_t.SHExpandDH(_dev(griddh), norm=norm,
                              sampling=sampling, csphase=csphase,
                              lmax_calc=lmax_calc))
 
@@ -69,7 +76,7 @@ def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
     """gridglq = MakeGridGLQ(cilm, [zero, lmax, norm, csphase, lmax_calc,
     extend]) -- see src/MakeGridGLQ.f95:1 and ducc0_wrapper.py:837.  With
     zero=None the nodes come from the GPU PreGLQ."""
-    return _np(_t.MakeGridGLQ(np.asarray(cilm, dtype=np.float64), zero=zero,
+    return _np(_t.MakeGridGLQ(_dev(cilm), zero=zero,
                               lmax=lmax, norm=norm, csphase=csphase,
                               lmax_calc=lmax_calc, extend=extend))
 
@@ -77,7 +84,7 @@ def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
 def SHExpandGLQ(gridglq, w=None, zero=None, norm=1, csphase=1, lmax_calc=None):
     """cilm = SHExpandGLQ(gridglq, [w, zero, norm, csphase, lmax_calc]) -- see
     src/SHExpandGLQ.f95:1 and ducc0_wrapper.py:1003."""
-    return _np(_t.SHExpandGLQ(np.asarray(gridglq, dtype=np.float64), w=w,
+    return _np(_t.SHExpandGLQ(_dev(gridglq), w=w,
                               zero=zero, norm=norm, csphase=csphase,
                               lmax_calc=lmax_calc))
 
@@ -131,7 +138,7 @@ def MakeGridDHC(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
                 extend=False):
     """griddh = MakeGridDHC(cilm, [lmax, norm, sampling, csphase, lmax_calc,
     extend]) -- see src/MakeGridDHC.f95:1 and ducc0_wrapper.py:552."""
-    return _np(_t.MakeGridDHC(np.asarray(cilm, dtype=np.complex128), lmax=lmax,
+    return _np(_t.MakeGridDHC(_dev(cilm, np.complex128), lmax=lmax,
                               norm=norm, sampling=sampling, csphase=csphase,
                               lmax_calc=lmax_calc, extend=extend))
 
@@ -139,7 +146,7 @@ def MakeGridDHC(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
 def SHExpandDHC(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None):
     """cilm = SHExpandDHC(griddh, [norm, sampling, csphase, lmax_calc]) -- see
     src/SHExpandDHC.f95:1 and ducc0_wrapper.py:745."""
-    return _np(_t.SHExpandDHC(np.asarray(griddh, dtype=np.complex128), norm=norm,
+    return _np(_t.SHExpandDHC(_dev(griddh, np.complex128), norm=norm,
                               sampling=sampling, csphase=csphase, lmax_calc=lmax_calc))
 
 
@@ -147,7 +154,7 @@ def MakeGridGLQC(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
                  extend=False):
     """gridglq = MakeGridGLQC(cilm, [zero, lmax, norm, csphase, lmax_calc,
     extend]) -- see src/MakeGridGLQC.f95:1 and ducc0_wrapper.py:917."""
-    return _np(_t.MakeGridGLQC(np.asarray(cilm, dtype=np.complex128), zero=zero,
+    return _np(_t.MakeGridGLQC(_dev(cilm, np.complex128), zero=zero,
                                lmax=lmax, norm=norm, csphase=csphase,
                                lmax_calc=lmax_calc, extend=extend))
 
@@ -155,7 +162,7 @@ def MakeGridGLQC(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
 def SHExpandGLQC(gridglq, w=None, zero=None, norm=1, csphase=1, lmax_calc=None):
     """cilm = SHExpandGLQC(gridglq, [w, zero, norm, csphase, lmax_calc]) -- see
     src/SHExpandGLQC.f95:1."""
-    return _np(_t.SHExpandGLQC(np.asarray(gridglq, dtype=np.complex128), w=w,
+    return _np(_t.SHExpandGLQC(_dev(gridglq, np.complex128), w=w,
                                zero=zero, norm=norm, csphase=csphase,
                                lmax_calc=lmax_calc))
 
@@ -164,7 +171,7 @@ def MakeGradientDH(cilm, lmax=None, sampling=1, lmax_calc=None, extend=False,
                    radius=None):
     """theta, phi = MakeGradientDH(cilm, [lmax, sampling, lmax_calc, extend,
     radius]) -- see src/MakeGradientDH.f95:1 and ducc0_wrapper.py:1164."""
-    th, ph = _t.MakeGradientDH(np.asarray(cilm, dtype=np.float64), lmax=lmax,
+    th, ph = _t.MakeGradientDH(_dev(cilm), lmax=lmax,
                                sampling=sampling, lmax_calc=lmax_calc, extend=extend,
                                radius=radius)
     return _np(th), _np(ph)
@@ -179,7 +186,7 @@ def MakeGravGridDH(cilm, gm, r0, lmax=None, a=None, f=0.0, sampling=2, lmax_calc
     None for an optional argument takes its default (omega 0.0, f 0.0,
     sampling 2, normal_gravity 1, extend 0), as SHGravCoeffs.expand() relies
     on (pyshtools/shclasses/shgravcoeffs.py:2574)."""
-    g = _t.MakeGravGridDH(np.asarray(cilm, dtype=np.float64), gm, r0, lmax=lmax, a=a,
+    g = _t.MakeGravGridDH(_dev(cilm), gm, r0, lmax=lmax, a=a,
                           f=0.0 if f is None else f,
                           sampling=2 if sampling is None else sampling,
                           lmax_calc=lmax_calc, omega=0.0 if omega is None else omega,

@@ -1,0 +1,131 @@
+"""Host <-> device copies of numpy arrays through pinned staging buffers.
+
+The pyshtools backend takes numpy arrays (pageable host memory) and returns
+new numpy arrays.  A plain ``torch.from_numpy(a).to("cuda")`` or
+``t.cpu().numpy()`` copies pageable memory, which the driver stages itself
+at a few GB/s.  Here the array moves in chunks through two reusable pinned
+buffers per device: the host copy of one chunk (numpy into the pinned
+buffer, or out of it) overlaps the PCIe transfer of the previous chunk on a
+dedicated copy stream, and each host copy is split over a small pool of
+threads (numpy releases the GIL while it copies), since one core copies
+well below what PCIe carries.  Small arrays take the plain path.
+
+Thread safety: one lock per device guards its staging buffers; calls from
+several threads are serialised on them.
+"""
+import os
+import threading
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+import torch
+
+CHUNK_BYTES = 16 << 20         # bytes per staging buffer
+SMALL_BYTES = 1 << 20          # arrays below this size are copied directly
+SLICE_BYTES = 2 << 20          # smallest share of a host copy given to one thread
+
+_lock = threading.Lock()
+_state = {}                    # device index -> (lock, stream, [buffers], [events])
+_pool = None
+
+
+def _threads():
+    return max(1, min(8, (os.cpu_count() or 1) // 2))
+
+
+def _copy(dst, src):
+    """dst[:] = src for flat uint8 arrays, split over the copy threads."""
+    global _pool
+    n = src.size
+    parts = min(_threads(), max(1, n // SLICE_BYTES))
+    if parts == 1:
+        np.copyto(dst, src)
+        return
+    with _lock:
+        if _pool is None:
+            _pool = ThreadPoolExecutor(_threads(), thread_name_prefix="shtc-hostio")
+        pool = _pool
+    step = -(-n // parts)
+    futs = [pool.submit(np.copyto, dst[o:o + step], src[o:o + step])
+            for o in range(0, n, step)]
+    for f in futs:
+        f.result()
+
+
+def _get(dev):
+    with _lock:
+        s = _state.get(dev.index)
+        if s is None:
+            bufs = [torch.empty(CHUNK_BYTES, dtype=torch.uint8, pin_memory=True)
+                    for _ in range(2)]
+            s = (threading.Lock(), torch.cuda.Stream(dev), bufs,
+                 [torch.cuda.Event(), torch.cuda.Event()])
+            _state[dev.index] = s
+        return s
+
+
+def to_device(a, device=None):
+    """A CUDA tensor holding the numpy array ``a`` (C-contiguous copy), ready
+    for work queued on the device's current stream."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None \
+        else torch.device(device)
+    if dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    a = np.ascontiguousarray(a)
+    if a.nbytes < SMALL_BYTES:
+        return torch.from_numpy(a).to(dev)
+    dst = torch.empty(a.shape, dtype=torch.from_numpy(a[:0]).dtype, device=dev)
+    src = a.reshape(-1).view(np.uint8)
+    dflat = dst.view(-1).view(torch.uint8)
+    lock, cs, bufs, evs = _get(dev)
+    cur = torch.cuda.current_stream(dev)
+    with lock:
+        cs.wait_stream(cur)                 # dst was allocated on the current stream
+        n = src.size
+        for k, off in enumerate(range(0, n, CHUNK_BYTES)):
+            b = k & 1
+            ln = min(CHUNK_BYTES, n - off)
+            evs[b].synchronize()            # earlier transfers have read buffer b
+            _copy(bufs[b].numpy()[:ln], src[off:off + ln])
+            with torch.cuda.stream(cs):
+                dflat[off:off + ln].copy_(bufs[b][:ln], non_blocking=True)
+                evs[b].record(cs)
+        cur.wait_stream(cs)
+        dst.record_stream(cs)
+    return dst
+
+
+def to_host(t):
+    """A new numpy array with the contents of the CUDA tensor ``t`` (after the
+    work queued on the device's current stream)."""
+    t = t.detach()
+    if not t.is_cuda or t.numel() * t.element_size() < SMALL_BYTES:
+        return t.cpu().numpy()
+    t = t.contiguous()
+    dev = t.device
+    out = np.empty(tuple(t.shape), dtype=t.new_empty(0).cpu().numpy().dtype)
+    dst = out.reshape(-1).view(np.uint8)
+    sflat = t.view(-1).view(torch.uint8)
+    lock, cs, bufs, evs = _get(dev)
+    cur = torch.cuda.current_stream(dev)
+    n = dst.size
+    offs = list(range(0, n, CHUNK_BYTES))
+    with lock:
+        cs.wait_stream(cur)                 # the producer of t ran on the current stream
+        pend = []                           # (buffer, offset, length) transferred, not read
+        for k, off in enumerate(offs):
+            b = k & 1
+            ln = min(CHUNK_BYTES, n - off)
+            if k >= 2:
+                pb, poff, pln = pend.pop(0)
+                evs[pb].synchronize()
+                _copy(dst[poff:poff + pln], bufs[pb].numpy()[:pln])
+            with torch.cuda.stream(cs):
+                bufs[b][:ln].copy_(sflat[off:off + ln], non_blocking=True)
+                evs[b].record(cs)
+            pend.append((b, off, ln))
+        for pb, poff, pln in pend:
+            evs[pb].synchronize()
+            _copy(dst[poff:poff + pln], bufs[pb].numpy()[:pln])
+        t.record_stream(cs)
+    return out

@@ -55,3 +55,23 @@ def test_pipelined_alternating_step_kinds(cuda, oracle):
     for i in range(3):
         assert torch.equal(outs[2 * i][0], grids[i])
         assert torch.equal(outs[2 * i + 1][0], cuda.SHExpandGLQ(grids[2 - i].cuda()).cpu())
+
+
+def test_hostio_staged_copies(cuda):
+    """numpy <-> device copies through the pinned staging buffers
+    (shtools_b200.hostio), at sizes below, at and above the chunk size, are
+    exact, and a device result read back right after being computed is the
+    computed one."""
+    from shtools_b200 import hostio
+    rng = np.random.default_rng(7)
+    for n in (10, hostio.SMALL_BYTES // 8 + 3, hostio.CHUNK_BYTES // 8,
+              5 * hostio.CHUNK_BYTES // 8 + 17):
+        a = rng.standard_normal(n)
+        t = hostio.to_device(a)
+        assert t.is_cuda and torch.equal(t.cpu(), torch.from_numpy(a))
+        t2 = t * 3.0
+        b = hostio.to_host(t2)
+        assert np.array_equal(b, a * 3.0)
+    g = hostio.to_device(rng.standard_normal((3, 700, 1401)))
+    assert g.shape == (3, 700, 1401) and g.is_contiguous()
+    assert np.array_equal(hostio.to_host(g[1]), g[1].cpu().numpy())

@@ -124,3 +124,18 @@ def test_max_over_ranks_gloo_two_ranks():
     assert res == {0: 11.0, 1: 11.0}
     import bench
     assert bench.max_over_ranks(3.5) == 3.5      # no process group: identity
+
+
+def test_hostio_threaded_copy_exact():
+    """The host side of the pinned staging (shtools_b200.hostio): the copy
+    split over threads reproduces the source for sizes below, at and above
+    one thread's share, including ragged tails."""
+    import numpy as np
+    from shtools_b200 import hostio
+    rng = np.random.default_rng(11)
+    for n in (0, 1, hostio.SLICE_BYTES - 1, hostio.SLICE_BYTES,
+              3 * hostio.SLICE_BYTES + 5, 17 * hostio.SLICE_BYTES + 12345):
+        src = rng.integers(0, 256, n, dtype=np.uint8)
+        dst = np.zeros(n, dtype=np.uint8)
+        hostio._copy(dst, src)
+        assert np.array_equal(dst, src)
