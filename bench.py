@@ -81,7 +81,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--workload", default="glq2047", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "int8x6", "int8x7"],
+    ap.add_argument("--precision", default="fp64",
+                    choices=["fp64", "int8x6", "int8x7", "int8x6-table", "int8x7-table"],
                     help="Legendre sums of the synthesis: FP64, or the INT8 tensor-core "
                          "error-free split with 6 or 7 byte digits (real DH/GLQ workloads)")
     ap.add_argument("--no-2799", action="store_true",
@@ -911,9 +912,12 @@ def compare_2799(dev, steps=3):
     c = torch.from_numpy(np.stack([power_law(L, w["seed"] + i, w["beta"])
                                    for i in range(F)])).to(dev)
     st = torch.cuda.current_stream(dev)
-    res, ref = {}, None
-    for prec in ("fp64", "int8x7"):
+    res, ref, grid_rec = {}, None, None
+    for prec in ("fp64", "int8x7", "int8x7-table"):
+        t_plan = time.perf_counter()
         ps = sht.get_plan(sht.GRID_DH, L, L, 1, 1, smp, 0, device=dev, precision=prec)
+        torch.cuda.synchronize(dev)
+        t_plan = time.perf_counter() - t_plan
         pa = sht.get_plan(sht.GRID_DH, L, L, 1, 1, smp, 0, device=dev)
         g = ps.synthesis(c)
         b = pa.analysis(g)
@@ -946,12 +950,28 @@ def compare_2799(dev, steps=3):
             e = torch.where(n > 0, d / n, d)
             entry["max_perdeg_rel_err_vs_fp64"] = float(e.max())
             entry["status"] = sht.mixed_status(dev)
+        if prec == "int8x7":
+            grid_rec = g.clone()
+        if prec == "int8x7-table":
+            entry["table_bytes"] = ps.table_bytes
+            entry["plan_build_s"] = t_plan
+            entry["bit_identical_to_int8x7"] = bool(torch.equal(g, grid_rec))
+            # the table streams once per call: HBM bytes of the dominant read
+            gbs = ps.table_bytes / (entry["legendre_synth_ms"] * 1e-3) / 1e9
+            peak = measured_peaks().get("hbm_gbs", 6650.0)
+            entry["table_stream"] = {"achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak}
+            grid_rec = None
         res[prec] = entry
         del g, b
+        if prec == "int8x7-table":
+            ps.legendre_table(False)          # frees the table's device memory
     res["workload"] = "16 DH fields, lmax 2799, sampling 2 (5600 x 11200), S(l)=(l+1)^-3"
-    res["step"] = "synthesis (FP64 or int8x7) + FP64 analysis, L2 not flushed"
+    res["step"] = ("synthesis (FP64, int8x7 from the recursion, or int8x7 streaming the "
+                   "plan's P_lm digit table) + FP64 analysis, L2 not flushed")
     res["synthesis_speedup_int8x7"] = (res["fp64"]["legendre_synth_ms"] /
                                        res["int8x7"]["legendre_synth_ms"])
+    res["synthesis_speedup_int8x7_table"] = (res["fp64"]["legendre_synth_ms"] /
+                                             res["int8x7-table"]["legendre_synth_ms"])
     return res
 
 

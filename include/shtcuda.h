@@ -68,6 +68,19 @@ typedef struct shtc_plan shtc_plan;
  * small table and synchronises. */
 SHTC_API int shtc_plan_set_precision(shtc_plan* plan, int precision);
 
+/* Table-driven mixed synthesis (no counterpart in the reference).  enable != 0
+ * computes, once, the fixed-point digits of every P_lm of the plan at its
+ * current mixed precision (INT8X6 or INT8X7) and keeps them in device memory
+ * in the tensor cores' operand layout; later syntheses of that precision
+ * stream the table instead of running the recursion (results bit-identical
+ * to the recursion path).  Leading degree tiles whose digits are all zero
+ * are not stored.  Size: about npair * (lmax+1)^2 / 2 * 7 bytes before that
+ * saving (lmax 2799, sampling 2: 77 GB; lmax 2047 GLQ: 15 GB).  enable == 0
+ * frees the table; so does switching the plan to the other mixed precision.
+ * bytes (may be NULL) receives the table size.  SHTC_EBOUND when the plan's
+ * precision is FP64, SHTC_EALLOC when the table does not fit.  Synchronises. */
+SHTC_API int shtc_plan_legendre_table(shtc_plan* plan, int enable, unsigned long long* bytes);
+
 /* Error word of the tensor-core kernels on the current device: 0 or
  * SHTC_ETIMEOUT (a bounded in-kernel wait ran out; the outputs of that call
  * are invalid).  Reads and clears it; synchronises the stream. */

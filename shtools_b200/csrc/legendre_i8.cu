@@ -751,12 +751,22 @@ __global__ void k_i8_rec2(const double2* __restrict__ rec, double4* __restrict__
     rec2[o + r] = make_double4(g, d, f.y, 0.0);
 }
 
+#include "legendre_i8_table.cuh"
+
 // --------------------------------------------------------------------------
 // host side
 // --------------------------------------------------------------------------
-// columns of a field group: 2 x 8 fields (MMA N of the weight window =
-// KW x 16 = 112 or 128; groups of fewer fields leave columns empty)
-static int group_cols(int) { return 16; }
+static bool has_table(const shtc_plan* P) {
+    return P->d_i8_tab != nullptr && P->i8_tab_prec == P->precision;
+}
+
+// columns of a field group: 2 x 8 fields (on-the-fly kernel: MMA N of the
+// weight window = KW x 16 = 112 or 128); the table-driven kernel takes
+// 2 x 16 fields when there are more than 8.  Groups of fewer fields leave
+// columns empty.
+static int group_cols(const shtc_plan* P, int nfield) {
+    return has_table(P) && nfield > 8 ? 32 : 16;
+}
 
 static int prec_digits(int precision) { return precision == SHTC_PREC_INT8X7 ? 7 : 6; }
 
@@ -768,7 +778,7 @@ using namespace i8;
 
 // scratch of the tensor-core synthesis: the coefficient image and the column scales
 size_t synth_i8_bytes(const shtc_plan* P, int nfield) {
-    const int N = group_cols(nfield), ngroups = (nfield + N / 2 - 1) / (N / 2);
+    const int N = group_cols(P, nfield), ngroups = (nfield + N / 2 - 1) / (N / 2);
     const int DB = prec_digits(P->precision);
     return align256((size_t)P->i8_ntot * ngroups * bimage_bytes(N, DB)) +
            align256((size_t)(P->lc + 1) * ngroups * N * sizeof(double));
@@ -781,6 +791,8 @@ int set_precision_tables(shtc_plan* P, int precision) {
     }
     if (precision != SHTC_PREC_INT8X6 && precision != SHTC_PREC_INT8X7) return SHTC_EBOUND;
     if (P->cplx || P->norm == 3) return SHTC_EUNSUP;
+    // a table of the other precision's digits is of no use
+    if (P->d_i8_tab && P->i8_tab_prec != precision) free_i8_table(P);
     if (!P->d_i8_toff) {
         std::vector<long long> toff(P->lc + 2);
         long long acc = 0;
@@ -824,6 +836,13 @@ int set_precision_tables(shtc_plan* P, int precision) {
     return SHTC_OK;
 }
 
+static int sm_count(int dev) {
+    static int nsm[64] = {0};
+    if (dev >= 0 && dev < 64 && nsm[dev] == 0)
+        cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
+    return dev >= 0 && dev < 64 && nsm[dev] > 0 ? nsm[dev] : 148;
+}
+
 template <int N, int DA>
 static int launch_synth_i8_n(const shtc_plan* P, const double2* coef, double2* spec, int nfield,
                              void* scratch, cudaStream_t st) {
@@ -842,11 +861,7 @@ static int launch_synth_i8_n(const shtc_plan* P, const double2* coef, double2* s
     const size_t smem = stages > 120 * 1024 ? stages : 120 * 1024;
     static_assert(stages <= 200 * 1024, "stages fit in shared memory");
     if ((rc = kernel_smem_attr((const void*)k_legendre_synth_i8<N, DA>, smem, true))) return rc;
-    static int nsm[64] = {0};
-    const int dev = P->device;
-    if (dev < 64 && nsm[dev] == 0)
-        cudaDeviceGetAttribute(&nsm[dev], cudaDevAttrMultiProcessorCount, dev);
-    const int sms = dev < 64 && nsm[dev] > 0 ? nsm[dev] : 148;
+    const int sms = sm_count(P->device);
     SynthArgs a;
     a.rec2 = P->d_i8_rec2;
     a.pmm = P->d_pmm;
@@ -868,13 +883,138 @@ static int launch_synth_i8_n(const shtc_plan* P, const double2* coef, double2* s
     return map_cuda(cudaGetLastError());
 }
 
+// the table-driven synthesis: coefficient image, then the streaming kernel
+template <int N, int DA>
+static int launch_synth_tab_n(const shtc_plan* P, const double2* coef, double2* spec, int nfield,
+                              void* scratch, cudaStream_t st) {
+    const int ngroups = (nfield + N / 2 - 1) / (N / 2);
+    uint8_t* image = (uint8_t*)scratch;
+    double* colinv =
+        (double*)((char*)scratch + align256((size_t)P->i8_ntot * ngroups * bimage_bytes(N, DA)));
+    k_i8_coef_image<N, DA><<<dim3(P->lc + 1, ngroups), 256, 0, st>>>(
+        coef, (uint32_t*)image, P->d_i8_toff, colinv, P->lc, nfield, ngroups);
+    int rc = map_cuda(cudaGetLastError());
+    if (rc) return rc;
+    constexpr size_t smem = (size_t)tab_stages(N, DA) * tab_stage_bytes(N, DA);
+    static_assert(smem >= 120 * 1024 && smem <= 220 * 1024, "one CTA per SM, stages fit");
+    if ((rc = kernel_smem_attr((const void*)k_legendre_synth_tab<N, DA>, smem, true))) return rc;
+    TabSynthArgs a;
+    a.tab = P->d_i8_tab;
+    a.off = P->d_i8_tab_off;
+    a.t0 = P->d_i8_tab_t0;
+    a.image = image;
+    a.toff = P->d_i8_toff;
+    a.colinv = colinv;
+    a.spec = spec;
+    a.lc = P->lc;
+    a.npair = P->npair;
+    a.nfield = nfield;
+    a.ngroups = ngroups;
+    a.ptiles = (P->npair + kPairs - 1) / kPairs;
+    a.ascale = P->i8_ascale;
+    const long long nitems = (long long)(P->lc + 1) * a.ptiles * ngroups;
+    const int sms = sm_count(P->device);
+    const int grid = (int)(nitems < sms ? nitems : sms);
+    k_legendre_synth_tab<N, DA><<<grid, kTabThreads, smem, st>>>(a);
+    return map_cuda(cudaGetLastError());
+}
+
 int launch_legendre_synth_i8(const shtc_plan* P, const double2* coef, double2* spec,
                              int nfield, void* scratch, cudaStream_t st) {
     if (!P->d_i8_toff) return SHTC_EBOUND;
     const bool seven = P->precision == SHTC_PREC_INT8X7;
     if (P->precision != SHTC_PREC_INT8X6 && !seven) return SHTC_EBOUND;
+    if (has_table(P)) {
+        if (group_cols(P, nfield) == 32)
+            return seven ? launch_synth_tab_n<32, 7>(P, coef, spec, nfield, scratch, st)
+                         : launch_synth_tab_n<32, 6>(P, coef, spec, nfield, scratch, st);
+        return seven ? launch_synth_tab_n<16, 7>(P, coef, spec, nfield, scratch, st)
+                     : launch_synth_tab_n<16, 6>(P, coef, spec, nfield, scratch, st);
+    }
     return seven ? launch_synth_i8_n<16, 7>(P, coef, spec, nfield, scratch, st)
                  : launch_synth_i8_n<16, 6>(P, coef, spec, nfield, scratch, st);
+}
+
+void free_i8_table(shtc_plan* P) {
+    if (P->d_i8_tab) P->device_bytes -= P->i8_tab_bytes;
+    cudaFree(P->d_i8_tab);
+    cudaFree(P->d_i8_tab_off);
+    cudaFree(P->d_i8_tab_t0);
+    P->d_i8_tab = nullptr;
+    P->d_i8_tab_off = nullptr;
+    P->d_i8_tab_t0 = nullptr;
+    P->i8_tab_bytes = 0;
+    P->i8_tab_prec = 0;
+}
+
+// Two passes of the recursion over every (m, pair tile): the first finds the
+// leading all-zero K-tiles, the second writes the stored ones.
+template <int DA>
+static int build_i8_table_n(shtc_plan* P) {
+    const int ptiles = (P->npair + kPairs - 1) / kPairs;
+    const long long nitem = (long long)(P->lc + 1) * ptiles;
+    TabBuildArgs a;
+    a.rec2 = P->d_i8_rec2;
+    a.pmm = P->d_pmm;
+    a.rtab = P->d_rtab;
+    a.zp = P->d_z;
+    a.lc = P->lc;
+    a.npair = P->npair;
+    a.ptiles = ptiles;
+    a.ascale = P->i8_ascale;
+    a.off = nullptr;
+    a.tab = nullptr;
+    int* t0 = nullptr;
+    long long* off = nullptr;
+    uint8_t* tab = nullptr;
+    std::vector<int> ht0((size_t)nitem);
+    std::vector<long long> hoff((size_t)nitem);
+    int rc = SHTC_OK;
+    auto fail = [&](int code) {
+        cudaFree(t0);
+        cudaFree(off);
+        cudaFree(tab);
+        return code;
+    };
+    if (cudaMalloc((void**)&t0, sizeof(int) * (size_t)nitem) != cudaSuccess) return fail(SHTC_EALLOC);
+    a.t0 = t0;
+    const dim3 grid(ptiles, P->lc + 1);
+    k_i8_table<DA, false><<<grid, 256>>>(a);
+    if ((rc = map_cuda(cudaGetLastError()))) return fail(rc);
+    if ((rc = map_cuda(cudaMemcpy(ht0.data(), t0, sizeof(int) * (size_t)nitem,
+                                  cudaMemcpyDeviceToHost))))
+        return fail(rc);
+    long long acc = 0;
+    for (int m = 0; m <= P->lc; ++m)
+        for (int pt = 0; pt < ptiles; ++pt) {
+            const long long i = (long long)m * ptiles + pt;
+            hoff[i] = acc;
+            acc += ntiles_of(P->lc, m) - ht0[i];
+        }
+    const unsigned long long bytes = (unsigned long long)acc * tab_ktile_bytes(DA);
+    if (cudaMalloc((void**)&off, sizeof(long long) * (size_t)nitem) != cudaSuccess)
+        return fail(SHTC_EALLOC);
+    if (cudaMalloc((void**)&tab, (size_t)(bytes ? bytes : 256)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SHTC_EALLOC);
+    }
+    if ((rc = map_cuda(cudaMemcpy(off, hoff.data(), sizeof(long long) * (size_t)nitem,
+                                  cudaMemcpyHostToDevice))))
+        return fail(rc);
+    a.off = off;
+    a.tab = tab;
+    if (bytes) {
+        k_i8_table<DA, true><<<grid, 256>>>(a);
+        if ((rc = map_cuda(cudaGetLastError()))) return fail(rc);
+    }
+    if ((rc = map_cuda(cudaDeviceSynchronize()))) return fail(rc);
+    P->d_i8_tab = tab;
+    P->d_i8_tab_off = off;
+    P->d_i8_tab_t0 = t0;
+    P->i8_tab_bytes = bytes;
+    P->i8_tab_prec = P->precision;
+    P->device_bytes += bytes;
+    return SHTC_OK;
 }
 
 }  // namespace shtc
@@ -887,6 +1027,24 @@ extern "C" int shtc_plan_set_precision(shtc_plan* P, int precision) {
     cudaGetDevice(&dev);
     if (dev != P->device) return SHTC_EHANDLE;
     return set_precision_tables(P, precision);
+}
+
+extern "C" int shtc_plan_legendre_table(shtc_plan* P, int enable, unsigned long long* bytes) {
+    if (!P) return SHTC_EHANDLE;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != P->device) return SHTC_EHANDLE;
+    int rc = SHTC_OK;
+    if (!enable) {
+        free_i8_table(P);
+    } else if (!has_table(P)) {
+        if (P->precision != SHTC_PREC_INT8X6 && P->precision != SHTC_PREC_INT8X7)
+            return SHTC_EBOUND;
+        free_i8_table(P);
+        rc = P->precision == SHTC_PREC_INT8X7 ? build_i8_table_n<7>(P) : build_i8_table_n<6>(P);
+    }
+    if (bytes) *bytes = P->i8_tab_bytes;
+    return rc;
 }
 
 extern "C" int shtc_mixed_status(int* status, void* stream) {

@@ -381,6 +381,7 @@ using namespace shtc;
 // plan creation (C ABI)
 // ---------------------------------------------------------------------------
 static void plan_free_tables(shtc_plan* P) {
+    free_i8_table(P);
     cudaFree(P->d_i8_toff);
     cudaFree(P->d_i8_rec2);
     cudaFree(P->d_rec);

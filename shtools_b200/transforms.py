@@ -15,6 +15,7 @@ All four are differentiable: the backward pass runs the hand-written
 adjoint kernels (the weighted transpose transforms, which recompute the
 Legendre functions).
 """
+import ctypes
 import threading
 
 import numpy as np
@@ -69,6 +70,8 @@ class Plan:
         if device.index is None:
             device = torch.device("cuda", torch.cuda.current_device())
         self.device = device
+        self.precision = 0
+        self.table_bytes = 0
         lc = -1 if lmax_calc is None else int(lmax_calc)
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
@@ -117,8 +120,24 @@ class Plan:
         with _on_device(self.device):
             _lib.check(self.lib.shtc_plan_set_precision(self.handle, int(code)),
                        "shtc_plan_set_precision")
+        if int(code) != self.precision:
+            self.table_bytes = 0          # the library freed a table of other digits
         self.precision = int(code)
         self.__dict__.pop("_wsb", None)
+
+    def legendre_table(self, enable=True):
+        """shtc_plan_legendre_table: build (or free) the plan's table of P_lm
+        digits for its mixed precision; the syntheses then stream it from
+        device memory instead of running the recursion.  Returns its size in
+        bytes."""
+        nb = ctypes.c_ulonglong(0)
+        with _on_device(self.device):
+            _lib.check(self.lib.shtc_plan_legendre_table(self.handle, int(bool(enable)),
+                                                         ctypes.byref(nb)),
+                       "shtc_plan_legendre_table")
+        self.table_bytes = int(nb.value)
+        self.__dict__.pop("_wsb", None)
+        return self.table_bytes
 
     def workspace_bytes(self, nfield):
         """shtc_workspace_bytes for nfield fields, cached per plan and tile
@@ -219,7 +238,9 @@ _cache_lock = threading.Lock()
 _plans = {}
 
 
-PRECISIONS = {"fp64": 0, "int8x6": 1, "int8x7": 2}
+# "-table": the synthesis streams a precomputed table of the P_lm digits
+# (Plan.legendre_table) instead of running the recursion
+PRECISIONS = {"fp64": 0, "int8x6": 1, "int8x7": 2, "int8x6-table": 1, "int8x7-table": 2}
 
 
 def _precision_code(precision):
@@ -234,8 +255,10 @@ def get_plan(kind, lmax, lmax_calc, norm, csphase, sampling=1, extend=0,
              zero=None, w=None, device=None, tune=None, cplx=False, precision="fp64"):
     """Cached Plan for the option set (thread-safe).  New plans are
     autotuned when ``tune`` is true or the environment sets SHTC_AUTOTUNE=1
-    (shtools_b200.autotune).  precision "int8x6" runs the plan's syntheses on
-    the INT8 tensor cores with an error-free 6-byte split (norms 1, 2, 4)."""
+    (shtools_b200.autotune).  precision "int8x6" ("int8x7") runs the plan's
+    syntheses on the INT8 tensor cores with an error-free 6-byte (7-byte)
+    split (norms 1, 2, 4); "int8x6-table" / "int8x7-table" in addition build
+    the plan's P_lm digit table once (Plan.legendre_table)."""
     import os
     dev = torch.device("cuda", torch.cuda.current_device()) if device is None \
         else torch.device(device)
@@ -245,7 +268,7 @@ def get_plan(kind, lmax, lmax_calc, norm, csphase, sampling=1, extend=0,
     wkey = None if w is None else np.asarray(w, dtype=np.float64).tobytes()
     prec = _precision_code(precision)
     key = (kind, int(lmax), int(lmax_calc), int(norm), int(csphase),
-           int(sampling), int(extend), dev.index, zkey, wkey, bool(cplx), prec)
+           int(sampling), int(extend), dev.index, zkey, wkey, bool(cplx), precision)
     with _cache_lock:
         p = _plans.get(key)
         if p is None:
@@ -253,6 +276,8 @@ def get_plan(kind, lmax, lmax_calc, norm, csphase, sampling=1, extend=0,
                      zero, w, dev, cplx=cplx)
             if prec:
                 p.set_precision(prec)
+                if precision.endswith("-table"):
+                    p.legendre_table(True)
             _plans[key] = p
             if tune or (tune is None and os.environ.get("SHTC_AUTOTUNE") == "1"):
                 from . import autotune

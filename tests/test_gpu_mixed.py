@@ -110,3 +110,62 @@ def test_mixed_synthesis_lmax2799_16_fields(cuda, oracle):
               % (prec, err, e.max()))
         assert e.max() <= DEG_TOL[prec], (prec, e.max())
         assert err <= GRID_TOL, (prec, err)
+
+
+@pytest.mark.parametrize("prec", ["int8x7", "int8x6"])
+@pytest.mark.parametrize("kind,L,nf,opts", [
+    ("dh", 63, 1, dict(sampling=2)),                                  # N = 16, one field
+    ("dh", 127, 6, dict(norm=2, csphase=-1, lmax_calc=100)),          # N = 16
+    ("glq", 150, 9, dict(norm=4, extend=True)),                       # N = 32, 9 of 16
+    ("dh", 200, 16, dict(sampling=2, extend=True)),                   # N = 32
+    ("glq", 255, 20, dict(norm=1, csphase=-1)),                       # 16 + 4 fields
+    ("dh", 64, 3, dict(norm=2, lmax_calc=40)),                        # ragged last tiles
+    ("dh", 383, 17, dict(sampling=2)),                                # 3 pair tiles, 2 groups
+])
+def test_table_synthesis_bit_identical(cuda, oracle, kind, L, nf, opts, prec):
+    """The table-driven synthesis (the P_lm digits computed once and streamed
+    from device memory) gives the same bits as the recursion-driven one:
+    same digits, same kept byte products, exact INT32 sums.  The table skips
+    leading all-zero degree tiles, so it is smaller than the full size."""
+    from shtools_b200 import transforms as T
+    c = torch.from_numpy(fields(oracle, L, nf, 500 + L)).cuda()
+    f = cuda.MakeGridDH if kind == "dh" else cuda.MakeGridGLQ
+    g_rec = f(c, precision=prec, **opts)
+    g_tab = f(c, precision=prec + "-table", **opts)
+    assert cuda.mixed_status() == 0
+    assert torch.equal(g_tab, g_rec), (g_tab - g_rec).abs().max().item()
+    # a second call streams the same table
+    assert torch.equal(f(c, precision=prec + "-table", **opts), g_rec)
+    plans = [p for k, p in T._plans.items() if k[-1] == prec + "-table" and k[1] == L]
+    assert plans and plans[-1].table_bytes > 0
+    p = plans[-1]
+    lc = p.lc
+    npad = -(-p.info["npair"] // 128) * 128
+    full = npad * sum(64 * ((lc - m + 64) // 64) for m in range(lc + 1)) \
+        * (7 if prec == "int8x7" else 6)
+    assert p.table_bytes <= full
+    print("%s %s L %d: table %.1f MB of %.1f MB" % (prec, kind, L, p.table_bytes / 2**20,
+                                                   full / 2**20))
+
+
+def test_table_freed_on_precision_switch(cuda, oracle):
+    """Switching a plan with a table to the other mixed precision frees the
+    table; the syntheses then take the recursion path and stay correct."""
+    from shtools_b200 import transforms as T
+    L = 95
+    p = T.Plan(T.GRID_DH, L, sampling=2)
+    p.set_precision(2)
+    nb = p.legendre_table(True)
+    assert nb > 0 and p.legendre_table(True) == nb          # built once
+    c = torch.from_numpy(fields(oracle, L, 4, 91)).cuda()
+    g7 = p.synthesis(c)
+    p.set_precision(1)
+    assert p.table_bytes == 0
+    g6 = p.synthesis(c)
+    assert cuda.mixed_status() == 0
+    ref = cuda.MakeGridDH(c, sampling=2, precision="int8x6")
+    assert torch.equal(g6, ref)
+    assert (g7 - g6).abs().max().item() <= 1e-9 * g7.abs().max().item()
+    p.set_precision(0)
+    with pytest.raises(RuntimeError):
+        p.legendre_table(True)
