@@ -83,11 +83,14 @@ def parse():
     ap.add_argument("--workload", default="glq2047", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64",
                     choices=["fp64", "int8x6", "int8x7", "int8x6-table", "int8x7-table"],
-                    help="Legendre sums of the synthesis: FP64, or the INT8 tensor-core "
-                         "error-free split with 6 or 7 byte digits (real DH/GLQ workloads)")
+                    help="Legendre sums: FP64, or the INT8 tensor-core error-free split "
+                         "with 6 or 7 byte digits (real DH/GLQ workloads): the synthesis "
+                         "from the recursion, or (-table) both directions from the "
+                         "plan's P_lm digit table")
     ap.add_argument("--no-2799", action="store_true",
-                    help="skip the lmax-2799 (16 DH fields) FP64 / int8x7 comparison "
-                         "that the default workload adds to its line")
+                    help="skip the FP64 / mixed-precision comparisons (glq2047 and "
+                         "16 DH fields at lmax 2799) that the default workload adds to "
+                         "its line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the default Legendre tile shapes instead of tuning "
@@ -879,46 +882,54 @@ def run_cuda_multiply(args, w, rank, world, local_rank):
     }
 
 
-def i8_tensor_ops(w, nfield, precision):
-    """INT8 multiply-add operations (2 per MAC) that one tensor-core synthesis
-    launch executes: per 64-degree K-tile of a 128-pair tile and a group of 8
-    fields, 2 x DA MMAs of M = 128, N = KW x 16, K = 32 (the weight windows
-    of shtools_b200/csrc/legendre_i8.cu)."""
-    DA, KW = (7, 8) if precision == "int8x7" else (6, 7)
-    L = w["lmax"]
-    # ring pairs: GLQ (L+1 rings) (L+2)//2, DH (2L+2 rings, with the pole
-    # and the equator) L+2
-    npair = (L + 2) // 2 if w["kind"] == "glq" else L + 2
-    ptiles = (npair + 127) // 128
-    groups = (nfield + 7) // 8
-    ktiles = sum((L - m + 1 + 63) // 64 for m in range(L + 1))
-    return 2.0 * ktiles * ptiles * groups * 2 * DA * (128 * KW * 16 * 32)
-
-
-def compare_2799(dev, steps=3):
-    """The lmax-2799 half of the metric, added to the default line: 16 DH
-    fields, lmax 2799, sampling 2 (5600 x 11200), S(l) = (l+1)^-3; synthesis
-    + FP64 analysis with the FP64 synthesis and with the int8x7 tensor-core
-    synthesis; transforms/s of each and the per-degree error of the int8x7
-    result against the FP64 one (both analysed in FP64)."""
+def compare_mixed(dev, wname, steps=3):
+    """The mixed-precision half of the metric, added to the default line:
+    synthesis + analysis of the workload in FP64, with the int8x7 synthesis
+    from the recursion (FP64 analysis), and with both directions on the INT8
+    tensor cores from the plan's P_lm digit table (int8x7-table); transforms/s
+    of each, per-launch Legendre times, the table stream's HBM rate and the
+    per-degree error against FP64: of the mixed round trip against the FP64
+    round trip, and of the mixed analysis of the FP64 grid against the FP64
+    analysis."""
     import ctypes
     import numpy as np
     import torch
     import shtools_b200 as sht
     from shtools_b200 import _lib
     lib = _lib.load()
-    w = WORKLOADS["dh2799x16"]
+    w = WORKLOADS[wname]
     L, F, smp = w["lmax"], w["nfield"], w["sampling"]
     c = torch.from_numpy(np.stack([power_law(L, w["seed"] + i, w["beta"])
                                    for i in range(F)])).to(dev)
     st = torch.cuda.current_stream(dev)
-    res, ref, grid_rec = {}, None, None
+    if w["kind"] == "glq":
+        zero_t, w_t = sht.PreGLQ(-1.0, 1.0, L + 1, device=dev)
+        zero, wts = zero_t.cpu().numpy(), w_t.cpu().numpy()
+
+        def plans(prec):
+            ps = sht.get_plan(sht.GRID_GLQ, L, L, 1, 1, 1, 0, zero=zero, device=dev,
+                              precision=prec)
+            pa = sht.get_plan(sht.GRID_GLQ, L, L, 1, 1, 1, 0, zero=zero, w=wts, device=dev,
+                              precision=prec if prec.endswith("-table") else "fp64")
+            return ps, pa
+    else:
+        def plans(prec):
+            ps = sht.get_plan(sht.GRID_DH, L, L, 1, 1, smp, 0, device=dev, precision=prec)
+            pa = ps if prec.endswith("-table") else \
+                sht.get_plan(sht.GRID_DH, L, L, 1, 1, smp, 0, device=dev)
+            return ps, pa
+
+    def perdeg(b, r):
+        d = (b - r).pow(2).sum(dim=(1, 3)).sqrt()
+        n = r.pow(2).sum(dim=(1, 3)).sqrt()
+        return float(torch.where(n > 0, d / n, d).max())
+
+    res, ref, g64 = {}, None, None
     for prec in ("fp64", "int8x7", "int8x7-table"):
         t_plan = time.perf_counter()
-        ps = sht.get_plan(sht.GRID_DH, L, L, 1, 1, smp, 0, device=dev, precision=prec)
+        ps, pa = plans(prec)
         torch.cuda.synchronize(dev)
         t_plan = time.perf_counter() - t_plan
-        pa = sht.get_plan(sht.GRID_DH, L, L, 1, 1, smp, 0, device=dev)
         g = ps.synthesis(c)
         b = pa.analysis(g)
         torch.cuda.synchronize(dev)
@@ -944,34 +955,50 @@ def compare_2799(dev, steps=3):
                  "fft_c2r_ms": ms[2] / max(1, cnt[2]), "fft_r2c_ms": ms[3] / max(1, cnt[3])}
         if prec == "fp64":
             ref = b.clone()
+            g64 = g.clone()
         else:
-            d = (b - ref).pow(2).sum(dim=(1, 3)).sqrt()
-            n = ref.pow(2).sum(dim=(1, 3)).sqrt()
-            e = torch.where(n > 0, d / n, d)
-            entry["max_perdeg_rel_err_vs_fp64"] = float(e.max())
+            entry["max_perdeg_rel_err_vs_fp64"] = perdeg(b, ref)
             entry["status"] = sht.mixed_status(dev)
         if prec == "int8x7":
             grid_rec = g.clone()
+            entry["directions"] = "synthesis int8x7 (recursion), analysis FP64"
         if prec == "int8x7-table":
+            entry["directions"] = "synthesis and analysis int8x7 from the P_lm digit table"
             entry["table_bytes"] = ps.table_bytes
             entry["plan_build_s"] = t_plan
-            entry["bit_identical_to_int8x7"] = bool(torch.equal(g, grid_rec))
-            # the table streams once per call: HBM bytes of the dominant read
-            gbs = ps.table_bytes / (entry["legendre_synth_ms"] * 1e-3) / 1e9
-            peak = measured_peaks().get("hbm_gbs", 6650.0)
-            entry["table_stream"] = {"achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak}
+            # the table holds the one-step FP64 recursion's P_lm, the
+            # recursion kernel runs a two-step form: close, not identical
+            entry["synthesis_max_abs_diff_vs_int8x7_rel"] = float(
+                (g - grid_rec).abs().max() / grid_rec.abs().max())
             grid_rec = None
+            # the analysis alone: the FP64 grid through the tensor-core analysis
+            entry["analysis_only_max_perdeg_rel_err_vs_fp64"] = perdeg(pa.analysis(g64), ref)
+            entry["status"] = sht.mixed_status(dev)
+            # the table streams once per Legendre launch: HBM rate of that read
+            peak = measured_peaks().get("hbm_gbs", 6650.0)
+            entry["table_stream"] = {}
+            for k in ("synth", "anal"):
+                tms = entry["legendre_%s_ms" % k]
+                gbs = ps.table_bytes / (tms * 1e-3) / 1e9
+                entry["table_stream"][k] = {"achieved_gbs": gbs, "peak_gbs": peak,
+                                            "frac": gbs / peak}
         res[prec] = entry
         del g, b
         if prec == "int8x7-table":
             ps.legendre_table(False)          # frees the table's device memory
-    res["workload"] = "16 DH fields, lmax 2799, sampling 2 (5600 x 11200), S(l)=(l+1)^-3"
-    res["step"] = ("synthesis (FP64, int8x7 from the recursion, or int8x7 streaming the "
-                   "plan's P_lm digit table) + FP64 analysis, L2 not flushed")
-    res["synthesis_speedup_int8x7"] = (res["fp64"]["legendre_synth_ms"] /
-                                       res["int8x7"]["legendre_synth_ms"])
-    res["synthesis_speedup_int8x7_table"] = (res["fp64"]["legendre_synth_ms"] /
-                                             res["int8x7-table"]["legendre_synth_ms"])
+            if pa is not ps:
+                pa.legendre_table(False)
+    del g64, ref
+    res["workload"] = "%s: %d field(s), lmax %d, %s, S(l)=(l+1)^-%g" % (
+        wname, F, L, "GLQ" if w["kind"] == "glq" else "DH sampling %d" % smp, w["beta"])
+    res["step"] = "synthesis + analysis, L2 not flushed, %d steps" % steps
+    f64, tab = res["fp64"], res["int8x7-table"]
+    res["speedup_int8x7_table_vs_fp64"] = {
+        "step": f64["ms_per_step"] / tab["ms_per_step"],
+        "legendre_synth": f64["legendre_synth_ms"] / tab["legendre_synth_ms"],
+        "legendre_anal": f64["legendre_anal_ms"] / tab["legendre_anal_ms"],
+        "legendre_both": (f64["legendre_synth_ms"] + f64["legendre_anal_ms"]) /
+                         (tab["legendre_synth_ms"] + tab["legendre_anal_ms"])}
     return res
 
 
@@ -998,11 +1025,11 @@ def run_cuda(args, w, rank, world, local_rank):
         zero_t, w_t = sht.PreGLQ(-1.0, 1.0, L + 1, device=dev)
         zero, wts = zero_t.cpu().numpy(), w_t.cpu().numpy()
         synth = lambda x: sht.MakeGridGLQ(x, zero=zero, precision=args.precision)
-        anal = lambda g: sht.SHExpandGLQ(g, w=wts, zero=zero)
+        anal = lambda g: sht.SHExpandGLQ(g, w=wts, zero=zero, precision=args.precision)
     else:
         s = w["sampling"]
         synth = lambda x: sht.MakeGridDH(x, sampling=s, precision=args.precision)
-        anal = lambda g: sht.SHExpandDH(g, sampling=s)
+        anal = lambda g: sht.SHExpandDH(g, sampling=s, precision=args.precision)
 
     def step(x):
         g = synth(x)
@@ -1141,6 +1168,25 @@ def run_cuda(args, w, rank, world, local_rank):
     fl = legendre_flops(w, F * (2 if cplx else 1))
     achieved = fl / (per_launch_ms * 1e-3) / 1e12
     traffic = load_traffic("%s_%s" % (names[dom], args.workload))
+    roof = {"kernel": names[dom], "bound": "fp64", "achieved": achieved,
+            "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak if peak else None,
+            "peak_source": "measured FP64 FMA probe, this run "
+                           "(MEASURED_PEAKS.json has no FP64 entry)",
+            "flops_per_launch": fl, "traffic": traffic}
+    if args.precision.endswith("-table") and not cplx:
+        # the table-driven tensor-core kernels stream the plan's P_lm digit
+        # table once per launch: HBM-bound on that read
+        sht_plans = [p for k, p in sht.transforms._plans.items()
+                     if k[-1] == args.precision and k[1] == L]
+        tb = max(p.table_bytes for p in sht_plans) if sht_plans else 0
+        gbs = tb / (per_launch_ms * 1e-3) / 1e9
+        hbm = measured_peaks().get("hbm_gbs", 6650.0)
+        roof = {"kernel": names[dom], "bound": "hbm", "achieved": gbs, "peak": hbm,
+                "unit": "GB/s", "frac": gbs / hbm,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs",
+                "bytes_per_launch": tb, "traffic": traffic,
+                "bytes_note": "the P_lm digit table, read once per launch"}
     stage = {names[i]: {"ms_per_launch": (ms[i] / cnt[i]) if cnt[i] else None,
                         "launches": cnt[i],
                         "share": ms[i] / max(1e-9, sum(ms))} for i in range(6)}
@@ -1159,12 +1205,7 @@ def run_cuda(args, w, rank, world, local_rank):
         "data": "synthetic seeded power-law coefficients, S(l)=(l+1)^-%g" % w["beta"],
         "config": bench_config(args, w, world),
         "l2": "flushed between steps (256 MiB write, outside step events)",
-        "roofline": {"kernel": names[dom], "bound": "fp64", "achieved": achieved,
-                     "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None,
-                     "peak_source": "measured FP64 FMA probe, this run "
-                                    "(MEASURED_PEAKS.json has no FP64 entry)",
-                     "flops_per_launch": fl, "traffic": traffic},
+        "roofline": roof,
         "stages": stage,
         "roundtrip_max_perdeg_err": rt_err,
         "e2e": {"value": plug_value, "unit": "transforms/s",
@@ -1184,19 +1225,9 @@ def run_cuda(args, w, rank, world, local_rank):
         "gpu_launches": int(sum(cnt)),
         "clocks": clk.summary(),
     }
-    if args.precision != "fp64" and not cplx:
-        ops = i8_tensor_ops(w, F, args.precision)
-        syn_ms = ms[1] / max(1, cnt[1])
-        tops = ops / (syn_ms * 1e-3) / 1e12
-        peak_i8 = 2.0 * measured_peaks().get("bf16_tflops", 1590.0)
-        res["tensor_synthesis"] = {
-            "kernel": "k_legendre_synth_i8", "precision": args.precision,
-            "ms_per_launch": syn_ms, "int8_ops_per_launch": ops, "achieved_tops": tops,
-            "peak_tops": peak_i8, "frac": tops / peak_i8,
-            "peak_source": "2 x the measured bf16 dense rate (MEASURED_PEAKS.json "
-                           "has no INT8 entry; B200 INT8 dense = 2 x BF16 nominal)"}
     if args.workload == "glq2047" and world == 1 and not args.no_2799:
-        res["lmax2799"] = compare_2799(dev)
+        res["mixed_glq2047"] = compare_mixed(dev, "glq2047", steps=5)
+        res["lmax2799"] = compare_mixed(dev, "dh2799x16")
     return res
 
 

@@ -68,14 +68,20 @@ typedef struct shtc_plan shtc_plan;
  * small table and synchronises. */
 SHTC_API int shtc_plan_set_precision(shtc_plan* plan, int precision);
 
-/* Table-driven mixed synthesis (no counterpart in the reference).  enable != 0
- * computes, once, the fixed-point digits of every P_lm of the plan at its
- * current mixed precision (INT8X6 or INT8X7) and keeps them in device memory
- * in the tensor cores' operand layout; later syntheses of that precision
- * stream the table instead of running the recursion (results bit-identical
- * to the recursion path).  Leading degree tiles whose digits are all zero
- * are not stored.  Size: about npair * (lmax+1)^2 / 2 * 7 bytes before that
- * saving (lmax 2799, sampling 2: 77 GB; lmax 2047 GLQ: 15 GB).  enable == 0
+/* Table-driven mixed transforms (no counterpart in the reference; the
+ * reference's plx table of MakeGridGLQ.f95:441-465 holds FP64 P_lm for the
+ * GLQ syntheses).  enable != 0 computes, once, the fixed-point digits of
+ * every P_lm of the plan at its current mixed precision (INT8X6 or INT8X7)
+ * and keeps them in device memory in a layout that is the tensor cores' A
+ * operand of both directions.  The digits are those of the FP64 kernels'
+ * recursion rounded to the fixed point.  Later syntheses of that precision
+ * stream the table instead of running the recursion, and the analyses and
+ * synthesis adjoints run their
+ * Legendre sums on the tensor cores from it (ring sums split into the same
+ * balanced digits; per-degree errors against FP64 are stated by the tests).
+ * Leading 256-degree tiles whose digits are all zero are not stored.  Size:
+ * about npair * (lmax+1)^2 / 2 * 7 bytes before that saving (lmax 2799,
+ * sampling 2: 77 GB; lmax 2047 GLQ: 15 GB).  enable == 0
  * frees the table; so does switching the plan to the other mixed precision.
  * bytes (may be NULL) receives the table size.  SHTC_EBOUND when the plan's
  * precision is FP64, SHTC_EALLOC when the table does not fit.  Synchronises. */

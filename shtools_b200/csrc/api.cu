@@ -59,6 +59,21 @@ static size_t i8_region(const shtc_plan* P, int nfield) {
     return P->precision != SHTC_PREC_F64 && !P->cplx ? align256(synth_i8_bytes(P, nfield)) : 0;
 }
 
+// Legendre analysis stage of a real plan: the tensor-core analysis when the
+// plan is mixed-precision and holds its P_lm digit table (its sums arrive as
+// one partial tile), else the FP64 kernels (anal_tiles partial tiles)
+static int legendre_anal_stage(const shtc_plan* P, const double2* spec, double2* partial,
+                               int nfield, void* work, int* tiles, cudaStream_t st) {
+    if (anal_i8_ready(P)) {
+        *tiles = 1;
+        return launch_legendre_anal_i8(
+            P, spec, partial, nfield,
+            (char*)work + coef_region(P, nfield) + spec_region(P, nfield) + fft_region(P), st);
+    }
+    *tiles = anal_tiles(P, nfield);
+    return launch_legendre_anal(P, spec, partial, *tiles, nfield, st);
+}
+
 extern "C" size_t shtc_workspace_bytes(const shtc_plan* P, int nfield) {
     if (!P || nfield < 1) return 0;
     const int nf = P->cplx ? 2 * nfield : nfield;
@@ -135,13 +150,13 @@ extern "C" int shtc_analysis_ex(const shtc_plan* P, const void* grid, int gdt,
     double2* partial = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
     double2* fbuf = fft_scratch(P, work, coef_region(P, nfield) + spec_region(P, nfield));
-    const int tiles = anal_tiles(P, nfield);
+    int tiles = 0;
     stage_begin(SHTC_STAGE_FFT_R2C, st);
     rc = launch_fft_r2c(P, grid, gdt, gsf, gsr, gsc, spec, nfield, 1, 0, st, fbuf);
     stage_end(SHTC_STAGE_FFT_R2C, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
-    rc = launch_legendre_anal(P, spec, partial, tiles, nfield, st);
+    rc = legendre_anal_stage(P, spec, partial, nfield, work, &tiles, st);
     stage_end(SHTC_STAGE_LEGENDRE_ANAL, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_UNPACK, st);
@@ -166,13 +181,13 @@ extern "C" int shtc_synthesis_adjoint_ex(const shtc_plan* P, const void* grid, i
     double2* partial = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
     double2* fbuf = fft_scratch(P, work, coef_region(P, nfield) + spec_region(P, nfield));
-    const int tiles = anal_tiles(P, nfield);
+    int tiles = 0;
     stage_begin(SHTC_STAGE_FFT_R2C, st);
     rc = launch_fft_r2c(P, grid, gdt, gsf, gsr, gsc, spec, nfield, 0, P->extend, st, fbuf);
     stage_end(SHTC_STAGE_FFT_R2C, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_ANAL, st);
-    rc = launch_legendre_anal(P, spec, partial, tiles, nfield, st);
+    rc = legendre_anal_stage(P, spec, partial, nfield, work, &tiles, st);
     stage_end(SHTC_STAGE_LEGENDRE_ANAL, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_UNPACK, st);
@@ -196,12 +211,19 @@ extern "C" int shtc_analysis_adjoint_ex(const shtc_plan* P, const void* cilm, in
     double2* packed = (double2*)work;
     double2* spec = (double2*)((char*)work + coef_region(P, nfield));
     double2* fbuf = fft_scratch(P, work, coef_region(P, nfield) + spec_region(P, nfield));
+    const bool i8 = P->precision != SHTC_PREC_F64;
     stage_begin(SHTC_STAGE_PACK, st);
-    rc = launch_pack_coef(P, cilm, cdt, csf, csk, csl, csm, cdim, packed, nfield, 1, st);
+    rc = launch_pack_coef(P, cilm, cdt, csf, csk, csl, csm, cdim, packed, nfield, i8 ? 3 : 1,
+                          st);
     stage_end(SHTC_STAGE_PACK, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_LEGENDRE_SYNTH, st);
-    rc = launch_legendre_synth(P, packed, spec, nfield, st);
+    if (i8)
+        rc = launch_legendre_synth_i8(
+            P, packed, spec, nfield,
+            (char*)work + coef_region(P, nfield) + spec_region(P, nfield) + fft_region(P), st);
+    else
+        rc = launch_legendre_synth(P, packed, spec, nfield, st);
     stage_end(SHTC_STAGE_LEGENDRE_SYNTH, st);
     if (rc) return rc;
     stage_begin(SHTC_STAGE_FFT_C2R, st);

@@ -38,7 +38,8 @@ int map_cuda(cudaError_t e) { return e == cudaSuccess ? SHTC_OK : SHTC_ECUDA; }
 // ---------------------------------------------------------------------------
 // scale_mode 0: copy; 1: multiply by the analysis normalisation factor
 // (the adjoint of the final divide of SHExpandDH.f95:674-702); 0 and 1 also
-// multiply by the recursion's D(l - m), 2 copies without it.
+// multiply by the recursion's D(l - m); 2 and 3 are 0 and 1 without it (the
+// INT8 tensor-core synthesis).
 __device__ __forceinline__ double anal_norm_factor(int norm, int l,
                                                    const double* nrm3,
                                                    long long idx) {
@@ -85,14 +86,14 @@ k_pack_coef(const CT* __restrict__ cilm, long long sf, long long sk, long long s
         if (m > l || l > lc) continue;
         const long long idx = packed_off(m, lc) + (l - m);
         double2 v = tile[j][tx];
-        if (scale_mode == 1) {
+        if (scale_mode == 1 || scale_mode == 3) {
             const double a = anal_norm_factor(norm, l, nrm3, idx);
             v.x *= a;
             v.y *= a;
         }
-        // D(l - m) of the rescaled recursion (legendre.cuh); scale_mode 2
-        // keeps the plain coefficients (the INT8 tensor-core synthesis)
-        const double d = scale_mode == 2 ? 1.0 : rec[idx].y;
+        // D(l - m) of the rescaled recursion (legendre.cuh); scale_modes 2
+        // and 3 keep the plain coefficients (the INT8 tensor-core synthesis)
+        const double d = scale_mode >= 2 ? 1.0 : rec[idx].y;
         packed[idx * nfield + f_off + f] = make_double2(v.x * d, v.y * d);
     }
 }

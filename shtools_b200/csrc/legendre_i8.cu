@@ -752,6 +752,7 @@ __global__ void k_i8_rec2(const double2* __restrict__ rec, double4* __restrict__
 }
 
 #include "legendre_i8_table.cuh"
+#include "legendre_i8_anal.cuh"
 
 // --------------------------------------------------------------------------
 // host side
@@ -776,12 +777,34 @@ static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 using namespace i8;
 
-// scratch of the tensor-core synthesis: the coefficient image and the column scales
-size_t synth_i8_bytes(const shtc_plan* P, int nfield) {
-    const int N = group_cols(P, nfield), ngroups = (nfield + N / 2 - 1) / (N / 2);
+// scratch of the tensor-core synthesis (the coefficient image and the column
+// scales) and of the tensor-core analysis (the ring-sum image and its
+// scales): one region serves both directions, so its size does not depend on
+// whether the plan holds its table
+static size_t synth_image_bytes(const shtc_plan* P, int nfield, int N) {
+    const int ngroups = (nfield + N / 2 - 1) / (N / 2);
     const int DB = prec_digits(P->precision);
     return align256((size_t)P->i8_ntot * ngroups * bimage_bytes(N, DB)) +
            align256((size_t)(P->lc + 1) * ngroups * N * sizeof(double));
+}
+
+static int anal_cols(int nfield) { return nfield > 8 ? 32 : 16; }
+
+static size_t anal_image_bytes(const shtc_plan* P, int nfield) {
+    const int N = anal_cols(nfield), ngroups = (nfield + N / 2 - 1) / (N / 2);
+    const int DB = prec_digits(P->precision);
+    const int ptiles = (P->npair + kPairs - 1) / kPairs;
+    return align256((size_t)(P->lc + 1) * ptiles * 2 * ngroups * gimage_bytes(N, DB)) +
+           align256((size_t)(P->lc + 1) * 2 * ngroups * N * sizeof(double));
+}
+
+size_t synth_i8_bytes(const shtc_plan* P, int nfield) {
+    // either column count of the synthesis (16 on the fly, 32 from the table
+    // for more than 8 fields), or the analysis
+    const size_t s16 = synth_image_bytes(P, nfield, 16), s32 = synth_image_bytes(P, nfield, 32);
+    const size_t s = s16 > s32 ? s16 : s32;
+    const size_t a = anal_image_bytes(P, nfield);
+    return s > a ? s : a;
 }
 
 int set_precision_tables(shtc_plan* P, int precision) {
@@ -811,6 +834,25 @@ int set_precision_tables(shtc_plan* P, int precision) {
         }
         P->d_i8_toff = d;
         P->i8_ntot = acc;
+    }
+    if (!P->d_i8_uoff) {
+        std::vector<long long> uoff(P->lc + 2);
+        long long acc = 0;
+        for (int m = 0; m <= P->lc; ++m) {
+            uoff[m] = acc;
+            acc += nsuper_of(P->lc, m);
+        }
+        uoff[P->lc + 1] = acc;
+        long long* d = nullptr;
+        if (cudaMalloc((void**)&d, sizeof(long long) * uoff.size()) != cudaSuccess)
+            return SHTC_EALLOC;
+        if (cudaMemcpy(d, uoff.data(), sizeof(long long) * uoff.size(),
+                       cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaFree(d);
+            return SHTC_ECUDA;
+        }
+        P->d_i8_uoff = d;
+        P->i8_utot = acc;
     }
     if (!P->d_i8_rec2) {
         double4* d = nullptr;
@@ -901,7 +943,7 @@ static int launch_synth_tab_n(const shtc_plan* P, const double2* coef, double2* 
     TabSynthArgs a;
     a.tab = P->d_i8_tab;
     a.off = P->d_i8_tab_off;
-    a.t0 = P->d_i8_tab_t0;
+    a.u0 = P->d_i8_tab_u0;
     a.image = image;
     a.toff = P->d_i8_toff;
     a.colinv = colinv;
@@ -935,26 +977,82 @@ int launch_legendre_synth_i8(const shtc_plan* P, const double2* coef, double2* s
                  : launch_synth_i8_n<16, 6>(P, coef, spec, nfield, scratch, st);
 }
 
+// the table-driven analysis: ring-sum image, then the streaming kernel
+template <int N, int DA>
+static int launch_anal_tab_n(const shtc_plan* P, const double2* spec, double2* partial,
+                             int nfield, void* scratch, cudaStream_t st) {
+    const int ngroups = (nfield + N / 2 - 1) / (N / 2);
+    const int ptiles = (P->npair + kPairs - 1) / kPairs;
+    uint8_t* image = (uint8_t*)scratch;
+    double* colinv = (double*)((char*)scratch +
+                               align256((size_t)(P->lc + 1) * ptiles * 2 * ngroups *
+                                        gimage_bytes(N, DA)));
+    k_i8_anal_image<N, DA><<<dim3(P->lc + 1, ngroups), 256, 0, st>>>(
+        spec, (uint32_t*)image, colinv, P->lc, P->npair, nfield, ngroups, ptiles);
+    int rc = map_cuda(cudaGetLastError());
+    if (rc) return rc;
+    constexpr size_t smem = anal_smem(N, DA);
+    static_assert(smem >= 120 * 1024, "one CTA per SM");
+    if ((rc = kernel_smem_attr((const void*)k_legendre_anal_tab<N, DA>, smem, true))) return rc;
+    TabAnalArgs a;
+    a.tab = P->d_i8_tab;
+    a.off = P->d_i8_tab_off;
+    a.u0 = P->d_i8_tab_u0;
+    a.uoff = P->d_i8_uoff;
+    a.image = image;
+    a.colinv = colinv;
+    a.partial = partial;
+    a.nlm = P->nlm;
+    a.lc = P->lc;
+    a.npair = P->npair;
+    a.nfield = nfield;
+    a.ngroups = ngroups;
+    a.ptiles = ptiles;
+    a.ascale = P->i8_ascale;
+    const long long nitems = 2LL * ngroups * P->i8_utot;
+    const int sms = sm_count(P->device);
+    const int grid = (int)(nitems < sms ? nitems : sms);
+    k_legendre_anal_tab<N, DA><<<grid, kTabThreads, smem, st>>>(a);
+    return map_cuda(cudaGetLastError());
+}
+
+bool anal_i8_ready(const shtc_plan* P) {
+    return (P->precision == SHTC_PREC_INT8X6 || P->precision == SHTC_PREC_INT8X7) &&
+           !P->cplx && has_table(P) && P->d_i8_uoff != nullptr;
+}
+
+int launch_legendre_anal_i8(const shtc_plan* P, const double2* spec, double2* partial,
+                            int nfield, void* scratch, cudaStream_t st) {
+    if (!anal_i8_ready(P)) return SHTC_EBOUND;
+    const bool seven = P->precision == SHTC_PREC_INT8X7;
+    if (anal_cols(nfield) == 32)
+        return seven ? launch_anal_tab_n<32, 7>(P, spec, partial, nfield, scratch, st)
+                     : launch_anal_tab_n<32, 6>(P, spec, partial, nfield, scratch, st);
+    return seven ? launch_anal_tab_n<16, 7>(P, spec, partial, nfield, scratch, st)
+                 : launch_anal_tab_n<16, 6>(P, spec, partial, nfield, scratch, st);
+}
+
 void free_i8_table(shtc_plan* P) {
     if (P->d_i8_tab) P->device_bytes -= P->i8_tab_bytes;
     cudaFree(P->d_i8_tab);
     cudaFree(P->d_i8_tab_off);
-    cudaFree(P->d_i8_tab_t0);
+    cudaFree(P->d_i8_tab_u0);
     P->d_i8_tab = nullptr;
     P->d_i8_tab_off = nullptr;
-    P->d_i8_tab_t0 = nullptr;
+    P->d_i8_tab_u0 = nullptr;
     P->i8_tab_bytes = 0;
     P->i8_tab_prec = 0;
 }
 
 // Two passes of the recursion over every (m, pair tile): the first finds the
-// leading all-zero K-tiles, the second writes the stored ones.
+// leading all-zero super-tiles, the second writes the stored ones into the
+// zeroed table.
 template <int DA>
 static int build_i8_table_n(shtc_plan* P) {
     const int ptiles = (P->npair + kPairs - 1) / kPairs;
     const long long nitem = (long long)(P->lc + 1) * ptiles;
     TabBuildArgs a;
-    a.rec2 = P->d_i8_rec2;
+    a.rec = P->d_rec;
     a.pmm = P->d_pmm;
     a.rtab = P->d_rtab;
     a.zp = P->d_z;
@@ -964,24 +1062,24 @@ static int build_i8_table_n(shtc_plan* P) {
     a.ascale = P->i8_ascale;
     a.off = nullptr;
     a.tab = nullptr;
-    int* t0 = nullptr;
+    int* u0 = nullptr;
     long long* off = nullptr;
     uint8_t* tab = nullptr;
-    std::vector<int> ht0((size_t)nitem);
+    std::vector<int> hu0((size_t)nitem);
     std::vector<long long> hoff((size_t)nitem);
     int rc = SHTC_OK;
     auto fail = [&](int code) {
-        cudaFree(t0);
+        cudaFree(u0);
         cudaFree(off);
         cudaFree(tab);
         return code;
     };
-    if (cudaMalloc((void**)&t0, sizeof(int) * (size_t)nitem) != cudaSuccess) return fail(SHTC_EALLOC);
-    a.t0 = t0;
+    if (cudaMalloc((void**)&u0, sizeof(int) * (size_t)nitem) != cudaSuccess) return fail(SHTC_EALLOC);
+    a.u0 = u0;
     const dim3 grid(ptiles, P->lc + 1);
-    k_i8_table<DA, false><<<grid, 256>>>(a);
+    k_i8_table<DA, false><<<grid, kPairs>>>(a);
     if ((rc = map_cuda(cudaGetLastError()))) return fail(rc);
-    if ((rc = map_cuda(cudaMemcpy(ht0.data(), t0, sizeof(int) * (size_t)nitem,
+    if ((rc = map_cuda(cudaMemcpy(hu0.data(), u0, sizeof(int) * (size_t)nitem,
                                   cudaMemcpyDeviceToHost))))
         return fail(rc);
     long long acc = 0;
@@ -989,9 +1087,9 @@ static int build_i8_table_n(shtc_plan* P) {
         for (int pt = 0; pt < ptiles; ++pt) {
             const long long i = (long long)m * ptiles + pt;
             hoff[i] = acc;
-            acc += ntiles_of(P->lc, m) - ht0[i];
+            acc += nsuper_of(P->lc, m) - hu0[i];
         }
-    const unsigned long long bytes = (unsigned long long)acc * tab_ktile_bytes(DA);
+    const unsigned long long bytes = (unsigned long long)acc * tab_super_bytes(DA);
     if (cudaMalloc((void**)&off, sizeof(long long) * (size_t)nitem) != cudaSuccess)
         return fail(SHTC_EALLOC);
     if (cudaMalloc((void**)&tab, (size_t)(bytes ? bytes : 256)) != cudaSuccess) {
@@ -1001,16 +1099,17 @@ static int build_i8_table_n(shtc_plan* P) {
     if ((rc = map_cuda(cudaMemcpy(off, hoff.data(), sizeof(long long) * (size_t)nitem,
                                   cudaMemcpyHostToDevice))))
         return fail(rc);
+    if ((rc = map_cuda(cudaMemset(tab, 0, (size_t)(bytes ? bytes : 256))))) return fail(rc);
     a.off = off;
     a.tab = tab;
     if (bytes) {
-        k_i8_table<DA, true><<<grid, 256>>>(a);
+        k_i8_table<DA, true><<<grid, kPairs>>>(a);
         if ((rc = map_cuda(cudaGetLastError()))) return fail(rc);
     }
     if ((rc = map_cuda(cudaDeviceSynchronize()))) return fail(rc);
     P->d_i8_tab = tab;
     P->d_i8_tab_off = off;
-    P->d_i8_tab_t0 = t0;
+    P->d_i8_tab_u0 = u0;
     P->i8_tab_bytes = bytes;
     P->i8_tab_prec = P->precision;
     P->device_bytes += bytes;

@@ -1,21 +1,33 @@
-// Table-driven tensor-core synthesis: the P_lm digits of a plan are computed
-// once (FP64 recursion, the same fixed point and balanced digits as the
-// on-the-fly kernel) and kept in HBM in the shared-memory layout of the MMA's
-// A operand; each call streams them with bulk copies and multiplies them with
-// the coefficient digits on the tensor cores.  The integer sums are the same
-// as those of k_legendre_synth_i8 (same digits, same kept products), so the
-// two paths give bit-identical results.
+// Table-driven tensor-core Legendre sums: the P_lm digits of a plan are
+// computed once and kept in HBM in a layout that is, at once, the K-major A
+// operand of the synthesis MMA (M = ring pairs, K = degrees) and the
+// MN-major A operand of the analysis MMA (M = degrees, K = ring pairs).
+// Each call streams the digits with bulk copies and multiplies them with the
+// coefficient (synthesis) or ring-sum (analysis) digits on the tensor cores.
+// The table holds the P_lm of the FP64 kernels' one-step recursion rounded to
+// the fixed point (same scale and balanced digits as the on-the-fly kernel,
+// whose same-parity two-step recursion rounds differently): the analysis of
+// the high degrees weighs every P_lm error by the whole field, and the
+// two-step values put the lmax-2799 analysis 1e-8 per degree away from FP64.
 //
 // Table layout.  Work item (m, ring-pair tile pt of 128 pairs) owns the
-// K-tiles t0(m, pt) .. nt(m) - 1 of 64 degrees; a K-tile is
-// [parity q][digit i] x 4096 bytes, one digit tile being 128 pairs x 32
-// degrees of that parity in the K-major core-matrix layout (pair r, degree
-// index k at (r % 8) * 16 + (r / 8) * 256 + (k / 16) * 128 + k % 16).  The
-// leading K-tiles whose digits are all zero (P_lm below half a unit of the
-// fixed point: high orders near the poles, where P_lm decays like sin^m of
-// the colatitude) are not stored; t0 is the first K-tile with a non-zero
-// digit over the item's 128 pairs and both parities, so the skipped tiles
-// contribute exactly nothing.
+// super-tiles u0(m, pt) .. nu(m) - 1 of 256 degrees (four K-tiles of 64); a
+// super-tile is [parity q][digit i] x 16384 bytes, one digit block holding
+// the 128 degrees d of that parity (s = l - m = 256 u + 2 d + q) of the 128
+// pairs r, byte (d, r) at
+//     (d / 16) * 2048 + (r / 8) * 128 + (r % 8) * 16 + d % 16.
+// Every 16-byte row is one pair's 16 consecutive same-parity degrees.  The
+// 4096 bytes of degrees d = 32 k .. 32 k + 31 (K-tile 4 u + k) are
+// contiguous: the synthesis A tile, K-major with the K core matrices 2048
+// bytes apart and the 8-pair groups 128 apart.  Read as M = 128 degrees x
+// K = 32 pairs the block is MN-major: degree chunks of 16 at 2048 bytes,
+// 8-pair groups at 128.  The leading super-tiles whose digits are all zero
+// (P_lm below half a unit of the fixed point: high orders near the poles,
+// where P_lm decays like sin^m of the colatitude) are not stored; u0 is the
+// first super-tile with a non-zero digit over the item's 128 pairs and both
+// parities, so the skipped ones contribute exactly nothing.  Degrees past
+// lc in the last super-tile hold finite garbage digits (synthesis: the
+// coefficient image is zero there; analysis: those rows are not written).
 //
 // Synthesis kernel: one CTA per SM, warps 0-7 the epilogue, warp 8 the MMA
 // issue, warp 9 the bulk-copy loader.  A stage holds one parity of one
@@ -28,8 +40,13 @@
 // until the epilogue of the previous item has read D, while the loader keeps
 // streaming the next stages.
 
-constexpr int kTabAT = kPairs * 32;              // bytes of one A digit tile
-__host__ __device__ constexpr int tab_ktile_bytes(int DA) { return 2 * DA * kTabAT; }
+constexpr int kTabAT = kPairs * 32;              // bytes of one A digit tile (32 degrees)
+constexpr int kTabSub = 4;                       // K-tiles per super-tile
+constexpr int kTabDigit = kTabSub * kTabAT;      // one digit block: 128 degrees x 128 pairs
+__host__ __device__ constexpr int tab_super_bytes(int DA) { return 2 * DA * kTabDigit; }
+__host__ __device__ inline int nsuper_of(int lc, int m) {
+    return (ntiles_of(lc, m) + kTabSub - 1) / kTabSub;
+}
 constexpr int kTabSmemBudget = 220 * 1024;
 __host__ __device__ constexpr int tab_stage_bytes(int N, int DA) {
     return DA * kTabAT + DA * btile_bytes(N);
@@ -40,91 +57,144 @@ __host__ __device__ constexpr int tab_stages(int N, int DA) {
 }
 
 struct TabBuildArgs {
-    const double4* rec2;     // {gamma, delta, D, 0} per packed (l, m)
+    const double2* rec;      // the plan's {beta, D} per packed (l, m) (FP64 path)
     const double* pmm;       // sectoral start values
     const double* rtab;      // u^m / 1e-280 per (m, pair)
     const double* zp;        // z of the northern ring of each pair
-    int* t0;                 // per item (m * ptiles + pt): first stored K-tile
-    const long long* off;    // per item: K-tiles stored before it (fill pass)
-    uint8_t* tab;            // the table (fill pass)
+    int* u0;                 // per item (m * ptiles + pt): first stored super-tile
+    const long long* off;    // per item: super-tiles stored before it (fill pass)
+    uint8_t* tab;            // the table (fill pass; zeroed beforehand)
     int lc, npair, ptiles;
     double ascale;
 };
 
-// Runs the recursion of item (pt = blockIdx.x, m = blockIdx.y) over all its
-// K-tiles.  FILL = false: records the first K-tile with a non-zero digit
-// (nt when there is none).  FILL = true: writes the digit tiles of K-tiles
-// t >= t0.  Warps w and w + 4 own the same 32 pairs; warp w the even
-// degrees (l - m), warp w + 4 the odd ones.
+// Digit words of one 64-degree K-tile of one pair from the one-step rescaled
+// recursion of the FP64 kernels (legendre.cuh: Q(s) = z Q(s-1) - beta(s)
+// Q(s-2), P(s) = Q(s) D(s), both values multiplied by D(s) at the end of
+// every 16-degree segment), so that the table holds the FP64 path's P_lm
+// rounded to the fixed point.  W0 / W1: the even / odd degrees, word i * 8 +
+// g of digit i holding the K indices 4 g .. 4 g + 3 of the parity.  q1, q2:
+// Q(s-1), Q(s-2) (at s = 0: 0 and the sectoral start, beta(0) = -1).
+template <int DA>
+__device__ __forceinline__ void tile_digits_1step(const double2* recs, double z, double rp,
+                                                  double& q1, double& q2, uint32_t* W0,
+                                                  uint32_t* W1) {
+    constexpr double kMagic6 = 6896688841130112.0;                // 1.5 * 2^52 + 0x80..80
+    constexpr double kMagic = 6755399441055744.0;                 // 1.5 * 2^52
+    constexpr unsigned long long kOffset7 = 0xBD48808080808080ull;
+#pragma unroll
+    for (int g8 = 0; g8 < 8; ++g8) {
+        uint32_t lo[2][4], hi[2][4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+#pragma unroll
+            for (int par = 0; par < 2; ++par) {
+                const int j = g8 * 8 + 2 * u + par;
+                const double2 f = recs[j];
+                const double pv = fma(z, q1, -(f.x * q2));
+                q2 = q1;
+                q1 = pv;
+                unsigned long long y;
+                if constexpr (DA == 6) {
+                    y = (unsigned long long)__double_as_longlong(fma(pv * f.y, rp, kMagic6));
+                } else {
+                    y = (unsigned long long)__double_as_longlong(fma(pv * f.y, rp, kMagic)) +
+                        kOffset7;
+                }
+                lo[par][u] = (uint32_t)y;
+                hi[par][u] = (uint32_t)(y >> 32);
+                if ((j & (kRecSegment - 1)) == 0) {
+                    q1 *= f.y;
+                    q2 *= f.y;
+                }
+            }
+        }
+        uint32_t w[DA];
+        pack4<DA>(lo[0], hi[0], w);
+#pragma unroll
+        for (int i = 0; i < DA; ++i) W0[i * 8 + g8] = w[i];
+        pack4<DA>(lo[1], hi[1], w);
+#pragma unroll
+        for (int i = 0; i < DA; ++i) W1[i * 8 + g8] = w[i];
+    }
+}
+
+// Runs the recursion of item (pt = blockIdx.x, m = blockIdx.y), one thread
+// per pair, over all its K-tiles.  FILL = false: records the first
+// super-tile with a non-zero digit (nu when there is none).  FILL = true:
+// writes the digit tiles of the K-tiles of super-tiles u >= u0 (K-tiles past
+// the last degree stay zero).
 template <int DA, bool FILL>
-__global__ void __launch_bounds__(256) k_i8_table(TabBuildArgs a) {
+__global__ void __launch_bounds__(kPairs) k_i8_table(TabBuildArgs a) {
     const int pt = blockIdx.x, m = blockIdx.y;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int lq = warp & 3, qrole = warp >> 2;
-    const int r = lq * 32 + lane;                 // row of the pair in the tile
+    const int r = threadIdx.x;                    // row of the pair in the tile
     const int p = pt * kPairs + r;
     const bool valid = p < a.npair;
     const int nsteps = a.lc - m + 1;
     const int nt = ntiles_of(a.lc, m);
+    const int nu = nsuper_of(a.lc, m);
     const long long item = (long long)m * a.ptiles + pt;
-    __shared__ double4 recs[kTileDeg];
+    __shared__ double2 recs[kTileDeg];
     __shared__ int tmin;
     const double z = valid ? a.zp[p] : 0.0;
     const double rp = valid ? a.rtab[(long long)m * a.npair + p] * a.ascale : 0.0;
-    const double start = a.pmm[m];
-    double c1 = qrole == 0 ? start : z * start;
-    double c2 = qrole == 0 ? start : 0.0;
-    const double z2 = z * z;
-    const double4* rsrc = a.rec2 + packed_off(m, a.lc);
-    int t0 = nt;
-    long long base = 0;                           // K-tile t sits at base + t - t0
+    double q1 = 0.0, q2 = a.pmm[m];
+    const double2* rsrc = a.rec + packed_off(m, a.lc);
+    int u0 = nu;
+    long long base = 0;                           // super-tile u sits at base + u - u0
     if (FILL) {
-        t0 = a.t0[item];
+        u0 = a.u0[item];
         base = a.off[item];
     } else if (threadIdx.x == 0) {
-        tmin = nt;
+        tmin = nu;
     }
-    const long long rowoff = (long long)qrole * DA * kTabAT + (r % 8) * 16 + (r / 8) * 256;
-    int first = nt;
+    const long long rowoff = (long long)(r / 8) * 128 + (r % 8) * 16;
+    int first = nu;
     for (int t = 0; t < nt; ++t) {
         __syncthreads();                          // the previous tile's entries are consumed
         for (int j = threadIdx.x; j < kTileDeg; j += blockDim.x) {
             const int s = kTileDeg * t + j;
-            recs[j] = s < nsteps ? rsrc[s] : make_double4(0.0, 0.0, 0.0, 0.0);
+            recs[j] = s < nsteps ? rsrc[s] : make_double2(0.0, 0.0);
         }
         __syncthreads();
-        // the chain advances through every tile, stored or not
-        uint32_t W[DA * 8];
-        if (qrole == 0) tile_digits<DA, 0, 0, 8>(recs, z2, rp, t == 0, c1, c2, W);
-        else tile_digits<DA, 1, 0, 8>(recs, z2, rp, t == 0, c1, c2, W);
+        // the recursion advances through every tile, stored or not
+        uint32_t W[2][DA * 8];
+        tile_digits_1step<DA>(recs, z, rp, q1, q2, W[0], W[1]);
+        const int u = t / kTabSub;
         if (!FILL) {
-            if (first == nt) {
+            if (first == nu) {
                 uint32_t any = 0u;
 #pragma unroll
-                for (int k = 0; k < DA * 8; ++k) any |= W[k];
-                if (any) first = t;
+                for (int k = 0; k < DA * 8; ++k) any |= W[0][k] | W[1][k];
+                if (any) first = u;
             }
-        } else if (t >= t0) {
-            uint8_t* tb = a.tab + (base + t - t0) * (long long)tab_ktile_bytes(DA) + rowoff;
+        } else if (u >= u0) {
+            // K-tile t = 4 u + k: degrees d = 32 k .. 32 k + 31 of each parity
+            uint8_t* tb = a.tab + (base + u - u0) * (long long)tab_super_bytes(DA) +
+                          (t % kTabSub) * kTabAT + rowoff;
 #pragma unroll
-            for (int i = 0; i < DA; ++i) {
-                uint4* d = reinterpret_cast<uint4*>(tb + i * kTabAT);
-                d[0] = make_uint4(W[i * 8 + 0], W[i * 8 + 1], W[i * 8 + 2], W[i * 8 + 3]);
-                d[8] = make_uint4(W[i * 8 + 4], W[i * 8 + 5], W[i * 8 + 6], W[i * 8 + 7]);
-            }
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int i = 0; i < DA; ++i) {
+                    uint4* d = reinterpret_cast<uint4*>(tb + (q * DA + i) * kTabDigit);
+                    d[0] = make_uint4(W[q][i * 8 + 0], W[q][i * 8 + 1], W[q][i * 8 + 2],
+                                      W[q][i * 8 + 3]);
+                    d[128] = make_uint4(W[q][i * 8 + 4], W[q][i * 8 + 5], W[q][i * 8 + 6],
+                                        W[q][i * 8 + 7]);
+                }
         }
     }
     if (!FILL) {
-        if (first < nt) atomicMin(&tmin, first);
+        if (first < nu) atomicMin(&tmin, first);
         __syncthreads();
-        if (threadIdx.x == 0) a.t0[item] = tmin;
+        if (threadIdx.x == 0) a.u0[item] = tmin;
     }
 }
 
 struct TabSynthArgs {
     const uint8_t* tab;      // the table (k_i8_table)
-    const long long* off;    // per item (m * ptiles + pt): K-tiles stored before it
-    const int* t0;           // per item: first stored K-tile
+    const long long* off;    // per item (m * ptiles + pt): super-tiles stored before it
+    const int* u0;           // per item: first stored super-tile
     const uint8_t* image;    // coefficient image (k_i8_coef_image<N, DB>)
     const long long* toff;   // K-tiles of the image before order m
     const double* colinv;    // 2^-b per (m, group, column)
@@ -213,11 +283,11 @@ __global__ void __launch_bounds__(kTabThreads, 1) k_legendre_synth_tab(TabSynthA
                 tab_item_decode(it, a.ptiles, a.ngroups, &m, &pt, &g);
                 const long long item = (long long)m * a.ptiles + pt;
                 const int nt = ntiles_of(a.lc, m);
-                const int t0 = a.t0[item];
-                const uint8_t* asrc = a.tab + a.off[item] * (long long)tab_ktile_bytes(DA);
+                const int t0 = kTabSub * a.u0[item];      // first K-tile stored
+                const uint8_t* asrc = a.tab + a.off[item] * (long long)tab_super_bytes(DA);
                 const uint8_t* bsrc = a.image + (a.toff[m] * a.ngroups + (long long)g * nt) *
                                                     (long long)bimage_bytes(N, DB);
-                const int ns = 2 * (nt - t0);
+                const int ns = nt > t0 ? 2 * (nt - t0) : 0;
                 for (int s = 0; s < ns && !abort_flag; ++s, ++L) {
                     const int st = (int)(L % NS);
                     if (L >= NS && !mbar_wait(&empty[st], (uint32_t)((L / NS - 1) & 1), &abort_flag))
@@ -225,7 +295,12 @@ __global__ void __launch_bounds__(kTabThreads, 1) k_legendre_synth_tab(TabSynthA
                     const int t = t0 + (s >> 1), q = s & 1;
                     uint8_t* sb = smem_tab + st * SB;
                     mbar_expect_tx(&full[st], (uint32_t)(ABYTES + BBYTES));
-                    bulk_g2s(sb, asrc + (long long)s * ABYTES, ABYTES, &full[st]);
+                    // the DA digit tiles of (t, q), 16 KB apart in the table
+                    const uint8_t* at = asrc + (long long)((t - t0) / kTabSub) * tab_super_bytes(DA) +
+                                        (long long)q * DA * kTabDigit + (t % kTabSub) * kTabAT;
+#pragma unroll
+                    for (int i = 0; i < DA; ++i)
+                        bulk_g2s(sb + i * kTabAT, at + (long long)i * kTabDigit, kTabAT, &full[st]);
                     bulk_g2s(sb + ABYTES, bsrc + (long long)t * bimage_bytes(N, DB) + q * BBYTES,
                              BBYTES, &full[st]);
                 }
@@ -240,7 +315,10 @@ __global__ void __launch_bounds__(kTabThreads, 1) k_legendre_synth_tab(TabSynthA
         // ------------------------------------------------ MMA issue
         const uint32_t tm = __shfl_sync(0xffffffffu, tmem, 0);
         const bool leader = elect_one();
-        const uint64_t desc0 = smem_desc(smem_u32(smem_tab), 128, 256);
+        // A tiles: K core matrices 2048 bytes apart, 8-pair groups 128;
+        // B (coefficient image): K core matrices 128 apart, column groups 256
+        const uint64_t adesc0 = smem_desc(smem_u32(smem_tab), 2048, 128);
+        const uint64_t bdesc0 = smem_desc(smem_u32(smem_tab) + ABYTES, 128, 256);
         long long T = 0;                      // stages consumed
         int kwork = 0;                        // items with MMAs
         bool ok = true;
@@ -248,7 +326,8 @@ __global__ void __launch_bounds__(kTabThreads, 1) k_legendre_synth_tab(TabSynthA
             int m, pt, g;
             tab_item_decode(it, a.ptiles, a.ngroups, &m, &pt, &g);
             const long long item = (long long)m * a.ptiles + pt;
-            const int ns = 2 * (ntiles_of(a.lc, m) - a.t0[item]);
+            const int nt = ntiles_of(a.lc, m), t0 = kTabSub * a.u0[item];
+            const int ns = nt > t0 ? 2 * (nt - t0) : 0;
             if (ns == 0) continue;
             // the epilogue of the previous item has read D
             ok = kwork == 0 || mbar_wait(&dfree, (uint32_t)((kwork - 1) & 1), &abort_flag);
@@ -260,8 +339,8 @@ __global__ void __launch_bounds__(kTabThreads, 1) k_legendre_synth_tab(TabSynthA
                 tc_fence_after();
                 const int q = s & 1;
                 const bool first = s < 2;
-                const uint64_t ad = desc0 + (uint64_t)((st * SB) >> 4);
-                const uint64_t bd = ad + (uint64_t)(ABYTES >> 4);
+                const uint64_t ad = adesc0 + (uint64_t)((st * SB) >> 4);
+                const uint64_t bd = bdesc0 + (uint64_t)((st * SB) >> 4);
                 const uint32_t dq = tm + (uint32_t)(q * KW * N);
                 // top A digit: coefficient digits 0 .. DB-1 -> blocks 1 .. KW-1
                 if (leader)
@@ -312,7 +391,7 @@ __global__ void __launch_bounds__(kTabThreads, 1) k_legendre_synth_tab(TabSynthA
             int m, pt, g;
             tab_item_decode(it, a.ptiles, a.ngroups, &m, &pt, &g);
             const long long item = (long long)m * a.ptiles + pt;
-            const bool work = ntiles_of(a.lc, m) > a.t0[item];
+            const bool work = ntiles_of(a.lc, m) > kTabSub * a.u0[item];
             const int p = pt * kPairs + lq * 32 + lane;
             const bool valid = p < a.npair;
             double v[2][CW];

@@ -383,6 +383,7 @@ using namespace shtc;
 static void plan_free_tables(shtc_plan* P) {
     free_i8_table(P);
     cudaFree(P->d_i8_toff);
+    cudaFree(P->d_i8_uoff);
     cudaFree(P->d_i8_rec2);
     cudaFree(P->d_rec);
     cudaFree(P->d_pmm);

@@ -102,11 +102,13 @@ struct shtc_plan {
     double4* d_i8_rec2;     // INT8X6: {gamma, delta, D, 0} per packed (l, m): the
                             // same-parity two-step form of the rescaled recursion
     long long i8_ntot;      // INT8X6: K-tiles of all orders
+    long long* d_i8_uoff;   // INT8X6: super-tiles of 256 degrees before each order (lc + 2)
+    long long i8_utot;      // INT8X6: super-tiles of all orders
     double i8_ascale;       // INT8X6: 2^a, fixed-point scale of the P_lm operand
     // table-driven tensor-core synthesis (shtc_plan_legendre_table)
     uint8_t* d_i8_tab;          // P_lm digit table (legendre_i8_table.cuh)
-    long long* d_i8_tab_off;    // per (m, pair tile): K-tiles stored before it
-    int* d_i8_tab_t0;           // per (m, pair tile): first stored K-tile
+    long long* d_i8_tab_off;    // per (m, pair tile): super-tiles stored before it
+    int* d_i8_tab_u0;           // per (m, pair tile): first stored super-tile
     unsigned long long i8_tab_bytes;
     int i8_tab_prec;            // precision the table holds digits of (0: none)
 };
@@ -205,6 +207,11 @@ size_t synth_i8_bytes(const shtc_plan* P, int nfield);
 int launch_legendre_synth_i8(const shtc_plan* P, const double2* coef, double2* spec,
                              int nfield, void* scratch, cudaStream_t st);
 int set_precision_tables(shtc_plan* P, int precision);
+// the analysis of a mixed plan runs on the tensor cores once the plan holds
+// its P_lm digit table (real plans)
+bool anal_i8_ready(const shtc_plan* P);
+int launch_legendre_anal_i8(const shtc_plan* P, const double2* spec, double2* partial,
+                            int nfield, void* scratch, cudaStream_t st);
 void free_i8_table(shtc_plan* P);
 
 // timing.cu: event brackets around kernel stages (SHTC_STAGE_* ids)

@@ -128,8 +128,9 @@ class Plan:
     def legendre_table(self, enable=True):
         """shtc_plan_legendre_table: build (or free) the plan's table of P_lm
         digits for its mixed precision; the syntheses then stream it from
-        device memory instead of running the recursion.  Returns its size in
-        bytes."""
+        device memory instead of running the recursion, and the analyses
+        (and the synthesis adjoints) run on the tensor cores from it.
+        Returns its size in bytes."""
         nb = ctypes.c_ulonglong(0)
         with _on_device(self.device):
             _lib.check(self.lib.shtc_plan_legendre_table(self.handle, int(bool(enable)),
@@ -239,7 +240,8 @@ _plans = {}
 
 
 # "-table": the synthesis streams a precomputed table of the P_lm digits
-# (Plan.legendre_table) instead of running the recursion
+# (Plan.legendre_table) instead of running the recursion, and the analysis
+# runs on the tensor cores from the same table
 PRECISIONS = {"fp64": 0, "int8x6": 1, "int8x7": 2, "int8x6-table": 1, "int8x7-table": 2}
 
 
@@ -507,18 +509,21 @@ def MakeGridDH(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
 
 
 def SHExpandDH(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None,
-               dtype=None):
+               dtype=None, precision="fp64"):
     """Driscoll-Healy analysis on the GPU (src/SHExpandDH.f95:1).
 
     griddh: (..., n, >= sampling*n) float64 or float32 with n even.  Returns
     (..., 2, lmax_calc+1, lmax_calc+1) of ``dtype`` (default: the grid's).
+    precision "int8x7-table" ("int8x6-table"): the Legendre sums on the INT8
+    tensor cores from the plan's P_lm digit table (norms 1, 2, 4); the
+    analysis of "int8x7" / "int8x6" plans without a table stays FP64.
     """
     _check_common(norm, csphase)
     lmax, lc = _resolve_anal_dh(np.shape(griddh), sampling, lmax_calc)
     dtype = _out_dtype(dtype)
     grid = _as_cuda(griddh, "griddh")
     plan = get_plan(GRID_DH, lmax, lc, norm, csphase, sampling, 0,
-                    device=grid.device)
+                    device=grid.device, precision=precision)
     return _analysis(grid, plan, lc + 1, dtype)
 
 
@@ -541,11 +546,12 @@ def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
 
 
 def SHExpandGLQ(gridglq, w=None, zero=None, norm=1, csphase=1,
-                lmax_calc=None, dtype=None):
+                lmax_calc=None, dtype=None, precision="fp64"):
     """Gauss-Legendre analysis on the GPU (src/SHExpandGLQ.f95:1).
 
     gridglq: (..., lmax+1, >= 2*lmax+1).  w, zero: weights and nodes from
-    SHGLQ; None computes them with the GPU PreGLQ.
+    SHGLQ; None computes them with the GPU PreGLQ.  precision: as for
+    SHExpandDH.
     """
     _check_common(norm, csphase)
     lmax, lc = _resolve_anal_glq(np.shape(gridglq), lmax_calc)
@@ -560,7 +566,7 @@ def SHExpandGLQ(gridglq, w=None, zero=None, norm=1, csphase=1,
         z = zz if z is None else z
         wh = ww if wh is None else wh
     plan = get_plan(GRID_GLQ, lmax, lc, norm, csphase, 1, 0, zero=z, w=wh,
-                    device=grid.device)
+                    device=grid.device, precision=precision)
     return _analysis(grid, plan, lc + 1, dtype)
 
 
