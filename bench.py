@@ -1095,6 +1095,8 @@ def run_cuda(args, w, rank, world, local_rank):
         b_synth = lambda x: B.MakeGridDH(x, sampling=s)
         b_anal = lambda x: B.SHExpandDH(x, sampling=s)
     plug_steps = max(2, min(args.steps, 4 if F > 1 else args.steps))
+    if not cplx:
+        B.set_precision(args.precision)
 
     def plug_step():
         out = []
@@ -1115,6 +1117,7 @@ def run_cuda(args, w, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     plug_ms = max_over_ranks(pa.elapsed_time(pb), dev)
     plug_value = 2.0 * F * plug_steps * world / (plug_ms * 1e-3)
+    B.set_precision("fp64")
     plug_ok = bool(np.array_equal(b_plug[-1], bb[-1]))
     plug_h2d = F * (cil[0].nbytes + g_last.nbytes)
     plug_d2h = F * (cil[0].nbytes + g_last.nbytes)

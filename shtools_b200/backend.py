@@ -24,7 +24,13 @@ __all__ = ["MakeGridDH", "SHExpandDH", "MakeGridGLQ", "SHExpandGLQ", "SHGLQ",
            "GLQGridCoord",
            "MakeGridDHC", "SHExpandDHC", "MakeGridGLQC", "SHExpandGLQC",
            "MakeGradientDH", "MakeGravGridDH", "NormalGravity", "SHRotateRealCoef",
-           "available", "register", "set_nthreads"]
+           "available", "register", "set_nthreads", "set_precision", "get_precision"]
+
+# Legendre arithmetic of the four real transforms (no counterpart in the
+# reference, whose backends are FP64): "fp64" (the default), or a mixed
+# precision of shtools_b200.transforms.PRECISIONS, e.g. "int8x7-table" for
+# the INT8 tensor-core sums from each plan's P_lm digit table
+_precision = "fp64"
 
 
 def available():
@@ -44,6 +50,20 @@ def set_nthreads(ntnew):
     return None
 
 
+def set_precision(precision="fp64"):
+    """Select the Legendre arithmetic of MakeGridDH, SHExpandDH, MakeGridGLQ
+    and SHExpandGLQ for later calls ("fp64", "int8x7", "int8x7-table", ...;
+    ValueError otherwise).  The mixed forms apply to norms 1, 2 and 4."""
+    global _precision
+    _t._precision_code(precision)
+    _precision = precision
+
+
+def get_precision():
+    """The Legendre arithmetic selected by set_precision."""
+    return _precision
+
+
 def _np(t):
     """The result as a new numpy array (through pinned staging buffers)."""
     return hostio.to_host(t)
@@ -60,7 +80,7 @@ def MakeGridDH(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
     extend]) -- see src/MakeGridDH.f95:1 and ducc0_wrapper.py:454."""
     return _np(_t.MakeGridDH(_dev(cilm), lmax=lmax,
                              norm=norm, sampling=sampling, csphase=csphase,
-                             lmax_calc=lmax_calc, extend=extend))
+                             lmax_calc=lmax_calc, extend=extend, precision=_precision))
 
 
 def SHExpandDH(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None):
@@ -68,7 +88,7 @@ def SHExpandDH(griddh, norm=1, sampling=1, csphase=1, lmax_calc=None):
     src/SHExpandDH.f95:1 and ducc0_wrapper.py:659."""
     return _np(_t.SHExpandDH(_dev(griddh), norm=norm,
                              sampling=sampling, csphase=csphase,
-                             lmax_calc=lmax_calc))
+                             lmax_calc=lmax_calc, precision=_precision))
 
 
 def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
@@ -78,7 +98,7 @@ def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
     zero=None the nodes come from the GPU PreGLQ."""
     return _np(_t.MakeGridGLQ(_dev(cilm), zero=zero,
                               lmax=lmax, norm=norm, csphase=csphase,
-                              lmax_calc=lmax_calc, extend=extend))
+                              lmax_calc=lmax_calc, extend=extend, precision=_precision))
 
 
 def SHExpandGLQ(gridglq, w=None, zero=None, norm=1, csphase=1, lmax_calc=None):
@@ -86,7 +106,7 @@ def SHExpandGLQ(gridglq, w=None, zero=None, norm=1, csphase=1, lmax_calc=None):
     src/SHExpandGLQ.f95:1 and ducc0_wrapper.py:1003."""
     return _np(_t.SHExpandGLQ(_dev(gridglq), w=w,
                               zero=zero, norm=norm, csphase=csphase,
-                              lmax_calc=lmax_calc))
+                              lmax_calc=lmax_calc, precision=_precision))
 
 
 def SHGLQ(lmax):

@@ -795,7 +795,8 @@ static size_t anal_image_bytes(const shtc_plan* P, int nfield) {
     const int DB = prec_digits(P->precision);
     const int ptiles = (P->npair + kPairs - 1) / kPairs;
     return align256((size_t)(P->lc + 1) * ptiles * 2 * ngroups * gimage_bytes(N, DB)) +
-           align256((size_t)(P->lc + 1) * 2 * ngroups * N * sizeof(double));
+           align256((size_t)(P->lc + 1) * 2 * ngroups * N * sizeof(double)) +
+           align256((size_t)(P->lc + 1) * nfield * 4 * sizeof(unsigned long long));
 }
 
 size_t synth_i8_bytes(const shtc_plan* P, int nfield) {
@@ -984,13 +985,18 @@ static int launch_anal_tab_n(const shtc_plan* P, const double2* spec, double2* p
     const int ngroups = (nfield + N / 2 - 1) / (N / 2);
     const int ptiles = (P->npair + kPairs - 1) / kPairs;
     uint8_t* image = (uint8_t*)scratch;
-    double* colinv = (double*)((char*)scratch +
-                               align256((size_t)(P->lc + 1) * ptiles * 2 * ngroups *
-                                        gimage_bytes(N, DA)));
-    k_i8_anal_image<N, DA><<<dim3(P->lc + 1, ngroups), 256, 0, st>>>(
-        spec, (uint32_t*)image, colinv, P->lc, P->npair, nfield, ngroups, ptiles);
-    int rc = map_cuda(cudaGetLastError());
+    const size_t ib = align256((size_t)(P->lc + 1) * ptiles * 2 * ngroups * gimage_bytes(N, DA));
+    double* colinv = (double*)((char*)scratch + ib);
+    unsigned long long* gmax = (unsigned long long*)(
+        (char*)scratch + ib + align256((size_t)(P->lc + 1) * 2 * ngroups * N * sizeof(double)));
+    const size_t gmb = (size_t)(P->lc + 1) * nfield * 4 * sizeof(unsigned long long);
+    int rc = map_cuda(cudaMemsetAsync(gmax, 0, gmb, st));
     if (rc) return rc;
+    k_i8_anal_max<<<dim3((P->lc + 1 + 127) / 128, nfield, (P->npair + kMaxPairs - 1) / kMaxPairs),
+                    128, 0, st>>>(spec, gmax, P->lc, P->npair);
+    k_i8_anal_digits<N, DA><<<dim3(P->lc + 1, ptiles, ngroups), 16 * N, 0, st>>>(
+        spec, gmax, (uint32_t*)image, colinv, P->lc, P->npair, nfield, ngroups, ptiles);
+    if ((rc = map_cuda(cudaGetLastError()))) return rc;
     constexpr size_t smem = anal_smem(N, DA);
     static_assert(smem >= 120 * 1024, "one CTA per SM");
     if ((rc = kernel_smem_attr((const void*)k_legendre_anal_tab<N, DA>, smem, true))) return rc;

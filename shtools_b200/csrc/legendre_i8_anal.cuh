@@ -11,7 +11,7 @@
 //   A = the table's digit block of (m, pair tile, u, q), read MN-major
 //       (M = 128 degrees, K = 32 pairs per MMA; legendre_i8_table.cuh);
 //   B = digits of round(G_q[p][n] 2^b(m, q, n)), one exponent per order,
-//       parity and column from max_p |G_q[p][n]| (k_i8_anal_image), K-major.
+//       parity and column from max_p |G_q[p][n]| (k_i8_anal_digits), K-major.
 // Digit i of A meets the window of B digits j = max(0, WB - i) .. DB - 1 in
 // one MMA whose (DB - j0) N columns land on the accumulator's weight blocks
 // w = i + j - WB, as in the synthesis.  The K loop runs over the pair tiles
@@ -41,86 +41,98 @@ __host__ __device__ constexpr int anal_smem(int N, int DB) {
 // tiles of B, tile index ((m * ptiles + pt) * 2 + q) * ngroups + g; byte =
 // balanced digit j of round(G_q[p][n] 2^b).  colinv[((m * 2 + q) * ngroups +
 // g) * N + n] = 2^-b.  spec: r2c output [field][pair][m][ring] (Re, Im).
+// Two passes over spec: the column maxima (k_i8_anal_max), then the digits
+// (k_i8_anal_digits), each reading every 32-byte ring pair once.
 // --------------------------------------------------------------------------
+constexpr int kMaxPairs = 64;     // ring pairs per block of the maxima pass
+
+// gmax[(f * (lc + 1) + m) * 4 + k] = max_p |G|, k = (q, Re/Im): the bits of
+// non-negative doubles, which order as integers (zeroed by the caller)
+__global__ void __launch_bounds__(128)
+k_i8_anal_max(const double2* __restrict__ spec, unsigned long long* __restrict__ gmax, int lc,
+              int npair) {
+    const int m = blockIdx.x * 128 + threadIdx.x;
+    const int f = blockIdx.y;
+    const int p0 = blockIdx.z * kMaxPairs;
+    if (m > lc) return;
+    const int p1 = min(npair, p0 + kMaxPairs);
+    const double4* x = reinterpret_cast<const double4*>(spec) +
+                       ((long long)f * npair + p0) * (lc + 1) + m;
+    double mx[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int p = p0; p < p1; ++p, x += lc + 1) {
+        const double4 v = *x;                     // north (Re, Im), south (Re, Im)
+        mx[0] = fmax(mx[0], fabs(v.x + v.z));
+        mx[1] = fmax(mx[1], fabs(v.y + v.w));
+        mx[2] = fmax(mx[2], fabs(v.x - v.z));
+        mx[3] = fmax(mx[3], fabs(v.y - v.w));
+    }
+    unsigned long long* o = gmax + ((long long)f * (lc + 1) + m) * 4;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (mx[k] > 0.0) atomicMax(&o[k], (unsigned long long)__double_as_longlong(mx[k]));
+}
+
+// Block (m, pt, g) of 32 NFG threads: thread (k4, fl, kc, ng) converts the
+// four pairs kc * 16 + k4 * 4 + 0..3 of field ng * 4 + fl, both parities and
+// both Re and Im, reading each pair's 32 bytes once.
 template <int N, int DB>
-__global__ void __launch_bounds__(256)
-k_i8_anal_image(const double2* __restrict__ spec, uint32_t* __restrict__ image,
-                double* __restrict__ colinv, int lc, int npair, int nfield, int ngroups,
-                int ptiles) {
+__global__ void __launch_bounds__(16 * N)
+k_i8_anal_digits(const double2* __restrict__ spec, const unsigned long long* __restrict__ gmax,
+                 uint32_t* __restrict__ image, double* __restrict__ colinv, int lc, int npair,
+                 int nfield, int ngroups, int ptiles) {
     constexpr int NFG = N / 2;
     constexpr int kBits = Digits<DB>::kBitsB;
-    static_assert(256 % NFG == 0, "fields of a group divide the block");
-    const int m = blockIdx.x, g = blockIdx.y;
-    const long long pstride = 2LL * (lc + 1);                    // double2 per pair
-    const long long fstride = (long long)npair * pstride;        // double2 per field
-    __shared__ unsigned long long cmax[2 * N];                   // [q][n]
-    __shared__ double cscale[2 * N];
-    for (int n = threadIdx.x; n < 2 * N; n += blockDim.x) cmax[n] = 0ull;
-    __syncthreads();
-    // column maxima of both ring combinations (non-negative doubles order as
-    // integers)
-    {
-        const int f = threadIdx.x % NFG, fg = g * NFG + f;
-        double mx[4] = {0.0, 0.0, 0.0, 0.0};   // sym Re, sym Im, anti Re, anti Im
-        if (fg < nfield) {
-            const double2* x = spec + fg * fstride + 2LL * m;
-            for (int p = threadIdx.x / NFG; p < npair; p += 256 / NFG) {
-                const double2 a = x[p * pstride], b = x[p * pstride + 1];
-                mx[0] = fmax(mx[0], fabs(a.x + b.x));
-                mx[1] = fmax(mx[1], fabs(a.y + b.y));
-                mx[2] = fmax(mx[2], fabs(a.x - b.x));
-                mx[3] = fmax(mx[3], fabs(a.y - b.y));
-            }
-        }
+    constexpr int WPT = gtile_bytes(N) / 4;
+    const int m = blockIdx.x, pt = blockIdx.y, g = blockIdx.z;
+    const int tid = threadIdx.x;
+    const int k4 = tid & 3, fl = (tid >> 2) & 3, kc = (tid >> 4) & 7, ng = tid >> 7;
+    const int fi = ng * 4 + fl, fg = g * NFG + fi;
+    const bool fok = fg < nfield;
+    double sc[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-            atomicMax(&cmax[(k >> 1) * N + 2 * f + (k & 1)],
-                      (unsigned long long)__double_as_longlong(mx[k]));
-    }
-    __syncthreads();
-    for (int n = threadIdx.x; n < 2 * N; n += blockDim.x) {
-        const double mx = __longlong_as_double((long long)cmax[n]);
-        double sc = 0.0, inv = 0.0;
+    for (int k = 0; k < 4; ++k) {
+        const double mx =
+            fok ? __longlong_as_double((long long)gmax[((long long)fg * (lc + 1) + m) * 4 + k])
+                : 0.0;
+        double inv = 0.0;
+        sc[k] = 0.0;
         if (mx > 0.0) {
             int e;
             frexp(mx, &e);                   // mx < 2^e
-            sc = ldexp(1.0, kBits - e);      // |G| sc < 2^kBits
+            sc[k] = ldexp(1.0, kBits - e);   // |G| sc < 2^kBits
             inv = ldexp(1.0, e - kBits);
         }
-        cscale[n] = sc;
-        const int q = n / N, c = n - q * N;
-        colinv[(((long long)m * 2 + q) * ngroups + g) * N + c] = inv;
+        if (pt == 0 && kc == 0 && k4 == 0)
+            colinv[(((long long)m * 2 + (k >> 1)) * ngroups + g) * N + 2 * fi + (k & 1)] = inv;
     }
-    __syncthreads();
-    // one thread per (pair tile, parity, word): 4 pairs of one column, DB words
-    constexpr int WPT = gtile_bytes(N) / 4;
-    for (int idx = threadIdx.x; idx < ptiles * 2 * WPT; idx += blockDim.x) {
-        const int wi = idx % WPT, tq = idx / WPT, pt = tq >> 1, q = tq & 1;
-        const int k4 = wi & 3, n8 = (wi >> 2) & 7, kc = (wi >> 5) & 7, ng = wi >> 8;
-        const int n = ng * 8 + n8, f = n >> 1, fg = g * NFG + f;
-        const double sc = cscale[q * N + n];
-        uint32_t w[DB];
+    uint32_t w[4][DB];
 #pragma unroll
-        for (int j = 0; j < DB; ++j) w[j] = 0u;
+    for (int k = 0; k < 4; ++k)
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int p = pt * kPairs + kc * 16 + k4 * 4 + u;
-            long long x = 0;
-            if (p < npair && fg < nfield) {
-                const double2* y = spec + fg * fstride + p * pstride + 2LL * m;
-                const double2 a = y[0], b = y[1];
-                const double va = (n & 1) ? a.y : a.x, vb = (n & 1) ? b.y : b.x;
-                x = __double2ll_rn((q ? va - vb : va + vb) * sc);
-            }
-            x += Digits<DB>::kBalance;
+        for (int j = 0; j < DB; ++j) w[k][j] = 0u;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int p = pt * kPairs + kc * 16 + k4 * 4 + u;
+        double4 v = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (fok && p < npair)
+            v = reinterpret_cast<const double4*>(spec)[((long long)fg * npair + p) * (lc + 1) + m];
+        const double gv[4] = {v.x + v.z, v.y + v.w, v.x - v.z, v.y - v.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const long long x = __double2ll_rn(gv[k] * sc[k]) + Digits<DB>::kBalance;
 #pragma unroll
             for (int j = 0; j < DB; ++j)
-                w[j] |= (uint32_t)(((x >> (8 * j)) & 0xFF) ^ 0x80) << (8 * u);
+                w[k][j] |= (uint32_t)(((x >> (8 * j)) & 0xFF) ^ 0x80) << (8 * u);
         }
-        uint32_t* tb = image + ((((long long)m * ptiles + pt) * 2 + q) * ngroups + g) *
-                                   (long long)(gimage_bytes(N, DB) / 4);
+    }
 #pragma unroll
-        for (int j = 0; j < DB; ++j) tb[j * WPT + wi] = w[j];
+    for (int k = 0; k < 4; ++k) {
+        const int q = k >> 1, n8 = 2 * fl + (k & 1);
+        uint32_t* tb = image + ((((long long)m * ptiles + pt) * 2 + q) * ngroups + g) *
+                                   (long long)(gimage_bytes(N, DB) / 4) +
+                       ng * 256 + kc * 32 + n8 * 4 + k4;
+#pragma unroll
+        for (int j = 0; j < DB; ++j) tb[j * WPT] = w[k][j];
     }
 }
 
@@ -129,7 +141,7 @@ struct TabAnalArgs {
     const long long* off;    // per (m * ptiles + pt): super-tiles stored before it
     const int* u0;           // per (m * ptiles + pt): first stored super-tile
     const long long* uoff;   // super-tiles of all orders before m (lc + 2 entries)
-    const uint8_t* image;    // ring-sum image (k_i8_anal_image<N, DB>)
+    const uint8_t* image;    // ring-sum image (k_i8_anal_digits<N, DB>)
     const double* colinv;    // 2^-b per (m, parity, group, column)
     double2* partial;        // [field][packed (l, m)] (Re, Im) sums
     long long nlm;

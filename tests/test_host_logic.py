@@ -139,3 +139,19 @@ def test_hostio_threaded_copy_exact():
         dst = np.zeros(n, dtype=np.uint8)
         hostio._copy(dst, src)
         assert np.array_equal(dst, src)
+
+
+def test_backend_precision_selection():
+    """The backend's Legendre arithmetic switch accepts the library's
+    precisions only and defaults to FP64 (no GPU needed)."""
+    from shtools_b200 import backend as B
+    assert B.get_precision() == "fp64"
+    try:
+        B.set_precision("int8x7-table")
+        assert B.get_precision() == "int8x7-table"
+        with pytest.raises(ValueError):
+            B.set_precision("fp16")
+        assert B.get_precision() == "int8x7-table"
+    finally:
+        B.set_precision("fp64")
+    assert B.get_precision() == "fp64"
