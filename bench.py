@@ -42,6 +42,10 @@ WORKLOADS = {
     # 16 DH fields, lmax 2799, sampling 2, FP64 grids
     "dh2799x16": dict(kind="dh", lmax=2799, nfield=16, sampling=2, beta=3.0,
                       seed=5000),
+    # 16 DH fields, lmax 1023, sampling 2 (2048 x 4096): the mixed-precision
+    # kernels at a size whose P_lm digit table (about 5 GB) profiles quickly
+    "dh1023x16": dict(kind="dh", lmax=1023, nfield=16, sampling=2, beta=3.0,
+                      seed=5500),
     # 8 DH fields, lmax 719, sampling 2
     "dh719x8": dict(kind="dh", lmax=719, nfield=8, sampling=2, beta=2.0,
                     seed=3000),

@@ -66,8 +66,11 @@ k_pack_coef(const CT* __restrict__ cilm, long long sf, long long sk, long long s
             int norm, const double* __restrict__ nrm3, int scale_mode,
             const double2* __restrict__ rec, int f_off) {
     __shared__ double2 tile[kCoefTile][kCoefTile + 1];   // [m - m0][l - l0]
-    const int l0 = blockIdx.x * kCoefTile, m0 = blockIdx.y * kCoefTile;
-    const int f = blockIdx.z;
+    // the fields of one tile are adjacent blocks: their 16-byte entries of
+    // the field-interleaved packed array share sectors, which L2 then
+    // writes to DRAM whole
+    const int f = blockIdx.x;
+    const int l0 = blockIdx.y * kCoefTile, m0 = blockIdx.z * kCoefTile;
     if (m0 > l0 + kCoefTile - 1) return;   // tile above the diagonal (uniform)
     const int tx = threadIdx.x;
     for (int j = threadIdx.y; j < kCoefTile; j += kCoefRows) {
@@ -354,7 +357,7 @@ int launch_pack_coef(const shtc_plan* P, const void* cilm, int dtype, long long 
     const int ntot = nfield_total > 0 ? nfield_total : nfield;
     const int lc = P->lc;
     const int nt = (lc + kCoefTile) / kCoefTile;
-    const dim3 grid(nt, nt, nfield), block(kCoefTile, kCoefRows);
+    const dim3 grid(nfield, nt, nt), block(kCoefTile, kCoefRows);
     if (dtype == SHTC_F32)
         k_pack_coef<float><<<grid, block, 0, st>>>((const float*)cilm, sf, sk, sl, sm, cdim,
                                                  packed, lc, ntot, P->norm, P->d_nrm,

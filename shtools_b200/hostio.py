@@ -10,6 +10,12 @@ dedicated copy stream, and each host copy is split over a small pool of
 threads (numpy releases the GIL while it copies), since one core copies
 well below what PCIe carries.  Small arrays take the plain path.
 
+Results of up to PINNED_MAX bytes come back without staging: they are
+copied straight into a new pinned host tensor whose memory the returned
+numpy array views (the array keeps it alive; freed blocks return to
+torch's pinned-memory cache).  Inputs that already live in pinned memory
+(for instance such a result, passed back in) are uploaded directly.
+
 Thread safety: one lock per device guards its staging buffers; calls from
 several threads are serialised on them.
 """
@@ -23,6 +29,7 @@ import torch
 CHUNK_BYTES = 16 << 20         # bytes per staging buffer
 SMALL_BYTES = 1 << 20          # arrays below this size are copied directly
 SLICE_BYTES = 2 << 20          # smallest share of a host copy given to one thread
+PINNED_MAX = 4 << 30           # results up to this size come back in pinned memory
 
 _lock = threading.Lock()
 _state = {}                    # device index -> (lock, stream, [buffers], [events])
@@ -74,7 +81,12 @@ def to_device(a, device=None):
     a = np.ascontiguousarray(a)
     if a.nbytes < SMALL_BYTES:
         return torch.from_numpy(a).to(dev)
-    dst = torch.empty(a.shape, dtype=torch.from_numpy(a[:0]).dtype, device=dev)
+    ta = torch.from_numpy(a)
+    if ta.is_pinned():
+        # one DMA on the current stream; torch's pinned-memory cache keeps
+        # blocks it allocated until the copy has completed
+        return ta.to(dev, non_blocking=True)
+    dst = torch.empty(a.shape, dtype=ta.dtype, device=dev)
     src = a.reshape(-1).view(np.uint8)
     dflat = dst.view(-1).view(torch.uint8)
     lock, cs, bufs, evs = _get(dev)
@@ -103,6 +115,11 @@ def to_host(t):
         return t.cpu().numpy()
     t = t.contiguous()
     dev = t.device
+    if t.numel() * t.element_size() <= PINNED_MAX:
+        h = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
+        h.copy_(t, non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        return h.numpy()
     out = np.empty(tuple(t.shape), dtype=t.new_empty(0).cpu().numpy().dtype)
     dst = out.reshape(-1).view(np.uint8)
     sflat = t.view(-1).view(torch.uint8)

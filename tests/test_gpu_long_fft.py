@@ -213,3 +213,50 @@ def test_long_rings_column_major_grids(cuda, oracle):
         plan.synthesis(c, out=gcm)
         assert torch.equal(gcm, g)
         assert torch.equal(plan.analysis(gcm), plan.analysis(g))
+
+
+# Even rings of more than 4096 complex points with radices <= 8 run the
+# 1024-thread register-capped FFT build with both buffers in shared memory:
+# DH lmax 2399, sampling 2, nlon 9600, half length 4800 = 2^6 * 3 * 5^2.
+@pytest.mark.parametrize("extend", [False, True])
+def test_dh2399_long_even_fft_all_rings_low_calc(cuda, oracle, extend):
+    L, lc = 2399, 48
+    c = oracle.power_law_cilm(L, 7101)
+    ext = 1 if extend else 0
+    g = cuda.MakeGridDH(torch.from_numpy(np.stack([c, 2 * c])).cuda(), sampling=2,
+                        lmax_calc=lc, extend=extend).cpu().numpy()
+    gref = oracle.makegrid_dh(c, sampling=2, lmax_calc=lc, extend=ext)
+    assert g.shape[1:] == gref.shape
+    assert grid_rel(g[0], gref) <= GRID_TOL
+    assert grid_rel(g[1], 2 * gref) <= GRID_TOL
+    rng = np.random.default_rng(7102)
+    grid = rng.standard_normal((2,) + gref.shape[:1] + (gref.shape[1],))
+    n = 2 * L + 2
+    b = cuda.SHExpandDH(torch.from_numpy(grid[:, :n, :2 * n]).cuda(), sampling=2,
+                        lmax_calc=lc).cpu().numpy()
+    for f in range(2):
+        bref = oracle.shexpand_dh(np.ascontiguousarray(grid[f, :n, :2 * n]), sampling=2,
+                                  lmax_calc=lc)
+        e = perdeg(b[f], bref)
+        assert e.max() <= DEG_TOL, (f, e.max(), e.argmax())
+
+
+def test_dh2399_long_even_fft_float32_and_adjoint(cuda, oracle):
+    """float32 grids through the long even-ring FFTs stay within float32
+    rounding of float64; the synthesis adjoint (r2c of the cotangent with
+    unit weights) satisfies <S c, y> = <c, S^T y>."""
+    L, lc = 2399, 48
+    c = torch.from_numpy(oracle.power_law_cilm(L, 7103)).cuda()
+    g64 = cuda.MakeGridDH(c, sampling=2, lmax_calc=lc)
+    g32 = cuda.MakeGridDH(c, sampling=2, lmax_calc=lc, dtype=torch.float32)
+    assert ((g32.double() - g64).abs().max() / g64.abs().max()).item() < 1e-6
+    b32 = cuda.SHExpandDH(g32, sampling=2, lmax_calc=lc)
+    b64 = cuda.SHExpandDH(g32.double(), sampling=2, lmax_calc=lc)
+    assert ((b32.double() - b64).abs().max() / b64.abs().max()).item() < 1e-6
+    cc = c.clone().requires_grad_(True)
+    g = cuda.MakeGridDH(cc, sampling=2, lmax_calc=lc)
+    y = torch.randn_like(g)
+    (g * y).sum().backward()
+    lhs = (g.detach() * y).sum().item()
+    rhs = (cc.grad * c).sum().item()
+    assert abs(lhs - rhs) <= 1e-10 * max(1.0, abs(lhs)), (lhs, rhs)

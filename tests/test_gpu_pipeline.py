@@ -75,3 +75,24 @@ def test_hostio_staged_copies(cuda):
     g = hostio.to_device(rng.standard_normal((3, 700, 1401)))
     assert g.shape == (3, 700, 1401) and g.is_contiguous()
     assert np.array_equal(hostio.to_host(g[1]), g[1].cpu().numpy())
+
+
+def test_hostio_pinned_results_and_staged_large(cuda, monkeypatch):
+    """Results come back in pinned memory viewed by numpy; such a result
+    passed back in is uploaded directly and stays exact; results above
+    PINNED_MAX take the staged path (forced here with a small limit)."""
+    from shtools_b200 import hostio
+    rng = np.random.default_rng(8)
+    a = rng.standard_normal(3 * hostio.CHUNK_BYTES // 8 + 5)
+    t = hostio.to_device(a)
+    b = hostio.to_host(t * 2.0)
+    assert torch.from_numpy(b).is_pinned()
+    assert np.array_equal(b, a * 2.0)
+    t2 = hostio.to_device(b)
+    t2 = t2 + 1.0                           # work queued after the direct upload
+    assert np.array_equal(hostio.to_host(t2), a * 2.0 + 1.0)
+    del b
+    monkeypatch.setattr(hostio, "PINNED_MAX", 0)
+    c = hostio.to_host(t * 5.0)
+    assert not torch.from_numpy(c).is_pinned()
+    assert np.array_equal(c, a * 5.0)
