@@ -1109,7 +1109,10 @@ def run_cuda(args, w, rank, world, local_rank):
             out.append(b_anal(gf))
         return gf, out
 
-    plug_step()     # warm-up
+    # warm-up: three calls, so that the pinned host blocks of the results
+    # (torch's pinned-memory cache) exist before the timed region
+    for _ in range(3):
+        plug_step()
     barrier()
     torch.cuda.synchronize(dev)
     pa = torch.cuda.Event(enable_timing=True)
@@ -1174,7 +1177,8 @@ def run_cuda(args, w, rank, world, local_rank):
     # complex fields: two coefficient sets (orders +m, -m) per field
     fl = legendre_flops(w, F * (2 if cplx else 1))
     achieved = fl / (per_launch_ms * 1e-3) / 1e12
-    traffic = load_traffic("%s_%s" % (names[dom], args.workload))
+    traffic = load_traffic("%s_%s" % (names[dom], args.workload) +
+                           ("" if args.precision == "fp64" else "_" + args.precision))
     roof = {"kernel": names[dom], "bound": "fp64", "achieved": achieved,
             "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak if peak else None,
