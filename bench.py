@@ -598,17 +598,32 @@ def run_cuda_grad(args, w, rank, world, local_rank):
                    / n)[:, None]
     st = torch.cuda.current_stream(dev)
 
-    def step():
+    def step(prec=args.precision):
         cr = c.detach().requires_grad_(True)
-        g = sht.MakeGridDH(cr, sampling=s_, dtype=torch.float32)
+        g = sht.MakeGridDH(cr, sampling=s_, dtype=torch.float32, precision=prec)
         loss = (wt * (g - d) ** 2).sum()
         loss.backward()
-        back = sht.SHExpandDH(g.detach(), sampling=s_, dtype=torch.float64)
+        back = sht.SHExpandDH(g.detach(), sampling=s_, dtype=torch.float64, precision=prec)
         return cr.grad, back
 
+    def perdeg(a, b):
+        dd = (a - b).pow(2).sum(dim=(1, 3)).sqrt()
+        nn = b.pow(2).sum(dim=(1, 3)).sqrt()
+        return float(torch.where(nn > 0, dd / nn, dd).max())
+
+    mixed_err = None
+    if args.precision != "fp64":
+        # the FP64 step once, as the reference of the mixed gradient and analysis
+        grad64, back64 = step("fp64")
+        grad64, back64 = grad64.clone(), back64.clone()
     for _ in range(args.warmup):
         grad, back = step()
     torch.cuda.synchronize(dev)
+    if args.precision != "fp64":
+        mixed_err = {"gradient_max_perdeg_rel_err_vs_fp64": perdeg(grad, grad64),
+                     "analysis_max_perdeg_rel_err_vs_fp64": perdeg(back, back64),
+                     "status": sht.mixed_status(dev)}
+        del grad64, back64
     bb = back.cpu().numpy()
     cc = c.cpu().numpy()
     num = np.sqrt(((bb - cc) ** 2).sum(axis=(1, 3)))
@@ -646,8 +661,9 @@ def run_cuda_grad(args, w, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 (float32 grids)",
         "data": "synthetic seeded power-law coefficients, S(l)=(l+1)^-%g" % w["beta"],
         "config": {"workload": args.workload, "kind": "dh", "lmax": L,
-                   "fields_per_gpu": F, "sampling": s_, "precision": "fp64 compute, "
-                   "float32 grids, float64 coefficients",
+                   "fields_per_gpu": F, "sampling": s_,
+                   "precision": ("fp64" if args.precision == "fp64" else args.precision) +
+                                " Legendre sums, float32 grids, float64 coefficients",
                    "step": "synthesis + weighted L2 misfit backward (adjoint) + analysis",
                    "l2": "flushed between steps (256 MiB write, outside step events)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
@@ -659,6 +675,7 @@ def run_cuda_grad(args, w, rank, world, local_rank):
         "stages": {names[i]: {"ms_per_launch": (ms[i] / cnt[i]) if cnt[i] else None,
                               "launches": cnt[i]} for i in range(6)},
         "roundtrip_max_perdeg_err": rt_err,
+        "mixed_vs_fp64": mixed_err,
         "gpu_launches": int(sum(cnt)),
         "clocks": clk.summary(),
     }
