@@ -11,16 +11,21 @@ threads (numpy releases the GIL while it copies), since one core copies
 well below what PCIe carries.  Small arrays take the plain path.
 
 Results of up to PINNED_MAX bytes come back without staging: they are
-copied straight into a new pinned host tensor whose memory the returned
-numpy array views (the array keeps it alive; freed blocks return to
-torch's pinned-memory cache).  Inputs that already live in pinned memory
-(for instance such a result, passed back in) are uploaded directly.
+copied straight into a pinned host buffer that the returned numpy array
+views.  The buffers come from a pool of this module, by byte size: a buffer
+returns to the pool when the array viewing it (and every view of that
+array) has been garbage-collected, so a loop of calls reuses the same few
+buffers instead of pinning new memory (cudaHostAlloc of tens of MB takes
+tens of ms).  The pool keeps at most POOL_MAX bytes of free buffers.
+Inputs that already live in pinned memory (for instance such a result,
+passed back in) are uploaded directly.
 
 Thread safety: one lock per device guards its staging buffers; calls from
 several threads are serialised on them.
 """
 import os
 import threading
+import weakref
 from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
@@ -30,10 +35,34 @@ CHUNK_BYTES = 16 << 20         # bytes per staging buffer
 SMALL_BYTES = 1 << 20          # arrays below this size are copied directly
 SLICE_BYTES = 2 << 20          # smallest share of a host copy given to one thread
 PINNED_MAX = 4 << 30           # results up to this size come back in pinned memory
+POOL_MAX = 8 << 30             # free pinned result buffers kept for reuse
 
 _lock = threading.Lock()
 _state = {}                    # device index -> (lock, stream, [buffers], [events])
 _pool = None
+_free = {}                     # byte size -> [pinned uint8 tensors] not viewed by any array
+_free_bytes = 0
+
+
+def _take(nbytes):
+    """A pinned uint8 host tensor of nbytes, from the pool or new."""
+    global _free_bytes
+    with _lock:
+        lst = _free.get(nbytes)
+        if lst:
+            _free_bytes -= nbytes
+            return lst.pop()
+    return torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+
+
+def _give(buf):
+    """Return a buffer whose array has died to the pool (or drop it)."""
+    global _free_bytes
+    n = buf.numel()
+    with _lock:
+        if _free_bytes + n <= POOL_MAX:
+            _free.setdefault(n, []).append(buf)
+            _free_bytes += n
 
 
 def _threads():
@@ -83,9 +112,11 @@ def to_device(a, device=None):
         return torch.from_numpy(a).to(dev)
     ta = torch.from_numpy(a)
     if ta.is_pinned():
-        # one DMA on the current stream; torch's pinned-memory cache keeps
-        # blocks it allocated until the copy has completed
-        return ta.to(dev, non_blocking=True)
+        # one DMA on the current stream, complete on return: the caller may
+        # reuse or free the host array at once
+        t = ta.to(dev, non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        return t
     dst = torch.empty(a.shape, dtype=ta.dtype, device=dev)
     src = a.reshape(-1).view(np.uint8)
     dflat = dst.view(-1).view(torch.uint8)
@@ -115,11 +146,15 @@ def to_host(t):
         return t.cpu().numpy()
     t = t.contiguous()
     dev = t.device
-    if t.numel() * t.element_size() <= PINNED_MAX:
-        h = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
+    nbytes = t.numel() * t.element_size()
+    if nbytes <= PINNED_MAX:
+        buf = _take(nbytes)
+        h = buf.view(t.dtype).view(tuple(t.shape))
         h.copy_(t, non_blocking=True)
         torch.cuda.current_stream(dev).synchronize()
-        return h.numpy()
+        out = h.numpy()
+        weakref.finalize(out, _give, buf)
+        return out
     out = np.empty(tuple(t.shape), dtype=t.new_empty(0).cpu().numpy().dtype)
     dst = out.reshape(-1).view(np.uint8)
     sflat = t.view(-1).view(torch.uint8)

@@ -91,7 +91,14 @@ def test_hostio_pinned_results_and_staged_large(cuda, monkeypatch):
     t2 = hostio.to_device(b)
     t2 = t2 + 1.0                           # work queued after the direct upload
     assert np.array_equal(hostio.to_host(t2), a * 2.0 + 1.0)
-    del b
+    # the buffer of a dead result is reused by the next result of its size
+    ptr = b.ctypes.data
+    del b, t2
+    import gc
+    gc.collect()
+    b2 = hostio.to_host(t * 4.0)
+    assert b2.ctypes.data == ptr and np.array_equal(b2, a * 4.0)
+    del b2
     monkeypatch.setattr(hostio, "PINNED_MAX", 0)
     c = hostio.to_host(t * 5.0)
     assert not torch.from_numpy(c).is_pinned()

@@ -155,3 +155,25 @@ def test_backend_precision_selection():
     finally:
         B.set_precision("fp64")
     assert B.get_precision() == "fp64"
+
+
+def test_hostio_pool_returns_buffers_when_views_die():
+    """A result buffer goes back to the pinned pool only once the returned
+    array and every view of it are gone (plain host tensors stand in for
+    pinned ones here)."""
+    import gc
+    import weakref
+    import torch
+    from shtools_b200 import hostio as H
+    before = H._free_bytes
+    buf = torch.empty(96, dtype=torch.uint8)
+    arr = buf.view(torch.float64).numpy()
+    weakref.finalize(arr, H._give, buf)
+    view = arr[3:5]
+    del arr
+    gc.collect()
+    assert H._free_bytes == before
+    del view
+    gc.collect()
+    assert H._free_bytes == before + 96
+    assert H._take(96) is buf and H._free_bytes == before
