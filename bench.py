@@ -46,6 +46,10 @@ WORKLOADS = {
     # kernels at a size whose P_lm digit table (about 5 GB) profiles quickly
     "dh1023x16": dict(kind="dh", lmax=1023, nfield=16, sampling=2, beta=3.0,
                       seed=5500),
+    # 2 DH fields, lmax 2399, sampling 2 (4800 x 9600): the long even-ring
+    # FFT build (complex half length 4800) at a size that profiles quickly
+    "dh2399x2": dict(kind="dh", lmax=2399, nfield=2, sampling=2, beta=3.0,
+                     seed=5700),
     # 8 DH fields, lmax 719, sampling 2
     "dh719x8": dict(kind="dh", lmax=719, nfield=8, sampling=2, beta=2.0,
                     seed=3000),
