@@ -92,6 +92,13 @@ SHTC_API int shtc_plan_legendre_table(shtc_plan* plan, int enable, unsigned long
  * are invalid).  Reads and clears it; synchronises the stream. */
 SHTC_API int shtc_mixed_status(int* status, void* stream);
 
+/* Self-test of that error path (no counterpart in the reference): one GPU
+ * thread waits, through the bounded wait of the tensor-core kernels, on an
+ * mbarrier that nothing completes; within about two seconds the wait gives up
+ * and records SHTC_ETIMEOUT, which the next shtc_mixed_status returns.  No fault
+ * and no trap: the context stays usable.  Synchronises the stream. */
+SHTC_API int shtc_mixed_wait_selftest(void* stream);
+
 /* Library version as 10000*major + 100*minor + patch. */
 SHTC_API int shtc_version(void);
 

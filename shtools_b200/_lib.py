@@ -28,7 +28,8 @@ EXPORTS = (
     "shtc_version", "shtc_status_string", "shtc_plan_create_dh",
     "shtc_plan_create_glq", "shtc_plan_destroy", "shtc_plan_info",
     "shtc_plan_set_tuning", "shtc_timing_enable", "shtc_timing_collect",
-    "shtc_plan_set_precision", "shtc_mixed_status", "shtc_plan_legendre_table",
+    "shtc_plan_set_precision", "shtc_mixed_status", "shtc_mixed_wait_selftest",
+    "shtc_plan_legendre_table",
     "shtc_synthesis_noalloc",
     "shtc_workspace_bytes", "shtc_synthesis", "shtc_analysis",
     "shtc_synthesis_adjoint", "shtc_analysis_adjoint", "shtc_synthesis_ex",
@@ -69,6 +70,7 @@ def _bind(L):
     L.shtc_plan_set_tuning.argtypes = [_P, _I, _I, _I]
     L.shtc_plan_set_precision.argtypes = [_P, _I]
     L.shtc_mixed_status.argtypes = [ctypes.POINTER(_I), _P]
+    L.shtc_mixed_wait_selftest.argtypes = [_P]
     L.shtc_plan_legendre_table.argtypes = [_P, _I, ctypes.POINTER(ctypes.c_ulonglong)]
     L.shtc_workspace_bytes.restype = _SZ
     L.shtc_workspace_bytes.argtypes = [_P, _I]

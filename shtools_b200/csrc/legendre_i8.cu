@@ -170,15 +170,28 @@ __device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
     return ok != 0;
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+constexpr unsigned long long kWaitNs = 2000000000ull;   // a wait gives up after 2 s
+
 // bounded wait: false on a timeout or when another thread raised the abort
 // flag.  Polls with test_wait first (no suspension when the phase is about
-// to complete), then suspends in try_wait.
+// to complete), then suspends in try_wait; every 256 tries it checks the
+// abort flag and the 2-second deadline, so the bound does not depend on how
+// long one try_wait may suspend.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
     for (int it = 0; it < 64; ++it)
         if (mbar_test(b, parity)) return true;
+    const unsigned long long t0 = global_ns();
     for (unsigned it = 0; it < kSpinLimit; ++it) {
         if (mbar_try(b, parity)) return true;
-        if ((it & 255) == 255 && *abort_flag) return false;
+        if ((it & 255) == 255) {
+            if (*abort_flag) return false;
+            if (global_ns() - t0 > kWaitNs) break;
+        }
     }
     raise_timeout(abort_flag);
     return false;
@@ -1149,6 +1162,29 @@ extern "C" int shtc_plan_legendre_table(shtc_plan* P, int enable, unsigned long 
         rc = P->precision == SHTC_PREC_INT8X7 ? build_i8_table_n<7>(P) : build_i8_table_n<6>(P);
     }
     if (bytes) *bytes = P->i8_tab_bytes;
+    return rc;
+}
+
+namespace shtc {
+namespace i8 {
+// One thread waits, through the tensor kernels' bounded wait, on an mbarrier
+// that nothing arrives on: the wait runs out, records SHTC_ETIMEOUT in the
+// error word and returns (no trap, no unbounded loop)
+__global__ void k_i8_wait_selftest() {
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ volatile int abort_flag;
+    mbar_init(&bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_wait(&bar, 0, &abort_flag);
+}
+}  // namespace i8
+}  // namespace shtc
+
+extern "C" int shtc_mixed_wait_selftest(void* stream) {
+    i8::k_i8_wait_selftest<<<1, 1, 0, (cudaStream_t)stream>>>();
+    int rc = map_cuda(cudaGetLastError());
+    if (!rc) rc = map_cuda(cudaStreamSynchronize((cudaStream_t)stream));
     return rc;
 }
 

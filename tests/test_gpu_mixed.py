@@ -295,3 +295,27 @@ def test_table_analysis_lmax2799_16_fields(cuda, oracle):
                 p.legendre_table(False)
                 del T._plans[k]
         assert e.max() <= DEG_TOL[prec], (prec, e.max())
+
+
+def test_bounded_wait_records_timeout_and_context_survives(cuda, oracle):
+    """A tensor-core wait that never completes (an mbarrier nothing arrives
+    on, shtc_mixed_wait_selftest) gives up, records SHTC_ETIMEOUT, and the
+    next status read returns it once; the context stays usable: a mixed
+    transform afterwards is correct and reports status 0."""
+    import time
+    from shtools_b200 import _lib
+    from shtools_b200.transforms import _stream_ptr
+    lib = _lib.load()
+    assert cuda.mixed_status() == 0
+    t0 = time.perf_counter()
+    _lib.check(lib.shtc_mixed_wait_selftest(_stream_ptr(torch.device("cuda", 0))),
+               "shtc_mixed_wait_selftest")
+    waited = time.perf_counter() - t0
+    assert cuda.mixed_status() == 10          # SHTC_ETIMEOUT
+    assert cuda.mixed_status() == 0           # read and cleared
+    c = torch.from_numpy(fields(oracle, 63, 2, 901)).cuda()
+    g = cuda.MakeGridDH(c, sampling=2, precision="int8x7")
+    g64 = cuda.MakeGridDH(c, sampling=2)
+    assert cuda.mixed_status() == 0
+    assert ((g - g64).abs().max() / g64.abs().max()).item() <= GRID_TOL
+    print("bounded wait gave up after %.2f s" % waited)
