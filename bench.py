@@ -1141,10 +1141,11 @@ def run_cuda(args, w, rank, world, local_rank):
             out.append(b_anal(gf))
         return gf, out
 
-    # warm-up: three calls, so that the pinned host blocks of the results
-    # (torch's pinned-memory cache) exist before the timed region
+    # warm-up: three steps that keep their results as the timed loop does
+    # (the previous step's arrays are alive while the next one runs), so the
+    # pinned result buffers of both exist before the timed region
     for _ in range(3):
-        plug_step()
+        g_last, b_plug = plug_step()
     barrier()
     torch.cuda.synchronize(dev)
     pa = torch.cuda.Event(enable_timing=True)
