@@ -334,6 +334,11 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t* v) {
           "=r"(v[7])
         : "r"(taddr));
 }
+__device__ __forceinline__ void tmem_ld2(uint32_t taddr, uint32_t* v) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];"
+                 : "=r"(v[0]), "=r"(v[1])
+                 : "r"(taddr));
+}
 __device__ __forceinline__ void tmem_wait_st() {
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
@@ -1010,9 +1015,10 @@ static int launch_anal_tab_n(const shtc_plan* P, const double2* spec, double2* p
     k_i8_anal_digits<N, DA><<<dim3(P->lc + 1, ptiles, ngroups), 16 * N, 0, st>>>(
         spec, gmax, (uint32_t*)image, colinv, P->lc, P->npair, nfield, ngroups, ptiles);
     if ((rc = map_cuda(cudaGetLastError()))) return rc;
-    constexpr size_t smem = anal_smem(N, DA);
-    static_assert(smem >= 120 * 1024, "one CTA per SM");
-    if ((rc = kernel_smem_attr((const void*)k_legendre_anal_tab<N, DA>, smem, true))) return rc;
+    constexpr int NBUF = 1;                   // two CTAs per SM, one accumulator buffer each
+    constexpr size_t smem = anal_smem(N, DA, NBUF);
+    if ((rc = kernel_smem_attr((const void*)k_legendre_anal_tab<N, DA, NBUF>, smem, true)))
+        return rc;
     TabAnalArgs a;
     a.tab = P->d_i8_tab;
     a.off = P->d_i8_tab_off;
@@ -1029,9 +1035,9 @@ static int launch_anal_tab_n(const shtc_plan* P, const double2* spec, double2* p
     a.ptiles = ptiles;
     a.ascale = P->i8_ascale;
     const long long nitems = 2LL * ngroups * P->i8_utot;
-    const int sms = sm_count(P->device);
-    const int grid = (int)(nitems < sms ? nitems : sms);
-    k_legendre_anal_tab<N, DA><<<grid, kTabThreads, smem, st>>>(a);
+    const int ctas = sm_count(P->device) * (NBUF == 1 ? 2 : 1);
+    const int grid = (int)(nitems < ctas ? nitems : ctas);
+    k_legendre_anal_tab<N, DA, NBUF><<<grid, kTabThreads, smem, st>>>(a);
     return map_cuda(cudaGetLastError());
 }
 

@@ -19,21 +19,34 @@
 // The INT32 sums are exact: at most DB products of 2^14 per weight and pair,
 // |sum| < DB 2^14 npair < 2^31 for npair < 18000.
 //
-// One CTA per SM: warp 9 streams the table's digit blocks (16 KB each, a
-// ring of NA) and the B tiles (a ring of NB) with bulk copies, warp 8 issues
-// the MMAs from one elected lane, warps 0-7 read the accumulators (two
-// buffers in tensor memory, so the epilogue of one item overlaps the MMAs of
-// the next), combine the weights in 64-bit integers and FP64, and write the
-// coefficients of the item's degrees.  Every wait is bounded (legendre_i8.cu).
+// Two CTAs per SM (NBUF = 1; 20% faster at lmax 2799 x16 than one CTA per SM
+// with two accumulator buffers, NBUF = 2): in each, warp 9 streams the
+// table's digit blocks (16 KB each, a ring of NA) and the B tiles (a ring of
+// NB) with bulk copies, warp 8 issues the MMAs from one elected lane, warps
+// 0-7 read the accumulators (256 tensor-memory columns per CTA), combine the
+// weights in 64-bit integers and FP64, and write the coefficients of the
+// item's degrees; while one CTA's epilogue holds its accumulators, the other
+// CTA's MMAs and copies keep the SM busy.  Every wait is bounded
+// (legendre_i8.cu).
 
 // one B digit tile: N columns x 128 pairs; byte (n, k) at
 // (n / 8) * 1024 + (k / 16) * 128 + (n % 8) * 16 + k % 16
 __host__ __device__ constexpr int gtile_bytes(int N) { return N * kPairs; }
 __host__ __device__ constexpr int gimage_bytes(int N, int DB) { return DB * gtile_bytes(N); }
-__host__ __device__ constexpr int anal_astages(int N) { return N == 32 ? 9 : 10; }
-__host__ __device__ constexpr int anal_bstages(int N) { return N == 32 ? 2 : 3; }
-__host__ __device__ constexpr int anal_smem(int N, int DB) {
-    return anal_astages(N) * kTabDigit + anal_bstages(N) * gimage_bytes(N, DB);
+// shared-memory slots: one CTA per SM with two accumulator buffers, or
+// (NBUF = 1) two CTAs per SM with one each
+__host__ __device__ constexpr int anal_astages(int N, int NBUF) {
+    return NBUF == 2 ? (N == 32 ? 9 : 10) : (N == 32 ? 3 : 5);
+}
+__host__ __device__ constexpr int anal_bstages(int N, int NBUF) {
+    return NBUF == 2 ? (N == 32 ? 2 : 3) : 2;
+}
+__host__ __device__ constexpr int anal_smem(int N, int DB, int NBUF) {
+    return anal_astages(N, NBUF) * kTabDigit + anal_bstages(N, NBUF) * gimage_bytes(N, DB);
+}
+// tensor-memory columns allocated by an analysis CTA (a power of two >= 32)
+__host__ __device__ constexpr int anal_tmem_cols(int DC, int NBUF) {
+    return NBUF == 2 ? 512 : (DC <= 128 ? 128 : 256);
 }
 
 // --------------------------------------------------------------------------
@@ -176,22 +189,24 @@ __device__ __forceinline__ bool anal_has_work(const int* u0, int m, int ptiles, 
     return false;
 }
 
-template <int N, int DA>
-__global__ void __launch_bounds__(kTabThreads, 1) k_legendre_anal_tab(TabAnalArgs a) {
+template <int N, int DA, int NBUF>
+__global__ void __launch_bounds__(kTabThreads, NBUF == 1 ? 2 : 1) k_legendre_anal_tab(TabAnalArgs a) {
     constexpr int DB = DA;
     constexpr int KW = Digits<DA>::KW;
     constexpr int TOP = DA + DB - 2;
     constexpr int WB = TOP - KW + 1;                 // weight of accumulator block 0
-    constexpr int NA = anal_astages(N), NB = anal_bstages(N);
+    constexpr int NA = anal_astages(N, NBUF), NB = anal_bstages(N, NBUF);
+    constexpr int kAlloc = anal_tmem_cols(KW * N, NBUF);
     constexpr int BT = gtile_bytes(N);
     constexpr int BB = gimage_bytes(N, DB);
     constexpr int DC = KW * N;                       // tensor-memory columns of one D buffer
     constexpr int NFG = N / 2;
     constexpr int CW = N / 2;                        // columns of one epilogue warp
-    static_assert(2 * DC <= kTmemAlloc, "tensor memory budget");
+    static_assert(NBUF * DC <= kAlloc && (NBUF == 1 || NBUF == 2), "tensor memory budget");
     static_assert(DB * N <= 256 && N % 16 == 0, "MMA N");
     static_assert(KW == DB + 1 && WB == DA - 2, "weight windows");
-    static_assert(anal_smem(N, DB) <= kTabSmemBudget, "stages fit");
+    static_assert(anal_smem(N, DB, NBUF) <= (NBUF == 1 ? 110 * 1024 : kTabSmemBudget),
+                  "stages fit");
     extern __shared__ __align__(1024) uint8_t smem_an[];   // NA A blocks | NB B tiles
     __shared__ __align__(8) uint64_t afull[NA], aempty[NA], bfull[NB], bempty[NB];
     __shared__ __align__(8) uint64_t dfull[2], dfree[2];
@@ -205,7 +220,7 @@ __global__ void __launch_bounds__(kTabThreads, 1) k_legendre_anal_tab(TabAnalArg
     if (warp == 8) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&tmem_base)),
-                     "r"(kTmemAlloc));
+                     "r"(kAlloc));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
@@ -293,10 +308,10 @@ __global__ void __launch_bounds__(kTabThreads, 1) k_legendre_anal_tab(TabAnalArg
             int m, u, q, g;
             anal_item_decode(it, a.uoff, a.lc, a.ngroups, &m, &u, &q, &g);
             if (!anal_has_work(a.u0, m, a.ptiles, u)) continue;
-            const int buf = kwork & 1;
+            const int buf = kwork % NBUF, use = kwork / NBUF;
             // the epilogue has read this buffer's previous item
-            ok = kwork < 2 ||
-                 mbar_wait(&dfree[buf], (uint32_t)(((kwork >> 1) - 1) & 1), &abort_flag);
+            ok = kwork < NBUF ||
+                 mbar_wait(&dfree[buf], (uint32_t)((use - 1) & 1), &abort_flag);
             if (!__all_sync(0xffffffffu, ok)) { ok = false; break; }
             tc_fence_after();
             const uint32_t d0 = tm + (uint32_t)(buf * DC);
@@ -359,7 +374,7 @@ __global__ void __launch_bounds__(kTabThreads, 1) k_legendre_anal_tab(TabAnalArg
         if (kwork > 0) {
             const int kl = kwork - 1;
             for (unsigned k = 0; k < kSpinLimit; ++k)
-                if (mbar_try(&dfull[kl & 1], (uint32_t)((kl >> 1) & 1))) break;
+                if (mbar_try(&dfull[kl % NBUF], (uint32_t)((kl / NBUF) & 1))) break;
         }
         __syncwarp();
     } else {
@@ -374,54 +389,99 @@ __global__ void __launch_bounds__(kTabThreads, 1) k_legendre_anal_tab(TabAnalArg
             anal_item_decode(it, a.uoff, a.lc, a.ngroups, &m, &u, &q, &g);
             const int s = 256 * u + 2 * d + q;
             const bool valid = s <= a.lc - m;
-            double v[CW];
-            if (anal_has_work(a.u0, m, a.ptiles, u)) {
-                double sc[CW];
-                {
-                    const double* ci =
-                        a.colinv + (((long long)m * 2 + q) * a.ngroups + g) * N + c0;
-                    const double k = pow2i(8 * WB) / a.ascale;
+            const bool work = anal_has_work(a.u0, m, a.ptiles, u);
+            const double kscale = pow2i(8 * WB) / a.ascale;
+            const double* ci = a.colinv + (((long long)m * 2 + q) * a.ngroups + g) * N + c0;
+            const long long o = packed_off(m, a.lc) + s;
+            if constexpr (NBUF == 2) {
+                double v[CW];
+                if (work) {
+                    double sc[CW];
 #pragma unroll
-                    for (int c = 0; c < CW; ++c) sc[c] = ci[c] * k;
-                }
-                const int buf = kwork & 1;
-                if (!__all_sync(0xffffffffu, mbar_wait(&dfull[buf], (uint32_t)((kwork >> 1) & 1),
-                                                       &abort_flag)))
-                    break;
-                tc_fence_after();
-                const uint32_t dcol = (uint32_t)(buf * DC + c0);
+                    for (int c = 0; c < CW; ++c) sc[c] = ci[c] * kscale;
+                    const int buf = kwork & 1;
+                    if (!__all_sync(0xffffffffu,
+                                    mbar_wait(&dfull[buf], (uint32_t)((kwork >> 1) & 1),
+                                              &abort_flag)))
+                        break;
+                    tc_fence_after();
+                    const uint32_t dcol = (uint32_t)(buf * DC + c0);
 #pragma unroll
-                for (int c8 = 0; c8 < CW; c8 += 8) {
-                    uint32_t acc[KW][8];
-#pragma unroll
-                    for (int w = 0; w < KW; ++w)
-                        tmem_ld8(lane_base + dcol + (uint32_t)(w * N + c8), acc[w]);
-                    tmem_wait_ld();
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) {
-                        long long gsum[3] = {0, 0, 0};
+                    for (int c8 = 0; c8 < CW; c8 += 8) {
+                        uint32_t acc[KW][8];
 #pragma unroll
                         for (int w = 0; w < KW; ++w)
-                            gsum[w / 3] += (long long)(int)acc[w][c] << (8 * (w % 3));
-                        v[c8 + c] = fma((double)gsum[2], 281474976710656.0,
-                                        fma((double)gsum[1], 16777216.0, (double)gsum[0])) *
-                                    sc[c8 + c];
+                            tmem_ld8(lane_base + dcol + (uint32_t)(w * N + c8), acc[w]);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {
+                            long long gsum[3] = {0, 0, 0};
+#pragma unroll
+                            for (int w = 0; w < KW; ++w)
+                                gsum[w / 3] += (long long)(int)acc[w][c] << (8 * (w % 3));
+                            v[c8 + c] = fma((double)gsum[2], 281474976710656.0,
+                                            fma((double)gsum[1], 16777216.0, (double)gsum[0])) *
+                                        sc[c8 + c];
+                        }
+                    }
+                    // D is in registers: the MMAs two items on may overwrite it
+                    tc_fence_before();
+                    mbar_arrive(&dfree[buf]);
+                    ++kwork;
+                } else {
+#pragma unroll
+                    for (int c = 0; c < CW; ++c) v[c] = 0.0;
+                }
+                if (valid) {
+#pragma unroll
+                    for (int c = 0; c < CW; c += 2) {
+                        const int fg = g * NFG + ((c0 + c) >> 1);
+                        if (fg < a.nfield)
+                            a.partial[(long long)fg * a.nlm + o] = make_double2(v[c], v[c + 1]);
                     }
                 }
-                // D is in registers: the MMAs two items on may overwrite it
-                tc_fence_before();
-                mbar_arrive(&dfree[buf]);
-                ++kwork;
             } else {
+                // one buffer: each column pair is read, combined and stored
+                // at once (few registers, two CTAs per SM); D is released
+                // after its last pair
+                if (work) {
+                    if (!__all_sync(0xffffffffu,
+                                    mbar_wait(&dfull[0], (uint32_t)(kwork & 1), &abort_flag)))
+                        break;
+                    tc_fence_after();
+                    const uint32_t dcol = (uint32_t)c0;
+#pragma unroll 1
+                    for (int c = 0; c < CW; c += 2) {
+                        uint32_t acc[KW][2];
 #pragma unroll
-                for (int c = 0; c < CW; ++c) v[c] = 0.0;
-            }
-            if (valid) {
-                const long long o = packed_off(m, a.lc) + s;
+                        for (int w = 0; w < KW; ++w)
+                            tmem_ld2(lane_base + dcol + (uint32_t)(w * N + c), acc[w]);
+                        tmem_wait_ld();
+                        double v2[2];
 #pragma unroll
-                for (int c = 0; c < CW; c += 2) {
-                    const int fg = g * NFG + ((c0 + c) >> 1);
-                    if (fg < a.nfield) a.partial[(long long)fg * a.nlm + o] = make_double2(v[c], v[c + 1]);
+                        for (int e = 0; e < 2; ++e) {
+                            long long gsum[3] = {0, 0, 0};
+#pragma unroll
+                            for (int w = 0; w < KW; ++w)
+                                gsum[w / 3] += (long long)(int)acc[w][e] << (8 * (w % 3));
+                            v2[e] = fma((double)gsum[2], 281474976710656.0,
+                                        fma((double)gsum[1], 16777216.0, (double)gsum[0])) *
+                                    (ci[c + e] * kscale);
+                        }
+                        const int fg = g * NFG + ((c0 + c) >> 1);
+                        if (valid && fg < a.nfield)
+                            a.partial[(long long)fg * a.nlm + o] = make_double2(v2[0], v2[1]);
+                    }
+                    tc_fence_before();
+                    mbar_arrive(&dfree[0]);
+                    ++kwork;
+                } else if (valid) {
+#pragma unroll 1
+                    for (int c = 0; c < CW; c += 2) {
+                        const int fg = g * NFG + ((c0 + c) >> 1);
+                        if (fg < a.nfield)
+                            a.partial[(long long)fg * a.nlm + o] = make_double2(0.0, 0.0);
+                    }
                 }
             }
         }
@@ -431,6 +491,6 @@ __global__ void __launch_bounds__(kTabThreads, 1) k_legendre_anal_tab(TabAnalArg
     if (warp == 8) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                     "r"(kTmemAlloc));
+                     "r"(kAlloc));
     }
 }

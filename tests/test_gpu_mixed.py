@@ -319,3 +319,27 @@ def test_bounded_wait_records_timeout_and_context_survives(cuda, oracle):
     assert cuda.mixed_status() == 0
     assert ((g - g64).abs().max() / g64.abs().max()).item() <= GRID_TOL
     print("bounded wait gave up after %.2f s" % waited)
+
+
+def test_backend_precision_switch(cuda, oracle):
+    """shtools_b200.backend.set_precision('int8x7-table') routes the numpy
+    backend calls (the calls pyshtools' classes make) through the
+    tensor-core path: the DH2 round trip of one field stays within the
+    mixed tolerances of the FP64 backend; 'fp64' restores the FP64 path
+    exactly."""
+    from shtools_b200 import backend as B
+    L = 95
+    c = fields(oracle, L, 1, 333)[0]
+    g64 = B.MakeGridDH(c, sampling=2)
+    b64 = B.SHExpandDH(g64, sampling=2)
+    try:
+        B.set_precision("int8x7-table")
+        gmx = B.MakeGridDH(c, sampling=2)
+        bmx = B.SHExpandDH(gmx, sampling=2)
+    finally:
+        B.set_precision("fp64")
+    assert cuda.mixed_status() == 0
+    assert np.abs(gmx - g64).max() / np.abs(g64).max() <= GRID_TOL
+    assert perdeg(bmx, b64).max() <= DEG_TOL["int8x7"]
+    assert not np.array_equal(gmx, g64)
+    assert np.array_equal(B.MakeGridDH(c, sampling=2), g64)
