@@ -76,10 +76,35 @@ __device__ __forceinline__ void dft4(double2& a, double2& b, double2& c, double2
     d = make_double2(d0.x - e.x, d0.y - e.y);
 }
 
-// radix-R DFT of v[] in place (R = 2, 4, 8, or an odd prime <= 13)
+// radix-R DFT of v[] in place (R = 2, 4, 8, 10, or an odd prime <= 13)
 template <int R, int SIGN>
 __device__ __forceinline__ void dft_small(double2* v) {
-    if (R == 8) {
+    if constexpr (R == 10) {
+        // two radix-5 DFTs of the even and odd samples, then
+        // X_k = E_k + w^k O_k, X_{k+5} = E_k - w^k O_k, w = exp(-+ 2 pi i / 10);
+        // cos and sin of 36 and 72 degrees are those of 144 and 72
+        double2 e[5], o[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            e[q] = v[2 * q];
+            o[q] = v[2 * q + 1];
+        }
+        dft_small<5, SIGN>(e);
+        dft_small<5, SIGN>(o);
+        constexpr double c36 = -root_cos(5, 2), s36 = root_sin(5, 2);
+        constexpr double c72 = root_cos(5, 1), s72 = root_sin(5, 1);
+        constexpr double ck[5] = {1.0, c36, c72, -c72, -c36};
+        constexpr double sk[5] = {0.0, s36, s72, s72, s36};
+        v[0] = make_double2(e[0].x + o[0].x, e[0].y + o[0].y);
+        v[5] = make_double2(e[0].x - o[0].x, e[0].y - o[0].y);
+#pragma unroll
+        for (int k = 1; k < 5; ++k) {
+            const double2 w = make_double2(ck[k], SIGN < 0 ? -sk[k] : sk[k]);
+            const double2 t = cmul(o[k], w);
+            v[k] = make_double2(e[k].x + t.x, e[k].y + t.y);
+            v[k + 5] = make_double2(e[k].x - t.x, e[k].y - t.y);
+        }
+    } else if (R == 8) {
         // two radix-4 DFTs of the even and odd samples, then
         // X_k = E_k + w^k O_k, X_{k+4} = E_k - w^k O_k, w = exp(-+ 2 pi i / 8)
         double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
@@ -161,6 +186,29 @@ __device__ __forceinline__ void dft_small(double2* v) {
     }
 }
 
+// v[q] *= w^q, q = 1 .. R-1.  Up to radix 8, w^q = w^(q/2) * w^(q - q/2): a
+// product tree of depth log2(R) instead of a chain of R-2 dependent
+// multiplications; radix 10 runs the chain, which keeps two powers live
+// instead of nine (the 64-register builds)
+template <int R, int SIGN>
+__device__ __forceinline__ void apply_twiddles(double2* v, double2 w) {
+    if constexpr (R >= 10) {
+        double2 wq = w;
+#pragma unroll
+        for (int q = 1; q < R; ++q) {
+            v[q] = cmul(v[q], wq);
+            if (q + 1 < R) wq = cmul(wq, w);
+        }
+    } else {
+        double2 wp[R];
+        wp[1] = w;
+#pragma unroll
+        for (int q = 2; q < R; ++q) wp[q] = cmul(wp[q / 2], wp[q - q / 2]);
+#pragma unroll
+        for (int q = 1; q < R; ++q) v[q] = cmul(v[q], wp[q]);
+    }
+}
+
 // One Stockham pass of radix R from x to y (ping-pong shared buffers).
 // tw: this pass's base twiddles, entry k < ns = exp(-2 pi i k/(ns R)); the
 // powers w^q, q >= 2, are formed by multiplication.
@@ -176,16 +224,7 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ x,
         double2 v[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = x[j + q * nr];
-        if (k != 0) {
-            // w^q = w^(q/2) * w^(q - q/2): a product tree of depth log2(R)
-            // instead of a chain of R-2 dependent multiplications
-            double2 wp[R];
-            wp[1] = twv<SIGN>(tw, k);
-#pragma unroll
-            for (int q = 2; q < R; ++q) wp[q] = cmul(wp[q / 2], wp[q - q / 2]);
-#pragma unroll
-            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], wp[q]);
-        }
+        if (k != 0) apply_twiddles<R, SIGN>(v, twv<SIGN>(tw, k));
         dft_small<R, SIGN>(v);
         const int d = (j - k) * R + k;
 #pragma unroll
@@ -211,14 +250,7 @@ __device__ __forceinline__ void fft_pass_io(Ld ld, St st, int M, int ns,
         double2 v[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = ld(j + q * nr);
-        if (k != 0) {
-            double2 wp[R];
-            wp[1] = twv<SIGN>(tw, k);
-#pragma unroll
-            for (int q = 2; q < R; ++q) wp[q] = cmul(wp[q / 2], wp[q - q / 2]);
-#pragma unroll
-            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], wp[q]);
-        }
+        if (k != 0) apply_twiddles<R, SIGN>(v, twv<SIGN>(tw, k));
         dft_small<R, SIGN>(v);
         const int d = (j - k) * R + k;
 #pragma unroll
@@ -236,6 +268,9 @@ __device__ __forceinline__ void fft_pass_io_r(int r, Ld ld, St st, int M, int ns
         case 3: fft_pass_io<3, SIGN>(ld, st, M, ns, t); break;
         case 4: fft_pass_io<4, SIGN>(ld, st, M, ns, t); break;
         case 8: fft_pass_io<8, SIGN>(ld, st, M, ns, t); break;
+        case 10:
+            if constexpr (MAXR >= 10) fft_pass_io<10, SIGN>(ld, st, M, ns, t);
+            break;
         case 5: fft_pass_io<5, SIGN>(ld, st, M, ns, t); break;
         case 7: fft_pass_io<7, SIGN>(ld, st, M, ns, t); break;
         case 11:
@@ -263,7 +298,8 @@ __device__ __forceinline__ void prefetch_l2_range(const void* p, size_t bytes) {
 
 // Runs the passes; the data starts in a, the result pointer is returned.
 // MAXR: the largest radix compiled in (8: plans whose factors are all <= 8,
-// which need far fewer registers than the radix-11/13 butterflies).
+// which need far fewer registers than the radix-11/13 butterflies; 10: the
+// same with the radix-10 pass of the long rings).
 template <int SIGN, int MAXR = 13>
 __device__ __forceinline__ double2* fft_run(double2* a, double2* b, int M, const int* fac,
                             int nfac, const double2* __restrict__ tw,
@@ -278,6 +314,9 @@ __device__ __forceinline__ double2* fft_run(double2* a, double2* b, int M, const
             case 3: fft_pass<3, SIGN>(a, b, M, ns, t); break;
             case 4: fft_pass<4, SIGN>(a, b, M, ns, t); break;
             case 8: fft_pass<8, SIGN>(a, b, M, ns, t); break;
+            case 10:
+                if constexpr (MAXR >= 10) fft_pass<10, SIGN>(a, b, M, ns, t);
+                break;
             case 5: fft_pass<5, SIGN>(a, b, M, ns, t); break;
             case 7: fft_pass<7, SIGN>(a, b, M, ns, t); break;
             case 11:
@@ -331,6 +370,9 @@ __device__ __forceinline__ double2* fft_run_io(double2* a, double2* b, int M, co
                 case 3: fft_pass<3, SIGN>(a, b, M, ns, t); break;
                 case 4: fft_pass<4, SIGN>(a, b, M, ns, t); break;
                 case 8: fft_pass<8, SIGN>(a, b, M, ns, t); break;
+                case 10:
+                    if constexpr (MAXR >= 10) fft_pass<10, SIGN>(a, b, M, ns, t);
+                    break;
                 case 5: fft_pass<5, SIGN>(a, b, M, ns, t); break;
                 case 7: fft_pass<7, SIGN>(a, b, M, ns, t); break;
                 case 11:

@@ -257,11 +257,11 @@ __device__ __forceinline__ double2* fft_buffers(const FftArgs& F, double2* smem_
 }
 
 // MAXR = 8: plans whose radices are all <= 8, built for <= 64 registers
-// (four 256-thread CTAs per SM, or one 1024-thread CTA for rings too long
-// for two CTAs' shared memory: MAXT = 1024); MAXR = 13 carries the
-// radix-11/13 passes
+// (four 256-thread CTAs per SM); MAXR = 10 the same with the radix-10 pass,
+// in one 1024-thread CTA for rings too long for two CTAs' shared memory
+// (MAXT = 1024); MAXR = 13 carries the radix-11/13 passes
 template <int MAXR, int MAXT>
-constexpr int fft_min_ctas() { return MAXR <= 8 ? 65536 / (64 * MAXT) : 1; }
+constexpr int fft_min_ctas() { return MAXR <= 10 ? 65536 / (64 * MAXT) : 1; }
 
 template <typename GT, int MAXR, int MAXT = 512>
 __global__ void __launch_bounds__(MAXT, fft_min_ctas<MAXR, MAXT>())
@@ -527,15 +527,19 @@ int launch_unpack_coef(const shtc_plan* P, const double2* partial, int ntiles,
 // Which FFT build runs a plan: 0 the full one (the plan's CTA size); 1 the
 // register-capped one (radices <= 8, every Bluestein length among them)
 // when shared memory leaves room for more than one CTA per SM; 2 the
-// register-capped one in 1024-thread CTAs for rings of more than 4096
-// points held in shared memory (one CTA per SM either way, but twice the
-// warps; with 512 threads the cap alone cost 2-3% at lmax 2799)
+// register-capped one in 1024-thread CTAs, with the radix-10 pass, for
+// rings of more than 4096 points held in shared memory (one CTA per SM
+// either way, but twice the warps; with 512 threads the cap alone cost 2-3%
+// at lmax 2799)
 static int fft_variant(const FftPlan& f) {
-    for (int i = 0; i < f.nfac; ++i)
-        if (f.fac[i] > 8) return 0;
-    if (f.smem <= 100 * 1024) return 1;
+    int maxr = 0;
+    for (int i = 0; i < f.nfac; ++i) maxr = std::max(maxr, f.fac[i]);
     const int len = f.bluestein ? f.mb : f.m;
-    return (!f.gmem && len > 4096) ? 2 : 0;
+    const bool long_ring = !f.gmem && len > 4096;
+    if (maxr > 10) return 0;
+    if (maxr == 10) return long_ring ? 2 : 0;
+    if (f.smem <= 100 * 1024) return 1;
+    return long_ring ? 2 : 0;
 }
 
 // the plan's FFT arguments with the CTA size of the build that runs them
@@ -620,9 +624,9 @@ int launch_fft_c2r(const shtc_plan* P, const double2* spec, void* grid, int dtyp
                                              weighted, st, gbuf);
     if (v == 2)
         return dtype == SHTC_F32
-                   ? launch_c2r_t<float, 8, 1024>(P, spec, (float*)grid, gf, grs, gcs, nfield,
+                   ? launch_c2r_t<float, 10, 1024>(P, spec, (float*)grid, gf, grs, gcs, nfield,
                                                   weighted, st, gbuf)
-                   : launch_c2r_t<double, 8, 1024>(P, spec, (double*)grid, gf, grs, gcs,
+                   : launch_c2r_t<double, 10, 1024>(P, spec, (double*)grid, gf, grs, gcs,
                                                    nfield, weighted, st, gbuf);
     return dtype == SHTC_F32
                ? launch_c2r_t<float, 13>(P, spec, (float*)grid, gf, grs, gcs, nfield, weighted,
@@ -668,7 +672,7 @@ int launch_fft_r2c_product(const shtc_plan* P, const double* grid, const double*
             return launch_r2c_t<double, 8>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st,
                                            grid2, gbuf);
         case 2:
-            return launch_r2c_t<double, 8, 1024>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st,
+            return launch_r2c_t<double, 10, 1024>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st,
                                                  grid2, gbuf);
         default:
             return launch_r2c_t<double, 13>(P, grid, gf, grs, gcs, spec, nfield, 1, 0, st,
@@ -688,10 +692,10 @@ int launch_fft_r2c(const shtc_plan* P, const void* grid, int dtype, long long gf
                                              nfield, weighted, fold_extend, st, nullptr, gbuf);
     if (v == 2)
         return dtype == SHTC_F32
-                   ? launch_r2c_t<float, 8, 1024>(P, (const float*)grid, gf, grs, gcs, spec,
+                   ? launch_r2c_t<float, 10, 1024>(P, (const float*)grid, gf, grs, gcs, spec,
                                                   nfield, weighted, fold_extend, st, nullptr,
                                                   gbuf)
-                   : launch_r2c_t<double, 8, 1024>(P, (const double*)grid, gf, grs, gcs, spec,
+                   : launch_r2c_t<double, 10, 1024>(P, (const double*)grid, gf, grs, gcs, spec,
                                                    nfield, weighted, fold_extend, st, nullptr,
                                                    gbuf);
     return dtype == SHTC_F32
@@ -880,7 +884,7 @@ int launch_fft_c2c_synth(const shtc_plan* P, const double2* spec, double2* grid,
     switch (fft_variant(P->fft)) {
         case 1: return launch_c2c_synth_t<8>(P, spec, grid, gf, grs, gcs, nfield, st, gbuf);
         case 2:
-            return launch_c2c_synth_t<8, 1024>(P, spec, grid, gf, grs, gcs, nfield, st, gbuf);
+            return launch_c2c_synth_t<10, 1024>(P, spec, grid, gf, grs, gcs, nfield, st, gbuf);
         default: return launch_c2c_synth_t<13>(P, spec, grid, gf, grs, gcs, nfield, st, gbuf);
     }
 }
@@ -891,7 +895,7 @@ int launch_fft_c2c_anal(const shtc_plan* P, const double2* grid, long long gf,
     switch (fft_variant(P->fft)) {
         case 1: return launch_c2c_anal_t<8>(P, grid, gf, grs, gcs, spec, nfield, st, gbuf);
         case 2:
-            return launch_c2c_anal_t<8, 1024>(P, grid, gf, grs, gcs, spec, nfield, st, gbuf);
+            return launch_c2c_anal_t<10, 1024>(P, grid, gf, grs, gcs, spec, nfield, st, gbuf);
         default: return launch_c2c_anal_t<13>(P, grid, gf, grs, gcs, spec, nfield, st, gbuf);
     }
 }

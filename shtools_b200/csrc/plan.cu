@@ -221,16 +221,36 @@ __global__ void k_ring_weights(const double* __restrict__ q,
 // write R elements apart, an R-way shared-memory bank conflict for R = 8
 // (16-byte elements, 8 threads per 128-byte wavefront) but none for odd R;
 // with ns >= 3 the writes of consecutive threads are contiguous runs.
-static int factor_len(int n, int* fac) {
+// with pair10, factors 5 and 2 are merged into radix-10 passes where that
+// lowers the number of passes (5600 = 10 * 10 * 7 * 8: four passes instead
+// of five, and no pass of more than 1024 butterflies)
+static int factor_len(int n, int* fac, bool pair10 = false) {
     int k = 0;
     int m = n;
     int p2 = 0;
     while (m % 2 == 0) { m /= 2; ++p2; }
+    auto groups2 = [](int e) { return e / 3 + (e % 3 ? 1 : 0); };
+    int n5 = 0;
+    {
+        int r = m;
+        while (r % 5 == 0) { r /= 5; ++n5; }
+    }
+    int tens = 0;
+    if (pair10) {
+        for (int t = 1; t <= std::min(n5, p2); ++t)
+            if (groups2(p2 - t) < groups2(p2 - tens)) tens = t;
+    }
+    p2 -= tens;
     for (int p = 3; p <= m; p += 2) {
         while (m % p == 0) {
             if (p > kMaxRadix || (p != 3 && p != 5 && p != 7 && p != 11 && p != 13))
                 return -1;
-            fac[k++] = p;
+            if (p == 5 && tens > 0) {
+                fac[k++] = 10;
+                --tens;
+            } else {
+                fac[k++] = p;
+            }
             m /= p;
         }
     }
@@ -315,6 +335,14 @@ int build_fft_plan(FftPlan* f, int n, int cplx, cudaStream_t st) {
         }
     }
     if (nf > kMaxFactors) return SHTC_EUNSUP;
+    int maxsmem = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    // rings of more than 4096 points held in shared memory run in
+    // 1024-thread CTAs, whose passes are short of butterflies with radices
+    // below 8: they take the radix-10 passes
+    if (!f->bluestein && f->m > 4096 && 2 * (size_t)f->m * sizeof(double2) <= (size_t)maxsmem)
+        nf = factor_len(f->m, fac, true);
     f->ntw = pass_twiddles(fac, nf, tw, f->tw_off);
     f->nfac = nf;
     for (int i = 0; i < nf; ++i) f->fac[i] = fac[i];
@@ -330,9 +358,6 @@ int build_fft_plan(FftPlan* f, int n, int cplx, cudaStream_t st) {
     // two shared buffers: Stockham passes ping-pong between them; the
     // per-plan kernels also keep the twiddles in shared memory when they fit
     f->smem_data = 2 * (size_t)len * sizeof(double2);
-    int maxsmem = 0, dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     f->threads = len > 2048 ? 512 : (len > 512 ? 256 : 128);
     if (maxsmem > 0 && f->smem_data > (size_t)maxsmem) {
         // too long for shared memory: the data buffers go to a global scratch

@@ -215,12 +215,14 @@ def test_long_rings_column_major_grids(cuda, oracle):
         assert torch.equal(plan.analysis(gcm), plan.analysis(g))
 
 
-# Even rings of more than 4096 complex points with radices <= 8 run the
+# Even rings of more than 4096 complex points with radices <= 10 run the
 # 1024-thread register-capped FFT build with both buffers in shared memory:
-# DH lmax 2399, sampling 2, nlon 9600, half length 4800 = 2^6 * 3 * 5^2.
-@pytest.mark.parametrize("extend", [False, True])
-def test_dh2399_long_even_fft_all_rings_low_calc(cuda, oracle, extend):
-    L, lc = 2399, 48
+# DH lmax 2399, sampling 2, nlon 9600, half length 4800 = 2^6 * 3 * 5^2
+# (passes 3, 5, 5, 8, 8); DH lmax 2799, sampling 2, nlon 11200, half length
+# 5600 = 2^5 * 5^2 * 7 (radix-10 passes: 10, 10, 7, 8).
+@pytest.mark.parametrize("L,extend", [(2399, False), (2399, True), (2799, False)])
+def test_dh2399_long_even_fft_all_rings_low_calc(cuda, oracle, L, extend):
+    lc = 48
     c = oracle.power_law_cilm(L, 7101)
     ext = 1 if extend else 0
     g = cuda.MakeGridDH(torch.from_numpy(np.stack([c, 2 * c])).cuda(), sampling=2,
@@ -241,11 +243,12 @@ def test_dh2399_long_even_fft_all_rings_low_calc(cuda, oracle, extend):
         assert e.max() <= DEG_TOL, (f, e.max(), e.argmax())
 
 
-def test_dh2399_long_even_fft_float32_and_adjoint(cuda, oracle):
+@pytest.mark.parametrize("L", [2399, 2799])
+def test_dh2399_long_even_fft_float32_and_adjoint(cuda, oracle, L):
     """float32 grids through the long even-ring FFTs stay within float32
     rounding of float64; the synthesis adjoint (r2c of the cotangent with
     unit weights) satisfies <S c, y> = <c, S^T y>."""
-    L, lc = 2399, 48
+    lc = 48
     c = torch.from_numpy(oracle.power_law_cilm(L, 7103)).cuda()
     g64 = cuda.MakeGridDH(c, sampling=2, lmax_calc=lc)
     g32 = cuda.MakeGridDH(c, sampling=2, lmax_calc=lc, dtype=torch.float32)
