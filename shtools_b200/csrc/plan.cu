@@ -222,8 +222,10 @@ __global__ void k_ring_weights(const double* __restrict__ q,
 // (16-byte elements, 8 threads per 128-byte wavefront) but none for odd R;
 // with ns >= 3 the writes of consecutive threads are contiguous runs.
 // with pair10, factors 5 and 2 are merged into radix-10 passes where that
-// lowers the number of passes (5600 = 10 * 10 * 7 * 8: four passes instead
-// of five, and no pass of more than 1024 butterflies)
+// lowers the number of passes (5600 = 7 * 10 * 10 * 8: four passes instead
+// of five, and no pass of more than 1024 butterflies).  Passes run odd
+// radices first, then 10, 8, 4, 2: with the radix-7 pass first the lmax
+// 2799 FFTs were 3-7% faster than with the radix-10 passes first.
 static int factor_len(int n, int* fac, bool pair10 = false) {
     int k = 0;
     int m = n;
@@ -241,19 +243,21 @@ static int factor_len(int n, int* fac, bool pair10 = false) {
             if (groups2(p2 - t) < groups2(p2 - tens)) tens = t;
     }
     p2 -= tens;
+    int t10 = 0;
     for (int p = 3; p <= m; p += 2) {
         while (m % p == 0) {
             if (p > kMaxRadix || (p != 3 && p != 5 && p != 7 && p != 11 && p != 13))
                 return -1;
             if (p == 5 && tens > 0) {
-                fac[k++] = 10;
                 --tens;
+                ++t10;
             } else {
                 fac[k++] = p;
             }
             m /= p;
         }
     }
+    while (t10-- > 0) fac[k++] = 10;
     while (p2 >= 3) { fac[k++] = 8; p2 -= 3; }
     if (p2 == 2) fac[k++] = 4;
     if (p2 == 1) fac[k++] = 2;
