@@ -50,6 +50,10 @@ WORKLOADS = {
     # FFT build (complex half length 4800) at a size that profiles quickly
     "dh2399x2": dict(kind="dh", lmax=2399, nfield=2, sampling=2, beta=3.0,
                      seed=5700),
+    # 2 DH fields, lmax 2799, sampling 2 (5600 x 11200): the radix-10 passes
+    # of the long even-ring FFT (half length 5600 = 7 * 10 * 10 * 8)
+    "dh2799x2": dict(kind="dh", lmax=2799, nfield=2, sampling=2, beta=3.0,
+                     seed=5800),
     # 8 DH fields, lmax 719, sampling 2
     "dh719x8": dict(kind="dh", lmax=719, nfield=8, sampling=2, beta=2.0,
                     seed=3000),
