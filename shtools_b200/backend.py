@@ -74,11 +74,18 @@ def _dev(a, dtype=np.float64):
     return hostio.to_device(np.asarray(a, dtype=dtype))
 
 
+def _dev_cilm(cilm):
+    """A real cilm on the current CUDA device: only its entries m <= l, the
+    ones the synthesis reads, cross the staging buffers (entries m > l are
+    zero on the device)."""
+    return hostio.to_device_lower(np.asarray(cilm, dtype=np.float64))
+
+
 def MakeGridDH(cilm, lmax=None, norm=1, sampling=1, csphase=1, lmax_calc=None,
                extend=False):
     """griddh = MakeGridDH(cilm, [lmax, norm, sampling, csphase, lmax_calc,
     extend]) -- see src/MakeGridDH.f95:1 and ducc0_wrapper.py:454."""
-    return _np(_t.MakeGridDH(_dev(cilm), lmax=lmax,
+    return _np(_t.MakeGridDH(_dev_cilm(cilm), lmax=lmax,
                              norm=norm, sampling=sampling, csphase=csphase,
                              lmax_calc=lmax_calc, extend=extend, precision=_precision))
 
@@ -96,7 +103,7 @@ def MakeGridGLQ(cilm, zero=None, lmax=None, norm=1, csphase=1, lmax_calc=None,
     """gridglq = MakeGridGLQ(cilm, [zero, lmax, norm, csphase, lmax_calc,
     extend]) -- see src/MakeGridGLQ.f95:1 and ducc0_wrapper.py:837.  With
     zero=None the nodes come from the GPU PreGLQ."""
-    return _np(_t.MakeGridGLQ(_dev(cilm), zero=zero,
+    return _np(_t.MakeGridGLQ(_dev_cilm(cilm), zero=zero,
                               lmax=lmax, norm=norm, csphase=csphase,
                               lmax_calc=lmax_calc, extend=extend, precision=_precision))
 

@@ -18,7 +18,8 @@ array) has been garbage-collected, so a loop of calls reuses the same few
 buffers instead of pinning new memory (cudaHostAlloc of tens of MB takes
 tens of ms).  The pool keeps at most POOL_MAX bytes of free buffers.
 Inputs that already live in pinned memory (for instance such a result,
-passed back in) are uploaded directly.
+passed back in) are uploaded directly.  Real coefficient arrays for the
+synthesis (to_device_lower) move only their entries m <= l.
 
 Thread safety: one lock per device guards its staging buffers; calls from
 several threads are serialised on them.
@@ -136,6 +137,74 @@ def to_device(a, device=None):
         cur.wait_stream(cs)
         dst.record_stream(cs)
     return dst
+
+
+def _copy_lower(dst, src, r0, n):
+    """dst[i, :l+1] = src[i, :l+1] for the 2-D row blocks of a coefficient
+    array, l = (r0 + i) mod n the degree of row i: the rows' valid prefixes
+    only, in bands of rows (each band copies the widest prefix it holds),
+    split over the copy threads."""
+    global _pool
+    nrow = src.shape[0]
+    band = max(1, n // 32)
+    jobs = []
+    i = 0
+    while i < nrow:
+        l = (r0 + i) % n
+        j = min(nrow, i + band, i + (n - l))   # a band ends at a degree wrap
+        cols = (r0 + j - 1) % n + 1            # widest prefix of the band
+        jobs.append((i, j, cols))
+        i = j
+    with _lock:
+        if _pool is None:
+            _pool = ThreadPoolExecutor(_threads(), thread_name_prefix="shtc-hostio")
+        pool = _pool
+    futs = [pool.submit(np.copyto, dst[a:b, :c], src[a:b, :c]) for a, b, c in jobs]
+    for f in futs:
+        f.result()
+
+
+def to_device_lower(a, device=None):
+    """to_device for real coefficient arrays [..., n, n] of which the
+    transforms read only the entries m <= l (the last index at most the one
+    before it): the host copies move only those (about half the bytes of a
+    square array); in the device copy the entries m > l are zero.  Other
+    shapes take to_device."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None \
+        else torch.device(device)
+    if dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    a = np.ascontiguousarray(a)
+    n = a.shape[-1] if a.ndim >= 2 else 0
+    rowb = n * a.itemsize
+    if (a.ndim < 2 or a.shape[-2] != n or a.nbytes < SMALL_BYTES or rowb > CHUNK_BYTES
+            or torch.from_numpy(a).is_pinned()):
+        t = to_device(a, dev)
+        return t.tril_() if a.ndim >= 2 and a.shape[-2] == a.shape[-1] else t
+    ta = torch.from_numpy(a)
+    dst = torch.empty(a.shape, dtype=ta.dtype, device=dev)
+    src = a.reshape(-1, n)
+    rows = src.shape[0]
+    per = CHUNK_BYTES // rowb               # whole rows per staging buffer
+    dflat = dst.view(-1).view(torch.uint8)
+    lock, cs, bufs, evs = _get(dev)
+    cur = torch.cuda.current_stream(dev)
+    with lock:
+        cs.wait_stream(cur)
+        for k, r0 in enumerate(range(0, rows, per)):
+            b = k & 1
+            nr = min(per, rows - r0)
+            evs[b].synchronize()
+            stage = bufs[b].numpy()[:nr * rowb].view(a.dtype).reshape(nr, n)
+            _copy_lower(stage, src[r0:r0 + nr], r0, n)
+            with torch.cuda.stream(cs):
+                dflat[r0 * rowb:(r0 + nr) * rowb].copy_(bufs[b][:nr * rowb],
+                                                        non_blocking=True)
+                evs[b].record(cs)
+        cur.wait_stream(cs)
+        dst.record_stream(cs)
+    # the staged rows' entries m > l hold whatever the buffers held before
+    return dst.tril_()
 
 
 def to_host(t):

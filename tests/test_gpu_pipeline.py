@@ -77,6 +77,33 @@ def test_hostio_staged_copies(cuda):
     assert np.array_equal(hostio.to_host(g[1]), g[1].cpu().numpy())
 
 
+def test_hostio_lower_triangle_upload(cuda, oracle):
+    """to_device_lower (the backend's cilm upload for the synthesis) gives
+    the array with its entries m > l zeroed, through the staged path (one
+    and several staging buffers, 3-D and 4-D) and the direct ones (small,
+    pinned); the backend's MakeGridDH / MakeGridGLQ results equal those of
+    the torch API on the same coefficients."""
+    from shtools_b200 import backend as B
+    from shtools_b200 import hostio
+    rng = np.random.default_rng(21)
+    for shape in ((2, 12, 12), (2, 700, 700), (2, 2048, 2048), (3, 2, 1100, 1100)):
+        a = rng.standard_normal(shape)
+        t = hostio.to_device_lower(a)
+        assert t.is_cuda and t.shape == shape
+        assert torch.equal(t.cpu(), torch.tril(torch.from_numpy(a)))
+    a = rng.standard_normal((2, 900, 900))
+    pinned = torch.from_numpy(a).pin_memory()
+    t = hostio.to_device_lower(pinned.numpy())
+    assert torch.equal(t.cpu(), torch.tril(torch.from_numpy(a)))
+    c = oracle.power_law_cilm(300, 2101)
+    c_up = c + np.triu(rng.standard_normal(c.shape), 1)   # entries m > l are ignored
+    g = B.MakeGridDH(c_up, sampling=2)
+    assert np.array_equal(g, cuda.MakeGridDH(torch.from_numpy(c).cuda(), sampling=2).cpu().numpy())
+    z, _ = oracle.shglq(300)
+    g = B.MakeGridGLQ(c_up, zero=z)
+    assert np.array_equal(g, cuda.MakeGridGLQ(torch.from_numpy(c).cuda(), zero=z).cpu().numpy())
+
+
 def test_hostio_pinned_results_and_staged_large(cuda, monkeypatch):
     """Results come back in pinned memory viewed by numpy; such a result
     passed back in is uploaded directly and stays exact; results above

@@ -177,3 +177,24 @@ def test_hostio_pool_returns_buffers_when_views_die():
     gc.collect()
     assert H._free_bytes == before + 96
     assert H._take(96) is buf and H._free_bytes == before
+
+
+def test_hostio_lower_band_copy():
+    """The staged copy of a coefficient array moves each row's entries
+    m <= l, for any split of the rows into staging blocks (the band logic of
+    shtools_b200.hostio._copy_lower, run on host arrays)."""
+    import numpy as np
+    from shtools_b200 import hostio as H
+    rng = np.random.default_rng(11)
+    for n in (1, 5, 37, 64, 300):
+        for lead in ((2,), (3, 2)):
+            src = rng.standard_normal(lead + (n, n)).reshape(-1, n)
+            rows = src.shape[0]
+            deg = np.arange(rows) % n
+            lower = np.arange(n)[None, :] <= deg[:, None]
+            for per in (1, 7, n, rows):
+                out = np.full_like(src, np.nan)
+                for r0 in range(0, rows, per):
+                    nr = min(per, rows - r0)
+                    H._copy_lower(out[r0:r0 + nr], src[r0:r0 + nr], r0, n)
+                assert np.array_equal(out[lower], src[lower]), (n, lead, per)
